@@ -1,0 +1,151 @@
+/* b200fmm -- Blackwell (sm_100a) implementation of the ScalFMM interpolation-FMM hot path.
+ *
+ * C ABI: plain pointers and sizes, no CUDA/PyTorch types.  Every function returns a b200fmm_status and
+ * never exits, traps or throws; b200fmm_last_error() gives the message of the last failure on the calling
+ * thread.  A handle is used by one host thread at a time and owns (or borrows) one CUDA stream.
+ *
+ * Reference interfaces replaced (paths relative to the ScalFMM project root):
+ *   - the kernel operator surface FAbstractKernels (Src/Components/FAbstractKernels.hpp:23-210):
+ *     P2M :36, M2M :50, M2L :81-83 (+ finishedLevelM2L :93-102), L2L :116, L2P :124, P2P :147-150,
+ *     P2POuter :171-174, P2PRemote :203-208 -- here level-batched: one call runs the operator over
+ *     every cell/leaf of a level, as FFmmAlgorithmThread's passes do (Src/Core/FFmmAlgorithmThread.hpp);
+ *   - the algorithm entry FAbstractAlgorithm::execute(operationsToProceed) (Src/Core/FCoreCommon.hpp:73-78)
+ *     with the FFmmOperations bits (FCoreCommon.hpp:17-29);
+ *   - the C API of Addons/CKernelApi (CScalfmmApi.h:103-802: scalfmm_init, scalfmm_tree_insert_particles_xyz,
+ *     scalfmm_set_physical_values, scalfmm_execute_fmm, scalfmm_get_potentials/forces_xyz) and the
+ *     Chebyshev extern "C" operators ChebKernel_P2M ... ChebKernel_P2PRemote (FChebInterface.h:37-76);
+ *   - the M2L operator file I/O of FChebSymM2LHandler (ComputeAndCompressAndStoreInBinaryFile /
+ *     ReadFromBinaryFile, Src/Kernels/Chebyshev/FChebSymM2LHandler.hpp:471-567).
+ */
+#ifndef B200FMM_H
+#define B200FMM_H
+
+#if defined(__GNUC__)
+#define B200FMM_API __attribute__((visibility("default")))
+#else
+#define B200FMM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  B200FMM_OK = 0,
+  B200FMM_ERR_INVALID = 1,     /* bad argument (null pointer, size, order/height out of range, ...) */
+  B200FMM_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+  B200FMM_ERR_OOM = 3,         /* device allocation failed */
+  B200FMM_ERR_STATE = 4,       /* call out of order (e.g. execute before set_particles) */
+  B200FMM_ERR_DOMAIN = 5,      /* particle outside the box, or a non-finite coordinate */
+  B200FMM_ERR_UNSUPPORTED = 6, /* configuration not built into this library */
+  B200FMM_ERR_NUMERIC = 7      /* operator precompute failed (SVD did not converge) */
+} b200fmm_status;
+
+/* Interpolation kernels (Src/Kernels/Chebyshev/FChebSymKernel.hpp, FChebDenseKernel.hpp,
+ * Src/Kernels/Uniform/FUnifKernel.hpp), all for the Laplace 1/r matrix kernel FInterpMatrixKernelR. */
+typedef enum { B200FMM_CHEB_SYM = 0, B200FMM_CHEB_DENSE = 1, B200FMM_LAGRANGE = 2 } b200fmm_kernel;
+
+/* FP64: every operator in FP64 (parity form).  MIXED: P2P in FP32 with per-target compensated sums,
+ * M2L as split-FP16 tensor-core GEMMs (tcgen05) over the dense per-transfer-vector operators with FP32
+ * accumulation and FP64 cross-group sums; P2M/M2M/L2L/L2P stay FP64. */
+typedef enum { B200FMM_FP64 = 0, B200FMM_MIXED = 1 } b200fmm_precision;
+
+/* FFmmOperations (FCoreCommon.hpp:17-29) */
+enum {
+  B200FMM_P2P = 1,
+  B200FMM_P2M = 2,
+  B200FMM_M2M = 4,
+  B200FMM_M2L = 8,
+  B200FMM_L2L = 16,
+  B200FMM_L2P = 32,
+  B200FMM_NEAR_FIELD = 1,
+  B200FMM_FAR_FIELD = 62,
+  B200FMM_ALL = 63
+};
+
+typedef struct {
+  int kernel;        /* b200fmm_kernel */
+  int order;         /* interpolation order p, 3..8 */
+  int height;        /* octree height (levels 0..height-1, leaves at height-1), 3..12 */
+  int nrhs;          /* charge vectors sharing one tree (the reference's NVALS), 1..32 */
+  int precision;     /* b200fmm_precision */
+  double box_width;  /* cubic simulation box (FOctree ctor, Src/Containers/FOctree.hpp:95) */
+  double center[3];
+  double epsilon;    /* M2L compression accuracy for CHEB_SYM; <= 0 selects 10^-order
+                        (FChebSymKernel.hpp:136-140) */
+  void *stream;      /* cudaStream_t to run on; NULL makes the handle create its own */
+  int device;        /* CUDA device ordinal; -1 keeps the calling thread's current device */
+} b200fmm_config;
+
+typedef struct b200fmm_context *b200fmm_handle;
+
+/* Lifecycle.  create() also builds the interpolation tables and, for CHEB_SYM, the 16 compressed
+ * operators (own FP64 precompute: kernel evaluation at the nodes on the GPU, pACA + QR + SVD on the host,
+ * following FChebSymM2LHandler.hpp:39-281); for CHEB_DENSE / LAGRANGE and MIXED it evaluates the
+ * dense per-transfer-vector operators on the GPU in FP64. */
+B200FMM_API b200fmm_status b200fmm_create(const b200fmm_config *cfg, b200fmm_handle *out);
+B200FMM_API b200fmm_status b200fmm_destroy(b200fmm_handle h);
+B200FMM_API const char *b200fmm_last_error(void);
+B200FMM_API const char *b200fmm_version(void);
+
+/* Compressed operators in the reference's storage layout: ranks[343] (non-zero for the 16 class slots),
+ * uv = for each class slot in increasing order U (p^3 x r, column-major) then V (p^3 x r, column-major).
+ * set_ replaces the handle's operators (ReadFromBinaryFile equivalent), get_ exports them. */
+B200FMM_API b200fmm_status b200fmm_set_sym_operators(b200fmm_handle h, const int *ranks, const double *uv, long long uv_len);
+B200FMM_API b200fmm_status b200fmm_get_sym_operators(b200fmm_handle h, int *ranks, double *uv, long long uv_cap,
+                                         long long *uv_len);
+
+/* Insert particles (FOctree::insert + FP2PParticleContainerIndexed, Src/Containers/FOctree.hpp:174-181)
+ * and build the tree on the GPU: Morton keys, stable radix sort, leaf ranges, upper levels, neighbour
+ * and interaction lists.  x, y, z: n doubles; q: nrhs*n doubles ([rhs][particle]).  Pointers are host
+ * memory when on_device == 0, device memory otherwise.  Resets all expansions and results. */
+B200FMM_API b200fmm_status b200fmm_set_particles(b200fmm_handle h, long long n, const double *x, const double *y,
+                                     const double *z, const double *q, int on_device);
+/* Replace the charges only (same positions, same tree). */
+B200FMM_API b200fmm_status b200fmm_set_charges(b200fmm_handle h, const double *q, int on_device);
+
+/* Whole evaluation (FFmmAlgorithmThread::executeCore, FFmmAlgorithmThread.hpp:118-159): zeroes the
+ * expansions and results, then runs the passes selected by ops. */
+B200FMM_API b200fmm_status b200fmm_execute(b200fmm_handle h, unsigned ops);
+
+/* Level-batched operators (FAbstractKernels).  They accumulate (+=) like the reference kernels.
+ * m2m/l2l take the parent level; m2l the level of the target cells (2..height-1). */
+B200FMM_API b200fmm_status b200fmm_reset_expansions(b200fmm_handle h);
+B200FMM_API b200fmm_status b200fmm_p2m(b200fmm_handle h);
+B200FMM_API b200fmm_status b200fmm_m2m(b200fmm_handle h, int level);
+B200FMM_API b200fmm_status b200fmm_m2l(b200fmm_handle h, int level);
+B200FMM_API b200fmm_status b200fmm_l2l(b200fmm_handle h, int level);
+B200FMM_API b200fmm_status b200fmm_l2p(b200fmm_handle h);
+/* variant 0: each leaf against itself and its <=26 neighbours (P2P with inTargets == inSources:
+ * P2POuter + P2PInner, FChebSymKernel.hpp:453-478); variant 1: neighbours only (P2PRemote, :481-486). */
+B200FMM_API b200fmm_status b200fmm_p2p(b200fmm_handle h, int variant);
+
+/* Results in the caller's original particle order, [rhs][particle]; host memory unless on_device. */
+B200FMM_API b200fmm_status b200fmm_get_results(b200fmm_handle h, double *phi, double *fx, double *fy, double *fz,
+                                   int on_device);
+B200FMM_API b200fmm_status b200fmm_synchronize(b200fmm_handle h);
+
+/* Tree inspection (host memory).  ncells: height entries.  get_cells returns the cells of one level in
+ * Morton order: keys[ncells[level]], multipoles/locals [ncells][nrhs][p^3] (either may be NULL). */
+B200FMM_API b200fmm_status b200fmm_tree_info(b200fmm_handle h, long long *ncells, long long *nparticles);
+B200FMM_API b200fmm_status b200fmm_get_cells(b200fmm_handle h, int level, long long *keys, double *multipoles,
+                                 double *locals);
+/* Sorted position -> original particle index. */
+B200FMM_API b200fmm_status b200fmm_get_permutation(b200fmm_handle h, long long *perm);
+
+/* Device time of the passes of the last execute(), milliseconds:
+ * [0] tree build (last set_particles), [1] P2M, [2] M2M, [3] M2L, [4] L2L, [5] L2P, [6] P2P, [7] total. */
+B200FMM_API b200fmm_status b200fmm_last_timings(b200fmm_handle h, double *ms8);
+/* Number of kernel launches issued by the last set_particles() plus the last execute(). */
+B200FMM_API b200fmm_status b200fmm_last_launch_count(b200fmm_handle h, long long *count);
+
+/* FP64 direct sum on the GPU (Examples/DirectComputation.cpp:104-142) for the listed targets (all if
+ * ntargets < 0).  Host pointers; outputs have ntargets (or n) entries. */
+B200FMM_API b200fmm_status b200fmm_direct(long long n, const double *x, const double *y, const double *z, const double *q,
+                              long long ntargets, const long long *targets, double *phi, double *fx,
+                              double *fy, double *fz);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

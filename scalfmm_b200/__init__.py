@@ -1,0 +1,281 @@
+"""scalfmm_b200: B200 (sm_100a) implementation of the ScalFMM interpolation-FMM hot path.
+
+The product is the C-ABI shared library ``libb200fmm.so`` (declared in include/b200fmm.h).  This module
+is a thin ctypes binding used by the tests and the benchmark; it mirrors the reference's flow
+(Examples/ChebyshevInterpolationFMM.cpp: build tree -> build kernel -> algo.execute()) and its operator
+surface (FAbstractKernels P2M/M2M/M2L/L2L/L2P/P2P, level-batched).  There is no CPU fallback: loading
+fails loudly when the library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libb200fmm.so"
+
+CHEB_SYM, CHEB_DENSE, LAGRANGE = 0, 1, 2
+FP64, MIXED = 0, 1
+P2P, P2M, M2M, M2L, L2L, L2P = 1, 2, 4, 8, 16, 32
+ALL = 63
+KERNELS = {"cheb_sym": CHEB_SYM, "cheb_dense": CHEB_DENSE, "lagrange": LAGRANGE}
+PRECISIONS = {"fp64": FP64, "mixed": MIXED}
+
+# every entry point declared in include/b200fmm.h
+EXPORTS = (
+    "b200fmm_create", "b200fmm_destroy", "b200fmm_last_error", "b200fmm_version", "b200fmm_set_sym_operators",
+    "b200fmm_get_sym_operators", "b200fmm_set_particles", "b200fmm_set_charges", "b200fmm_execute",
+    "b200fmm_reset_expansions", "b200fmm_p2m", "b200fmm_m2m", "b200fmm_m2l", "b200fmm_l2l", "b200fmm_l2p",
+    "b200fmm_p2p", "b200fmm_get_results", "b200fmm_synchronize", "b200fmm_tree_info", "b200fmm_get_cells",
+    "b200fmm_get_permutation", "b200fmm_last_timings", "b200fmm_last_launch_count", "b200fmm_direct",
+)
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_lp = ctypes.POINTER(ctypes.c_longlong)
+
+
+class B200FmmError(RuntimeError):
+    pass
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("kernel", ctypes.c_int),
+        ("order", ctypes.c_int),
+        ("height", ctypes.c_int),
+        ("nrhs", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("box_width", ctypes.c_double),
+        ("center", ctypes.c_double * 3),
+        ("epsilon", ctypes.c_double),
+        ("stream", ctypes.c_void_p),
+        ("device", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+
+def build(verbose: bool = False) -> None:
+    """Compile libb200fmm.so for sm_100a (nvcc; works without a GPU)."""
+    import subprocess
+
+    subprocess.run(["make", "-s", "-C", str(HERE / "csrc"), "-j8"], check=True,
+                   stdout=None if verbose else subprocess.DEVNULL)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise B200FmmError(f"{LIB_PATH} is missing: build it with `make -C scalfmm_b200/csrc`")
+        L = ctypes.CDLL(str(LIB_PATH))
+        for name in EXPORTS:
+            getattr(L, name).restype = ctypes.c_int
+        L.b200fmm_last_error.restype = ctypes.c_char_p
+        L.b200fmm_version.restype = ctypes.c_char_p
+        L.b200fmm_create.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(ctypes.c_void_p)]
+        L.b200fmm_destroy.argtypes = [ctypes.c_void_p]
+        L.b200fmm_set_sym_operators.argtypes = [ctypes.c_void_p, _ip, _dp, ctypes.c_longlong]
+        L.b200fmm_get_sym_operators.argtypes = [ctypes.c_void_p, _ip, _dp, ctypes.c_longlong, _lp]
+        L.b200fmm_set_particles.argtypes = [ctypes.c_void_p, ctypes.c_longlong] + [ctypes.c_void_p] * 4 + [ctypes.c_int]
+        L.b200fmm_set_charges.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        L.b200fmm_execute.argtypes = [ctypes.c_void_p, ctypes.c_uint]
+        for n in ("b200fmm_reset_expansions", "b200fmm_p2m", "b200fmm_l2p", "b200fmm_synchronize"):
+            getattr(L, n).argtypes = [ctypes.c_void_p]
+        for n in ("b200fmm_m2m", "b200fmm_m2l", "b200fmm_l2l", "b200fmm_p2p"):
+            getattr(L, n).argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.b200fmm_get_results.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 4 + [ctypes.c_int]
+        L.b200fmm_tree_info.argtypes = [ctypes.c_void_p, _lp, _lp]
+        L.b200fmm_get_cells.argtypes = [ctypes.c_void_p, ctypes.c_int, _lp, _dp, _dp]
+        L.b200fmm_get_permutation.argtypes = [ctypes.c_void_p, _lp]
+        L.b200fmm_last_timings.argtypes = [ctypes.c_void_p, _dp]
+        L.b200fmm_last_launch_count.argtypes = [ctypes.c_void_p, _lp]
+        L.b200fmm_direct.argtypes = [ctypes.c_longlong, _dp, _dp, _dp, _dp, ctypes.c_longlong, _lp, _dp, _dp, _dp, _dp]
+        _lib = L
+    return _lib
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != 0:
+        msg = lib().b200fmm_last_error().decode(errors="replace")
+        raise B200FmmError(f"{what} failed (status {rc}): {msg}")
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _ptr(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+class FMM:
+    """One FMM configuration on one GPU (a b200fmm handle).
+
+    kernel: 'cheb_sym' (FChebSymKernel), 'cheb_dense' (FChebDenseKernel) or 'lagrange' (FUnifKernel);
+    precision: 'fp64' or 'mixed'.
+    """
+
+    def __init__(self, kernel="cheb_sym", order=7, height=6, nrhs=1, precision="fp64", box_width=1.0,
+                 center=(0.5, 0.5, 0.5), epsilon=0.0, device=-1, stream=None):
+        self.order, self.height, self.nrhs = order, height, nrhs
+        self.nn = order ** 3
+        cfg = Config(KERNELS[kernel] if isinstance(kernel, str) else kernel, order, height, nrhs,
+                     PRECISIONS[precision] if isinstance(precision, str) else precision, box_width,
+                     (ctypes.c_double * 3)(*center), epsilon, stream, device)
+        h = ctypes.c_void_p()
+        _check(lib().b200fmm_create(ctypes.byref(cfg), ctypes.byref(h)), "b200fmm_create")
+        self._h = h
+        self.n = 0
+
+    # -- lifecycle --------------------------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().b200fmm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- operators --------------------------------------------------------------------------------------
+    def set_sym_operators(self, ranks, uv):
+        ranks = np.ascontiguousarray(ranks, dtype=np.int32)
+        uv = _f64(uv)
+        _check(lib().b200fmm_set_sym_operators(self._h, _ptr(ranks, _ip), _ptr(uv), uv.size), "set_sym_operators")
+
+    def get_sym_operators(self):
+        n = ctypes.c_longlong()
+        ranks = np.zeros(343, np.int32)
+        _check(lib().b200fmm_get_sym_operators(self._h, _ptr(ranks, _ip), None, 0, ctypes.byref(n)), "get_sym_operators")
+        uv = np.zeros(n.value)
+        _check(lib().b200fmm_get_sym_operators(self._h, _ptr(ranks, _ip), _ptr(uv), uv.size, ctypes.byref(n)),
+               "get_sym_operators")
+        return ranks, uv
+
+    # -- particles --------------------------------------------------------------------------------------
+    def set_particles(self, x, y, z, q):
+        """Host numpy arrays, or CUDA tensors (anything with data_ptr()) for device-resident inputs."""
+        if hasattr(x, "data_ptr"):
+            n = x.numel()
+            args = [ctypes.c_void_p(t.data_ptr()) for t in (x, y, z, q)]
+            _check(lib().b200fmm_set_particles(self._h, n, *args, 1), "set_particles")
+        else:
+            x, y, z, q = _f64(x), _f64(y), _f64(z), _f64(q)
+            n = x.size
+            self._keep = (x, y, z, q)
+            _check(lib().b200fmm_set_particles(self._h, n, *[ctypes.c_void_p(a.ctypes.data) for a in (x, y, z, q)], 0),
+                   "set_particles")
+        self.n = n
+
+    def set_charges(self, q):
+        if hasattr(q, "data_ptr"):
+            _check(lib().b200fmm_set_charges(self._h, ctypes.c_void_p(q.data_ptr()), 1), "set_charges")
+        else:
+            q = _f64(q)
+            _check(lib().b200fmm_set_charges(self._h, ctypes.c_void_p(q.ctypes.data), 0), "set_charges")
+
+    # -- algorithm --------------------------------------------------------------------------------------
+    def execute(self, ops=ALL):
+        _check(lib().b200fmm_execute(self._h, ops), "execute")
+
+    def reset_expansions(self):
+        _check(lib().b200fmm_reset_expansions(self._h), "reset_expansions")
+
+    def p2m(self):
+        _check(lib().b200fmm_p2m(self._h), "p2m")
+
+    def m2m(self, level):
+        _check(lib().b200fmm_m2m(self._h, level), "m2m")
+
+    def m2l(self, level):
+        _check(lib().b200fmm_m2l(self._h, level), "m2l")
+
+    def l2l(self, level):
+        _check(lib().b200fmm_l2l(self._h, level), "l2l")
+
+    def l2p(self):
+        _check(lib().b200fmm_l2p(self._h), "l2p")
+
+    def p2p(self, variant=0):
+        _check(lib().b200fmm_p2p(self._h, variant), "p2p")
+
+    def synchronize(self):
+        _check(lib().b200fmm_synchronize(self._h), "synchronize")
+
+    # -- outputs ----------------------------------------------------------------------------------------
+    def results(self):
+        R, n = self.nrhs, self.n
+        out = [np.zeros(R * n) for _ in range(4)]
+        _check(lib().b200fmm_get_results(self._h, *[ctypes.c_void_p(o.ctypes.data) for o in out], 0), "get_results")
+        shape = (R, n) if R > 1 else (n,)
+        return dict(zip(("phi", "fx", "fy", "fz"), (o.reshape(shape) for o in out)))
+
+    def results_device(self, phi, fx, fy, fz):
+        _check(lib().b200fmm_get_results(self._h, *[ctypes.c_void_p(t.data_ptr()) for t in (phi, fx, fy, fz)], 1),
+               "get_results")
+
+    def tree_info(self):
+        nc = np.zeros(self.height, np.int64)
+        npart = ctypes.c_longlong()
+        _check(lib().b200fmm_tree_info(self._h, _ptr(nc, _lp), ctypes.byref(npart)), "tree_info")
+        return nc, npart.value
+
+    def cells(self, level, expansions=True):
+        nc, _ = self.tree_info()
+        n = int(nc[level])
+        keys = np.zeros(n, np.int64)
+        M = np.zeros(n * self.nrhs * self.nn) if expansions else None
+        L = np.zeros(n * self.nrhs * self.nn) if expansions else None
+        _check(lib().b200fmm_get_cells(self._h, level, _ptr(keys, _lp), _ptr(M) if expansions else None,
+                                       _ptr(L) if expansions else None), "get_cells")
+        if not expansions:
+            return keys, None, None
+        return keys, M.reshape(n, self.nrhs, self.nn), L.reshape(n, self.nrhs, self.nn)
+
+    def permutation(self):
+        perm = np.zeros(self.n, np.int64)
+        _check(lib().b200fmm_get_permutation(self._h, _ptr(perm, _lp)), "get_permutation")
+        return perm
+
+    def timings(self):
+        ms = np.zeros(8)
+        _check(lib().b200fmm_last_timings(self._h, _ptr(ms)), "last_timings")
+        return dict(zip(("tree", "p2m", "m2m", "m2l", "l2l", "l2p", "p2p", "total"), ms.tolist()))
+
+    def launch_count(self):
+        c = ctypes.c_longlong()
+        _check(lib().b200fmm_last_launch_count(self._h, ctypes.byref(c)), "last_launch_count")
+        return c.value
+
+
+def direct(x, y, z, q, targets=None):
+    """FP64 direct sum on the GPU for the listed targets (all when None)."""
+    x, y, z, q = _f64(x), _f64(y), _f64(z), _f64(q)
+    t = None if targets is None else np.ascontiguousarray(targets, dtype=np.int64)
+    nt = x.size if t is None else t.size
+    out = [np.zeros(nt) for _ in range(4)]
+    _check(lib().b200fmm_direct(x.size, _ptr(x), _ptr(y), _ptr(z), _ptr(q), -1 if t is None else nt,
+                                None if t is None else _ptr(t, _lp), *[_ptr(o) for o in out]), "direct")
+    return dict(zip(("phi", "fx", "fy", "fz"), out))
+
+
+def rel_l2(a, b):
+    """Relative L2 norm sqrt(sum (b-a)^2 / sum b^2) (FMath::FAccurater, Src/Utils/FMath.hpp:590-592)."""
+    a = np.asarray(a, dtype=np.float64).ravel()
+    b = np.asarray(b, dtype=np.float64).ravel()
+    den = float((b * b).sum())
+    return float(np.sqrt(((a - b) ** 2).sum() / den)) if den > 0 else float(np.sqrt(((a - b) ** 2).sum()))

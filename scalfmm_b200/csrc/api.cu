@@ -1,0 +1,493 @@
+// The C ABI of include/b200fmm.h: handle lifecycle, particle insertion, the algorithm driver and the
+// level-batched operators.  The driver follows FFmmAlgorithmThread::executeCore
+// (Src/Core/FFmmAlgorithmThread.hpp:118-159): bottom pass (P2M), upward pass (M2M, levels height-2..2),
+// transfer pass (M2L, levels 2..height-1), downward pass (L2L, parents at levels 2..height-2), direct
+// pass (L2P + P2P).
+#include "common.cuh"
+
+#include <cmath>
+#include <cstring>
+#include <new>
+
+namespace b200 {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+b200fmm_status fail(b200fmm_status st, const std::string &msg) {
+  g_last_error = msg;
+  return st;
+}
+
+b200fmm_status ensure_scratch(Context &c, size_t bytes) {
+  if (c.scratch_bytes >= bytes) return B200FMM_OK;
+  if (c.d_scratch) cudaFree(c.d_scratch);
+  c.d_scratch = nullptr;
+  c.scratch_bytes = 0;
+  B200_CUDA(cudaMalloc(&c.d_scratch, bytes));
+  c.scratch_bytes = bytes;
+  return B200FMM_OK;
+}
+
+b200fmm_status check_status(Context &c) {
+  int st[4] = {0, 0, 0, 0};
+  B200_CUDA(cudaMemcpyAsync(st, c.d_status, sizeof(st), cudaMemcpyDeviceToHost, c.stream));
+  B200_CUDA(cudaStreamSynchronize(c.stream));
+  if (st[0] || st[1] || st[2] || st[3]) {
+    cudaMemsetAsync(c.d_status, 0, sizeof(st), c.stream);
+    return fail(B200FMM_ERR_CUDA, std::string("a device wait ran out of its iteration budget (") +
+                                      (st[0] ? "P2P" : st[1] ? "M2L" : "kernel") + ")");
+  }
+  return B200FMM_OK;
+}
+
+namespace {
+
+__global__ void scatter_to_original(long long n, int R, const long long *__restrict__ perm,
+                                    const double *__restrict__ a, const double *__restrict__ b,
+                                    const double *__restrict__ c, const double *__restrict__ d, double *__restrict__ oa,
+                                    double *__restrict__ ob, double *__restrict__ oc, double *__restrict__ od) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long long j = perm[i];
+  for (int r = 0; r < R; ++r) {
+    const long long s = (long long)r * n + i, t = (long long)r * n + j;
+    if (oa) oa[t] = a[s];
+    if (ob) ob[t] = b[s];
+    if (oc) oc[t] = c[s];
+    if (od) od[t] = d[s];
+  }
+}
+
+b200fmm_status check_handle(b200fmm_handle h) {
+  if (!h) return fail(B200FMM_ERR_INVALID, "null handle");
+  return B200FMM_OK;
+}
+
+b200fmm_status set_device(Context &c) {
+  B200_CUDA(cudaSetDevice(c.device));
+  return B200FMM_OK;
+}
+
+b200fmm_status need_particles(Context &c) {
+  if (!c.has_particles) return fail(B200FMM_ERR_STATE, "no particles: call b200fmm_set_particles first");
+  return B200FMM_OK;
+}
+
+b200fmm_status zero_state(Context &c) {
+  for (int l = 2; l < c.H; ++l) {
+    const size_t bytes = sizeof(double) * (size_t)c.lv[l].n * c.R * c.nn;
+    if (bytes) {
+      B200_CUDA(cudaMemsetAsync(c.lv[l].M, 0, bytes, c.stream));
+      B200_CUDA(cudaMemsetAsync(c.lv[l].L, 0, bytes, c.stream));
+    }
+  }
+  const size_t pb = sizeof(double) * (size_t)c.N * c.R;
+  for (double *p : {c.d_phi, c.d_fx, c.d_fy, c.d_fz}) B200_CUDA(cudaMemsetAsync(p, 0, pb, c.stream));
+  return B200FMM_OK;
+}
+
+b200fmm_status record(Context &c, int k) {
+  B200_CUDA(cudaEventRecord(c.ev[k], c.stream));
+  return B200FMM_OK;
+}
+
+b200fmm_status run_m2l(Context &c, int level) {
+  if (c.cfg.precision == B200FMM_MIXED) return run_m2l_tc(c, level);
+  return run_m2l_fp64(c, level);
+}
+
+void destroy_context(b200fmm_context *c) {
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_tree(*c);
+  tc_free(*c);
+  for (void *p : {(void *)c->d_roots, (void *)c->d_Troots, (void *)c->d_S, (void *)c->d_pindices, (void *)c->d_pvec,
+                  (void *)c->d_symU, (void *)c->d_symV, (void *)c->d_symoff, (void *)c->d_symrank,
+                  (void *)c->d_dense, (void *)c->d_itab, (void *)c->d_class_order, (void *)c->d_cls_bounds,
+                  (void *)c->d_cls_slots, (void *)c->d_status, c->d_scratch})
+    if (p) cudaFree(p);
+  if (c->events_ready)
+    for (auto &e : c->ev) cudaEventDestroy(e);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+}  // namespace
+}  // namespace b200
+
+using namespace b200;
+
+extern "C" {
+
+const char *b200fmm_last_error(void) { return g_last_error.c_str(); }
+
+const char *b200fmm_version(void) { return "b200fmm 0.1 (sm_100a)"; }
+
+b200fmm_status b200fmm_create(const b200fmm_config *cfg, b200fmm_handle *out) {
+  if (!cfg || !out) return fail(B200FMM_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (cfg->kernel < 0 || cfg->kernel > 2) return fail(B200FMM_ERR_INVALID, "unknown kernel");
+  if (cfg->order < 3 || cfg->order > kMaxOrder) return fail(B200FMM_ERR_INVALID, "order must be in [3, 8]");
+  if (cfg->height < 3 || cfg->height > kMaxHeight) return fail(B200FMM_ERR_INVALID, "height must be in [3, 12]");
+  if (cfg->nrhs < 1 || cfg->nrhs > kMaxNrhs) return fail(B200FMM_ERR_INVALID, "nrhs must be in [1, 32]");
+  if (cfg->precision != B200FMM_FP64 && cfg->precision != B200FMM_MIXED)
+    return fail(B200FMM_ERR_INVALID, "unknown precision");
+  if (!(cfg->box_width > 0) || !std::isfinite(cfg->box_width)) return fail(B200FMM_ERR_INVALID, "bad box width");
+  for (int d = 0; d < 3; ++d)
+    if (!std::isfinite(cfg->center[d])) return fail(B200FMM_ERR_INVALID, "bad box centre");
+  b200fmm_context *c = new (std::nothrow) b200fmm_context();
+  if (!c) return fail(B200FMM_ERR_OOM, "host allocation failed");
+  c->cfg = *cfg;
+  c->p = cfg->order;
+  c->nn = c->p * c->p * c->p;
+  c->H = cfg->height;
+  c->R = cfg->nrhs;
+  if (cfg->device >= 0) {
+    c->device = cfg->device;
+  } else if (cudaGetDevice(&c->device) != cudaSuccess) {
+    delete c;
+    return fail(B200FMM_ERR_CUDA, "no CUDA device");
+  }
+  b200fmm_status st = set_device(*c);
+  if (st == B200FMM_OK) {
+    if (cfg->stream) {
+      c->stream = (cudaStream_t)cfg->stream;
+    } else {
+      if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+        st = fail(B200FMM_ERR_CUDA, "stream creation failed");
+      c->own_stream = true;
+    }
+  }
+  if (st == B200FMM_OK) {
+    bool ok = true;
+    for (auto &e : c->ev) ok = ok && cudaEventCreate(&e) == cudaSuccess;
+    c->events_ready = ok;
+    if (!ok) st = fail(B200FMM_ERR_CUDA, "event creation failed");
+  }
+  if (st == B200FMM_OK) {
+    if (cudaMalloc(&c->d_status, 16 * sizeof(int)) != cudaSuccess ||
+        cudaMemset(c->d_status, 0, 16 * sizeof(int)) != cudaSuccess)
+      st = fail(B200FMM_ERR_OOM, "status allocation failed");
+  }
+  if (st == B200FMM_OK) st = build_tables(*c);
+  if (st == B200FMM_OK && cfg->kernel == B200FMM_CHEB_SYM && cfg->precision == B200FMM_FP64) {
+    st = compress_sym_operators(*c);
+    if (st == B200FMM_OK) st = upload_sym_operators(*c);
+  }
+  if (st == B200FMM_OK && cfg->kernel != B200FMM_CHEB_SYM && cfg->precision == B200FMM_FP64)
+    st = build_dense_operators(*c);
+  if (st == B200FMM_OK && cfg->precision == B200FMM_MIXED) st = tc_init(*c);
+  if (st != B200FMM_OK) {
+    destroy_context(c);
+    return st;
+  }
+  *out = c;
+  return B200FMM_OK;
+}
+
+b200fmm_status b200fmm_destroy(b200fmm_handle h) {
+  if (!h) return B200FMM_OK;
+  destroy_context(h);
+  return B200FMM_OK;
+}
+
+b200fmm_status b200fmm_set_sym_operators(b200fmm_handle h, const int *ranks, const double *uv, long long uv_len) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  if (c.cfg.kernel != B200FMM_CHEB_SYM || c.cfg.precision != B200FMM_FP64)
+    return fail(B200FMM_ERR_STATE, "symmetric operators apply to the FP64 CHEB_SYM kernel only");
+  if (!ranks || !uv) return fail(B200FMM_ERR_INVALID, "null argument");
+  long long need = 0;
+  int nclass = 0;
+  for (int t = 0; t < 343; ++t) {
+    if (ranks[t] < 0 || ranks[t] > c.nn) return fail(B200FMM_ERR_INVALID, "rank out of range");
+    if (ranks[t] > 0) ++nclass;
+    need += 2LL * ranks[t] * c.nn;
+  }
+  if (nclass != 16) return fail(B200FMM_ERR_INVALID, "expected operators for exactly 16 class slots");
+  if (uv_len != need) return fail(B200FMM_ERR_INVALID, "uv length does not match the ranks");
+  B200_CHECK(set_device(c));
+  c.sym_ranks.assign(ranks, ranks + 343);
+  c.sym_uv.assign(uv, uv + need);
+  return upload_sym_operators(c);
+}
+
+b200fmm_status b200fmm_get_sym_operators(b200fmm_handle h, int *ranks, double *uv, long long uv_cap,
+                                         long long *uv_len) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  if (c.sym_ranks.empty()) return fail(B200FMM_ERR_STATE, "this handle has no symmetric operators");
+  if (uv_len) *uv_len = (long long)c.sym_uv.size();
+  if (ranks) std::memcpy(ranks, c.sym_ranks.data(), sizeof(int) * 343);
+  if (uv) {
+    if (uv_cap < (long long)c.sym_uv.size()) return fail(B200FMM_ERR_INVALID, "uv buffer too small");
+    std::memcpy(uv, c.sym_uv.data(), sizeof(double) * c.sym_uv.size());
+  }
+  return B200FMM_OK;
+}
+
+b200fmm_status b200fmm_set_particles(b200fmm_handle h, long long n, const double *x, const double *y,
+                                     const double *z, const double *q, int on_device) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  if (n < 1 || n > 2000000000LL) return fail(B200FMM_ERR_INVALID, "particle count must be in [1, 2e9]");
+  if (!x || !y || !z || !q) return fail(B200FMM_ERR_INVALID, "null particle array");
+  B200_CHECK(set_device(c));
+  B200_CUDA(cudaStreamSynchronize(c.stream));
+  free_tree(c);
+  c.N = n;
+  B200_CUDA(cudaEventRecord(c.ev[14], c.stream));
+  b200fmm_status st = build_tree(c, x, y, z, q, on_device != 0);
+  if (st != B200FMM_OK) {
+    free_tree(c);
+    return st;
+  }
+  B200_CUDA(cudaEventRecord(c.ev[15], c.stream));
+  B200_CUDA(cudaEventSynchronize(c.ev[15]));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c.ev[14], c.ev[15]);
+  c.ms[0] = ms;
+  c.has_particles = true;
+  return B200FMM_OK;
+}
+
+b200fmm_status b200fmm_set_charges(b200fmm_handle h, const double *q, int on_device) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  B200_CHECK(need_particles(c));
+  if (!q) return fail(B200FMM_ERR_INVALID, "null charges");
+  B200_CHECK(set_device(c));
+  B200_CHECK(upload_charges(c, q, on_device != 0));
+  if (c.d_pq32) {
+    cudaFreeAsync(c.d_pq32, c.stream);
+    c.d_pq32 = nullptr;
+  }
+  return B200FMM_OK;
+}
+
+b200fmm_status b200fmm_reset_expansions(b200fmm_handle h) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  B200_CHECK(need_particles(c));
+  B200_CHECK(set_device(c));
+  return zero_state(c);
+}
+
+b200fmm_status b200fmm_execute(b200fmm_handle h, unsigned ops) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  B200_CHECK(need_particles(c));
+  B200_CHECK(set_device(c));
+  c.launches = 0;
+  const int LL = c.H - 1;
+  B200_CHECK(record(c, 0));
+  B200_CHECK(zero_state(c));
+  B200_CHECK(record(c, 1));
+  if (ops & B200FMM_P2M) B200_CHECK(run_p2m(c));
+  B200_CHECK(record(c, 2));
+  if (ops & B200FMM_M2M)
+    for (int l = LL - 1; l >= 2; --l) B200_CHECK(run_m2m(c, l));
+  B200_CHECK(record(c, 3));
+  if (ops & B200FMM_M2L) {
+    if (c.cfg.precision == B200FMM_MIXED)
+      B200_CHECK(run_m2l_tc(c, -1));  // one launch for every level
+    else
+      for (int l = 2; l <= LL; ++l) B200_CHECK(run_m2l_fp64(c, l));
+  }
+  B200_CHECK(record(c, 4));
+  if (ops & B200FMM_L2L)
+    for (int l = 2; l <= LL - 1; ++l) B200_CHECK(run_l2l(c, l));
+  B200_CHECK(record(c, 5));
+  if (ops & B200FMM_L2P) B200_CHECK(run_l2p(c));
+  B200_CHECK(record(c, 6));
+  if (ops & B200FMM_P2P) B200_CHECK(run_p2p(c, 0));
+  B200_CHECK(record(c, 7));
+  return B200FMM_OK;
+}
+
+b200fmm_status b200fmm_p2m(b200fmm_handle h) {
+  B200_CHECK(check_handle(h));
+  B200_CHECK(need_particles(*h));
+  B200_CHECK(set_device(*h));
+  return run_p2m(*h);
+}
+
+b200fmm_status b200fmm_m2m(b200fmm_handle h, int level) {
+  B200_CHECK(check_handle(h));
+  B200_CHECK(need_particles(*h));
+  B200_CHECK(set_device(*h));
+  return run_m2m(*h, level);
+}
+
+b200fmm_status b200fmm_m2l(b200fmm_handle h, int level) {
+  B200_CHECK(check_handle(h));
+  B200_CHECK(need_particles(*h));
+  B200_CHECK(set_device(*h));
+  if (level < 2 || level > h->H - 1) return fail(B200FMM_ERR_INVALID, "m2l: level must be in [2, height-1]");
+  return run_m2l(*h, level);
+}
+
+b200fmm_status b200fmm_l2l(b200fmm_handle h, int level) {
+  B200_CHECK(check_handle(h));
+  B200_CHECK(need_particles(*h));
+  B200_CHECK(set_device(*h));
+  return run_l2l(*h, level);
+}
+
+b200fmm_status b200fmm_l2p(b200fmm_handle h) {
+  B200_CHECK(check_handle(h));
+  B200_CHECK(need_particles(*h));
+  B200_CHECK(set_device(*h));
+  return run_l2p(*h);
+}
+
+b200fmm_status b200fmm_p2p(b200fmm_handle h, int variant) {
+  B200_CHECK(check_handle(h));
+  B200_CHECK(need_particles(*h));
+  if (variant != 0 && variant != 1) return fail(B200FMM_ERR_INVALID, "p2p variant must be 0 or 1");
+  B200_CHECK(set_device(*h));
+  return run_p2p(*h, variant);
+}
+
+b200fmm_status b200fmm_get_results(b200fmm_handle h, double *phi, double *fx, double *fy, double *fz,
+                                   int on_device) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  B200_CHECK(need_particles(c));
+  B200_CHECK(set_device(c));
+  const long long n = c.N;
+  const size_t bytes = sizeof(double) * n * c.R;
+  if (on_device) {
+    scatter_to_original<<<grid_for(n, 256), 256, 0, c.stream>>>(n, c.R, c.d_perm, c.d_phi, c.d_fx, c.d_fy, c.d_fz, phi,
+                                                                fx, fy, fz);
+    B200_CUDA(cudaGetLastError());
+    return B200FMM_OK;
+  }
+  B200_CHECK(ensure_scratch(c, 4 * bytes + 4096));
+  double *o = (double *)((char *)c.d_scratch + 4096);
+  scatter_to_original<<<grid_for(n, 256), 256, 0, c.stream>>>(n, c.R, c.d_perm, c.d_phi, c.d_fx, c.d_fy, c.d_fz, o,
+                                                              o + n * c.R, o + 2 * n * c.R, o + 3 * n * c.R);
+  B200_CUDA(cudaGetLastError());
+  double *dst[4] = {phi, fx, fy, fz};
+  for (int k = 0; k < 4; ++k)
+    if (dst[k]) B200_CUDA(cudaMemcpyAsync(dst[k], o + k * n * c.R, bytes, cudaMemcpyDeviceToHost, c.stream));
+  B200_CUDA(cudaStreamSynchronize(c.stream));
+  return check_status(c);
+}
+
+b200fmm_status b200fmm_synchronize(b200fmm_handle h) {
+  B200_CHECK(check_handle(h));
+  B200_CHECK(set_device(*h));
+  B200_CUDA(cudaStreamSynchronize(h->stream));
+  return check_status(*h);
+}
+
+b200fmm_status b200fmm_tree_info(b200fmm_handle h, long long *ncells, long long *nparticles) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  B200_CHECK(need_particles(c));
+  if (ncells)
+    for (int l = 0; l < c.H; ++l) ncells[l] = c.lv[l].n;
+  if (nparticles) *nparticles = c.N;
+  return B200FMM_OK;
+}
+
+b200fmm_status b200fmm_get_cells(b200fmm_handle h, int level, long long *keys, double *multipoles, double *locals) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  B200_CHECK(need_particles(c));
+  if (level < 0 || level >= c.H) return fail(B200FMM_ERR_INVALID, "level out of range");
+  B200_CHECK(set_device(c));
+  const Level &L = c.lv[level];
+  if (keys) B200_CUDA(cudaMemcpyAsync(keys, L.keys, sizeof(long long) * L.n, cudaMemcpyDeviceToHost, c.stream));
+  const size_t bytes = sizeof(double) * (size_t)L.n * c.R * c.nn;
+  if (multipoles) {
+    if (!L.M) return fail(B200FMM_ERR_INVALID, "no expansions above level 2");
+    B200_CUDA(cudaMemcpyAsync(multipoles, L.M, bytes, cudaMemcpyDeviceToHost, c.stream));
+  }
+  if (locals) {
+    if (!L.L) return fail(B200FMM_ERR_INVALID, "no expansions above level 2");
+    B200_CUDA(cudaMemcpyAsync(locals, L.L, bytes, cudaMemcpyDeviceToHost, c.stream));
+  }
+  B200_CUDA(cudaStreamSynchronize(c.stream));
+  return B200FMM_OK;
+}
+
+b200fmm_status b200fmm_get_permutation(b200fmm_handle h, long long *perm) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  B200_CHECK(need_particles(c));
+  if (!perm) return fail(B200FMM_ERR_INVALID, "null argument");
+  B200_CHECK(set_device(c));
+  B200_CUDA(cudaMemcpyAsync(perm, c.d_perm, sizeof(long long) * c.N, cudaMemcpyDeviceToHost, c.stream));
+  B200_CUDA(cudaStreamSynchronize(c.stream));
+  return B200FMM_OK;
+}
+
+b200fmm_status b200fmm_last_timings(b200fmm_handle h, double *ms8) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  if (!ms8) return fail(B200FMM_ERR_INVALID, "null argument");
+  B200_CHECK(set_device(c));
+  B200_CUDA(cudaEventSynchronize(c.ev[7]));
+  ms8[0] = c.ms[0];
+  for (int k = 1; k <= 6; ++k) {
+    float t = 0;
+    if (cudaEventElapsedTime(&t, c.ev[k], c.ev[k + 1]) != cudaSuccess) t = 0;
+    ms8[k] = t;
+  }
+  float tot = 0;
+  if (cudaEventElapsedTime(&tot, c.ev[0], c.ev[7]) != cudaSuccess) tot = 0;
+  ms8[7] = tot;
+  return B200FMM_OK;
+}
+
+b200fmm_status b200fmm_last_launch_count(b200fmm_handle h, long long *count) {
+  B200_CHECK(check_handle(h));
+  if (!count) return fail(B200FMM_ERR_INVALID, "null argument");
+  *count = h->launches + h->tree_launches;
+  return B200FMM_OK;
+}
+
+b200fmm_status b200fmm_direct(long long n, const double *x, const double *y, const double *z, const double *q,
+                              long long ntargets, const long long *targets, double *phi, double *fx, double *fy,
+                              double *fz) {
+  if (n < 1 || !x || !y || !z || !q || !phi || !fx || !fy || !fz) return fail(B200FMM_ERR_INVALID, "bad argument");
+  const long long nt = ntargets < 0 ? n : ntargets;
+  if (ntargets >= 0 && !targets) return fail(B200FMM_ERR_INVALID, "null target list");
+  for (long long k = 0; ntargets >= 0 && k < nt; ++k)
+    if (targets[k] < 0 || targets[k] >= n) return fail(B200FMM_ERR_INVALID, "target index out of range");
+  cudaStream_t s;
+  B200_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  double *d = nullptr;
+  long long *dt = nullptr;
+  const size_t in_bytes = sizeof(double) * n * 4, out_bytes = sizeof(double) * nt * 4;
+  cudaError_t e = cudaMallocAsync(&d, in_bytes + out_bytes, s);
+  if (e == cudaSuccess && ntargets >= 0) e = cudaMallocAsync(&dt, sizeof(long long) * nt, s);
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(s);
+    return fail(B200FMM_ERR_OOM, "device allocation failed");
+  }
+  cudaMemcpyAsync(d, x, sizeof(double) * n, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(d + n, y, sizeof(double) * n, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(d + 2 * n, z, sizeof(double) * n, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(d + 3 * n, q, sizeof(double) * n, cudaMemcpyHostToDevice, s);
+  if (dt) cudaMemcpyAsync(dt, targets, sizeof(long long) * nt, cudaMemcpyHostToDevice, s);
+  double *o = d + 4 * n;
+  b200fmm_status st = run_direct(n, d, d + n, d + 2 * n, d + 3 * n, nt, dt, o, o + nt, o + 2 * nt, o + 3 * nt, s);
+  if (st == B200FMM_OK) {
+    double *dst[4] = {phi, fx, fy, fz};
+    for (int k = 0; k < 4; ++k) cudaMemcpyAsync(dst[k], o + k * nt, sizeof(double) * nt, cudaMemcpyDeviceToHost, s);
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = fail(B200FMM_ERR_CUDA, cudaGetErrorString(e));
+  }
+  cudaFreeAsync(d, s);
+  if (dt) cudaFreeAsync(dt, s);
+  cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  return st;
+}
+
+}  // extern "C"

@@ -1,0 +1,203 @@
+// Shared definitions of the b200fmm library: the handle (context), the per-level tree storage,
+// error plumbing and small device helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/b200fmm.h"
+
+namespace b200 {
+
+constexpr int kMaxOrder = 8;
+constexpr int kMaxHeight = 12;
+constexpr int kMaxNrhs = 32;
+
+// Error reporting: the last message per host thread.
+void set_error(const std::string &msg);
+b200fmm_status fail(b200fmm_status st, const std::string &msg);
+
+#define B200_CUDA(call)                                                                                   \
+  do {                                                                                                    \
+    cudaError_t e_ = (call);                                                                              \
+    if (e_ != cudaSuccess)                                                                                \
+      return ::b200::fail(e_ == cudaErrorMemoryAllocation ? B200FMM_ERR_OOM : B200FMM_ERR_CUDA,          \
+                          std::string(#call) + ": " + cudaGetErrorString(e_));                          \
+  } while (0)
+
+#define B200_CHECK(st)                  \
+  do {                                  \
+    b200fmm_status s_ = (st);           \
+    if (s_ != B200FMM_OK) return s_;    \
+  } while (0)
+
+// One level of the octree.  Cells are the non-empty cells of the level in Morton order.
+struct Level {
+  long long n = 0;
+  long long *keys = nullptr;  // [n] Morton keys (device)
+  int *parent = nullptr;      // [n] index of the parent cell at level-1 (device)
+  int *child = nullptr;       // [n][8] index of child cells at level+1, -1 if empty (device)
+  int *ilist = nullptr;       // [n][189] source cell of each interaction-list entry, -1 if empty (device)
+  double *M = nullptr;        // [n][nrhs][p^3] multipole expansions (device)
+  double *L = nullptr;        // [n][nrhs][p^3] local expansions (device)
+  int *grid = nullptr;        // [side^3] cell index by (x,y,z) grid position, -1 if empty (device, MIXED)
+};
+
+// Interaction-list candidates of a target with Morton child index c (0..7): the children of the
+// parent's 26 neighbours that are not adjacent to the target (FTreeCoordinate.hpp:219-264).
+struct IListTable {
+  int n[8];                  // 189 for every child type
+  signed char off[8][189][3];
+  short slot[8][189];        // ((dx+3)*7+(dy+3))*7+(dz+3)
+};
+
+struct DenseTC;  // tensor-core M2L state (m2l_tc.cu)
+
+struct Context {
+  b200fmm_config cfg{};
+  int p = 0, nn = 0, H = 0, R = 1;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int device = 0;
+
+  // interpolation tables (device)
+  double *d_roots = nullptr;     // [p]
+  double *d_Troots = nullptr;    // [p][p]  T_o(root_j) (Chebyshev only)
+  double *d_S = nullptr;         // [8][3][p][p] child->parent 1-D interpolators
+
+  // symmetric compressed operators (host copy + device)
+  std::vector<int> sym_ranks;        // [343]
+  std::vector<double> sym_uv;        // reference layout
+  int *d_pindices = nullptr;         // [343]
+  int *d_pvec = nullptr;             // [343][nn]
+  double *d_symU = nullptr;          // per class slot: U^T stored [r][nn] (= the reference's column-major U)
+  double *d_symV = nullptr;          // per class slot: V^T stored [r][nn]
+  long long *d_symoff = nullptr;     // [343] element offset of slot's U/V in d_symU/d_symV, -1 if none
+  int *d_symrank = nullptr;          // [343]
+  int max_rank = 0;
+
+  // dense FP64 operators (CHEB_DENSE / LAGRANGE in FP64): [343][nn][nn], zero for near slots
+  double *d_dense = nullptr;
+
+  IListTable itab{};
+  IListTable *d_itab = nullptr;
+  int *d_class_order = nullptr;  // [8][189] list entries of child type c ordered by symmetry class
+  int *d_cls_bounds = nullptr;   // [8][17] start of each class's run in d_class_order (16 classes + end)
+  std::vector<int> cls_slots;    // the 16 class slots in increasing order
+  int *d_cls_slots = nullptr;    // same, on the device
+
+  // particles (sorted by Morton key, stable)
+  long long N = 0;
+  double *d_x = nullptr, *d_y = nullptr, *d_z = nullptr;  // sorted positions
+  double *d_q = nullptr;                                  // [R][N] sorted charges
+  long long *d_perm = nullptr;                            // sorted -> original
+  long long *d_leaf_start = nullptr;                      // [nleaves+1]
+  int *d_leaf_nbr = nullptr;                              // [nleaves][27] (13 = self), -1 if empty
+  float4 *d_pq32 = nullptr;                               // [R][N] leaf-local FP32 (x,y,z,q) (MIXED)
+  double *d_phi = nullptr, *d_fx = nullptr, *d_fy = nullptr, *d_fz = nullptr;  // [R][N] sorted results
+  Level lv[kMaxHeight];
+  bool has_particles = false;
+
+  // device status words set by kernels whose bounded waits ran out (0 = fine); checked by the host at
+  // every synchronising call
+  int *d_status = nullptr;
+
+  // scratch
+  void *d_scratch = nullptr;
+  size_t scratch_bytes = 0;
+
+  DenseTC *tc = nullptr;
+
+  // timings / counters
+  cudaEvent_t ev[16];
+  bool events_ready = false;
+  double ms[8] = {0};
+  long long launches = 0;       // kernel launches of the last execute()
+  long long tree_launches = 0;  // kernel launches of the last set_particles()
+};
+
+b200fmm_status ensure_scratch(Context &c, size_t bytes);
+b200fmm_status check_status(Context &c);
+
+// ---- module entry points -------------------------------------------------------------------------
+// precompute.cu
+b200fmm_status build_tables(Context &c);
+b200fmm_status compress_sym_operators(Context &c);
+b200fmm_status upload_sym_operators(Context &c);
+b200fmm_status build_dense_operators(Context &c);
+// tree.cu
+b200fmm_status build_tree(Context &c, const double *x, const double *y, const double *z, const double *q,
+                          bool on_device);
+b200fmm_status upload_charges(Context &c, const double *q, bool on_device);
+void free_tree(Context &c);
+// interp.cu
+b200fmm_status run_p2m(Context &c);
+b200fmm_status run_m2m(Context &c, int level);
+b200fmm_status run_l2l(Context &c, int level);
+b200fmm_status run_l2p(Context &c);
+// p2p.cu
+b200fmm_status run_p2p(Context &c, int variant);
+// m2l_fp64.cu
+b200fmm_status run_m2l_fp64(Context &c, int level);
+// m2l_tc.cu
+b200fmm_status tc_init(Context &c);
+void tc_free(Context &c);
+b200fmm_status run_m2l_tc(Context &c, int level);
+// direct.cu
+b200fmm_status run_direct(long long n, const double *x, const double *y, const double *z, const double *q,
+                          long long nt, const long long *targets, double *phi, double *fx, double *fy, double *fz,
+                          cudaStream_t s);
+
+// ---- device helpers --------------------------------------------------------------------------------
+__host__ __device__ inline long long morton_encode3(int ix, int iy, int iz) {
+  long long key = 0;
+#pragma unroll
+  for (int b = 0; b < 21; ++b) {
+    key |= (long long)((iz >> b) & 1) << (3 * b);
+    key |= (long long)((iy >> b) & 1) << (3 * b + 1);
+    key |= (long long)((ix >> b) & 1) << (3 * b + 2);
+  }
+  return key;
+}
+
+__host__ __device__ inline void morton_decode3(long long key, int &ix, int &iy, int &iz) {
+  int x = 0, y = 0, z = 0;
+#pragma unroll
+  for (int b = 0; b < 21; ++b) {
+    z |= (int)((key >> (3 * b)) & 1) << b;
+    y |= (int)((key >> (3 * b + 1)) & 1) << b;
+    x |= (int)((key >> (3 * b + 2)) & 1) << b;
+  }
+  ix = x;
+  iy = y;
+  iz = z;
+}
+
+// Index of key in sorted keys[0..n), or -1.
+__device__ inline int find_key(const long long *keys, long long n, long long key) {
+  long long lo = 0, hi = n;
+  while (lo < hi) {
+    const long long mid = (lo + hi) >> 1;
+    if (keys[mid] < key)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return (lo < n && keys[lo] == key) ? (int)lo : -1;
+}
+
+inline unsigned grid_for(long long n, int block) {
+  long long g = (n + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > 2147483647LL) g = 2147483647LL;
+  return (unsigned)g;
+}
+
+}  // namespace b200
+
+// The opaque handle type of the C ABI is the context itself.
+struct b200fmm_context : public b200::Context {};

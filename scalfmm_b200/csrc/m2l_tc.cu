@@ -1,0 +1,654 @@
+// Tensor-core M2L (MIXED precision) on tcgen05 / TMEM, fed by TMA.
+//
+// The transfer pass of FFmmAlgorithmThread (Src/Core/FFmmAlgorithmThread.hpp:271-322) applies, for every
+// target cell and every source of its interaction list, L_target += scale * K_t M_source with K_t the dense
+// p^3 x p^3 operator of transfer vector t (FChebDenseM2LHandler.hpp:178-215; FUnifM2LHandler applies the same
+// operator for the Lagrange basis).  Here this is recast as GEMMs:
+//
+//   * Cells of a level are stored as a dense grid split by parity (the Morton child index c of the cell):
+//     A[rhs*8 + c][z/2][y/2][x/2][node].  All targets of parity c share the same 189 transfer vectors, and
+//     for a fixed (c, t) every source lies in parity c' = c + t (mod 2) at a constant half-grid shift, so a
+//     tile of 8x4x4 targets maps to a tile of 8x4x4 sources that one 5-D TMA box load fetches (out-of-range
+//     boxes are zero-filled by the TMA unit, which supplies the domain boundary).
+//   * One work item = (level, rhs, parity, 128-target tile, a range of the 189 transfer vectors).  The
+//     accumulator D (128 targets x p^3 nodes, FP32) lives in TMEM; per transfer vector and 32-node K chunk
+//     the MMA warp issues D += A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T (split FP16: a = hi + lo carries
+//     22 significant bits; operands are pre-scaled by powers of two so that lo stays normal).
+//   * The MMA accumulator is reset at the start of every segment of a transfer vector's K chunks (a
+//     segment is NK / nseg chunks): the tensor-core FP32 accumulation loses about a third of an ulp of the
+//     running value per instruction, always in the same direction, so its error grows linearly with the
+//     chain length.  After each segment the epilogue warps read D with tcgen05.ld and add it to running
+//     sums held in registers with ordinary IEEE FP32 adds; at the end of a work item they add
+//     scale * 2^-(sA+sB) * sum into the FP64 locals (atomic adds: several items of the same tile contribute).
+//
+// Roles: warp 0 = TMA producer (one elected thread), warp 1 = MMA issuer (one thread) and TMEM owner,
+// warps 2..9 = epilogue (TMEM lane quarter = warp % 4, column half = (warp - 2) / 4).  Shared memory: STAGES x {A_hi, A_lo, B_hi, B_lo}
+// K-chunks with the 64-byte swizzle the UMMA descriptors describe.  Every mbarrier wait is bounded; a wait
+// that runs out sets a device status word, the CTA abandons its work, frees its TMEM and returns.
+#include "common.cuh"
+
+#include <cuda.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+
+namespace b200 {
+
+namespace {
+
+constexpr int TC_THREADS = 320;
+constexpr int TILE_X = 8, TILE_Y = 4, TILE_Z = 4;  // 128 targets
+constexpr int KCHUNK = 32;                          // fp16 elements per 64-byte swizzle row
+constexpr int SB = 15;                              // operator pre-scale 2^15
+constexpr int MAX_STAGES = 4;
+constexpr long long WAIT_LIMIT = 1LL << 22;
+
+struct TcItem {
+  short level, rhs, parity, split;
+  short bx, by, bz;
+  short t0, t1;
+};
+
+struct TcLevel {
+  int HX, HY, HZ;      // padded half-grid extents
+  int side;            // real grid side 2^level
+  int *grid;           // [side^3] cell index or -1
+  double *L;           // locals of the level
+  double *scale_out;   // device scalar: scale_l * 2^-(sA + SB)
+};
+
+struct __align__(64) TcParams {
+  CUtensorMap mapA_hi[kMaxHeight];
+  CUtensorMap mapA_lo[kMaxHeight];
+  CUtensorMap mapB_hi;
+  CUtensorMap mapB_lo;
+  TcLevel lv[kMaxHeight];
+  const TcItem *items;
+  int item0, nitems;  // items [item0, item0 + nitems) of the list run in this launch
+  int R, nn, KP, NP, NH, NHALF, NK, stages, ncols;
+  int nseg;  // accumulator resets per transfer vector (the K chunks are split into nseg segments)
+  int stage_bytes;
+  signed char off[8][189][3];
+  short slot[8][189];
+  int *status;
+};
+
+// ---- PTX helpers ----------------------------------------------------------------------------------
+__device__ __forceinline__ unsigned su32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *b, unsigned n) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(b)), "r"(n));
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long *b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity) {
+  for (long long it = 0; it < WAIT_LIMIT; ++it) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(su32(b)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, unsigned long long *bar, int c0, int c1,
+                                            int c2, int c3, int c4) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6, %7}], "
+      "[%2];" ::"r"(su32(dst)),
+      "l"(map), "r"(su32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4)
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, unsigned long long *bar, int c0, int c1,
+                                            int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(
+          su32(dst)),
+      "l"(map), "r"(su32(bar)), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+// UMMA shared-memory descriptor: K-major, 64-byte swizzle, rows of 64 B in 8-row groups 512 B apart.
+__device__ __forceinline__ unsigned long long sdesc(const void *p) {
+  const unsigned long long a = su32(p);
+  return ((a >> 4) & 0x3FFFull) | (1ull << 16) | (32ull << 32) | (1ull << 46) | (4ull << 61);
+}
+__device__ __forceinline__ void mma_f16(unsigned d_tmem, unsigned long long da, unsigned long long db, unsigned idesc,
+                                        unsigned accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+          d_tmem),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+}
+__device__ __forceinline__ void mma_commit(unsigned long long *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(unsigned taddr, float *v) {
+  unsigned r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_ld16(unsigned taddr, unsigned *r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+      "[%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+
+// ---- the kernel -------------------------------------------------------------------------------------
+// CW: accumulator columns owned by one epilogue thread (NP / 2), a compile-time constant so that the
+// running sums stay in registers.
+template <int CW>
+__global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_constant__ TcParams P) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // 1024-byte aligned stage buffers (the swizzle pattern repeats every 512 B)
+  unsigned char *smem = (unsigned char *)(((unsigned long long)smem_raw + 1023) & ~1023ull);
+  __shared__ __align__(8) unsigned long long full_bar[MAX_STAGES], empty_bar[MAX_STAGES];
+  __shared__ __align__(8) unsigned long long acc_full, acc_empty;
+  __shared__ unsigned tmem_base_sh;
+  __shared__ volatile int abort_sh;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int S = P.stages;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(&acc_full, 1);
+    mbar_init(&acc_empty, 8);  // one arrive per epilogue warp
+    abort_sh = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_base_sh)),
+                 "r"(P.ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const unsigned tmem = tmem_base_sh;
+
+  const int a_bytes = TILE_X * TILE_Y * TILE_Z * KCHUNK * 2;  // 8 KB
+  const int b_bytes = P.NP * KCHUNK * 2;
+
+  if (warp == 0) {
+    // ------------------------------------------------ TMA producer
+    if (lane == 0) {
+      int stage = 0;
+      unsigned phase = 0;
+      for (int it = blockIdx.x; it < P.nitems && !abort_sh; it += gridDim.x) {
+        const TcItem w = P.items[P.item0 + it];
+        const int c = w.parity;
+        const int cx = (c >> 2) & 1, cy = (c >> 1) & 1, cz = c & 1;
+        for (int e = w.t0; e < w.t1 && !abort_sh; ++e) {
+          const int dx = P.off[c][e][0], dy = P.off[c][e][1], dz = P.off[c][e][2];
+          const int sp = (((cx + dx) & 1) << 2) | (((cy + dy) & 1) << 1) | ((cz + dz) & 1);
+          const int ox = w.bx * TILE_X + ((cx + dx) >> 1), oy = w.by * TILE_Y + ((cy + dy) >> 1),
+                    oz = w.bz * TILE_Z + ((cz + dz) >> 1);
+          const int slot = P.slot[c][e];
+          for (int kc = 0; kc < P.NK; ++kc) {
+            if (!mbar_wait(&empty_bar[stage], phase ^ 1)) {
+              atomicExch(P.status + 1, 1);
+              abort_sh = 1;
+              break;
+            }
+            unsigned char *sbuf = smem + (size_t)stage * P.stage_bytes;
+            mbar_expect_tx(&full_bar[stage], 2 * a_bytes + 2 * b_bytes);
+            tma_load_5d(sbuf, &P.mapA_hi[w.level], &full_bar[stage], kc * KCHUNK, ox, oy, oz, w.rhs * 8 + sp);
+            tma_load_5d(sbuf + a_bytes, &P.mapA_lo[w.level], &full_bar[stage], kc * KCHUNK, ox, oy, oz,
+                        w.rhs * 8 + sp);
+            for (int h = 0; h < P.NHALF; ++h) {
+              tma_load_3d(sbuf + 2 * a_bytes + h * P.NH * 64, &P.mapB_hi, &full_bar[stage], kc * KCHUNK, h * P.NH, slot);
+              tma_load_3d(sbuf + 2 * a_bytes + b_bytes + h * P.NH * 64, &P.mapB_lo, &full_bar[stage], kc * KCHUNK,
+                          h * P.NH, slot);
+            }
+            if (++stage == S) {
+              stage = 0;
+              phase ^= 1;
+            }
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      const unsigned idesc = (1u << 4) | ((unsigned)(P.NH >> 3) << 17) | ((unsigned)(128 >> 4) << 24);
+      int stage = 0;
+      unsigned phase = 0, acc_phase = 0;
+      for (int it = blockIdx.x; it < P.nitems && !abort_sh; it += gridDim.x) {
+        const TcItem w = P.items[P.item0 + it];
+        for (int e = w.t0; e < w.t1 && !abort_sh; ++e) {
+          for (int sg = 0; sg < P.nseg && !abort_sh; ++sg) {
+            const int k0 = sg * P.NK / P.nseg, k1 = (sg + 1) * P.NK / P.nseg;
+            // the epilogue has drained the accumulator of the previous segment
+            if (!mbar_wait(&acc_empty, acc_phase ^ 1)) {
+              atomicExch(P.status + 1, 1);
+              abort_sh = 1;
+              break;
+            }
+            acc_phase ^= 1;
+            tc_fence_after();
+            bool first = true;
+            for (int kc = k0; kc < k1; ++kc) {
+              if (!mbar_wait(&full_bar[stage], phase)) {
+                atomicExch(P.status + 1, 1);
+                abort_sh = 1;
+                break;
+              }
+              tc_fence_after();
+              const unsigned char *sbuf = smem + (size_t)stage * P.stage_bytes;
+              const unsigned char *ahi = sbuf, *alo = sbuf + a_bytes;
+              const unsigned char *bhi = sbuf + 2 * a_bytes, *blo = sbuf + 2 * a_bytes + b_bytes;
+#pragma unroll
+              for (int ks = 0; ks < 2; ++ks) {
+                for (int h = 0; h < P.NHALF; ++h) {
+                  const unsigned d = tmem + h * P.NH;
+                  const int bo = h * P.NH * 64 + ks * 32;
+                  // the small cross terms first, the leading term last
+                  mma_f16(d, sdesc(ahi + ks * 32), sdesc(blo + bo), idesc, first ? 0u : 1u);
+                  mma_f16(d, sdesc(alo + ks * 32), sdesc(bhi + bo), idesc, 1u);
+                  mma_f16(d, sdesc(ahi + ks * 32), sdesc(bhi + bo), idesc, 1u);
+                }
+                first = false;
+              }
+              mma_commit(&empty_bar[stage]);  // frees the stage once these MMAs have read it
+              if (++stage == S) {
+                stage = 0;
+                phase ^= 1;
+              }
+            }
+            mma_commit(&acc_full);  // segment accumulated
+          }
+        }
+      }
+    }
+  } else {
+    // ------------------------------------------------ epilogue (warps 2..9)
+    const int q = warp & 3;              // TMEM lane quarter this warp may access
+    const int ch = (warp - 2) >> 2;      // column half
+    const int row = q * 32 + lane;       // target within the tile
+    const unsigned tbase = tmem + ((unsigned)(q * 32) << 16) + (unsigned)(ch * CW);
+    unsigned acc_phase = 0;
+    float acc[CW];
+#pragma unroll
+    for (int i = 0; i < CW; ++i) acc[i] = 0.f;
+    for (int it = blockIdx.x; it < P.nitems && !abort_sh; it += gridDim.x) {
+      const TcItem w = P.items[P.item0 + it];
+      const int nseg_item = (w.t1 - w.t0) * P.nseg;
+      for (int sgi = 0; sgi < nseg_item; ++sgi) {
+        if (!mbar_wait(&acc_full, acc_phase)) {
+          atomicExch(P.status + 1, 1);
+          abort_sh = 1;
+          break;
+        }
+        acc_phase ^= 1;
+        tc_fence_after();
+#pragma unroll
+        for (int c0 = 0; c0 < CW; c0 += 16) {
+          unsigned r[16];
+          tmem_ld16(tbase + c0, r);
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+          for (int i = 0; i < 16; ++i) acc[c0 + i] += __uint_as_float(r[i]);
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acc_empty);
+      }
+      if (abort_sh) break;
+      // flush the item's sums into the FP64 locals
+      const TcLevel &Lv = P.lv[w.level];
+      const int c = w.parity;
+      const int hx = w.bx * TILE_X + (row & 7), hy = w.by * TILE_Y + ((row >> 3) & 3), hz = w.bz * TILE_Z + (row >> 5);
+      const int gx = 2 * hx + ((c >> 2) & 1), gy = 2 * hy + ((c >> 1) & 1), gz = 2 * hz + (c & 1);
+      int cell = -1;
+      if (gx < Lv.side && gy < Lv.side && gz < Lv.side) cell = Lv.grid[((long long)gz * Lv.side + gy) * Lv.side + gx];
+      if (cell >= 0) {
+        const double sc = *Lv.scale_out;
+        double *Lrow = Lv.L + ((long long)cell * P.R + w.rhs) * P.nn + ch * CW;
+        const int lim = P.nn - ch * CW;
+#pragma unroll
+        for (int i = 0; i < CW; ++i)
+          if (i < lim) atomicAdd(Lrow + i, (double)acc[i] * sc);
+      }
+#pragma unroll
+      for (int i = 0; i < CW; ++i) acc[i] = 0.f;
+    }
+  }
+  __syncthreads();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P.ncols));
+  }
+}
+
+// ---- conversion kernels -----------------------------------------------------------------------------
+
+// max |M| of a level -> bit pattern (non-negative doubles order like their bit patterns)
+__global__ void absmax_kernel(long long n, const double *__restrict__ v, unsigned long long *__restrict__ out) {
+  double m = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    m = fmax(m, fabs(v[i]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// 2^sA with sA chosen so that max|M| * 2^sA ~ 2^14, and the epilogue factor scale_l * 2^-(sA + SB)
+__global__ void level_scale_kernel(const unsigned long long *__restrict__ amax, double scale_l,
+                                   double *__restrict__ pre, double *__restrict__ post) {
+  const double m = __longlong_as_double((long long)*amax);
+  int e = 0;
+  if (m > 0) frexp(m, &e);  // m = f * 2^e, f in [0.5, 1)
+  const int sA = 14 - e;
+  *pre = ldexp(1.0, sA);
+  *post = scale_l * ldexp(1.0, -(sA + SB));
+}
+
+__global__ void pack_multipoles(long long ncells, int R, int nn, int KP, int HX, int HY, int HZ,
+                                const long long *__restrict__ keys, const double *__restrict__ M,
+                                const double *__restrict__ pre, __half *__restrict__ hi, __half *__restrict__ lo) {
+  const long long cell = blockIdx.x;
+  int ix, iy, iz;
+  morton_decode3(keys[cell], ix, iy, iz);
+  const int c = ((ix & 1) << 2) | ((iy & 1) << 1) | (iz & 1);
+  const double s = *pre;
+  for (int r = 0; r < R; ++r) {
+    const long long base = ((((long long)(r * 8 + c) * HZ + (iz >> 1)) * HY + (iy >> 1)) * HX + (ix >> 1)) * KP;
+    for (int n = threadIdx.x; n < nn; n += blockDim.x) {
+      const double a = M[(cell * R + r) * nn + n] * s;
+      const __half h = __double2half(a);
+      hi[base + n] = h;
+      lo[base + n] = __double2half(a - (double)__half2float(h));
+    }
+  }
+}
+
+// operators: K[t][n][m] (FP64, source node n, target node m) -> B[t][m][n] split fp16, scaled by 2^SB
+__global__ void pack_operators(int nn, int KP, int NP, const double *__restrict__ K, __half *__restrict__ hi,
+                               __half *__restrict__ lo) {
+  const int t = blockIdx.y;
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (e >= (long long)NP * KP) return;
+  const int m = (int)(e / KP), n = (int)(e % KP);
+  double v = 0.0;
+  if (m < nn && n < nn) v = ldexp(K[((long long)t * nn + n) * nn + m], SB);
+  const __half h = __double2half(v);
+  hi[(long long)t * NP * KP + e] = h;
+  lo[(long long)t * NP * KP + e] = __double2half(v - (double)__half2float(h));
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+
+}  // namespace
+
+struct DenseTC {
+  int KP = 0, NP = 0, NH = 0, NHALF = 0, NK = 0, stages = 0, ncols = 0, stage_bytes = 0;
+  __half *Bhi = nullptr, *Blo = nullptr;
+  // per level
+  __half *Ahi[kMaxHeight] = {}, *Alo[kMaxHeight] = {};
+  size_t Abytes[kMaxHeight] = {};
+  int HX[kMaxHeight] = {}, HY[kMaxHeight] = {}, HZ[kMaxHeight] = {};
+  double *scal = nullptr;                 // [kMaxHeight][2]: pre, post
+  unsigned long long *amax = nullptr;     // [kMaxHeight]
+  TcItem *items = nullptr;
+  int nitems = 0;
+  int lvl_begin[kMaxHeight] = {}, lvl_end[kMaxHeight] = {};
+  long long built_for_N = -1;             // tree the per-level buffers were sized for
+  TcParams *params = nullptr;             // host copy
+  int grid = 0;
+};
+
+static b200fmm_status encode(CUtensorMap *map, void *base, int rank, const cuuint64_t *dims, const cuuint64_t *strides,
+                             const cuuint32_t *box) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return fail(B200FMM_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is not available");
+  cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, (cuuint32_t)rank, base, dims, strides, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(B200FMM_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return B200FMM_OK;
+}
+
+b200fmm_status tc_init(Context &c) {
+  B200_CHECK(build_dense_operators(c));  // FP64 K on the device
+  DenseTC *t = new DenseTC();
+  c.tc = t;
+  const int nn = c.nn;
+  t->KP = (nn + KCHUNK - 1) / KCHUNK * KCHUNK;
+  t->NP = t->KP;
+  t->NHALF = t->NP > 256 ? 2 : 1;
+  t->NH = t->NP / t->NHALF;
+  if (t->NH % 16 != 0 || t->NH > 256) return fail(B200FMM_ERR_UNSUPPORTED, "unsupported node count for the MMA tile");
+  if (t->NP > 352) return fail(B200FMM_ERR_UNSUPPORTED, "the tensor-core M2L supports orders up to 7");
+  t->NK = t->KP / KCHUNK;
+  t->stage_bytes = 2 * (TILE_X * TILE_Y * TILE_Z * KCHUNK * 2) + 2 * t->NP * KCHUNK * 2;
+  t->stages = std::min(MAX_STAGES, (220 * 1024) / t->stage_bytes);
+  if (t->stages < 2) return fail(B200FMM_ERR_UNSUPPORTED, "stage buffers do not fit in shared memory");
+  t->ncols = 32;
+  while (t->ncols < t->NP) t->ncols *= 2;
+  const size_t bsz = (size_t)343 * t->NP * t->KP;
+  B200_CUDA(cudaMalloc(&t->Bhi, bsz * sizeof(__half)));
+  B200_CUDA(cudaMalloc(&t->Blo, bsz * sizeof(__half)));
+  pack_operators<<<dim3(grid_for((long long)t->NP * t->KP, 256), 343), 256>>>(nn, t->KP, t->NP, c.d_dense, t->Bhi,
+                                                                            t->Blo);
+  B200_CUDA(cudaGetLastError());
+  B200_CUDA(cudaDeviceSynchronize());
+  // the FP64 dense operators are not needed by the mixed path after packing
+  cudaFree(c.d_dense);
+  c.d_dense = nullptr;
+  B200_CUDA(cudaMalloc(&t->scal, sizeof(double) * kMaxHeight * 2));
+  B200_CUDA(cudaMalloc(&t->amax, sizeof(unsigned long long) * kMaxHeight));
+  t->params = new TcParams();
+  std::memset(t->params, 0, sizeof(TcParams));
+  cuuint64_t dims[3] = {(cuuint64_t)t->KP, (cuuint64_t)t->NP, 343};
+  cuuint64_t strides[2] = {(cuuint64_t)t->KP * 2, (cuuint64_t)t->KP * 2 * t->NP};
+  cuuint32_t box[3] = {KCHUNK, (cuuint32_t)t->NH, 1};
+  B200_CHECK(encode(&t->params->mapB_hi, t->Bhi, 3, dims, strides, box));
+  B200_CHECK(encode(&t->params->mapB_lo, t->Blo, 3, dims, strides, box));
+  int dev_sms = 148;
+  cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c.device);
+  t->grid = dev_sms;
+  return B200FMM_OK;
+}
+
+void tc_free(Context &c) {
+  DenseTC *t = c.tc;
+  if (!t) return;
+  for (void *p : {(void *)t->Bhi, (void *)t->Blo, (void *)t->scal, (void *)t->amax, (void *)t->items})
+    if (p) cudaFree(p);
+  for (int l = 0; l < kMaxHeight; ++l) {
+    if (t->Ahi[l]) cudaFree(t->Ahi[l]);
+    if (t->Alo[l]) cudaFree(t->Alo[l]);
+  }
+  delete t->params;
+  delete t;
+  c.tc = nullptr;
+}
+
+// (Re)build the per-level A buffers, tensor maps and the work-item list for the current tree.
+static b200fmm_status tc_prepare(Context &c) {
+  DenseTC *t = c.tc;
+  TcParams &P = *t->params;
+  const int LL = c.H - 1;
+  std::vector<TcItem> items;
+  long long ntiles = 0;
+  for (int l = 2; l <= LL; ++l) {
+    const int h = 1 << (l - 1);
+    t->HX[l] = std::max(h, TILE_X);
+    t->HY[l] = std::max(h, TILE_Y);
+    t->HZ[l] = std::max(h, TILE_Z);
+    const size_t elems = (size_t)c.R * 8 * t->HZ[l] * t->HY[l] * t->HX[l] * t->KP;
+    if (t->Abytes[l] != elems * sizeof(__half)) {
+      if (t->Ahi[l]) cudaFree(t->Ahi[l]);
+      if (t->Alo[l]) cudaFree(t->Alo[l]);
+      B200_CUDA(cudaMalloc(&t->Ahi[l], elems * sizeof(__half)));
+      B200_CUDA(cudaMalloc(&t->Alo[l], elems * sizeof(__half)));
+      t->Abytes[l] = elems * sizeof(__half);
+    }
+    cuuint64_t dims[5] = {(cuuint64_t)t->KP, (cuuint64_t)t->HX[l], (cuuint64_t)t->HY[l], (cuuint64_t)t->HZ[l],
+                          (cuuint64_t)(8 * c.R)};
+    cuuint64_t st[4] = {(cuuint64_t)t->KP * 2, (cuuint64_t)t->KP * 2 * t->HX[l],
+                        (cuuint64_t)t->KP * 2 * t->HX[l] * t->HY[l],
+                        (cuuint64_t)t->KP * 2 * t->HX[l] * t->HY[l] * t->HZ[l]};
+    cuuint32_t box[5] = {KCHUNK, TILE_X, TILE_Y, TILE_Z, 1};
+    B200_CHECK(encode(&P.mapA_hi[l], t->Ahi[l], 5, dims, st, box));
+    B200_CHECK(encode(&P.mapA_lo[l], t->Alo[l], 5, dims, st, box));
+    P.lv[l].HX = t->HX[l];
+    P.lv[l].HY = t->HY[l];
+    P.lv[l].HZ = t->HZ[l];
+    P.lv[l].side = 1 << l;
+    P.lv[l].grid = c.lv[l].grid;
+    P.lv[l].L = c.lv[l].L;
+    P.lv[l].scale_out = t->scal + 2 * l + 1;
+    ntiles += (long long)c.R * 8 * (t->HX[l] / TILE_X) * (t->HY[l] / TILE_Y) * (t->HZ[l] / TILE_Z);
+  }
+  // split the 189 transfer vectors of each tile so that the items fill the SMs evenly
+  int ns = 1;
+  for (int k = 1; k <= 8; ++k) {
+    const long long n = ntiles * k;
+    const long long rounds = (n + t->grid - 1) / t->grid;
+    ns = k;
+    if ((double)n / (double)(rounds * t->grid) >= 0.9) break;
+  }
+  if (const char *e = getenv("B200FMM_TC_SPLITS")) ns = std::max(1, std::min(189, atoi(e)));
+  for (int l = LL; l >= 2; --l) {
+    t->lvl_begin[l] = (int)items.size();
+    for (int r = 0; r < c.R; ++r)
+      for (int par = 0; par < 8; ++par)
+        for (int bz = 0; bz < t->HZ[l] / TILE_Z; ++bz)
+          for (int by = 0; by < t->HY[l] / TILE_Y; ++by)
+            for (int bx = 0; bx < t->HX[l] / TILE_X; ++bx)
+              for (int s = 0; s < ns; ++s) {
+                TcItem w;
+                w.level = (short)l;
+                w.rhs = (short)r;
+                w.parity = (short)par;
+                w.split = (short)s;
+                w.bx = (short)bx;
+                w.by = (short)by;
+                w.bz = (short)bz;
+                w.t0 = (short)(189 * s / ns);
+                w.t1 = (short)(189 * (s + 1) / ns);
+                items.push_back(w);
+              }
+    t->lvl_end[l] = (int)items.size();
+  }
+  if (t->items) cudaFree(t->items);
+  B200_CUDA(cudaMalloc(&t->items, sizeof(TcItem) * items.size()));
+  B200_CUDA(cudaMemcpy(t->items, items.data(), sizeof(TcItem) * items.size(), cudaMemcpyHostToDevice));
+  t->nitems = (int)items.size();
+  P.items = t->items;
+  P.item0 = 0;
+  P.nitems = t->nitems;
+  P.R = c.R;
+  P.nn = c.nn;
+  P.KP = t->KP;
+  P.NP = t->NP;
+  P.NH = t->NH;
+  P.NHALF = t->NHALF;
+  P.NK = t->NK;
+  P.stages = t->stages;
+  P.ncols = t->ncols;
+  P.stage_bytes = t->stage_bytes;
+  // accumulator resets per transfer vector: 2 for p >= 6 keeps the M2L within ~1e-6 of FP64
+  P.nseg = std::min(t->NK, c.p >= 6 ? 2 : 1);
+  if (const char *e = getenv("B200FMM_TC_SEGMENTS")) P.nseg = std::max(1, std::min(t->NK, atoi(e)));
+  std::memcpy(P.off, c.itab.off, sizeof(P.off));
+  std::memcpy(P.slot, c.itab.slot, sizeof(P.slot));
+  P.status = c.d_status;
+  t->built_for_N = c.N;
+  return B200FMM_OK;
+}
+
+b200fmm_status run_m2l_tc(Context &c, int level) {
+  DenseTC *t = c.tc;
+  if (!t) return fail(B200FMM_ERR_STATE, "tensor-core M2L not initialised");
+  const int LL = c.H - 1;
+  if (level != -1 && (level < 2 || level > LL)) return fail(B200FMM_ERR_INVALID, "m2l: level out of range");
+  if (t->built_for_N != c.N || t->params->lv[LL].grid != c.lv[LL].grid) B200_CHECK(tc_prepare(c));
+  const int l0 = level == -1 ? 2 : level, l1 = level == -1 ? LL : level;
+  for (int l = l0; l <= l1; ++l) {
+    const Level &Lv = c.lv[l];
+    B200_CUDA(cudaMemsetAsync(t->amax + l, 0, sizeof(unsigned long long), c.stream));
+    B200_CUDA(cudaMemsetAsync(t->Ahi[l], 0, t->Abytes[l], c.stream));
+    B200_CUDA(cudaMemsetAsync(t->Alo[l], 0, t->Abytes[l], c.stream));
+    if (Lv.n == 0) continue;
+    const long long cnt = Lv.n * c.R * c.nn;
+    absmax_kernel<<<std::min<long long>(1024, grid_for(cnt, 256)), 256, 0, c.stream>>>(cnt, Lv.M, t->amax + l);
+    level_scale_kernel<<<1, 1, 0, c.stream>>>(t->amax + l, 2.0 / (c.cfg.box_width / (double)(1LL << l)),
+                                              t->scal + 2 * l, t->scal + 2 * l + 1);
+    pack_multipoles<<<(unsigned)Lv.n, 128, 0, c.stream>>>(Lv.n, c.R, c.nn, t->KP, t->HX[l], t->HY[l], t->HZ[l],
+                                                          Lv.keys, Lv.M, t->scal + 2 * l, t->Ahi[l], t->Alo[l]);
+    c.launches += 3;
+  }
+  // items are ordered by level, finest first: levels [l0, l1] are one contiguous range
+  TcParams &P = *t->params;
+  P.item0 = t->lvl_begin[l1];
+  P.nitems = t->lvl_end[l0] - t->lvl_begin[l1];
+  if (P.nitems <= 0) return B200FMM_OK;
+  const size_t smem = (size_t)t->stages * t->stage_bytes + 1024;
+  const int grid = std::min(t->grid, P.nitems);
+  switch (t->NP / 2) {
+#define B200_TC_CASE(CWV)                                                                                      \
+  case CWV:                                                                                                    \
+    B200_CUDA(cudaFuncSetAttribute(m2l_tc_kernel<CWV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    m2l_tc_kernel<CWV><<<grid, TC_THREADS, smem, c.stream>>>(P);                                               \
+    break;
+    B200_TC_CASE(16)
+    B200_TC_CASE(32)
+    B200_TC_CASE(64)
+    B200_TC_CASE(112)
+    B200_TC_CASE(176)
+#undef B200_TC_CASE
+    default:
+      return fail(B200FMM_ERR_UNSUPPORTED, "no tensor-core M2L instance for this order");
+  }
+  ++c.launches;
+  B200_CUDA(cudaGetLastError());
+  return B200FMM_OK;
+}
+
+}  // namespace b200

@@ -1,0 +1,323 @@
+// Near field P2P for the Laplace 1/r kernel over each leaf and its <=26 neighbour leaves.
+//
+// Pair math (FP2PR::MutualParticles / NonMutualParticles, Src/Kernels/P2P/FP2PR.hpp:14-69):
+//   phi_t += q_s / r,   F_t += -q_t q_s (x_t - x_s) / r^3.
+// The reference evaluates each unordered pair once (mutual half shell, FChebSymKernel.hpp:468-478);
+// the ordered pairs summed here per target are the same set.
+//
+//  * FP64 (parity form): one CTA per target leaf, source leaves staged through shared memory, the
+//    reference's arithmetic sequence (1/r^2, sqrt, products).
+//  * FP32 (mixed form): positions are stored relative to their own leaf centre as a float pair
+//    (hi, lo) with hi + lo exact to ~2^-48 of the leaf width.  For each source leaf the target is moved into
+//    that leaf's frame in FP64 once and split again, so that per pair dx = (t_hi - s_hi) + (t_lo - s_lo):
+//    the first difference is exact for nearby particles (Sterbenz), which keeps the close pairs -- the ones
+//    that dominate the forces -- accurate to a few ulp.  One warp per target leaf; the source leaves are
+//    copied into shared memory by the bulk-copy engine (cp.async.bulk + mbarrier, double buffered); rsqrt on
+//    the SFU; per-target compensated (two-sum) accumulation of the per-leaf partial sums; the result is added
+//    in FP64 to the far field.
+#include "common.cuh"
+
+namespace b200 {
+
+namespace {
+
+constexpr int P2P64_THREADS = 64;
+
+__global__ void p2p_fp64_kernel(int R, long long N, const long long *__restrict__ leaf_start,
+                                const int *__restrict__ nbr, int variant, const double *__restrict__ x,
+                                const double *__restrict__ y, const double *__restrict__ z,
+                                const double *__restrict__ q, double *__restrict__ phi, double *__restrict__ fx,
+                                double *__restrict__ fy, double *__restrict__ fz) {
+  __shared__ double sx[P2P64_THREADS], sy[P2P64_THREADS], sz[P2P64_THREADS], sq[P2P64_THREADS];
+  __shared__ long long sidx[P2P64_THREADS];
+  const long long leaf = blockIdx.x;
+  const long long t0 = leaf_start[leaf], t1 = leaf_start[leaf + 1];
+  for (int r = 0; r < R; ++r) {
+    const double *qr = q + (long long)r * N;
+    for (long long tb = t0; tb < t1; tb += blockDim.x) {
+      const long long i = tb + threadIdx.x;
+      const bool active = i < t1;
+      const double tx = active ? x[i] : 0, ty = active ? y[i] : 0, tz = active ? z[i] : 0;
+      const double tq = active ? qr[i] : 0;
+      double pv = 0, gx = 0, gy = 0, gz = 0;
+      for (int e = 0; e < 27; ++e) {
+        if (variant == 1 && e == 13) continue;
+        const int sl = nbr[leaf * 27 + e];
+        if (sl < 0) continue;
+        const long long s0 = leaf_start[sl], s1 = leaf_start[sl + 1];
+        for (long long sb = s0; sb < s1; sb += blockDim.x) {
+          __syncthreads();
+          const long long j = sb + threadIdx.x;
+          if (j < s1) {
+            sx[threadIdx.x] = x[j];
+            sy[threadIdx.x] = y[j];
+            sz[threadIdx.x] = z[j];
+            sq[threadIdx.x] = qr[j];
+            sidx[threadIdx.x] = j;
+          }
+          __syncthreads();
+          const int cnt = (int)min((long long)blockDim.x, s1 - sb);
+          if (active) {
+            for (int k = 0; k < cnt; ++k) {
+              if (sidx[k] == i) continue;
+              double dx = tx - sx[k], dy = ty - sy[k], dz = tz - sz[k];
+              double inv2 = 1.0 / (dx * dx + dy * dy + dz * dz);
+              const double inv = sqrt(inv2);
+              inv2 *= inv;
+              inv2 *= tq * sq[k];
+              gx += -dx * inv2;
+              gy += -dy * inv2;
+              gz += -dz * inv2;
+              pv += inv * sq[k];
+            }
+          }
+        }
+      }
+      if (active) {
+        const long long j = (long long)r * N + i;
+        phi[j] += pv;
+        fx[j] += gx;
+        fy[j] += gy;
+        fz[j] += gz;
+      }
+    }
+  }
+}
+
+// ---- FP32 compensated ------------------------------------------------------------------------------
+
+__global__ void pack_local32(long long N, int R, const long long *__restrict__ keys_leaf,
+                             const long long *__restrict__ leaf_start, const double *__restrict__ x,
+                             const double *__restrict__ y, const double *__restrict__ z, const double *__restrict__ q,
+                             double cx0, double cy0, double cz0, double leaf_w, float4 *__restrict__ hi,
+                             float4 *__restrict__ lo) {
+  const long long leaf = blockIdx.x;
+  int ix, iy, iz;
+  morton_decode3(keys_leaf[leaf], ix, iy, iz);
+  const double c0 = cx0 + (ix + 0.5) * leaf_w, c1 = cy0 + (iy + 0.5) * leaf_w, c2 = cz0 + (iz + 0.5) * leaf_w;
+  for (long long i = leaf_start[leaf] + threadIdx.x; i < leaf_start[leaf + 1]; i += blockDim.x) {
+    const double lx = x[i] - c0, ly = y[i] - c1, lz = z[i] - c2;
+    const float hx = (float)lx, hy = (float)ly, hz = (float)lz;
+    lo[i] = make_float4((float)(lx - (double)hx), (float)(ly - (double)hy), (float)(lz - (double)hz), 0.f);
+    for (int r = 0; r < R; ++r) hi[(long long)r * N + i] = make_float4(hx, hy, hz, (float)q[(long long)r * N + i]);
+  }
+}
+
+__device__ __forceinline__ void two_sum(float &hi, float &lo, float v) {
+  const float s = hi + v;
+  const float bp = s - hi;
+  const float err = (hi - (s - bp)) + (v - bp);
+  hi = s;
+  lo += err;
+}
+
+constexpr int P2P32_WARPS = 4;        // target leaves per CTA (one warp each)
+constexpr int P2P32_STAGE = 128;      // source particles per bulk-copy stage
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+// Bounded wait on an mbarrier phase; returns false when the iteration budget runs out.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned phase) {
+  for (int it = 0; it < (1 << 22); ++it) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(phase)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
+// One warp per target leaf.  The source ranges of the 27 neighbour slots are walked as a sequence of
+// stages of <= P2P32_STAGE particles, each copied by one bulk copy (16-byte float4 records, so address and
+// size are 16-byte multiples).  Two stage buffers per warp: the copy of stage k+1 overlaps the math of k.
+__global__ void __launch_bounds__(P2P32_WARPS * 32) p2p_fp32_kernel(
+    int R, long long N, long long nleaves, const long long *__restrict__ leaf_start, const int *__restrict__ nbr,
+    int variant, const float4 *__restrict__ pq, const float4 *__restrict__ plo, double leaf_w,
+    double *__restrict__ phi, double *__restrict__ fx, double *__restrict__ fy, double *__restrict__ fz,
+    int *__restrict__ status) {
+  __shared__ __align__(128) float4 buf[P2P32_WARPS][2][P2P32_STAGE];
+  __shared__ __align__(128) float4 blo[P2P32_WARPS][2][P2P32_STAGE];
+  __shared__ __align__(8) unsigned long long bar[P2P32_WARPS][2];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long leaf = (long long)blockIdx.x * P2P32_WARPS + w;
+  if (lane == 0) {
+    mbar_init(&bar[w][0], 1);
+    mbar_init(&bar[w][1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  if (leaf >= nleaves) return;
+  const long long t0 = leaf_start[leaf], t1 = leaf_start[leaf + 1];
+  // the list of (slot, begin, end) stages
+  int slots[27];
+  int ns = 0;
+  for (int e = 0; e < 27; ++e) {
+    if (variant == 1 && e == 13) continue;
+    const int sl = nbr[leaf * 27 + e];
+    if (sl >= 0) slots[ns++] = e;
+  }
+  unsigned phase[2] = {0, 0};
+  for (int r = 0; r < R; ++r) {
+    const float4 *pr = pq + (long long)r * N;
+    for (long long tb = t0; tb < t1; tb += 32) {
+      const long long i = tb + lane;
+      const bool active = i < t1;
+      const float4 me = active ? pr[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 mel = active ? plo[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+      const double mx = (double)me.x + (double)mel.x, my = (double)me.y + (double)mel.y,
+                   mz = (double)me.z + (double)mel.z;
+      float ph_hi = 0.f, ph_lo = 0.f, gx_hi = 0.f, gx_lo = 0.f, gy_hi = 0.f, gy_lo = 0.f, gz_hi = 0.f, gz_lo = 0.f;
+      // stage iterator: (slot index e, begin b) -> next
+      int se = 0;
+      long long sb = ns > 0 ? leaf_start[nbr[leaf * 27 + slots[0]]] : 0;
+      auto stage_end = [&](int e) { return leaf_start[nbr[leaf * 27 + slots[e]] + 1]; };
+      // issue the first stage
+      int buf_id = 0;
+      long long cur_b = sb;
+      int cur_e = se;
+      int cur_n = 0;
+      if (ns > 0) {
+        const long long e1 = stage_end(0);
+        cur_n = (int)min((long long)P2P32_STAGE, e1 - sb);
+        if (lane == 0) {
+          mbar_expect_tx(&bar[w][0], cur_n * 32);
+          bulk_g2s(&buf[w][0][0], pr + sb, cur_n * 16, &bar[w][0]);
+          bulk_g2s(&blo[w][0][0], plo + sb, cur_n * 16, &bar[w][0]);
+        }
+      }
+      while (cur_n > 0) {
+        // next stage
+        long long nb = cur_b + cur_n;
+        int ne = cur_e;
+        if (nb >= stage_end(ne)) {
+          ++ne;
+          if (ne < ns) nb = leaf_start[nbr[leaf * 27 + slots[ne]]];
+        }
+        int nxt_n = 0;
+        if (ne < ns) {
+          nxt_n = (int)min((long long)P2P32_STAGE, stage_end(ne) - nb);
+          if (lane == 0) {
+            mbar_expect_tx(&bar[w][buf_id ^ 1], nxt_n * 32);
+            bulk_g2s(&buf[w][buf_id ^ 1][0], pr + nb, nxt_n * 16, &bar[w][buf_id ^ 1]);
+            bulk_g2s(&blo[w][buf_id ^ 1][0], plo + nb, nxt_n * 16, &bar[w][buf_id ^ 1]);
+          }
+        }
+        // wait for the current stage
+        if (!mbar_wait(&bar[w][buf_id], phase[buf_id])) {
+          if (lane == 0) atomicExch(status, 1);
+          return;
+        }
+        phase[buf_id] ^= 1;
+        // the target moved into the source leaf's frame (FP64, exact multiples of the leaf width), split into
+        // a float pair
+        const int sl_pos = slots[cur_e];
+        const double tdx = mx - (double)(sl_pos / 9 - 1) * leaf_w, tdy = my - (double)((sl_pos / 3) % 3 - 1) * leaf_w,
+                     tdz = mz - (double)(sl_pos % 3 - 1) * leaf_w;
+        const float thx = (float)tdx, thy = (float)tdy, thz = (float)tdz;
+        const float tlx = (float)(tdx - (double)thx), tly = (float)(tdy - (double)thy), tlz = (float)(tdz - (double)thz);
+        float pv = 0.f, ax = 0.f, ay = 0.f, az = 0.f;
+        const float4 *s = buf[w][buf_id];
+        const float4 *sl = blo[w][buf_id];
+        if (sl_pos == 13) {
+          const int self = (int)(i - cur_b);
+#pragma unroll 4
+          for (int k = 0; k < cur_n; ++k) {
+            const float4 v = s[k];
+            const float4 u = sl[k];
+            const float dx = (thx - v.x) + (tlx - u.x), dy = (thy - v.y) + (tly - u.y), dz = (thz - v.z) + (tlz - u.z);
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const float inv = (k == self) ? 0.f : rsqrtf(r2);
+            const float qi = v.w * inv;
+            const float qi3 = qi * inv * inv;
+            pv += qi;
+            ax = fmaf(dx, qi3, ax);
+            ay = fmaf(dy, qi3, ay);
+            az = fmaf(dz, qi3, az);
+          }
+        } else {
+#pragma unroll 8
+          for (int k = 0; k < cur_n; ++k) {
+            const float4 v = s[k];
+            const float4 u = sl[k];
+            const float dx = (thx - v.x) + (tlx - u.x), dy = (thy - v.y) + (tly - u.y), dz = (thz - v.z) + (tlz - u.z);
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const float inv = rsqrtf(r2);
+            const float qi = v.w * inv;
+            const float qi3 = qi * inv * inv;
+            pv += qi;
+            ax = fmaf(dx, qi3, ax);
+            ay = fmaf(dy, qi3, ay);
+            az = fmaf(dz, qi3, az);
+          }
+        }
+        two_sum(ph_hi, ph_lo, pv);
+        two_sum(gx_hi, gx_lo, ax);
+        two_sum(gy_hi, gy_lo, ay);
+        two_sum(gz_hi, gz_lo, az);
+        __syncwarp();  // every lane is done with this buffer before it is refilled
+        buf_id ^= 1;
+        cur_b = nb;
+        cur_e = ne;
+        cur_n = nxt_n;
+      }
+      if (active) {
+        const long long j = (long long)r * N + i;
+        const double tq = -(double)me.w;
+        phi[j] += (double)ph_hi + (double)ph_lo;
+        fx[j] += tq * ((double)gx_hi + (double)gx_lo);
+        fy[j] += tq * ((double)gy_hi + (double)gy_lo);
+        fz[j] += tq * ((double)gz_hi + (double)gz_lo);
+      }
+    }
+  }
+}
+
+}  // namespace
+
+b200fmm_status run_p2p(Context &c, int variant) {
+  const int LL = c.H - 1;
+  const Level &L = c.lv[LL];
+  if (L.n == 0) return B200FMM_OK;
+  if (c.cfg.precision == B200FMM_MIXED) {
+    if (!c.d_pq32) {
+      B200_CUDA(cudaMallocAsync(&c.d_pq32, sizeof(float4) * c.N * (c.R + 1), c.stream));
+      const double W = c.cfg.box_width;
+      pack_local32<<<(unsigned)L.n, 64, 0, c.stream>>>(c.N, c.R, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q,
+                                                       c.cfg.center[0] - W / 2, c.cfg.center[1] - W / 2,
+                                                       c.cfg.center[2] - W / 2, W / (double)(1 << LL), c.d_pq32,
+                                                       c.d_pq32 + c.N * c.R);
+      ++c.launches;
+    }
+    int *status = c.d_status;
+    const unsigned blocks = grid_for(L.n, P2P32_WARPS);
+    p2p_fp32_kernel<<<blocks, P2P32_WARPS * 32, 0, c.stream>>>(c.R, c.N, L.n, c.d_leaf_start, c.d_leaf_nbr, variant,
+                                                               c.d_pq32, c.d_pq32 + c.N * c.R,
+                                                               c.cfg.box_width / (double)(1 << LL), c.d_phi,
+                                                               c.d_fx, c.d_fy, c.d_fz, status);
+    ++c.launches;
+  } else {
+    p2p_fp64_kernel<<<(unsigned)L.n, P2P64_THREADS, 0, c.stream>>>(c.R, c.N, c.d_leaf_start, c.d_leaf_nbr, variant,
+                                                                   c.d_x, c.d_y, c.d_z, c.d_q, c.d_phi, c.d_fx,
+                                                                   c.d_fy, c.d_fz);
+    ++c.launches;
+  }
+  B200_CUDA(cudaGetLastError());
+  return B200FMM_OK;
+}
+
+}  // namespace b200

@@ -1,0 +1,549 @@
+// Tree construction on the GPU -- integer work, bit-exact with the reference's rules:
+//   leaf coordinate  FCoordinateComputer::GetTreeCoordinate (Src/Containers/FCoordinateComputer.hpp:16-40)
+//   Morton key       FTreeCoordinate::getMortonIndex (Src/Containers/FTreeCoordinate.hpp:91-113)
+//   leaf order       FOctree::insert appends in input order -> a stable sort by key
+//   leaf neighbours  FTreeCoordinate::getNeighborsIndexes (FTreeCoordinate.hpp:189-216)
+//   interaction list FTreeCoordinate::getInteractionNeighbors (FTreeCoordinate.hpp:219-264)
+//
+// The sort is a stable LSD radix sort with 4-bit digits (histogram / scan / scatter per digit); keys
+// have 3*(height-1) significant bits.
+#include "common.cuh"
+
+#include <algorithm>
+
+namespace b200 {
+
+namespace {
+
+constexpr int RS_THREADS = 256;
+constexpr int RS_ITEMS = 8;
+constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
+constexpr int RS_BINS = 16;
+
+// --------------------------------------------------------------------------------------------------
+// keys
+// --------------------------------------------------------------------------------------------------
+__global__ void keys_kernel(long long n, const double *__restrict__ x, const double *__restrict__ y,
+                            const double *__restrict__ z, double cx, double cy, double cz, double box_width,
+                            double leaf_width, int height, unsigned long long *__restrict__ keys,
+                            int *__restrict__ vals, int *__restrict__ err) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double r[3] = {x[i] - cx, y[i] - cy, z[i] - cz};
+  int c[3];
+  const int last = (1 << (height - 1)) - 1;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    if (!(r[d] >= 0.0 && r[d] <= box_width)) {  // also rejects NaN
+      atomicExch(err, 1);
+      c[d] = 0;
+    } else if (r[d] == box_width) {
+      c[d] = last;
+    } else {
+      c[d] = (int)(r[d] / leaf_width);
+      if (c[d] > last) c[d] = last;  // unreachable for in-box input; keeps the key in range
+    }
+  }
+  keys[i] = (unsigned long long)morton_encode3(c[0], c[1], c[2]);
+  vals[i] = (int)i;
+}
+
+// --------------------------------------------------------------------------------------------------
+// radix sort
+// --------------------------------------------------------------------------------------------------
+__global__ void rs_hist(const unsigned long long *__restrict__ keys, long long n, int shift, int nblocks,
+                        unsigned *__restrict__ counts) {
+  __shared__ unsigned h[RS_BINS];
+  if (threadIdx.x < RS_BINS) h[threadIdx.x] = 0;
+  __syncthreads();
+  const long long base = (long long)blockIdx.x * RS_TILE;
+#pragma unroll
+  for (int k = 0; k < RS_ITEMS; ++k) {
+    const long long i = base + k * RS_THREADS + threadIdx.x;
+    if (i < n) atomicAdd(&h[(keys[i] >> shift) & (RS_BINS - 1)], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x < RS_BINS) counts[(long long)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+// Exclusive scan of an unsigned array in tiles of 1024 (one block per tile), block sums out.
+__global__ void scan_tiles_u32(const unsigned *__restrict__ in, unsigned *__restrict__ out, long long n,
+                               unsigned *__restrict__ sums) {
+  __shared__ unsigned s[1024];
+  __shared__ unsigned wsum[32];
+  const long long i = (long long)blockIdx.x * 1024 + threadIdx.x;
+  const unsigned v = i < n ? in[i] : 0u;
+  // warp inclusive scan
+  unsigned x = v;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned t = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += t;
+  }
+  if (lane == 31) wsum[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    unsigned y = wsum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned t = __shfl_up_sync(0xffffffffu, y, o);
+      if (lane >= o) y += t;
+    }
+    wsum[lane] = y;
+  }
+  __syncthreads();
+  const unsigned incl = x + (w > 0 ? wsum[w - 1] : 0u);
+  if (i < n) out[i] = incl - v;
+  if (threadIdx.x == 1023 && sums) sums[blockIdx.x] = incl;
+  (void)s;
+}
+
+__global__ void add_tile_offsets_u32(unsigned *__restrict__ out, long long n, const unsigned *__restrict__ offs) {
+  const long long i = (long long)blockIdx.x * 1024 + threadIdx.x;
+  if (i < n) out[i] += offs[blockIdx.x];
+}
+
+// Same for long long.
+__global__ void scan_tiles_i64(const long long *__restrict__ in, long long *__restrict__ out, long long n,
+                               long long *__restrict__ sums) {
+  __shared__ long long wsum[32];
+  const long long i = (long long)blockIdx.x * 1024 + threadIdx.x;
+  const long long v = i < n ? in[i] : 0;
+  long long x = v;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long t = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += t;
+  }
+  if (lane == 31) wsum[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    long long y = wsum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long t = __shfl_up_sync(0xffffffffu, y, o);
+      if (lane >= o) y += t;
+    }
+    wsum[lane] = y;
+  }
+  __syncthreads();
+  const long long incl = x + (w > 0 ? wsum[w - 1] : 0);
+  if (i < n) out[i] = incl - v;
+  if (threadIdx.x == 1023 && sums) sums[blockIdx.x] = incl;
+}
+
+__global__ void add_tile_offsets_i64(long long *__restrict__ out, long long n, const long long *__restrict__ offs) {
+  const long long i = (long long)blockIdx.x * 1024 + threadIdx.x;
+  if (i < n) out[i] += offs[blockIdx.x];
+}
+
+__global__ void rs_scatter(const unsigned long long *__restrict__ kin, const int *__restrict__ vin,
+                           unsigned long long *__restrict__ kout, int *__restrict__ vout, long long n, int shift,
+                           int nblocks, const unsigned *__restrict__ offsets) {
+  __shared__ unsigned cnt[RS_BINS][RS_THREADS + 1];
+  __shared__ unsigned base_off[RS_BINS];
+  const int t = threadIdx.x;
+  const long long base = (long long)blockIdx.x * RS_TILE + (long long)t * RS_ITEMS;  // blocked: items in order
+  unsigned long long k[RS_ITEMS];
+  int v[RS_ITEMS];
+  int dg[RS_ITEMS];
+  unsigned rank[RS_ITEMS];
+  unsigned c[RS_BINS];
+#pragma unroll
+  for (int b = 0; b < RS_BINS; ++b) c[b] = 0;
+#pragma unroll
+  for (int j = 0; j < RS_ITEMS; ++j) {
+    const long long i = base + j;
+    if (i < n) {
+      k[j] = kin[i];
+      v[j] = vin[i];
+      dg[j] = (int)((k[j] >> shift) & (RS_BINS - 1));
+    } else {
+      dg[j] = -1;
+    }
+    rank[j] = 0;
+#pragma unroll
+    for (int b = 0; b < RS_BINS; ++b)
+      if (dg[j] == b) rank[j] = c[b]++;
+  }
+#pragma unroll
+  for (int b = 0; b < RS_BINS; ++b) cnt[b][t] = c[b];
+  if (t < RS_BINS) base_off[t] = offsets[(long long)t * nblocks + blockIdx.x];
+  __syncthreads();
+  // exclusive scan over threads of each digit's counts: warp w scans digits 2w and 2w+1
+  {
+    const int lane = t & 31, w = t >> 5;
+    for (int b = 2 * w; b < 2 * w + 2; ++b) {
+      unsigned loc[RS_THREADS / 32];
+      unsigned s = 0;
+#pragma unroll
+      for (int e = 0; e < RS_THREADS / 32; ++e) {
+        loc[e] = cnt[b][lane * (RS_THREADS / 32) + e];
+        s += loc[e];
+      }
+      unsigned x = s;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      unsigned run = x - s;
+#pragma unroll
+      for (int e = 0; e < RS_THREADS / 32; ++e) {
+        cnt[b][lane * (RS_THREADS / 32) + e] = run;
+        run += loc[e];
+      }
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < RS_ITEMS; ++j) {
+    if (dg[j] < 0) continue;
+    const unsigned pos = base_off[dg[j]] + cnt[dg[j]][t] + rank[j];
+    kout[pos] = k[j];
+    vout[pos] = v[j];
+  }
+}
+
+// --------------------------------------------------------------------------------------------------
+// tree arrays
+// --------------------------------------------------------------------------------------------------
+__global__ void gather_particles(long long n, int R, const int *__restrict__ perm, const double *__restrict__ x,
+                                 const double *__restrict__ y, const double *__restrict__ z,
+                                 const double *__restrict__ q, double *__restrict__ xs, double *__restrict__ ys,
+                                 double *__restrict__ zs, double *__restrict__ qs, long long *__restrict__ perm64) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long long j = perm[i];
+  xs[i] = x[j];
+  ys[i] = y[j];
+  zs[i] = z[j];
+  for (int r = 0; r < R; ++r) qs[(long long)r * n + i] = q[(long long)r * n + j];
+  perm64[i] = j;
+}
+
+__global__ void gather_charges(long long n, int R, const long long *__restrict__ perm, const double *__restrict__ q,
+                               double *__restrict__ qs) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long long j = perm[i];
+  for (int r = 0; r < R; ++r) qs[(long long)r * n + i] = q[(long long)r * n + j];
+}
+
+// head[i] = 1 when keys[i] (shifted) differs from its predecessor
+__global__ void head_flags(long long n, const unsigned long long *__restrict__ keys, int shift,
+                           long long *__restrict__ flags) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  flags[i] = (i == 0 || (keys[i] >> shift) != (keys[i - 1] >> shift)) ? 1 : 0;
+}
+
+__global__ void head_flags_i64(long long n, const long long *__restrict__ keys, long long *__restrict__ flags) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  flags[i] = (i == 0 || (keys[i] >> 3) != (keys[i - 1] >> 3)) ? 1 : 0;
+}
+
+__global__ void compact_leaves(long long n, const unsigned long long *__restrict__ keys,
+                               const long long *__restrict__ flags, const long long *__restrict__ idx,
+                               long long *__restrict__ leaf_keys, long long *__restrict__ leaf_start) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (flags[i]) {
+    leaf_keys[idx[i]] = (long long)keys[i];
+    leaf_start[idx[i]] = i;
+  }
+}
+
+__global__ void compact_parents(long long n, const long long *__restrict__ ckeys, const long long *__restrict__ flags,
+                                const long long *__restrict__ idx, long long *__restrict__ pkeys,
+                                int *__restrict__ parent, int *__restrict__ pchild) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long long pi = idx[i] + flags[i] - 1;  // inclusive index of this child's parent
+  if (flags[i]) pkeys[pi] = ckeys[i] >> 3;
+  parent[i] = (int)pi;
+  pchild[pi * 8 + (ckeys[i] & 7)] = (int)i;
+}
+
+__global__ void leaf_neighbors_kernel(long long nleaves, const long long *__restrict__ keys, int height,
+                                      int *__restrict__ nbr) {
+  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= nleaves) return;
+  int ix, iy, iz;
+  morton_decode3(keys[c], ix, iy, iz);
+  const int lim = 1 << (height - 1);
+  for (int p = 0; p < 27; ++p) {
+    const int dx = p / 9 - 1, dy = (p / 3) % 3 - 1, dz = p % 3 - 1;
+    int v = -1;
+    if (p == 13) {
+      v = (int)c;
+    } else if (ix + dx >= 0 && ix + dx < lim && iy + dy >= 0 && iy + dy < lim && iz + dz >= 0 && iz + dz < lim) {
+      v = find_key(keys, nleaves, morton_encode3(ix + dx, iy + dy, iz + dz));
+    }
+    nbr[c * 27 + p] = v;
+  }
+}
+
+__global__ void ilist_kernel(long long ncells, const long long *__restrict__ keys, int level,
+                             const IListTable *__restrict__ tab, int *__restrict__ ilist) {
+  const long long c = blockIdx.x;
+  if (c >= ncells) return;
+  int ix, iy, iz;
+  const long long key = keys[c];
+  morton_decode3(key, ix, iy, iz);
+  const int ct = (int)(key & 7);
+  const int lim = 1 << level;
+  for (int e = threadIdx.x; e < 189; e += blockDim.x) {
+    const int sx = ix + tab->off[ct][e][0], sy = iy + tab->off[ct][e][1], sz = iz + tab->off[ct][e][2];
+    int v = -1;
+    if (sx >= 0 && sx < lim && sy >= 0 && sy < lim && sz >= 0 && sz < lim)
+      v = find_key(keys, ncells, morton_encode3(sx, sy, sz));
+    ilist[c * 189 + e] = v;
+  }
+}
+
+__global__ void grid_index_kernel(long long ncells, const long long *__restrict__ keys, int level,
+                                  int *__restrict__ grid) {
+  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= ncells) return;
+  int ix, iy, iz;
+  morton_decode3(keys[c], ix, iy, iz);
+  const long long side = 1LL << level;
+  grid[((long long)iz * side + iy) * side + ix] = (int)c;
+}
+
+__global__ void fill_int(long long n, int *p, int v) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+// exclusive scan (host driver, recursive over tiles of 1024)
+b200fmm_status scan_u32(Context &c, const unsigned *in, unsigned *out, long long n) {
+  const long long tiles = (n + 1023) / 1024;
+  c.tree_launches += tiles > 1 ? 2 : 1;
+  unsigned *sums = nullptr;
+  if (tiles > 1) B200_CUDA(cudaMallocAsync(&sums, sizeof(unsigned) * tiles * 2, c.stream));
+  scan_tiles_u32<<<(unsigned)tiles, 1024, 0, c.stream>>>(in, out, n, sums);
+  if (tiles > 1) {
+    B200_CHECK(scan_u32(c, sums, sums + tiles, tiles));
+    add_tile_offsets_u32<<<(unsigned)tiles, 1024, 0, c.stream>>>(out, n, sums + tiles);
+    B200_CUDA(cudaFreeAsync(sums, c.stream));
+  }
+  return B200FMM_OK;
+}
+
+b200fmm_status scan_i64(Context &c, const long long *in, long long *out, long long n) {
+  const long long tiles = (n + 1023) / 1024;
+  c.tree_launches += tiles > 1 ? 2 : 1;
+  long long *sums = nullptr;
+  if (tiles > 1) B200_CUDA(cudaMallocAsync(&sums, sizeof(long long) * tiles * 2, c.stream));
+  scan_tiles_i64<<<(unsigned)tiles, 1024, 0, c.stream>>>(in, out, n, sums);
+  if (tiles > 1) {
+    B200_CHECK(scan_i64(c, sums, sums + tiles, tiles));
+    add_tile_offsets_i64<<<(unsigned)tiles, 1024, 0, c.stream>>>(out, n, sums + tiles);
+    B200_CUDA(cudaFreeAsync(sums, c.stream));
+  }
+  return B200FMM_OK;
+}
+
+template <class T>
+void dfree(T *&p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+}  // namespace
+
+void free_tree(Context &c) {
+  dfree(c.d_x);
+  dfree(c.d_y);
+  dfree(c.d_z);
+  dfree(c.d_q);
+  dfree(c.d_perm);
+  dfree(c.d_leaf_start);
+  dfree(c.d_leaf_nbr);
+  dfree(c.d_pq32);
+  dfree(c.d_phi);
+  dfree(c.d_fx);
+  dfree(c.d_fy);
+  dfree(c.d_fz);
+  for (int l = 0; l < kMaxHeight; ++l) {
+    Level &L = c.lv[l];
+    dfree(L.keys);
+    dfree(L.parent);
+    dfree(L.child);
+    dfree(L.ilist);
+    dfree(L.M);
+    dfree(L.L);
+    dfree(L.grid);
+    L.n = 0;
+  }
+  c.N = 0;
+  c.has_particles = false;
+}
+
+b200fmm_status upload_charges(Context &c, const double *q, bool on_device) {
+  const long long n = c.N;
+  double *dq = nullptr;
+  if (!on_device) {
+    B200_CUDA(cudaMallocAsync(&dq, sizeof(double) * n * c.R, c.stream));
+    B200_CUDA(cudaMemcpyAsync(dq, q, sizeof(double) * n * c.R, cudaMemcpyHostToDevice, c.stream));
+    q = dq;
+  }
+  gather_charges<<<grid_for(n, 256), 256, 0, c.stream>>>(n, c.R, c.d_perm, q, c.d_q);
+  if (dq) B200_CUDA(cudaFreeAsync(dq, c.stream));
+  B200_CUDA(cudaGetLastError());
+  return B200FMM_OK;
+}
+
+b200fmm_status build_tree(Context &c, const double *x, const double *y, const double *z, const double *q,
+                          bool on_device) {
+  const long long n = c.N;
+  const int H = c.H, LL = H - 1;
+  cudaStream_t s = c.stream;
+  c.tree_launches = 0;
+  // inputs on the device
+  const double *dx = x, *dy = y, *dz = z, *dq = q;
+  double *own = nullptr;
+  if (!on_device) {
+    B200_CUDA(cudaMallocAsync(&own, sizeof(double) * n * (3 + c.R), s));
+    B200_CUDA(cudaMemcpyAsync(own, x, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    B200_CUDA(cudaMemcpyAsync(own + n, y, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    B200_CUDA(cudaMemcpyAsync(own + 2 * n, z, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    B200_CUDA(cudaMemcpyAsync(own + 3 * n, q, sizeof(double) * n * c.R, cudaMemcpyHostToDevice, s));
+    dx = own;
+    dy = own + n;
+    dz = own + 2 * n;
+    dq = own + 3 * n;
+  }
+  // keys
+  unsigned long long *k0 = nullptr, *k1 = nullptr;
+  int *v0 = nullptr, *v1 = nullptr, *err = nullptr;
+  const long long nb = (n + RS_TILE - 1) / RS_TILE;
+  unsigned *cnt = nullptr, *off = nullptr;
+  B200_CUDA(cudaMallocAsync(&k0, sizeof(unsigned long long) * n * 2, s));
+  B200_CUDA(cudaMallocAsync(&v0, sizeof(int) * n * 2, s));
+  B200_CUDA(cudaMallocAsync(&err, sizeof(int), s));
+  B200_CUDA(cudaMallocAsync(&cnt, sizeof(unsigned) * RS_BINS * nb * 2, s));
+  k1 = k0 + n;
+  v1 = v0 + n;
+  off = cnt + RS_BINS * nb;
+  B200_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+  const double W = c.cfg.box_width;
+  const double leaf_w = W / (double)(1 << LL);
+  keys_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, dx, dy, dz, c.cfg.center[0] - W / 2, c.cfg.center[1] - W / 2,
+                                               c.cfg.center[2] - W / 2, W, leaf_w, H, k0, v0, err);
+  ++c.tree_launches;
+  int herr = 0;
+  B200_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  B200_CUDA(cudaStreamSynchronize(s));
+  if (herr) {
+    cudaFreeAsync(k0, s);
+    cudaFreeAsync(v0, s);
+    cudaFreeAsync(err, s);
+    cudaFreeAsync(cnt, s);
+    if (own) cudaFreeAsync(own, s);
+    cudaStreamSynchronize(s);
+    return fail(B200FMM_ERR_DOMAIN, "a particle lies outside the box or has a non-finite coordinate");
+  }
+  // sort
+  const int bits = 3 * LL;
+  for (int sh = 0; sh < bits; sh += 4) {
+    rs_hist<<<(unsigned)nb, RS_THREADS, 0, s>>>(k0, n, sh, (int)nb, cnt);
+    ++c.tree_launches;
+    B200_CHECK(scan_u32(c, cnt, off, RS_BINS * nb));
+    rs_scatter<<<(unsigned)nb, RS_THREADS, 0, s>>>(k0, v0, k1, v1, n, sh, (int)nb, off);
+    ++c.tree_launches;
+    std::swap(k0, k1);
+    std::swap(v0, v1);
+  }
+  // particle arrays
+  B200_CUDA(cudaMallocAsync(&c.d_x, sizeof(double) * n, s));
+  B200_CUDA(cudaMallocAsync(&c.d_y, sizeof(double) * n, s));
+  B200_CUDA(cudaMallocAsync(&c.d_z, sizeof(double) * n, s));
+  B200_CUDA(cudaMallocAsync(&c.d_q, sizeof(double) * n * c.R, s));
+  B200_CUDA(cudaMallocAsync(&c.d_perm, sizeof(long long) * n, s));
+  for (double **p : {&c.d_phi, &c.d_fx, &c.d_fy, &c.d_fz}) B200_CUDA(cudaMallocAsync(p, sizeof(double) * n * c.R, s));
+  gather_particles<<<grid_for(n, 256), 256, 0, s>>>(n, c.R, v0, dx, dy, dz, dq, c.d_x, c.d_y, c.d_z, c.d_q, c.d_perm);
+  ++c.tree_launches;
+  // leaves
+  long long *flags = nullptr, *idx = nullptr;
+  B200_CUDA(cudaMallocAsync(&flags, sizeof(long long) * (n + 1) * 2, s));
+  idx = flags + (n + 1);
+  head_flags<<<grid_for(n, 256), 256, 0, s>>>(n, k0, 0, flags);
+  ++c.tree_launches;
+  B200_CHECK(scan_i64(c, flags, idx, n));
+  long long last_idx = 0, last_flag = 0;
+  B200_CUDA(cudaMemcpyAsync(&last_idx, idx + n - 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  B200_CUDA(cudaMemcpyAsync(&last_flag, flags + n - 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  B200_CUDA(cudaStreamSynchronize(s));
+  const long long nleaves = last_idx + last_flag;
+  Level &leaf = c.lv[LL];
+  leaf.n = nleaves;
+  B200_CUDA(cudaMallocAsync(&leaf.keys, sizeof(long long) * nleaves, s));
+  B200_CUDA(cudaMallocAsync(&c.d_leaf_start, sizeof(long long) * (nleaves + 1), s));
+  compact_leaves<<<grid_for(n, 256), 256, 0, s>>>(n, k0, flags, idx, leaf.keys, c.d_leaf_start);
+  ++c.tree_launches;
+  B200_CUDA(cudaMemcpyAsync(c.d_leaf_start + nleaves, &c.N, sizeof(long long), cudaMemcpyHostToDevice, s));
+  // upper levels
+  for (int l = LL - 1; l >= 0; --l) {
+    Level &ch = c.lv[l + 1];
+    Level &pa = c.lv[l];
+    const long long nc = ch.n;
+    head_flags_i64<<<grid_for(nc, 256), 256, 0, s>>>(nc, ch.keys, flags);
+    ++c.tree_launches;
+    B200_CHECK(scan_i64(c, flags, idx, nc));
+    long long li = 0, lf = 0;
+    B200_CUDA(cudaMemcpyAsync(&li, idx + nc - 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    B200_CUDA(cudaMemcpyAsync(&lf, flags + nc - 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    B200_CUDA(cudaStreamSynchronize(s));
+    pa.n = li + lf;
+    B200_CUDA(cudaMallocAsync(&pa.keys, sizeof(long long) * pa.n, s));
+    B200_CUDA(cudaMallocAsync(&ch.parent, sizeof(int) * nc, s));
+    B200_CUDA(cudaMallocAsync(&pa.child, sizeof(int) * pa.n * 8, s));
+    fill_int<<<grid_for(pa.n * 8, 256), 256, 0, s>>>(pa.n * 8, pa.child, -1);
+    ++c.tree_launches;
+    compact_parents<<<grid_for(nc, 256), 256, 0, s>>>(nc, ch.keys, flags, idx, pa.keys, ch.parent, pa.child);
+    ++c.tree_launches;
+  }
+  // expansions
+  for (int l = 2; l <= LL; ++l) {
+    Level &L = c.lv[l];
+    const size_t bytes = sizeof(double) * (size_t)L.n * c.R * c.nn;
+    B200_CUDA(cudaMallocAsync(&L.M, bytes, s));
+    B200_CUDA(cudaMallocAsync(&L.L, bytes, s));
+    B200_CUDA(cudaMemsetAsync(L.M, 0, bytes, s));
+    B200_CUDA(cudaMemsetAsync(L.L, 0, bytes, s));
+  }
+  // neighbour and interaction lists
+  B200_CUDA(cudaMallocAsync(&c.d_leaf_nbr, sizeof(int) * nleaves * 27, s));
+  leaf_neighbors_kernel<<<grid_for(nleaves, 128), 128, 0, s>>>(nleaves, leaf.keys, H, c.d_leaf_nbr);
+  ++c.tree_launches;
+  for (int l = 2; l <= LL; ++l) {
+    Level &L = c.lv[l];
+    B200_CUDA(cudaMallocAsync(&L.ilist, sizeof(int) * L.n * 189, s));
+    ilist_kernel<<<(unsigned)L.n, 192, 0, s>>>(L.n, L.keys, l, c.d_itab, L.ilist);
+    ++c.tree_launches;
+    if (c.cfg.precision == B200FMM_MIXED) {
+      const long long side = 1LL << l;
+      B200_CUDA(cudaMallocAsync(&L.grid, sizeof(int) * side * side * side, s));
+      fill_int<<<grid_for(side * side * side, 256), 256, 0, s>>>(side * side * side, L.grid, -1);
+      ++c.tree_launches;
+      grid_index_kernel<<<grid_for(L.n, 256), 256, 0, s>>>(L.n, L.keys, l, L.grid);
+      ++c.tree_launches;
+    }
+  }
+  B200_CUDA(cudaFreeAsync(flags, s));
+  B200_CUDA(cudaFreeAsync(k0 < k1 ? k0 : k1, s));
+  B200_CUDA(cudaFreeAsync(v0 < v1 ? v0 : v1, s));
+  B200_CUDA(cudaFreeAsync(err, s));
+  B200_CUDA(cudaFreeAsync(cnt, s));
+  if (own) B200_CUDA(cudaFreeAsync(own, s));
+  B200_CUDA(cudaGetLastError());
+  return B200FMM_OK;
+}
+
+}  // namespace b200

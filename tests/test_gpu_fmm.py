@@ -1,0 +1,267 @@
+"""Parity of the CUDA FMM (through the C ABI) with the reference and with the CPU oracle.
+
+Tolerances (relative L2 over the whole vector, FMath::FAccurater):
+  * FP64 path with the reference's own compressed operators: 1e-12 against the reference's outputs;
+  * FP64 path with this library's own operator compression: the compression tolerance 10^-p can move the
+    factors (pivot ties), so 50 * 10^-p against the reference;
+  * integer tree work (keys, permutation, lists): exact;
+  * MIXED path: 2e-6 against the FP64 path (FP32 P2P + split-FP16 tensor-core M2L).
+"""
+import numpy as np
+import pytest
+
+import scalfmm_b200 as S
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("phi", "fx", "fy", "fz")
+CENTER = (0.5, 0.5, 0.5)
+
+
+def run(g, kernel="cheb_sym", precision="fp64", ops=S.ALL, sym=None, nrhs=1):
+    f = S.FMM(kernel, int(g["order"]), int(g["height"]), nrhs=nrhs, precision=precision)
+    if sym is not None:
+        f.set_sym_operators(sym["ranks"], sym["uv"])
+    f.set_particles(g["x"], g["y"], g["z"], g["q"])
+    f.execute(ops)
+    r = f.results()
+    f.close()
+    return r
+
+
+SYM_CASES = ["sym_p5_h4_n2000", "sym_p7_h4_n2000", "sym_p4_h5_n3000", "sym_p6_h3_n500"]
+
+
+@pytest.mark.parametrize("name", SYM_CASES)
+def test_fp64_sym_matches_reference_with_reference_operators(golden, name):
+    g = golden(f"fmm_{name}.npz")
+    sym = golden(f"sym_ops_p{int(g['order'])}.npz")
+    r = run(g, sym=sym)
+    for f in FIELDS:
+        assert S.rel_l2(r[f], g[f]) < 1e-12, (f, S.rel_l2(r[f], g[f]))
+
+
+@pytest.mark.parametrize("name", SYM_CASES)
+def test_fp64_sym_own_operators_close_to_reference(golden, name):
+    g = golden(f"fmm_{name}.npz")
+    r = run(g)
+    tol = 50 * 10.0 ** (-int(g["order"]))
+    for f in FIELDS:
+        assert S.rel_l2(r[f], g[f]) < tol, (f, S.rel_l2(r[f], g[f]))
+
+
+@pytest.mark.parametrize("order", [4, 5, 7])
+def test_own_operator_compression_matches_reference(golden, order):
+    sym = golden(f"sym_ops_p{order}.npz")
+    f = S.FMM("cheb_sym", order, 3)
+    ranks, uv = f.get_sym_operators()
+    f.close()
+    assert (ranks == sym["ranks"]).all()
+    mine, ref = O.unpack_sym(ranks, uv, order), O.unpack_sym(sym["ranks"], sym["uv"], order)
+    for slot in ref:
+        A = mine[slot][0] @ mine[slot][1].T
+        B = ref[slot][0] @ ref[slot][1].T
+        assert np.linalg.norm(A - B) / np.linalg.norm(B) < 10 * 10.0 ** (-order)
+
+
+@pytest.mark.parametrize("name", ["dense_p4_h4_n2000", "dense_p5_h3_n1000"])
+def test_fp64_dense_matches_reference(golden, name):
+    g = golden(f"fmm_{name}.npz")
+    r = run(g, kernel="cheb_dense")
+    for f in FIELDS:
+        assert S.rel_l2(r[f], g[f]) < 1e-12, (f, S.rel_l2(r[f], g[f]))
+
+
+def test_multi_rhs_matches_reference(golden):
+    g = golden("fmm_sym_p5_h4_n1500_rhs16.npz")
+    sym = golden("sym_ops_p5.npz")
+    r = run(g, sym=sym, nrhs=16)
+    for f in FIELDS:
+        assert r[f].shape == (16, g["x"].size)
+        assert S.rel_l2(r[f], g[f]) < 1e-12, f
+
+
+def test_expansions_per_level_match_reference(golden):
+    g = golden("expansions_sym_p4_h4_n1000.npz")
+    sym = golden("sym_ops_p4.npz")
+    f = S.FMM("cheb_sym", 4, 4)
+    f.set_sym_operators(sym["ranks"], sym["uv"])
+    f.set_particles(g["x"], g["y"], g["z"], g["q"])
+    f.execute()
+    for lvl in (2, 3):
+        keys, M, L = f.cells(lvl)
+        ref = {int(k): i for i, k in enumerate(g["mortons"]) if g["levels"][i] == lvl}
+        assert sorted(ref) == sorted(keys.tolist())
+        idx = [ref[int(k)] for k in keys]
+        assert S.rel_l2(M[:, 0], g["multipoles"][idx]) < 1e-12
+        assert S.rel_l2(L[:, 0], g["locals"][idx]) < 1e-12
+    f.close()
+
+
+def test_tree_is_bit_exact_with_oracle():
+    rng = np.random.default_rng(5)
+    n, H = 20000, 6
+    x, y, z = rng.random((3, n))
+    x[:50] = 1.0  # the upper face maps to the last cell
+    y[50:100] = 0.0
+    q = rng.uniform(-1, 1, n)
+    f = S.FMM("cheb_sym", 3, H)
+    f.set_particles(x, y, z, q)
+    keys = O.morton_keys(x, y, z, 1.0, CENTER, H)
+    order = np.lexsort((np.arange(n), keys))  # stable sort by key
+    assert (f.permutation() == order).all()
+    leaf_keys = np.unique(keys)
+    nc, npart = f.tree_info()
+    assert npart == n and nc[H - 1] == leaf_keys.size
+    for lvl in range(H):
+        k, _, _ = f.cells(lvl, expansions=False)
+        assert (k == np.unique(leaf_keys >> (3 * (H - 1 - lvl)))).all()
+    f.close()
+
+
+def test_direct_gpu_matches_reference(golden):
+    g = golden("direct_n1500.npz")
+    d = S.direct(g["x"], g["y"], g["z"], g["q"])
+    for k in FIELDS:
+        assert S.rel_l2(d[k], g[k]) < 1e-13
+    t = np.array([0, 7, 1499, 300])
+    d2 = S.direct(g["x"], g["y"], g["z"], g["q"], targets=t)
+    for k in FIELDS:
+        assert np.allclose(d2[k], g[k][t], rtol=1e-13, atol=0)
+
+
+@pytest.mark.parametrize("ops", [S.P2P, S.P2M | S.M2M | S.M2L | S.L2L | S.L2P, S.P2M | S.M2M | S.M2L | S.L2L])
+def test_operation_masks_match_oracle(golden, ops):
+    g = golden("fmm_sym_p5_h4_n2000.npz")
+    sym = golden("sym_ops_p5.npz")
+    r = run(g, sym=sym, ops=ops)
+    o = O.fmm(O.CHEB_SYM, 5, 4, 1.0, CENTER, g["x"], g["y"], g["z"], g["q"], ops=ops, sym_ranks=sym["ranks"],
+              sym_uv=sym["uv"])
+    for f in FIELDS:
+        if not np.any(o[f]):
+            assert not np.any(r[f])
+        else:
+            assert S.rel_l2(r[f], o[f]) < 1e-12, f
+
+
+def test_level_batched_operators_equal_execute(golden):
+    g = golden("fmm_sym_p4_h5_n3000.npz")
+    sym = golden("sym_ops_p4.npz")
+    f = S.FMM("cheb_sym", 4, 5)
+    f.set_sym_operators(sym["ranks"], sym["uv"])
+    f.set_particles(g["x"], g["y"], g["z"], g["q"])
+    f.reset_expansions()
+    f.p2m()
+    for lvl in (3, 2):
+        f.m2m(lvl)
+    for lvl in (2, 3, 4):
+        f.m2l(lvl)
+    for lvl in (2, 3):
+        f.l2l(lvl)
+    f.l2p()
+    f.p2p(0)
+    r = f.results()
+    for k in FIELDS:
+        assert S.rel_l2(r[k], g[k]) < 1e-12
+    # P2PRemote variant: neighbours only = full P2P minus the leaf's own pairs
+    f.reset_expansions()
+    f.p2p(1)
+    remote = f.results()
+    f.reset_expansions()
+    f.p2p(0)
+    full = f.results()
+    o_self = O.fmm(O.CHEB_SYM, 4, 5, 1.0, CENTER, g["x"], g["y"], g["z"], g["q"], ops=O.P2P, sym_ranks=sym["ranks"],
+                   sym_uv=sym["uv"])
+    assert S.rel_l2(full["phi"], o_self["phi"]) < 1e-12
+    assert S.rel_l2(remote["phi"], full["phi"]) > 1e-3  # the self-leaf pairs are missing
+    f.close()
+
+
+def test_edge_cases():
+    # one particle: no interactions at all
+    f = S.FMM("cheb_sym", 4, 3)
+    f.set_particles([0.3], [0.3], [0.3], [1.0])
+    f.execute()
+    r = f.results()
+    assert r["phi"][0] == 0 and r["fx"][0] == 0
+    # two particles in one leaf: exact pair
+    f.set_particles([0.1, 0.12], [0.1, 0.1], [0.1, 0.1], [1.0, -2.0])
+    f.execute()
+    r = f.results()
+    assert abs(r["phi"][0] - (-2.0 / 0.02)) < 1e-9 and abs(r["phi"][1] - 1.0 / 0.02) < 1e-9
+    # particles outside the box are rejected with a status code
+    with pytest.raises(S.B200FmmError):
+        f.set_particles([1.5], [0.5], [0.5], [1.0])
+    with pytest.raises(S.B200FmmError):
+        f.set_particles([np.nan], [0.5], [0.5], [1.0])
+    f.close()
+    # clustered particles (many empty leaves) against the oracle
+    rng = np.random.default_rng(9)
+    n = 3000
+    pos = np.clip(0.2 + 0.05 * rng.standard_normal((3, n)), 0, 1)
+    pos[:, :300] = rng.random((3, 300))
+    q = rng.uniform(-1, 1, n)
+    sym = O.unpack_sym  # noqa: F841 (operators below come from the library itself)
+    f = S.FMM("cheb_sym", 5, 6)
+    ranks, uv = f.get_sym_operators()
+    f.set_particles(pos[0], pos[1], pos[2], q)
+    f.execute()
+    r = f.results()
+    o = O.fmm(O.CHEB_SYM, 5, 6, 1.0, CENTER, pos[0], pos[1], pos[2], q, sym_ranks=ranks, sym_uv=uv)
+    for k in FIELDS:
+        assert S.rel_l2(r[k], o[k]) < 1e-12
+    f.close()
+
+
+@pytest.mark.parametrize("kernel", ["cheb_sym", "lagrange"])
+def test_mixed_close_to_fp64(kernel):
+    rng = np.random.default_rng(3)
+    n = 30000
+    x, y, z = rng.random((3, n))
+    q = rng.uniform(-1, 1, n)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        f = S.FMM("cheb_dense" if (kernel == "cheb_sym" and prec == "fp64") else kernel, 5, 5, precision=prec)
+        f.set_particles(x, y, z, q)
+        f.execute()
+        out[prec] = f.results()
+        f.close()
+    for k in FIELDS:
+        assert S.rel_l2(out["mixed"][k], out["fp64"][k]) < 2e-6, (k, S.rel_l2(out["mixed"][k], out["fp64"][k]))
+
+
+def test_lagrange_fp64_matches_oracle():
+    rng = np.random.default_rng(4)
+    n = 2000
+    x, y, z = rng.random((3, n))
+    q = rng.uniform(-1, 1, n)
+    f = S.FMM("lagrange", 5, 4)
+    f.set_particles(x, y, z, q)
+    f.execute()
+    r = f.results()
+    f.close()
+    o = O.fmm(O.LAGRANGE, 5, 4, 1.0, CENTER, x, y, z, q)
+    for k in FIELDS:
+        assert S.rel_l2(r[k], o[k]) < 1e-12, k
+
+
+@pytest.mark.parametrize("order,height", [(5, 5), (7, 4), (4, 6)])
+def test_mixed_m2l_locals_match_fp64_dense(order, height):
+    """Isolates the tensor-core M2L: same multipoles (FP64 P2M/M2M in both), locals after M2L compared per
+    level against the FP64 dense M2L."""
+    rng = np.random.default_rng(order * 10 + height)
+    n = 20000
+    x, y, z = rng.random((3, n))
+    q = rng.uniform(-1, 1, n)
+    ops = S.P2M | S.M2M | S.M2L
+    loc = {}
+    for prec in ("fp64", "mixed"):
+        f = S.FMM("cheb_dense", order, height, precision=prec)
+        f.set_particles(x, y, z, q)
+        f.execute(ops)
+        loc[prec] = {lvl: f.cells(lvl)[2] for lvl in range(2, height)}
+        f.close()
+    for lvl in range(2, height):
+        err = S.rel_l2(loc["mixed"][lvl], loc["fp64"][lvl])
+        assert err < 1e-6, (lvl, err)
