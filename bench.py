@@ -1,0 +1,376 @@
+"""Benchmark of the FMM hot path on B200 (one JSON line on rank 0).
+
+Workload (the headline configuration): 1,000,000 particles uniform in [0,1)^3 (seeded), charges uniform in
+[-1,1], Laplace 1/r, Chebyshev order 7, octree height 6, MIXED precision (FP32 compensated P2P, split-FP16
+tcgen05 M2L with FP32 accumulation).  One step = one FMM evaluation from particles: GPU tree build
+(Morton keys, radix sort, lists) + P2M, M2M, M2L, L2L, L2P, P2P.
+
+  value  particles/s with the particles resident in HBM (device-pointer b200fmm_set_particles + execute),
+         device time from CUDA events on the library's stream, summed over the K timed steps, max over ranks;
+  e2e    the same through host buffers: pinned x, y, z, q copied in by b200fmm_set_particles, results
+         (phi, fx, fy, fz) copied back by b200fmm_get_results, every step;
+L2 is flushed (a 512 MiB write) between timed steps, outside the timed intervals.
+
+Multi-GPU (torchrun): replicas only -- every rank evaluates its own copy of the workload, no collective in
+the data path ("scaling": "weak"); NCCL is used only for the barrier and the max-over-ranks reduction.
+
+--impl reference times the reference's own CPU implementation (ScalFMM FFmmAlgorithmThread +
+FChebSymKernel, compiled from its sources into oracle/_ref) on the host cores: one step = one evaluation
+of the same workload (tree insertion and kernel construction untimed, as the reference's own drivers time
+algo.execute()).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+
+METRIC = "particles/s per FMM eval (1M uniform, Chebyshev p=7, height 6, mixed precision)"
+N_PART, ORDER, HEIGHT, SEED = 1_000_000, 7, 6, 42
+FLOPS_PER_P2P_PAIR = 20  # SURVEY 8(d) work unit
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=N_PART)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
+    return ap.parse_args()
+
+
+def particles(n, seed=SEED):
+    rng = np.random.default_rng(seed)
+    pos = rng.random((3, n))
+    q = rng.uniform(-1.0, 1.0, n)
+    return pos[0].copy(), pos[1].copy(), pos[2].copy(), q
+
+
+def workload_config(n):
+    return {"workload": f"{n} particles uniform in [0,1)^3, q~U[-1,1] (seed {SEED}), Laplace 1/r, Chebyshev order "
+                        f"{ORDER}, height {HEIGHT}", "particles": n, "order": ORDER, "height": HEIGHT,
+            "precision": "mixed: FP32 compensated P2P, split-FP16 x3 tcgen05 M2L, FP64 P2M/M2M/L2L/L2P",
+            "l2": "flushed between timed steps (512 MiB write)", "parallelism": "replicas"}
+
+
+# ------------------------------------------------------------------------------------------------------
+# clocks
+# ------------------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm", "clocks.max.sm", "clocks_event_reasons.hw_slowdown",
+              "clocks_event_reasons.hw_thermal_slowdown", "clocks_event_reasons.sw_thermal_slowdown",
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + ",".join(self.FIELDS),
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                vals = [v.strip() for v in out.stdout.strip().split(",")]
+                if len(vals) == len(self.FIELDS):
+                    self.samples.append(vals)
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[2 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops_sustained", 1400.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1400.0, 1590.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the tensor-core M2L kernel, from the committed ncu summary (None if absent)."""
+    f = ROOT / "profiles" / "m2l_tc_kernel_traffic.txt"
+    if f.exists():
+        for line in f.read_text().splitlines():
+            if line.startswith("bytes_per_launch_scaled_to_bench_workload"):
+                return float(line.split("=")[1].strip())
+    return None
+
+
+# ------------------------------------------------------------------------------------------------------
+# CPU baseline: the reference itself (oracle/_ref), else the CPU restatement
+# ------------------------------------------------------------------------------------------------------
+class _StdoutToStderr:
+    """The reference library prints progress lines on stdout; keep stdout for the JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+
+    def __exit__(self, *a):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
+def cpu_eval(x, y, z, q, steps=1):
+    with _StdoutToStderr():
+        return _cpu_eval(x, y, z, q, steps)
+
+
+def _cpu_eval(x, y, z, q, steps=1):
+    from oracle import oracle as O
+
+    threads = os.cpu_count() or 1
+    if O.ref_available():
+        times = []
+        for _ in range(steps):
+            r = O.ref_fmm(O.CHEB_SYM, ORDER, HEIGHT, 1.0, (0.5, 0.5, 0.5), x, y, z, q, nthreads=threads)
+            times.append(r["times"]["execute"])
+        return times, "reference", threads, "ScalFMM FFmmAlgorithmThread + FChebSymKernel (order 7, height 6) built from " \
+                                            "its sources, algo.execute() of the full workload"
+    from oracle import precompute as PC
+
+    ranks, uv = PC.pack_reference_layout(PC.sym_operators(ORDER), ORDER)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        O.fmm(O.CHEB_SYM, ORDER, HEIGHT, 1.0, (0.5, 0.5, 0.5), x, y, z, q, sym_ranks=ranks, sym_uv=uv, nthreads=threads)
+        times.append(time.perf_counter() - t0)
+    return times, "port", threads, "CPU restatement (oracle/fmm_oracle.c) of the full workload"
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    n = args.n
+    x, y, z, q = particles(n)
+    from oracle import oracle as O
+
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libscalfmm_ref.so was not built"}))
+        return 0
+    cpu_eval(x, y, z, q, steps=args.warmup)
+    times, kind, cores, sample = cpu_eval(x, y, z, q, steps=args.steps)
+    total = sum(times)
+    value = n * args.steps / total
+    line = {"metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(n), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "particles/s", "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------------------------------------------
+# GPU arm
+# ------------------------------------------------------------------------------------------------------
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+
+    import scalfmm_b200 as S
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+    stream = torch.cuda.current_stream(dev)
+    n = args.n
+    x, y, z, q = particles(n)
+    dx, dy, dz, dq = (torch.from_numpy(a).to(dev) for a in (x, y, z, q))
+    hx, hy, hz, hq = (torch.from_numpy(a).pin_memory() for a in (x, y, z, q))
+    out_h = [torch.empty(n, dtype=torch.float64).pin_memory() for _ in range(4)]
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    f = S.FMM("cheb_sym", ORDER, HEIGHT, precision="mixed", device=local, stream=stream.cuda_stream)
+
+    def step_device():
+        f.set_particles(dx, dy, dz, dq)
+        f.execute()
+
+    def step_e2e():
+        f.set_particles(hx, hy, hz, hq)
+        f.execute()
+        f.results_into(*out_h)
+
+    for _ in range(args.warmup):
+        step_device()
+        step_e2e()
+    torch.cuda.synchronize()
+    m2l_pairs, p2p_pairs = f.tree_stats()
+
+    def timed(fn, sampler_index=None):
+        ms = []
+        kernel = []
+        launches = 0
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            fn()
+            e.record(stream)
+            e.synchronize()
+            ms.append(s.elapsed_time(e))
+            kernel.append(f.kernel_times())
+            launches += f.launch_count()
+        return ms, kernel, launches
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ms_dev, ktimes, launches = timed(step_device)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ms_e2e, _, launches_e2e = timed(step_e2e)
+    torch.cuda.synchronize()
+    t_dev = sum(ms_dev)
+    t_e2e = sum(ms_e2e)
+    if world > 1:
+        t = torch.tensor([t_dev, t_e2e], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_dev, t_e2e = t.tolist()
+
+    hbm, bf16_sus, bf16_burst, peak_src = measured_peaks()
+    m2l_ms = statistics.mean(k["m2l"] for k in ktimes)
+    p2p_ms = statistics.mean(k["p2p"] for k in ktimes)
+    nn = ORDER ** 3
+    m2l_flops = m2l_pairs * 2.0 * nn * nn  # logical: split products counted once
+    achieved = m2l_flops / (m2l_ms * 1e-3) / 1e12
+    peak = bf16_sus / 3.0  # three FP16 products per logical product
+    traffic = profile_traffic()
+    p2p_tflops = p2p_pairs * FLOPS_PER_P2P_PAIR / (p2p_ms * 1e-3) / 1e12
+    fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12
+
+    line = {
+        "metric": METRIC, "value": world * n * args.steps / (t_dev * 1e-3), "unit": "particles/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_dev / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32/f16x3 (mixed), f64 far-field bookkeeping",
+        "data": "synthetic", "config": workload_config(n),
+        "e2e": {"value": world * n * args.steps / (t_e2e * 1e-3), "unit": "particles/s",
+                "h2d_bytes_per_step": 4 * 8 * n, "d2h_bytes_per_step": 4 * 8 * n},
+        "gpu_launches": launches + launches_e2e,
+        "roofline": {"bound": "tensor", "kernel": "m2l_tc_kernel (tcgen05 split-FP16 M2L)",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": traffic,
+                     "note": f"logical M2L flops = {m2l_pairs} pairs x 2 x {nn}^2 per launch; peak = {peak_src} "
+                             f"sustained bf16 {bf16_sus} TFLOP/s / 3 (three FP16 products per logical product); "
+                             f"kernel time {m2l_ms:.3f} ms (CUDA events on the launching stream)"},
+        "p2p": {"pairs": p2p_pairs, "kernel_ms": p2p_ms, "gpairs_per_s": p2p_pairs / (p2p_ms * 1e-3) / 1e9,
+                "tflops_at_20_per_pair": p2p_tflops, "frac_fp32_peak": p2p_tflops / fp32_peak,
+                "fp32_peak_note": "148 SMs x 128 FP32 lanes x 2 x 1965 MHz (nominal)"},
+        "pass_ms": f.timings(),
+        "clocks": clk.summary(),
+    }
+    f.close()
+
+    if rank == 0 and not args.no_accuracy:
+        line["accuracy"] = accuracy(S, torch, dev, stream, x, y, z, q, line)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            times, kind, cores, sample = cpu_eval(x, y, z, q, steps=1)
+            line["cpu_baseline"] = {"value": n / times[0], "unit": "particles/s", "cores": cores, "kind": kind,
+                                    "sample": sample}
+        except Exception as exc:  # the baseline is reported, never the target
+            line["cpu_baseline"] = {"value": None, "unit": "particles/s", "cores": os.cpu_count(), "kind": "reference",
+                                    "sample": f"failed: {exc}"}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def accuracy(S, torch, dev, stream, x, y, z, q, line):
+    """Mixed vs the plain FP64 GPU FMM (same tree) over all particles, and both against the FP64 direct sum on
+    a seeded 10,000-target subsample; also times the plain FP64 GPU FMM (same step definition)."""
+    n = x.size
+    out = {}
+    res = {}
+    for prec in ("fp64", "mixed"):
+        f = S.FMM("cheb_sym", ORDER, HEIGHT, precision=prec, device=dev.index, stream=stream.cuda_stream)
+        dx, dy, dz, dq = (torch.from_numpy(a).to(dev) for a in (x, y, z, q))
+        f.set_particles(dx, dy, dz, dq)
+        f.execute()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(3):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            f.set_particles(dx, dy, dz, dq)
+            f.execute()
+            e.record(stream)
+            e.synchronize()
+            ms.append(s.elapsed_time(e))
+        res[prec] = f.results()
+        out[f"{prec}_ms_per_eval"] = min(ms)
+        out[f"{prec}_pass_ms"] = f.timings()
+        f.close()
+    out["fp64_particles_per_s"] = n / (out["fp64_ms_per_eval"] * 1e-3)
+    out["mixed_over_fp64_speedup"] = out["fp64_ms_per_eval"] / out["mixed_ms_per_eval"]
+    for k in ("phi", "fx", "fy", "fz"):
+        out[f"mixed_vs_fp64_rel_l2_{k}"] = S.rel_l2(res["mixed"][k], res["fp64"][k])
+    t = np.random.default_rng(7).choice(n, 10000, replace=False)
+    d = S.direct(x, y, z, q, targets=t)
+    for prec in ("fp64", "mixed"):
+        for k in ("phi", "fx"):
+            out[f"{prec}_vs_direct_rel_l2_{k}"] = S.rel_l2(res[prec][k][t], d[k])
+    out["gate_mixed_vs_fp64_le_1e-6"] = bool(out["mixed_vs_fp64_rel_l2_phi"] <= 1e-6)
+    return out
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -136,6 +136,12 @@ B200FMM_API b200fmm_status b200fmm_get_permutation(b200fmm_handle h, long long *
 /* Device time of the passes of the last execute(), milliseconds:
  * [0] tree build (last set_particles), [1] P2M, [2] M2M, [3] M2L, [4] L2L, [5] L2P, [6] P2P, [7] total. */
 B200FMM_API b200fmm_status b200fmm_last_timings(b200fmm_handle h, double *ms8);
+/* Device time of single kernels of the last execute(), milliseconds: [0] the M2L kernel (the tensor-core
+ * kernel alone in MIXED, the whole M2L pass in FP64), [1] the P2P kernel, [2] P2M, [3] L2P. */
+B200FMM_API b200fmm_status b200fmm_last_kernel_times(b200fmm_handle h, double *ms4);
+/* Work counts of the current tree: M2L (target, source) pairs over levels 2..height-1 and ordered P2P
+ * particle pairs (i != j) over each leaf and its neighbours. */
+B200FMM_API b200fmm_status b200fmm_tree_stats(b200fmm_handle h, long long *m2l_pairs, long long *p2p_pairs);
 /* Number of kernel launches issued by the last set_particles() plus the last execute(). */
 B200FMM_API b200fmm_status b200fmm_last_launch_count(b200fmm_handle h, long long *count);
 

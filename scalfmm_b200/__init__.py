@@ -30,7 +30,8 @@ EXPORTS = (
     "b200fmm_get_sym_operators", "b200fmm_set_particles", "b200fmm_set_charges", "b200fmm_execute",
     "b200fmm_reset_expansions", "b200fmm_p2m", "b200fmm_m2m", "b200fmm_m2l", "b200fmm_l2l", "b200fmm_l2p",
     "b200fmm_p2p", "b200fmm_get_results", "b200fmm_synchronize", "b200fmm_tree_info", "b200fmm_get_cells",
-    "b200fmm_get_permutation", "b200fmm_last_timings", "b200fmm_last_launch_count", "b200fmm_direct",
+    "b200fmm_get_permutation", "b200fmm_last_timings", "b200fmm_last_kernel_times", "b200fmm_tree_stats",
+    "b200fmm_last_launch_count", "b200fmm_direct",
 )
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -95,6 +96,8 @@ def lib():
         L.b200fmm_get_permutation.argtypes = [ctypes.c_void_p, _lp]
         L.b200fmm_last_timings.argtypes = [ctypes.c_void_p, _dp]
         L.b200fmm_last_launch_count.argtypes = [ctypes.c_void_p, _lp]
+        L.b200fmm_last_kernel_times.argtypes = [ctypes.c_void_p, _dp]
+        L.b200fmm_tree_stats.argtypes = [ctypes.c_void_p, _lp, _lp]
         L.b200fmm_direct.argtypes = [ctypes.c_longlong, _dp, _dp, _dp, _dp, ctypes.c_longlong, _lp, _dp, _dp, _dp, _dp]
         _lib = L
     return _lib
@@ -172,7 +175,7 @@ class FMM:
         if hasattr(x, "data_ptr"):
             n = x.numel()
             args = [ctypes.c_void_p(t.data_ptr()) for t in (x, y, z, q)]
-            _check(lib().b200fmm_set_particles(self._h, n, *args, 1), "set_particles")
+            _check(lib().b200fmm_set_particles(self._h, n, *args, 1 if x.is_cuda else 0), "set_particles")
         else:
             x, y, z, q = _f64(x), _f64(y), _f64(z), _f64(q)
             n = x.size
@@ -224,9 +227,10 @@ class FMM:
         shape = (R, n) if R > 1 else (n,)
         return dict(zip(("phi", "fx", "fy", "fz"), (o.reshape(shape) for o in out)))
 
-    def results_device(self, phi, fx, fy, fz):
-        _check(lib().b200fmm_get_results(self._h, *[ctypes.c_void_p(t.data_ptr()) for t in (phi, fx, fy, fz)], 1),
-               "get_results")
+    def results_into(self, phi, fx, fy, fz):
+        """Write the results into four tensors (CUDA tensors, or pinned host tensors)."""
+        _check(lib().b200fmm_get_results(self._h, *[ctypes.c_void_p(t.data_ptr()) for t in (phi, fx, fy, fz)],
+                                         1 if phi.is_cuda else 0), "get_results")
 
     def tree_info(self):
         nc = np.zeros(self.height, np.int64)
@@ -255,6 +259,16 @@ class FMM:
         ms = np.zeros(8)
         _check(lib().b200fmm_last_timings(self._h, _ptr(ms)), "last_timings")
         return dict(zip(("tree", "p2m", "m2m", "m2l", "l2l", "l2p", "p2p", "total"), ms.tolist()))
+
+    def kernel_times(self):
+        ms = np.zeros(4)
+        _check(lib().b200fmm_last_kernel_times(self._h, _ptr(ms)), "last_kernel_times")
+        return dict(zip(("m2l", "p2p", "p2m", "l2p"), ms.tolist()))
+
+    def tree_stats(self):
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        _check(lib().b200fmm_tree_stats(self._h, ctypes.byref(a), ctypes.byref(b)), "tree_stats")
+        return a.value, b.value
 
     def launch_count(self):
         c = ctypes.c_longlong()

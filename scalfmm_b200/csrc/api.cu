@@ -44,6 +44,27 @@ b200fmm_status check_status(Context &c) {
 
 namespace {
 
+// counts: [0] M2L pairs (existing interaction-list entries), [1] ordered P2P pairs
+__global__ void count_m2l_pairs(long long ncells, const int *__restrict__ ilist, unsigned long long *__restrict__ out) {
+  unsigned long long n = 0;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ncells * 189;
+       e += (long long)gridDim.x * blockDim.x)
+    n += ilist[e] >= 0;
+  atomicAdd(out, n);
+}
+__global__ void count_p2p_pairs(long long nleaves, const long long *__restrict__ start, const int *__restrict__ nbr,
+                                unsigned long long *__restrict__ out) {
+  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= nleaves) return;
+  const long long nt = start[c + 1] - start[c];
+  long long ns = 0;
+  for (int e = 0; e < 27; ++e) {
+    const int s = nbr[c * 27 + e];
+    if (s >= 0) ns += start[s + 1] - start[s];
+  }
+  atomicAdd(out + 1, (unsigned long long)(nt * ns - nt));
+}
+
 __global__ void scatter_to_original(long long n, int R, const long long *__restrict__ perm,
                                     const double *__restrict__ a, const double *__restrict__ b,
                                     const double *__restrict__ c, const double *__restrict__ d, double *__restrict__ oa,
@@ -441,6 +462,47 @@ b200fmm_status b200fmm_last_timings(b200fmm_handle h, double *ms8) {
   float tot = 0;
   if (cudaEventElapsedTime(&tot, c.ev[0], c.ev[7]) != cudaSuccess) tot = 0;
   ms8[7] = tot;
+  return B200FMM_OK;
+}
+
+b200fmm_status b200fmm_last_kernel_times(b200fmm_handle h, double *ms4) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  if (!ms4) return fail(B200FMM_ERR_INVALID, "null argument");
+  B200_CHECK(set_device(c));
+  B200_CUDA(cudaEventSynchronize(c.ev[7]));
+  float t = 0;
+  if (c.cfg.precision == B200FMM_MIXED && cudaEventElapsedTime(&t, c.ev[8], c.ev[9]) == cudaSuccess)
+    ms4[0] = t;
+  else
+    ms4[0] = (cudaEventElapsedTime(&t, c.ev[3], c.ev[4]) == cudaSuccess) ? t : 0;
+  ms4[1] = (cudaEventElapsedTime(&t, c.ev[10], c.ev[11]) == cudaSuccess) ? t : 0;
+  ms4[2] = (cudaEventElapsedTime(&t, c.ev[1], c.ev[2]) == cudaSuccess) ? t : 0;
+  ms4[3] = (cudaEventElapsedTime(&t, c.ev[5], c.ev[6]) == cudaSuccess) ? t : 0;
+  cudaGetLastError();
+  return B200FMM_OK;
+}
+
+b200fmm_status b200fmm_tree_stats(b200fmm_handle h, long long *m2l_pairs, long long *p2p_pairs) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  B200_CHECK(need_particles(c));
+  B200_CHECK(set_device(c));
+  B200_CHECK(ensure_scratch(c, 4096));
+  unsigned long long *d = (unsigned long long *)((char *)c.d_scratch + 2048);
+  B200_CUDA(cudaMemsetAsync(d, 0, 2 * sizeof(unsigned long long), c.stream));
+  for (int l = 2; l < c.H; ++l)
+    if (c.lv[l].n)
+      count_m2l_pairs<<<grid_for(c.lv[l].n * 189, 256) < 1024 ? grid_for(c.lv[l].n * 189, 256) : 1024, 256, 0,
+                        c.stream>>>(c.lv[l].n, c.lv[l].ilist, d);
+  const Level &lf = c.lv[c.H - 1];
+  count_p2p_pairs<<<grid_for(lf.n, 256), 256, 0, c.stream>>>(lf.n, c.d_leaf_start, c.d_leaf_nbr, d);
+  B200_CUDA(cudaGetLastError());
+  unsigned long long hv[2];
+  B200_CUDA(cudaMemcpyAsync(hv, d, sizeof(hv), cudaMemcpyDeviceToHost, c.stream));
+  B200_CUDA(cudaStreamSynchronize(c.stream));
+  if (m2l_pairs) *m2l_pairs = (long long)hv[0];
+  if (p2p_pairs) *p2p_pairs = (long long)hv[1];
   return B200FMM_OK;
 }
 

@@ -631,6 +631,7 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
   if (P.nitems <= 0) return B200FMM_OK;
   const size_t smem = (size_t)t->stages * t->stage_bytes + 1024;
   const int grid = std::min(t->grid, P.nitems);
+  B200_CUDA(cudaEventRecord(c.ev[8], c.stream));
   switch (t->NP / 2) {
 #define B200_TC_CASE(CWV)                                                                                      \
   case CWV:                                                                                                    \
@@ -646,6 +647,7 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
     default:
       return fail(B200FMM_ERR_UNSUPPORTED, "no tensor-core M2L instance for this order");
   }
+  B200_CUDA(cudaEventRecord(c.ev[9], c.stream));
   ++c.launches;
   B200_CUDA(cudaGetLastError());
   return B200FMM_OK;

@@ -305,15 +305,19 @@ b200fmm_status run_p2p(Context &c, int variant) {
     }
     int *status = c.d_status;
     const unsigned blocks = grid_for(L.n, P2P32_WARPS);
+    B200_CUDA(cudaEventRecord(c.ev[10], c.stream));
     p2p_fp32_kernel<<<blocks, P2P32_WARPS * 32, 0, c.stream>>>(c.R, c.N, L.n, c.d_leaf_start, c.d_leaf_nbr, variant,
                                                                c.d_pq32, c.d_pq32 + c.N * c.R,
                                                                c.cfg.box_width / (double)(1 << LL), c.d_phi,
                                                                c.d_fx, c.d_fy, c.d_fz, status);
+    B200_CUDA(cudaEventRecord(c.ev[11], c.stream));
     ++c.launches;
   } else {
+    B200_CUDA(cudaEventRecord(c.ev[10], c.stream));
     p2p_fp64_kernel<<<(unsigned)L.n, P2P64_THREADS, 0, c.stream>>>(c.R, c.N, c.d_leaf_start, c.d_leaf_nbr, variant,
                                                                    c.d_x, c.d_y, c.d_z, c.d_q, c.d_phi, c.d_fx,
                                                                    c.d_fy, c.d_fz);
+    B200_CUDA(cudaEventRecord(c.ev[11], c.stream));
     ++c.launches;
   }
   B200_CUDA(cudaGetLastError());
