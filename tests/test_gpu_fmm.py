@@ -5,7 +5,8 @@ Tolerances (relative L2 over the whole vector, FMath::FAccurater):
   * FP64 path with this library's own operator compression: the compression tolerance 10^-p can move the
     factors (pivot ties), so 50 * 10^-p against the reference;
   * integer tree work (keys, permutation, lists): exact;
-  * MIXED path: 2e-6 against the FP64 path (FP32 P2P + split-FP16 tensor-core M2L).
+  * MIXED path: 2e-6 against the FP64 path (FP32 P2P + split-FP16 tensor-core M2L); the bench gates the
+    1M-particle headline case at 1e-6 on the potential.
 """
 import numpy as np
 import pytest
@@ -249,7 +250,8 @@ def test_lagrange_fp64_matches_oracle():
 @pytest.mark.parametrize("order,height", [(5, 5), (7, 4), (4, 6)])
 def test_mixed_m2l_locals_match_fp64_dense(order, height):
     """Isolates the tensor-core M2L: same multipoles (FP64 P2M/M2M in both), locals after M2L compared per
-    level against the FP64 dense M2L."""
+    level against the FP64 dense M2L.  Tolerance 2e-6: split-FP16 operands carry 22 bits and each transfer
+    vector's tensor-core FP32 accumulation chain adds ~1e-6 at p = 7 (measured 1.1e-6 at level 2)."""
     rng = np.random.default_rng(order * 10 + height)
     n = 20000
     x, y, z = rng.random((3, n))
@@ -264,4 +266,4 @@ def test_mixed_m2l_locals_match_fp64_dense(order, height):
         f.close()
     for lvl in range(2, height):
         err = S.rel_l2(loc["mixed"][lvl], loc["fp64"][lvl])
-        assert err < 1e-6, (lvl, err)
+        assert err < 2e-6, (lvl, err)
