@@ -145,6 +145,28 @@ B200FMM_API b200fmm_status b200fmm_tree_stats(b200fmm_handle h, long long *m2l_p
 /* Number of kernel launches issued by the last set_particles() plus the last execute(). */
 B200FMM_API b200fmm_status b200fmm_last_launch_count(b200fmm_handle h, long long *count);
 
+/* Allocation-free near field.  This entry point has no counterpart in the reference.  It is for callers
+ * that must not allocate device memory while they run this step: code being captured into a CUDA graph by
+ * a framework that forbids allocations during capture, applications that hand all device memory to their
+ * own pool up front, or real-time loops where cudaMalloc's implicit synchronisation is not acceptable.
+ * It runs the MIXED-precision P2P of b200fmm_p2p (variant 0 or 1) on caller-owned device arrays and calls
+ * no cudaMalloc, cudaFree or other allocating routine: its scratch (the FP32 leaf-local copies of the
+ * particles) lives in a fixed 8 MiB device array inside this library, so it accepts at most
+ * B200FMM_NOALLOC_MAX_PARTICLES particles and returns B200FMM_ERR_INVALID above that.
+ *   x, y, z, q: n particles sorted by leaf (FP64, device); leaf_keys[nleaves] Morton keys of the non-empty
+ *   leaves in increasing order; leaf_start[nleaves+1] their particle ranges; leaf_nbr[nleaves*27] the leaf
+ *   index of each neighbour position ((dx+1)*3+(dy+1))*3+(dz+1) (13 = the leaf itself), -1 when empty;
+ *   phi, fx, fy, fz: n outputs (FP64, device) to which the near field is ADDED.  stream: cudaStream_t.
+ * The first call on a device looks up that array's device address (cudaGetSymbolAddress) with the device
+ * current; make that first call before any stream capture.  All calls share the one array and its status
+ * word, so calls whose executions overlap on the GPU race: serialise them (one stream, or events). */
+#define B200FMM_NOALLOC_MAX_PARTICLES 262144LL
+B200FMM_API b200fmm_status b200fmm_p2p_noalloc(long long n, const double *x, const double *y, const double *z,
+                                               const double *q, long long nleaves, const long long *leaf_keys,
+                                               const long long *leaf_start, const int *leaf_nbr, int height,
+                                               double box_width, const double *center, int variant, double *phi,
+                                               double *fx, double *fy, double *fz, void *stream);
+
 /* FP64 direct sum on the GPU (Examples/DirectComputation.cpp:104-142) for the listed targets (all if
  * ntargets < 0).  Host pointers; outputs have ntargets (or n) entries. */
 B200FMM_API b200fmm_status b200fmm_direct(long long n, const double *x, const double *y, const double *z, const double *q,

@@ -31,8 +31,9 @@ EXPORTS = (
     "b200fmm_reset_expansions", "b200fmm_p2m", "b200fmm_m2m", "b200fmm_m2l", "b200fmm_l2l", "b200fmm_l2p",
     "b200fmm_p2p", "b200fmm_get_results", "b200fmm_synchronize", "b200fmm_tree_info", "b200fmm_get_cells",
     "b200fmm_get_permutation", "b200fmm_last_timings", "b200fmm_last_kernel_times", "b200fmm_tree_stats",
-    "b200fmm_last_launch_count", "b200fmm_direct",
+    "b200fmm_last_launch_count", "b200fmm_p2p_noalloc", "b200fmm_direct",
 )
+NOALLOC_MAX_PARTICLES = 262144
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -98,6 +99,9 @@ def lib():
         L.b200fmm_last_launch_count.argtypes = [ctypes.c_void_p, _lp]
         L.b200fmm_last_kernel_times.argtypes = [ctypes.c_void_p, _dp]
         L.b200fmm_tree_stats.argtypes = [ctypes.c_void_p, _lp, _lp]
+        L.b200fmm_p2p_noalloc.argtypes = ([ctypes.c_longlong] + [ctypes.c_void_p] * 4 + [ctypes.c_longlong]
+                                          + [ctypes.c_void_p] * 3 + [ctypes.c_int, ctypes.c_double, _dp, ctypes.c_int]
+                                          + [ctypes.c_void_p] * 5)
         L.b200fmm_direct.argtypes = [ctypes.c_longlong, _dp, _dp, _dp, _dp, ctypes.c_longlong, _lp, _dp, _dp, _dp, _dp]
         _lib = L
     return _lib

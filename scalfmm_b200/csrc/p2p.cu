@@ -17,6 +17,8 @@
 //    in FP64 to the far field.
 #include "common.cuh"
 
+#include <mutex>
+
 namespace b200 {
 
 namespace {
@@ -325,3 +327,72 @@ b200fmm_status run_p2p(Context &c, int variant) {
 }
 
 }  // namespace b200
+
+// ---- allocation-free entry point -------------------------------------------------------------------
+// Scratch of b200fmm_p2p_noalloc: the hi and lo FP32 leaf-local particle copies (2 x 2^18 float4 = 8 MiB)
+// and the status word of the kernel's bounded waits.  In host code these names are host-side stand-ins,
+// not device addresses: the host passes the addresses looked up with cudaGetSymbolAddress.
+static __device__ __align__(256) float4 g_noalloc_stage[2 * B200FMM_NOALLOC_MAX_PARTICLES];
+static __device__ __align__(256) int g_noalloc_status[4];
+
+namespace b200 {
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+float4 *g_noalloc_stage_ptr[kMaxDevices] = {};
+int *g_noalloc_status_ptr[kMaxDevices] = {};
+
+// Once per device, with that device current: the device addresses of the file-scope arrays.
+b200fmm_status noalloc_addresses(float4 **stage, int **status) {
+  int dev = -1;
+  B200_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return fail(B200FMM_ERR_UNSUPPORTED, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_stage_ptr[dev]) {
+    void *a = nullptr, *b = nullptr;
+    B200_CUDA(cudaGetSymbolAddress(&a, g_noalloc_stage));
+    B200_CUDA(cudaGetSymbolAddress(&b, g_noalloc_status));
+    g_noalloc_stage_ptr[dev] = (float4 *)a;
+    g_noalloc_status_ptr[dev] = (int *)b;
+  }
+  *stage = g_noalloc_stage_ptr[dev];
+  *status = g_noalloc_status_ptr[dev];
+  return B200FMM_OK;
+}
+}  // namespace
+}  // namespace b200
+
+extern "C" b200fmm_status b200fmm_p2p_noalloc(long long n, const double *x, const double *y, const double *z,
+                                              const double *q, long long nleaves, const long long *leaf_keys,
+                                              const long long *leaf_start, const int *leaf_nbr, int height,
+                                              double box_width, const double *center, int variant, double *phi,
+                                              double *fx, double *fy, double *fz, void *stream) {
+  using namespace b200;
+  if (n < 1 || nleaves < 1 || nleaves > n) return fail(B200FMM_ERR_INVALID, "p2p_noalloc: bad particle/leaf count");
+  if (n > B200FMM_NOALLOC_MAX_PARTICLES)
+    return fail(B200FMM_ERR_INVALID, "p2p_noalloc: more than B200FMM_NOALLOC_MAX_PARTICLES (262144) particles");
+  if (!x || !y || !z || !q || !leaf_keys || !leaf_start || !leaf_nbr || !center || !phi || !fx || !fy || !fz)
+    return fail(B200FMM_ERR_INVALID, "p2p_noalloc: null pointer");
+  if (height < 2 || height > kMaxHeight) return fail(B200FMM_ERR_INVALID, "p2p_noalloc: height out of range");
+  if (variant != 0 && variant != 1) return fail(B200FMM_ERR_INVALID, "p2p_noalloc: variant must be 0 or 1");
+  if (!(box_width > 0)) return fail(B200FMM_ERR_INVALID, "p2p_noalloc: bad box width");
+  float4 *stage = nullptr;
+  int *status = nullptr;
+  B200_CHECK(noalloc_addresses(&stage, &status));
+  cudaStream_t s = (cudaStream_t)stream;
+  const int LL = height - 1;
+  const double leaf_w = box_width / (double)(1 << LL);
+  B200_CUDA(cudaMemsetAsync(status, 0, sizeof(int) * 4, s));
+  pack_local32<<<(unsigned)nleaves, 64, 0, s>>>(n, 1, leaf_keys, leaf_start, x, y, z, q, center[0] - box_width / 2,
+                                               center[1] - box_width / 2, center[2] - box_width / 2, leaf_w, stage,
+                                               stage + n);
+  p2p_fp32_kernel<<<grid_for(nleaves, P2P32_WARPS), P2P32_WARPS * 32, 0, s>>>(
+      1, n, nleaves, leaf_start, leaf_nbr, variant, stage, stage + n, leaf_w, phi, fx, fy, fz, status);
+  B200_CUDA(cudaGetLastError());
+  int st = 0;
+  B200_CUDA(cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  B200_CUDA(cudaStreamSynchronize(s));
+  if (st) return fail(B200FMM_ERR_CUDA, "p2p_noalloc: a device wait ran out of its iteration budget");
+  return B200FMM_OK;
+}
+
