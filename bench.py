@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=N_PART)
+    ap.add_argument("--height", type=int, default=HEIGHT, help="octree height (profiling of small cases only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
     return ap.parse_args()
@@ -61,9 +62,9 @@ def particles(n, seed=SEED):
     return pos[0].copy(), pos[1].copy(), pos[2].copy(), q
 
 
-def workload_config(n):
+def workload_config(n, height=HEIGHT):
     return {"workload": f"{n} particles uniform in [0,1)^3, q~U[-1,1] (seed {SEED}), Laplace 1/r, Chebyshev order "
-                        f"{ORDER}, height {HEIGHT}", "particles": n, "order": ORDER, "height": HEIGHT,
+                        f"{ORDER}, height {height}", "particles": n, "order": ORDER, "height": height,
             "precision": "mixed: FP32 compensated P2P, split-FP16 x3 tcgen05 M2L, FP64 P2M/M2M/L2L/L2P",
             "l2": "flushed between timed steps (512 MiB write)", "parallelism": "replicas"}
 
@@ -228,7 +229,7 @@ def run_gpu(args):
     out_h = [torch.empty(n, dtype=torch.float64).pin_memory() for _ in range(4)]
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
-    f = S.FMM("cheb_sym", ORDER, HEIGHT, precision="mixed", device=local, stream=stream.cuda_stream)
+    f = S.FMM("cheb_sym", ORDER, args.height, precision="mixed", device=local, stream=stream.cuda_stream)
 
     def step_device():
         f.set_particles(dx, dy, dz, dq)
@@ -294,7 +295,7 @@ def run_gpu(args):
         "metric": METRIC, "value": world * n * args.steps / (t_dev * 1e-3), "unit": "particles/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_dev / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32/f16x3 (mixed), f64 far-field bookkeeping",
-        "data": "synthetic", "config": workload_config(n),
+        "data": "synthetic", "config": workload_config(n, args.height),
         "e2e": {"value": world * n * args.steps / (t_e2e * 1e-3), "unit": "particles/s",
                 "h2d_bytes_per_step": 4 * 8 * n, "d2h_bytes_per_step": 4 * 8 * n},
         "gpu_launches": launches + launches_e2e,

@@ -127,7 +127,8 @@ void destroy_context(b200fmm_context *c) {
   for (void *p : {(void *)c->d_roots, (void *)c->d_Troots, (void *)c->d_S, (void *)c->d_pindices, (void *)c->d_pvec,
                   (void *)c->d_symU, (void *)c->d_symV, (void *)c->d_symoff, (void *)c->d_symrank,
                   (void *)c->d_dense, (void *)c->d_itab, (void *)c->d_class_order, (void *)c->d_cls_bounds,
-                  (void *)c->d_cls_slots, (void *)c->d_status, c->d_scratch})
+                  (void *)c->d_cls_slots, (void *)c->d_status, (void *)c->d_Ut, (void *)c->d_Vt,
+                  (void *)c->d_toff, (void *)c->d_trank, c->d_scratch})
     if (p) cudaFree(p);
   if (c->events_ready)
     for (auto &e : c->ev) cudaEventDestroy(e);
@@ -256,15 +257,11 @@ b200fmm_status b200fmm_set_particles(b200fmm_handle h, long long n, const double
   if (n < 1 || n > 2000000000LL) return fail(B200FMM_ERR_INVALID, "particle count must be in [1, 2e9]");
   if (!x || !y || !z || !q) return fail(B200FMM_ERR_INVALID, "null particle array");
   B200_CHECK(set_device(c));
-  B200_CUDA(cudaStreamSynchronize(c.stream));
-  free_tree(c);
+  c.has_particles = false;
   c.N = n;
   B200_CUDA(cudaEventRecord(c.ev[14], c.stream));
   b200fmm_status st = build_tree(c, x, y, z, q, on_device != 0);
-  if (st != B200FMM_OK) {
-    free_tree(c);
-    return st;
-  }
+  if (st != B200FMM_OK) return st;
   B200_CUDA(cudaEventRecord(c.ev[15], c.stream));
   B200_CUDA(cudaEventSynchronize(c.ev[15]));
   float ms = 0;
@@ -280,12 +277,7 @@ b200fmm_status b200fmm_set_charges(b200fmm_handle h, const double *q, int on_dev
   B200_CHECK(need_particles(c));
   if (!q) return fail(B200FMM_ERR_INVALID, "null charges");
   B200_CHECK(set_device(c));
-  B200_CHECK(upload_charges(c, q, on_device != 0));
-  if (c.d_pq32) {
-    cudaFreeAsync(c.d_pq32, c.stream);
-    c.d_pq32 = nullptr;
-  }
-  return B200FMM_OK;
+  return upload_charges(c, q, on_device != 0);
 }
 
 b200fmm_status b200fmm_reset_expansions(b200fmm_handle h) {

@@ -38,6 +38,8 @@ b200fmm_status fail(b200fmm_status st, const std::string &msg);
 // One level of the octree.  Cells are the non-empty cells of the level in Morton order.
 struct Level {
   long long n = 0;
+  size_t cap = 0;             // allocated cells (grow-only)
+  bool grid_ready = false;
   long long *keys = nullptr;  // [n] Morton keys (device)
   int *parent = nullptr;      // [n] index of the parent cell at level-1 (device)
   int *child = nullptr;       // [n][8] index of child cells at level+1, -1 if empty (device)
@@ -79,6 +81,11 @@ struct Context {
   long long *d_symoff = nullptr;     // [343] element offset of slot's U/V in d_symU/d_symV, -1 if none
   int *d_symrank = nullptr;          // [343]
   int max_rank = 0;
+  // the same operators expanded per transfer-vector slot t through its permutation:
+  // Ut[t][n][a] = U_c[pvec_t[n]][a] (row-major p^3 x r), Vt[t][a][m] = V_c[pvec_t[m]][a] (row-major r x p^3)
+  double *d_Ut = nullptr, *d_Vt = nullptr;
+  long long *d_toff = nullptr;       // [343] element offset of slot t's Ut / Vt, -1 for near slots
+  int *d_trank = nullptr;            // [343] rank of slot t (its class's rank)
 
   // dense FP64 operators (CHEB_DENSE / LAGRANGE in FP64): [343][nn][nn], zero for near slots
   double *d_dense = nullptr;
@@ -101,6 +108,19 @@ struct Context {
   double *d_phi = nullptr, *d_fx = nullptr, *d_fy = nullptr, *d_fz = nullptr;  // [R][N] sorted results
   Level lv[kMaxHeight];
   bool has_particles = false;
+  bool packed32 = false;      // d_pq32 holds the current particles
+
+  // grow-only buffers of the tree build (capacities in elements)
+  size_t cap_N = 0, cap_leaf = 0, cap_sort = 0, cap_cnt = 0, cap_stage = 0, cap_scan = 0;
+  unsigned long long *d_sortk = nullptr;  // [2N] radix-sort keys (ping-pong)
+  int *d_sortv = nullptr;                 // [2N] radix-sort values
+  long long *d_flags = nullptr;           // [2(N+1)] head flags and their scan
+  unsigned *d_cnt = nullptr;              // radix histograms and offsets
+  double *d_stage = nullptr;              // host input staged on the device
+  long long *d_scan = nullptr;            // scan block sums
+  int *d_err = nullptr;                   // domain error flag
+  long long *h_pinned = nullptr;          // small pinned host buffer for counts
+  int tree_gen = 0;                       // bumped whenever a tree buffer moves
 
   // device status words set by kernels whose bounded waits ran out (0 = fine); checked by the host at
   // every synchronising call

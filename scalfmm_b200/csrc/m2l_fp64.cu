@@ -3,8 +3,9 @@
 //  * CHEB_SYM: FChebSymKernel::M2L (Src/Kernels/Chebyshev/FChebSymKernel.hpp:210-328).  For each target the
 //    reference permutes every source multipole into its symmetry class frame (pvectors, pindices), applies the
 //    16 compressed operators as Y = V^T M' then scale * U Y per class, and adds the result back through the
-//    same permutation.  Here one CTA handles the (up to) 8 children of one parent, so each class operator is
-//    read once for 8 targets; pairs are processed class by class in chunks.
+//    same permutation.  Here the permutation is folded into per-slot factors U_t, V_t once (precompute.cu),
+//    and one CTA applies them for 32 targets of one child type -- which share their 189 slots -- keeping the
+//    local sums in registers.
 //  * CHEB_DENSE / LAGRANGE: L[m] += scale * sum_n K_t(X_m, Y_n) M[n] (FChebDenseKernel::M2L,
 //    FChebDenseKernel.hpp:116-127; FUnifKernel applies the same Toeplitz operator through FFTs).
 //  scale = 2 / cell width (FInterpMatrixKernelR::getScaleFactor, FInterpMatrixKernel.hpp:124-133).
@@ -14,120 +15,98 @@ namespace b200 {
 
 namespace {
 
-constexpr int SYM_CHUNK = 16;
+constexpr int SYM_T = 32;         // targets per CTA (children of one type of SYM_T consecutive parents)
 constexpr int SYM_THREADS = 256;
+constexpr int SYM_ACC = (SYM_T * 512 + SYM_THREADS - 1) / SYM_THREADS;  // outputs per thread, p <= 8
 
 struct SymArgs {
-  int p, nn, R;
+  int nn, R, rhs;
   double scale;
+  long long nparents;
   const int *child;        // parents' [8] children at the target level
-  const long long *keys;   // target keys (child type = key & 7)
   const int *ilist;        // [ntargets][189]
-  const int *class_order;  // [8][189]
-  const int *cls_bounds;   // [8][17]
-  const int *cls_slot;     // [16] class slot ids
-  const int *pvec;         // [343][nn]
-  const int *pind;         // [343]
-  const double *U, *V;     // per class [r][nn]
-  const long long *off;    // [343]
-  const int *rank;         // [343]
   const IListTable *itab;
+  const double *Ut, *Vt;   // per-slot permuted factors
+  const long long *toff;   // [343]
+  const int *trank;        // [343]
   const double *M;         // source multipoles at this level
   double *L;               // target locals at this level
   int max_rank;
 };
 
+// One CTA: the SYM_T targets of child type blockIdx.y among SYM_T consecutive parents.  For each of the
+// 189 transfer vectors of that child type: gather the source multipoles, Y = V_t^T M (rank r), then
+// L += scale * U_t Y, with the targets' local sums held in registers across all transfer vectors.
 __global__ void __launch_bounds__(SYM_THREADS) m2l_sym_kernel(SymArgs a) {
   extern __shared__ double sh[];
   const int nn = a.nn;
-  double *Lacc = sh;                          // [8][nn]
-  double *Mb = Lacc + 8 * nn;                 // [SYM_CHUNK][nn]
-  double *Y = Mb + SYM_CHUNK * nn;            // [SYM_CHUNK][max_rank]
-  int *pchild = (int *)(Y + SYM_CHUNK * a.max_rank);  // [SYM_CHUNK]
-  int *psrc = pchild + SYM_CHUNK;
-  int *pslot = psrc + SYM_CHUNK;
-  __shared__ int tgt[8];
-  const long long parent = blockIdx.x;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  if (threadIdx.x < 8) tgt[threadIdx.x] = a.child[parent * 8 + threadIdx.x];
-  for (int r = 0; r < a.R; ++r) {
-    __syncthreads();
-    for (int e = threadIdx.x; e < 8 * nn; e += blockDim.x) Lacc[e] = 0.0;
-    for (int ci = 0; ci < 16; ++ci) {
-      const int cls = a.cls_slot[ci];
-      const int rk = a.rank[cls];
-      const double *U = a.U + a.off[cls];
-      const double *V = a.V + a.off[cls];
-      // walk the class-ci entries of the 8 children as one sequence, chunk by chunk
-      int k = 0, pos = 0;  // child, position within its class run
-      while (true) {
-        __syncthreads();
-        // the next SYM_CHUNK existing pairs (thread 0 builds the chunk list)
-        if (threadIdx.x == 0) {
-          int cnt = 0;
-          while (k < 8 && cnt < SYM_CHUNK) {
-            const int tc = tgt[k];
-            if (tc < 0) {
-              ++k;
-              pos = 0;
-              continue;
-            }
-            const int b0 = a.cls_bounds[k * 17 + ci], b1 = a.cls_bounds[k * 17 + ci + 1];
-            if (b0 + pos >= b1) {
-              ++k;
-              pos = 0;
-              continue;
-            }
-            const int e = a.class_order[k * 189 + b0 + pos];
-            ++pos;
-            const int src = a.ilist[(long long)tc * 189 + e];
-            if (src < 0) continue;
-            pchild[cnt] = k;
-            psrc[cnt] = src;
-            pslot[cnt] = a.itab->slot[k][e];
-            ++cnt;
-          }
-          for (int j = cnt; j < SYM_CHUNK; ++j) pchild[j] = -1;
-        }
-        __syncthreads();
-        if (pchild[0] < 0) break;
-        // gather the permuted source multipoles: Mb[j][pvec[t][m]] = M[src][m]
-        for (int e = threadIdx.x; e < SYM_CHUNK * nn; e += blockDim.x) {
-          const int j = e / nn, m = e % nn;
-          if (pchild[j] < 0) continue;
-          Mb[j * nn + a.pvec[pslot[j] * nn + m]] = a.M[((long long)psrc[j] * a.R + r) * nn + m];
-        }
-        __syncthreads();
-        // Y[j][q] = sum_m V[q][m] Mb[j][m]   (one warp per dot product)
-        for (int d = warp; d < SYM_CHUNK * rk; d += nwarps) {
-          const int j = d / rk, q = d % rk;
-          double s = 0.0;
-          if (pchild[j] >= 0)
-            for (int m = lane; m < nn; m += 32) s += V[(long long)q * nn + m] * Mb[j * nn + m];
+  double *Ms = sh;                        // [SYM_T][nn]
+  double *Y = Ms + SYM_T * nn;            // [SYM_T][max_rank]
+  __shared__ int tgt[SYM_T], src[SYM_T];
+  __shared__ int any;
+  const int ct = blockIdx.y;
+  const long long p0 = (long long)blockIdx.x * SYM_T;
+  if (threadIdx.x < SYM_T) {
+    const long long p = p0 + threadIdx.x;
+    tgt[threadIdx.x] = p < a.nparents ? a.child[p * 8 + ct] : -1;
+  }
+  double acc[SYM_ACC];
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-          if (lane == 0) Y[j * a.max_rank + q] = s;
-        }
-        __syncthreads();
-        // Lacc[child][n] += scale * sum_q U[q][pvec[t][n]] Y[j][q]  (each thread owns outputs; deterministic)
-        for (int e = threadIdx.x; e < 8 * nn; e += blockDim.x) {
-          const int kk = e / nn, n = e % nn;
-          double acc = 0.0;
-          for (int j = 0; j < SYM_CHUNK; ++j) {
-            if (pchild[j] != kk) continue;
-            const int idx = a.pvec[pslot[j] * nn + n];
-            double s = 0.0;
-            for (int q = 0; q < rk; ++q) s += U[(long long)q * nn + idx] * Y[j * a.max_rank + q];
-            acc += s;
-          }
-          Lacc[e] += a.scale * acc;
+  for (int j = 0; j < SYM_ACC; ++j) acc[j] = 0.0;
+  const int nout = SYM_T * nn;
+  for (int e = 0; e < 189; ++e) {
+    __syncthreads();
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    if (threadIdx.x < SYM_T) {
+      const int tg = tgt[threadIdx.x];
+      const int sc = tg >= 0 ? a.ilist[(long long)tg * 189 + e] : -1;
+      src[threadIdx.x] = sc;
+      if (sc >= 0) any = 1;
+    }
+    __syncthreads();
+    if (!any) continue;
+    const int t = a.itab->slot[ct][e];
+    const int r = a.trank[t];
+    const double *Ut = a.Ut + a.toff[t];
+    const double *Vt = a.Vt + a.toff[t];
+    for (int idx = threadIdx.x; idx < nout; idx += blockDim.x) {
+      const int k = idx / nn, m = idx - k * nn;
+      const int sc = src[k];
+      Ms[idx] = sc >= 0 ? a.M[((long long)sc * a.R + a.rhs) * nn + m] : 0.0;
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < SYM_T * r; idx += blockDim.x) {
+      const int q = idx / SYM_T, k = idx - q * SYM_T;  // lanes share the operator row q
+      const double *v = Vt + (long long)q * nn;
+      const double *mk = Ms + k * nn;
+      double s = 0.0;
+      if (src[k] >= 0)
+        for (int m = 0; m < nn; ++m) s += v[m] * mk[m];
+      Y[k * a.max_rank + q] = s;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < SYM_ACC; ++j) {
+      const int o = threadIdx.x + j * SYM_THREADS;
+      if (o < nout) {
+        const int k = o / nn, n = o - k * nn;
+        if (src[k] >= 0) {
+          const double *u = Ut + (long long)n * r;
+          const double *y = Y + k * a.max_rank;
+          double s = 0.0;
+          for (int q = 0; q < r; ++q) s += u[q] * y[q];
+          acc[j] += s;
         }
       }
     }
-    __syncthreads();
-    for (int e = threadIdx.x; e < 8 * nn; e += blockDim.x) {
-      const int kk = e / nn, n = e % nn;
-      if (tgt[kk] >= 0) a.L[((long long)tgt[kk] * a.R + r) * nn + n] += Lacc[e];
+  }
+#pragma unroll
+  for (int j = 0; j < SYM_ACC; ++j) {
+    const int o = threadIdx.x + j * SYM_THREADS;
+    if (o < nout) {
+      const int k = o / nn, n = o - k * nn;
+      if (tgt[k] >= 0) a.L[((long long)tgt[k] * a.R + a.rhs) * nn + n] += a.scale * acc[j];
     }
   }
 }
@@ -173,30 +152,28 @@ b200fmm_status run_m2l_fp64(Context &c, int level) {
   const double scale = 2.0 / (c.cfg.box_width / (double)(1LL << level));
   if (c.cfg.kernel == B200FMM_CHEB_SYM && c.cfg.precision == B200FMM_FP64) {
     SymArgs a;
-    a.p = c.p;
     a.nn = c.nn;
     a.R = c.R;
     a.scale = scale;
+    a.nparents = c.lv[level - 1].n;
     a.child = c.lv[level - 1].child;
-    a.keys = T.keys;
     a.ilist = T.ilist;
-    a.class_order = c.d_class_order;
-    a.cls_bounds = c.d_cls_bounds;
-    a.cls_slot = c.d_cls_slots;
-    a.pvec = c.d_pvec;
-    a.pind = c.d_pindices;
-    a.U = c.d_symU;
-    a.V = c.d_symV;
-    a.off = c.d_symoff;
-    a.rank = c.d_symrank;
     a.itab = c.d_itab;
+    a.Ut = c.d_Ut;
+    a.Vt = c.d_Vt;
+    a.toff = c.d_toff;
+    a.trank = c.d_trank;
     a.M = T.M;
     a.L = T.L;
     a.max_rank = c.max_rank;
-    const size_t sh = sizeof(double) * (8 * c.nn + SYM_CHUNK * c.nn + SYM_CHUNK * c.max_rank) + sizeof(int) * 3 * SYM_CHUNK;
+    const size_t sh = sizeof(double) * ((size_t)SYM_T * c.nn + (size_t)SYM_T * c.max_rank);
     B200_CUDA(cudaFuncSetAttribute(m2l_sym_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
-    m2l_sym_kernel<<<(unsigned)c.lv[level - 1].n, SYM_THREADS, sh, c.stream>>>(a);
-    ++c.launches;
+    const dim3 grid((unsigned)((a.nparents + SYM_T - 1) / SYM_T), 8);
+    for (int r = 0; r < c.R; ++r) {
+      a.rhs = r;
+      m2l_sym_kernel<<<grid, SYM_THREADS, sh, c.stream>>>(a);
+      ++c.launches;
+    }
   } else {
     m2l_dense_kernel<<<(unsigned)T.n, 128, sizeof(double) * c.nn, c.stream>>>(
         c.p, c.R, scale, T.keys, T.ilist, c.d_itab, c.d_dense, T.M, T.L);

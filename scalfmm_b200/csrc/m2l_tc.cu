@@ -436,6 +436,7 @@ struct DenseTC {
   int nitems = 0;
   int lvl_begin[kMaxHeight] = {}, lvl_end[kMaxHeight] = {};
   long long built_for_N = -1;             // tree the per-level buffers were sized for
+  int built_for_gen = -1;                 // tree generation the tensor maps / pointers belong to
   TcParams *params = nullptr;             // host copy
   int grid = 0;
 };
@@ -600,6 +601,7 @@ static b200fmm_status tc_prepare(Context &c) {
   std::memcpy(P.slot, c.itab.slot, sizeof(P.slot));
   P.status = c.d_status;
   t->built_for_N = c.N;
+  t->built_for_gen = c.tree_gen;
   return B200FMM_OK;
 }
 
@@ -608,7 +610,7 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
   if (!t) return fail(B200FMM_ERR_STATE, "tensor-core M2L not initialised");
   const int LL = c.H - 1;
   if (level != -1 && (level < 2 || level > LL)) return fail(B200FMM_ERR_INVALID, "m2l: level out of range");
-  if (t->built_for_N != c.N || t->params->lv[LL].grid != c.lv[LL].grid) B200_CHECK(tc_prepare(c));
+  if (t->built_for_gen != c.tree_gen) B200_CHECK(tc_prepare(c));
   const int l0 = level == -1 ? 2 : level, l1 = level == -1 ? LL : level;
   for (int l = l0; l <= l1; ++l) {
     const Level &Lv = c.lv[l];

@@ -296,8 +296,8 @@ b200fmm_status run_p2p(Context &c, int variant) {
   const Level &L = c.lv[LL];
   if (L.n == 0) return B200FMM_OK;
   if (c.cfg.precision == B200FMM_MIXED) {
-    if (!c.d_pq32) {
-      B200_CUDA(cudaMallocAsync(&c.d_pq32, sizeof(float4) * c.N * (c.R + 1), c.stream));
+    if (!c.packed32) {
+      c.packed32 = true;
       const double W = c.cfg.box_width;
       pack_local32<<<(unsigned)L.n, 64, 0, c.stream>>>(c.N, c.R, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q,
                                                        c.cfg.center[0] - W / 2, c.cfg.center[1] - W / 2,

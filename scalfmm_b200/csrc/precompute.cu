@@ -433,8 +433,40 @@ b200fmm_status upload_sym_operators(Context &c) {
       used += 2LL * rk[t] * nn;
     }
   for (void *p : {(void *)c.d_pindices, (void *)c.d_pvec, (void *)c.d_symU, (void *)c.d_symV, (void *)c.d_symoff,
-                  (void *)c.d_symrank})
+                  (void *)c.d_symrank, (void *)c.d_Ut, (void *)c.d_Vt, (void *)c.d_toff, (void *)c.d_trank})
     if (p) cudaFree(p);
+  // per-slot permuted factors (FChebSymKernel::M2L applies the permutation around the class operator;
+  // folding it into the factors once gives plain per-slot operators)
+  std::vector<long long> toff(343, -1);
+  std::vector<int> trank(343, 0);
+  long long tot = 0;
+  for (int t = 0; t < 343; ++t) {
+    const int i = t / 49 - 3, j = (t / 7) % 7 - 3, k = t % 7 - 3;
+    if (!(std::abs(i) > 1 || std::abs(j) > 1 || std::abs(k) > 1)) continue;
+    toff[t] = tot;
+    trank[t] = rk[pind[t]];
+    tot += (long long)trank[t] * nn;
+  }
+  std::vector<double> Ut(tot), Vt(tot);
+  for (int t = 0; t < 343; ++t) {
+    if (toff[t] < 0) continue;
+    const int cls = pind[t], r = trank[t];
+    const double *Uc = U.data() + off[cls], *Vc = V.data() + off[cls];  // [a][j] = U_c[j][a]
+    const int *pv = pvec.data() + (size_t)t * nn;
+    for (int n = 0; n < nn; ++n)
+      for (int a = 0; a < r; ++a) {
+        Ut[toff[t] + (size_t)n * r + a] = Uc[(size_t)a * nn + pv[n]];
+        Vt[toff[t] + (size_t)a * nn + n] = Vc[(size_t)a * nn + pv[n]];
+      }
+  }
+  B200_CUDA(cudaMalloc(&c.d_Ut, sizeof(double) * std::max<long long>(tot, 1)));
+  B200_CUDA(cudaMalloc(&c.d_Vt, sizeof(double) * std::max<long long>(tot, 1)));
+  B200_CUDA(cudaMalloc(&c.d_toff, sizeof(long long) * 343));
+  B200_CUDA(cudaMalloc(&c.d_trank, sizeof(int) * 343));
+  B200_CUDA(cudaMemcpy(c.d_Ut, Ut.data(), sizeof(double) * tot, cudaMemcpyHostToDevice));
+  B200_CUDA(cudaMemcpy(c.d_Vt, Vt.data(), sizeof(double) * tot, cudaMemcpyHostToDevice));
+  B200_CUDA(cudaMemcpy(c.d_toff, toff.data(), sizeof(long long) * 343, cudaMemcpyHostToDevice));
+  B200_CUDA(cudaMemcpy(c.d_trank, trank.data(), sizeof(int) * 343, cudaMemcpyHostToDevice));
   B200_CUDA(cudaMalloc(&c.d_pindices, sizeof(int) * 343));
   B200_CUDA(cudaMalloc(&c.d_pvec, sizeof(int) * 343 * nn));
   B200_CUDA(cudaMalloc(&c.d_symU, sizeof(double) * std::max<long long>(o, 1)));

@@ -320,31 +320,49 @@ __global__ void fill_int(long long n, int *p, int v) {
   if (i < n) p[i] = v;
 }
 
-// exclusive scan (host driver, recursive over tiles of 1024)
-b200fmm_status scan_u32(Context &c, const unsigned *in, unsigned *out, long long n) {
+// grow-only device buffer: reallocates (and bumps the tree generation) only when n exceeds the capacity
+template <class T>
+b200fmm_status grow(Context &c, T *&p, size_t &cap, size_t n) {
+  if (p && n <= cap) return B200FMM_OK;
+  if (p) cudaFree(p);
+  p = nullptr;
+  const size_t nc = std::max<size_t>(n, cap + cap / 4);
+  B200_CUDA(cudaMalloc((void **)&p, sizeof(T) * std::max<size_t>(nc, 1)));
+  cap = nc;
+  ++c.tree_gen;
+  return B200FMM_OK;
+}
+
+// exclusive scans (host driver over tiles of 1024, block sums in a persistent buffer)
+template <class T>
+size_t scan_tmp_elems(long long n) {
+  size_t tot = 0;
+  long long tiles = (n + 1023) / 1024;
+  while (tiles > 1) {
+    tot += 2 * tiles;
+    tiles = (tiles + 1023) / 1024;
+  }
+  return tot + 2;
+}
+
+b200fmm_status scan_u32(Context &c, const unsigned *in, unsigned *out, long long n, unsigned *tmp) {
   const long long tiles = (n + 1023) / 1024;
   c.tree_launches += tiles > 1 ? 2 : 1;
-  unsigned *sums = nullptr;
-  if (tiles > 1) B200_CUDA(cudaMallocAsync(&sums, sizeof(unsigned) * tiles * 2, c.stream));
-  scan_tiles_u32<<<(unsigned)tiles, 1024, 0, c.stream>>>(in, out, n, sums);
+  scan_tiles_u32<<<(unsigned)tiles, 1024, 0, c.stream>>>(in, out, n, tiles > 1 ? tmp : nullptr);
   if (tiles > 1) {
-    B200_CHECK(scan_u32(c, sums, sums + tiles, tiles));
-    add_tile_offsets_u32<<<(unsigned)tiles, 1024, 0, c.stream>>>(out, n, sums + tiles);
-    B200_CUDA(cudaFreeAsync(sums, c.stream));
+    B200_CHECK(scan_u32(c, tmp, tmp + tiles, tiles, tmp + 2 * tiles));
+    add_tile_offsets_u32<<<(unsigned)tiles, 1024, 0, c.stream>>>(out, n, tmp + tiles);
   }
   return B200FMM_OK;
 }
 
-b200fmm_status scan_i64(Context &c, const long long *in, long long *out, long long n) {
+b200fmm_status scan_i64(Context &c, const long long *in, long long *out, long long n, long long *tmp) {
   const long long tiles = (n + 1023) / 1024;
   c.tree_launches += tiles > 1 ? 2 : 1;
-  long long *sums = nullptr;
-  if (tiles > 1) B200_CUDA(cudaMallocAsync(&sums, sizeof(long long) * tiles * 2, c.stream));
-  scan_tiles_i64<<<(unsigned)tiles, 1024, 0, c.stream>>>(in, out, n, sums);
+  scan_tiles_i64<<<(unsigned)tiles, 1024, 0, c.stream>>>(in, out, n, tiles > 1 ? tmp : nullptr);
   if (tiles > 1) {
-    B200_CHECK(scan_i64(c, sums, sums + tiles, tiles));
-    add_tile_offsets_i64<<<(unsigned)tiles, 1024, 0, c.stream>>>(out, n, sums + tiles);
-    B200_CUDA(cudaFreeAsync(sums, c.stream));
+    B200_CHECK(scan_i64(c, tmp, tmp + tiles, tiles, tmp + 2 * tiles));
+    add_tile_offsets_i64<<<(unsigned)tiles, 1024, 0, c.stream>>>(out, n, tmp + tiles);
   }
   return B200FMM_OK;
 }
@@ -370,6 +388,15 @@ void free_tree(Context &c) {
   dfree(c.d_fx);
   dfree(c.d_fy);
   dfree(c.d_fz);
+  dfree(c.d_sortk);
+  dfree(c.d_sortv);
+  dfree(c.d_flags);
+  dfree(c.d_cnt);
+  dfree(c.d_stage);
+  dfree(c.d_scan);
+  dfree(c.d_err);
+  if (c.h_pinned) cudaFreeHost(c.h_pinned);
+  c.h_pinned = nullptr;
   for (int l = 0; l < kMaxHeight; ++l) {
     Level &L = c.lv[l];
     dfree(L.keys);
@@ -380,22 +407,46 @@ void free_tree(Context &c) {
     dfree(L.L);
     dfree(L.grid);
     L.n = 0;
+    L.cap = 0;
+    L.grid_ready = false;
   }
+  c.cap_N = c.cap_leaf = c.cap_sort = c.cap_cnt = c.cap_stage = c.cap_scan = 0;
   c.N = 0;
   c.has_particles = false;
+  c.packed32 = false;
+  ++c.tree_gen;
 }
 
 b200fmm_status upload_charges(Context &c, const double *q, bool on_device) {
   const long long n = c.N;
-  double *dq = nullptr;
   if (!on_device) {
-    B200_CUDA(cudaMallocAsync(&dq, sizeof(double) * n * c.R, c.stream));
-    B200_CUDA(cudaMemcpyAsync(dq, q, sizeof(double) * n * c.R, cudaMemcpyHostToDevice, c.stream));
-    q = dq;
+    B200_CHECK(grow(c, c.d_stage, c.cap_stage, (size_t)n * (3 + c.R)));
+    B200_CUDA(cudaMemcpyAsync(c.d_stage, q, sizeof(double) * n * c.R, cudaMemcpyHostToDevice, c.stream));
+    q = c.d_stage;
   }
   gather_charges<<<grid_for(n, 256), 256, 0, c.stream>>>(n, c.R, c.d_perm, q, c.d_q);
-  if (dq) B200_CUDA(cudaFreeAsync(dq, c.stream));
   B200_CUDA(cudaGetLastError());
+  c.packed32 = false;
+  return B200FMM_OK;
+}
+
+// Level storage for n cells (grow-only; M and L are zeroed by execute / reset_expansions).
+static b200fmm_status level_storage(Context &c, Level &L, long long n) {
+  L.n = n;
+  if (L.keys && (size_t)n <= L.cap) return B200FMM_OK;
+  size_t cap = L.cap, tmp;
+  B200_CHECK(grow(c, L.keys, cap, (size_t)n));
+  tmp = L.cap;
+  B200_CHECK(grow(c, L.parent, tmp, cap));
+  tmp = 8 * L.cap;
+  B200_CHECK(grow(c, L.child, tmp, 8 * cap));
+  tmp = 189 * L.cap;
+  B200_CHECK(grow(c, L.ilist, tmp, 189 * cap));
+  tmp = (size_t)c.R * c.nn * L.cap;
+  B200_CHECK(grow(c, L.M, tmp, (size_t)c.R * c.nn * cap));
+  tmp = (size_t)c.R * c.nn * L.cap;
+  B200_CHECK(grow(c, L.L, tmp, (size_t)c.R * c.nn * cap));
+  L.cap = cap;
   return B200FMM_OK;
 }
 
@@ -405,89 +456,99 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
   const int H = c.H, LL = H - 1;
   cudaStream_t s = c.stream;
   c.tree_launches = 0;
+  c.packed32 = false;
+  if (!c.h_pinned) B200_CUDA(cudaMallocHost((void **)&c.h_pinned, sizeof(long long) * 64));
+  // particle-sized buffers
+  size_t cap;
+  cap = c.cap_N;
+  B200_CHECK(grow(c, c.d_x, cap, (size_t)n));
+  cap = c.cap_N;
+  B200_CHECK(grow(c, c.d_y, cap, (size_t)n));
+  cap = c.cap_N;
+  B200_CHECK(grow(c, c.d_z, cap, (size_t)n));
+  cap = c.cap_N;
+  B200_CHECK(grow(c, c.d_perm, cap, (size_t)n));
+  for (double **p : {&c.d_q, &c.d_phi, &c.d_fx, &c.d_fy, &c.d_fz}) {
+    size_t cr = c.cap_N * c.R;
+    B200_CHECK(grow(c, *p, cr, (size_t)n * c.R));
+  }
+  {
+    size_t cp = c.cap_N * (c.R + 1);
+    B200_CHECK(grow(c, c.d_pq32, cp, (size_t)n * (c.R + 1)));
+  }
+  c.cap_N = std::max(c.cap_N, (size_t)n);
+  {
+    // the three sort buffers share one capacity: each compares against the old value
+    size_t cs = c.cap_sort;
+    B200_CHECK(grow(c, c.d_sortk, cs, (size_t)2 * (n + 1)));
+    cs = c.cap_sort;
+    B200_CHECK(grow(c, c.d_sortv, cs, (size_t)2 * (n + 1)));
+    cs = c.cap_sort;
+    B200_CHECK(grow(c, c.d_flags, cs, (size_t)2 * (n + 1)));
+    c.cap_sort = std::max(c.cap_sort, (size_t)(2 * (n + 1)));
+  }
+  const long long nb = (n + RS_TILE - 1) / RS_TILE;
+  B200_CHECK(grow(c, c.d_cnt, c.cap_cnt, (size_t)2 * RS_BINS * nb));
+  B200_CHECK(grow(c, c.d_scan, c.cap_scan,
+                  std::max(scan_tmp_elems<long long>(n + 1), scan_tmp_elems<unsigned>(RS_BINS * nb))));
+  if (!c.d_err) B200_CUDA(cudaMalloc(&c.d_err, sizeof(int)));
   // inputs on the device
   const double *dx = x, *dy = y, *dz = z, *dq = q;
-  double *own = nullptr;
   if (!on_device) {
-    B200_CUDA(cudaMallocAsync(&own, sizeof(double) * n * (3 + c.R), s));
-    B200_CUDA(cudaMemcpyAsync(own, x, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    B200_CUDA(cudaMemcpyAsync(own + n, y, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    B200_CUDA(cudaMemcpyAsync(own + 2 * n, z, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    B200_CUDA(cudaMemcpyAsync(own + 3 * n, q, sizeof(double) * n * c.R, cudaMemcpyHostToDevice, s));
-    dx = own;
-    dy = own + n;
-    dz = own + 2 * n;
-    dq = own + 3 * n;
+    B200_CHECK(grow(c, c.d_stage, c.cap_stage, (size_t)n * (3 + c.R)));
+    B200_CUDA(cudaMemcpyAsync(c.d_stage, x, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    B200_CUDA(cudaMemcpyAsync(c.d_stage + n, y, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    B200_CUDA(cudaMemcpyAsync(c.d_stage + 2 * n, z, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    B200_CUDA(cudaMemcpyAsync(c.d_stage + 3 * n, q, sizeof(double) * n * c.R, cudaMemcpyHostToDevice, s));
+    dx = c.d_stage;
+    dy = c.d_stage + n;
+    dz = c.d_stage + 2 * n;
+    dq = c.d_stage + 3 * n;
   }
-  // keys
-  unsigned long long *k0 = nullptr, *k1 = nullptr;
-  int *v0 = nullptr, *v1 = nullptr, *err = nullptr;
-  const long long nb = (n + RS_TILE - 1) / RS_TILE;
-  unsigned *cnt = nullptr, *off = nullptr;
-  B200_CUDA(cudaMallocAsync(&k0, sizeof(unsigned long long) * n * 2, s));
-  B200_CUDA(cudaMallocAsync(&v0, sizeof(int) * n * 2, s));
-  B200_CUDA(cudaMallocAsync(&err, sizeof(int), s));
-  B200_CUDA(cudaMallocAsync(&cnt, sizeof(unsigned) * RS_BINS * nb * 2, s));
-  k1 = k0 + n;
-  v1 = v0 + n;
-  off = cnt + RS_BINS * nb;
-  B200_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+  unsigned long long *k0 = c.d_sortk, *k1 = c.d_sortk + n;
+  int *v0 = c.d_sortv, *v1 = c.d_sortv + n;
+  unsigned *cnt = c.d_cnt, *off = c.d_cnt + RS_BINS * nb;
+  long long *flags = c.d_flags, *idx = c.d_flags + (n + 1);
+  B200_CUDA(cudaMemsetAsync(c.d_err, 0, sizeof(int), s));
   const double W = c.cfg.box_width;
   const double leaf_w = W / (double)(1 << LL);
   keys_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, dx, dy, dz, c.cfg.center[0] - W / 2, c.cfg.center[1] - W / 2,
-                                               c.cfg.center[2] - W / 2, W, leaf_w, H, k0, v0, err);
+                                               c.cfg.center[2] - W / 2, W, leaf_w, H, k0, v0, c.d_err);
   ++c.tree_launches;
-  int herr = 0;
-  B200_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s));
-  B200_CUDA(cudaStreamSynchronize(s));
-  if (herr) {
-    cudaFreeAsync(k0, s);
-    cudaFreeAsync(v0, s);
-    cudaFreeAsync(err, s);
-    cudaFreeAsync(cnt, s);
-    if (own) cudaFreeAsync(own, s);
-    cudaStreamSynchronize(s);
-    return fail(B200FMM_ERR_DOMAIN, "a particle lies outside the box or has a non-finite coordinate");
-  }
-  // sort
+  // stable LSD radix sort of (key, original index)
   const int bits = 3 * LL;
   for (int sh = 0; sh < bits; sh += 4) {
     rs_hist<<<(unsigned)nb, RS_THREADS, 0, s>>>(k0, n, sh, (int)nb, cnt);
-    ++c.tree_launches;
-    B200_CHECK(scan_u32(c, cnt, off, RS_BINS * nb));
+    B200_CHECK(scan_u32(c, cnt, off, RS_BINS * nb, (unsigned *)c.d_scan));
     rs_scatter<<<(unsigned)nb, RS_THREADS, 0, s>>>(k0, v0, k1, v1, n, sh, (int)nb, off);
-    ++c.tree_launches;
+    c.tree_launches += 2;
     std::swap(k0, k1);
     std::swap(v0, v1);
   }
-  // particle arrays
-  B200_CUDA(cudaMallocAsync(&c.d_x, sizeof(double) * n, s));
-  B200_CUDA(cudaMallocAsync(&c.d_y, sizeof(double) * n, s));
-  B200_CUDA(cudaMallocAsync(&c.d_z, sizeof(double) * n, s));
-  B200_CUDA(cudaMallocAsync(&c.d_q, sizeof(double) * n * c.R, s));
-  B200_CUDA(cudaMallocAsync(&c.d_perm, sizeof(long long) * n, s));
-  for (double **p : {&c.d_phi, &c.d_fx, &c.d_fy, &c.d_fz}) B200_CUDA(cudaMallocAsync(p, sizeof(double) * n * c.R, s));
   gather_particles<<<grid_for(n, 256), 256, 0, s>>>(n, c.R, v0, dx, dy, dz, dq, c.d_x, c.d_y, c.d_z, c.d_q, c.d_perm);
-  ++c.tree_launches;
-  // leaves
-  long long *flags = nullptr, *idx = nullptr;
-  B200_CUDA(cudaMallocAsync(&flags, sizeof(long long) * (n + 1) * 2, s));
-  idx = flags + (n + 1);
   head_flags<<<grid_for(n, 256), 256, 0, s>>>(n, k0, 0, flags);
-  ++c.tree_launches;
-  B200_CHECK(scan_i64(c, flags, idx, n));
-  long long last_idx = 0, last_flag = 0;
-  B200_CUDA(cudaMemcpyAsync(&last_idx, idx + n - 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
-  B200_CUDA(cudaMemcpyAsync(&last_flag, flags + n - 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  c.tree_launches += 2;
+  B200_CHECK(scan_i64(c, flags, idx, n, (long long *)c.d_scan));
+  // one synchronisation: the leaf count and the domain error flag
+  B200_CUDA(cudaMemcpyAsync(c.h_pinned, idx + n - 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  B200_CUDA(cudaMemcpyAsync(c.h_pinned + 1, flags + n - 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  B200_CUDA(cudaMemcpyAsync(c.h_pinned + 2, c.d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
   B200_CUDA(cudaStreamSynchronize(s));
-  const long long nleaves = last_idx + last_flag;
+  if ((int)c.h_pinned[2]) return fail(B200FMM_ERR_DOMAIN, "a particle lies outside the box or has a non-finite coordinate");
+  const long long nleaves = c.h_pinned[0] + c.h_pinned[1];
   Level &leaf = c.lv[LL];
-  leaf.n = nleaves;
-  B200_CUDA(cudaMallocAsync(&leaf.keys, sizeof(long long) * nleaves, s));
-  B200_CUDA(cudaMallocAsync(&c.d_leaf_start, sizeof(long long) * (nleaves + 1), s));
+  B200_CHECK(level_storage(c, leaf, nleaves));
+  {
+    size_t cl = c.cap_leaf;
+    B200_CHECK(grow(c, c.d_leaf_start, cl, (size_t)nleaves + 1));
+    cl = c.cap_leaf * 27;
+    B200_CHECK(grow(c, c.d_leaf_nbr, cl, (size_t)(nleaves + 1) * 27));
+    c.cap_leaf = std::max(c.cap_leaf, (size_t)nleaves + 1);
+  }
   compact_leaves<<<grid_for(n, 256), 256, 0, s>>>(n, k0, flags, idx, leaf.keys, c.d_leaf_start);
   ++c.tree_launches;
-  B200_CUDA(cudaMemcpyAsync(c.d_leaf_start + nleaves, &c.N, sizeof(long long), cudaMemcpyHostToDevice, s));
+  c.h_pinned[3] = c.N;
+  B200_CUDA(cudaMemcpyAsync(c.d_leaf_start + nleaves, c.h_pinned + 3, sizeof(long long), cudaMemcpyHostToDevice, s));
   // upper levels
   for (int l = LL - 1; l >= 0; --l) {
     Level &ch = c.lv[l + 1];
@@ -495,53 +556,33 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
     const long long nc = ch.n;
     head_flags_i64<<<grid_for(nc, 256), 256, 0, s>>>(nc, ch.keys, flags);
     ++c.tree_launches;
-    B200_CHECK(scan_i64(c, flags, idx, nc));
-    long long li = 0, lf = 0;
-    B200_CUDA(cudaMemcpyAsync(&li, idx + nc - 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
-    B200_CUDA(cudaMemcpyAsync(&lf, flags + nc - 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    B200_CHECK(scan_i64(c, flags, idx, nc, (long long *)c.d_scan));
+    B200_CUDA(cudaMemcpyAsync(c.h_pinned + 4, idx + nc - 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    B200_CUDA(cudaMemcpyAsync(c.h_pinned + 5, flags + nc - 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
     B200_CUDA(cudaStreamSynchronize(s));
-    pa.n = li + lf;
-    B200_CUDA(cudaMallocAsync(&pa.keys, sizeof(long long) * pa.n, s));
-    B200_CUDA(cudaMallocAsync(&ch.parent, sizeof(int) * nc, s));
-    B200_CUDA(cudaMallocAsync(&pa.child, sizeof(int) * pa.n * 8, s));
+    B200_CHECK(level_storage(c, pa, c.h_pinned[4] + c.h_pinned[5]));
     fill_int<<<grid_for(pa.n * 8, 256), 256, 0, s>>>(pa.n * 8, pa.child, -1);
-    ++c.tree_launches;
     compact_parents<<<grid_for(nc, 256), 256, 0, s>>>(nc, ch.keys, flags, idx, pa.keys, ch.parent, pa.child);
-    ++c.tree_launches;
-  }
-  // expansions
-  for (int l = 2; l <= LL; ++l) {
-    Level &L = c.lv[l];
-    const size_t bytes = sizeof(double) * (size_t)L.n * c.R * c.nn;
-    B200_CUDA(cudaMallocAsync(&L.M, bytes, s));
-    B200_CUDA(cudaMallocAsync(&L.L, bytes, s));
-    B200_CUDA(cudaMemsetAsync(L.M, 0, bytes, s));
-    B200_CUDA(cudaMemsetAsync(L.L, 0, bytes, s));
+    c.tree_launches += 2;
   }
   // neighbour and interaction lists
-  B200_CUDA(cudaMallocAsync(&c.d_leaf_nbr, sizeof(int) * nleaves * 27, s));
   leaf_neighbors_kernel<<<grid_for(nleaves, 128), 128, 0, s>>>(nleaves, leaf.keys, H, c.d_leaf_nbr);
   ++c.tree_launches;
   for (int l = 2; l <= LL; ++l) {
     Level &L = c.lv[l];
-    B200_CUDA(cudaMallocAsync(&L.ilist, sizeof(int) * L.n * 189, s));
     ilist_kernel<<<(unsigned)L.n, 192, 0, s>>>(L.n, L.keys, l, c.d_itab, L.ilist);
     ++c.tree_launches;
     if (c.cfg.precision == B200FMM_MIXED) {
       const long long side = 1LL << l;
-      B200_CUDA(cudaMallocAsync(&L.grid, sizeof(int) * side * side * side, s));
+      if (!L.grid) {
+        B200_CUDA(cudaMalloc(&L.grid, sizeof(int) * side * side * side));
+        ++c.tree_gen;
+      }
       fill_int<<<grid_for(side * side * side, 256), 256, 0, s>>>(side * side * side, L.grid, -1);
-      ++c.tree_launches;
       grid_index_kernel<<<grid_for(L.n, 256), 256, 0, s>>>(L.n, L.keys, l, L.grid);
-      ++c.tree_launches;
+      c.tree_launches += 2;
     }
   }
-  B200_CUDA(cudaFreeAsync(flags, s));
-  B200_CUDA(cudaFreeAsync(k0 < k1 ? k0 : k1, s));
-  B200_CUDA(cudaFreeAsync(v0 < v1 ? v0 : v1, s));
-  B200_CUDA(cudaFreeAsync(err, s));
-  B200_CUDA(cudaFreeAsync(cnt, s));
-  if (own) B200_CUDA(cudaFreeAsync(own, s));
   B200_CUDA(cudaGetLastError());
   return B200FMM_OK;
 }
