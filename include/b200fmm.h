@@ -151,7 +151,7 @@ B200FMM_API b200fmm_status b200fmm_last_launch_count(b200fmm_handle h, long long
  * own pool up front, or real-time loops where cudaMalloc's implicit synchronisation is not acceptable.
  * It runs the MIXED-precision P2P of b200fmm_p2p (variant 0 or 1) on caller-owned device arrays and calls
  * no cudaMalloc, cudaFree or other allocating routine: its scratch (the FP32 leaf-local copies of the
- * particles) lives in a fixed 8 MiB device array inside this library, so it accepts at most
+ * particles) lives in a fixed 24 MiB device array inside this library, so it accepts at most
  * B200FMM_NOALLOC_MAX_PARTICLES particles and returns B200FMM_ERR_INVALID above that.
  *   x, y, z, q: n particles sorted by leaf (FP64, device); leaf_keys[nleaves] Morton keys of the non-empty
  *   leaves in increasing order; leaf_start[nleaves+1] their particle ranges; leaf_nbr[nleaves*27] the leaf

@@ -82,7 +82,7 @@ struct Context {
   int *d_symrank = nullptr;          // [343]
   int max_rank = 0;
   // the same operators expanded per transfer-vector slot t through its permutation:
-  // Ut[t][n][a] = U_c[pvec_t[n]][a] (row-major p^3 x r), Vt[t][a][m] = V_c[pvec_t[m]][a] (row-major r x p^3)
+  // Ut[t][n][a] = U_c[pvec_t[n]][a], Vt[t][m][a] = V_c[pvec_t[m]][a] (both row-major p^3 x r)
   double *d_Ut = nullptr, *d_Vt = nullptr;
   long long *d_toff = nullptr;       // [343] element offset of slot t's Ut / Vt, -1 for near slots
   int *d_trank = nullptr;            // [343] rank of slot t (its class's rank)

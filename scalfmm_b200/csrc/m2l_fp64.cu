@@ -15,18 +15,16 @@ namespace b200 {
 
 namespace {
 
-constexpr int SYM_T = 32;         // targets per CTA (children of one type of SYM_T consecutive parents)
-constexpr int SYM_THREADS = 256;
-constexpr int SYM_ACC = (SYM_T * 512 + SYM_THREADS - 1) / SYM_THREADS;  // outputs per thread, p <= 8
+constexpr int SYM_THREADS = 512;
 
 struct SymArgs {
-  int nn, R, rhs;
+  int R, rhs;
   double scale;
   long long nparents;
   const int *child;        // parents' [8] children at the target level
   const int *ilist;        // [ntargets][189]
   const IListTable *itab;
-  const double *Ut, *Vt;   // per-slot permuted factors
+  const double *Ut, *Vt;   // per-slot permuted factors, both [p^3][r]
   const long long *toff;   // [343]
   const int *trank;        // [343]
   const double *M;         // source multipoles at this level
@@ -34,31 +32,35 @@ struct SymArgs {
   int max_rank;
 };
 
-// One CTA: the SYM_T targets of child type blockIdx.y among SYM_T consecutive parents.  For each of the
-// 189 transfer vectors of that child type: gather the source multipoles, Y = V_t^T M (rank r), then
-// L += scale * U_t Y, with the targets' local sums held in registers across all transfer vectors.
+template <int P>
+__host__ __device__ constexpr int sym_targets() { return P >= 8 ? 16 : 32; }
+
+// One CTA: the T targets of child type blockIdx.y among T consecutive parents.  For each of the 189 transfer
+// vectors of that child type: gather the source multipoles, Y = V_t^T M (rank r), then L += U_t Y, with the
+// targets' local sums kept in shared memory across all transfer vectors (each owned by one thread).  Both
+// phases give every thread independent FMA chains (two targets x two partial sums).
+template <int P>
 __global__ void __launch_bounds__(SYM_THREADS) m2l_sym_kernel(SymArgs a) {
+  constexpr int nn = P * P * P, T = sym_targets<P>();
   extern __shared__ double sh[];
-  const int nn = a.nn;
-  double *Ms = sh;                        // [SYM_T][nn]
-  double *Y = Ms + SYM_T * nn;            // [SYM_T][max_rank]
-  __shared__ int tgt[SYM_T], src[SYM_T];
+  double *Ms = sh;                        // [T][nn] gathered source multipoles
+  double *Lacc = Ms + T * nn;             // [T][nn] local sums
+  double *Y = Lacc + T * nn;              // [T][max_rank]
+  __shared__ int tgt[T], src[T];
   __shared__ int any;
   const int ct = blockIdx.y;
-  const long long p0 = (long long)blockIdx.x * SYM_T;
-  if (threadIdx.x < SYM_T) {
+  const long long p0 = (long long)blockIdx.x * T;
+  if (threadIdx.x < T) {
     const long long p = p0 + threadIdx.x;
     tgt[threadIdx.x] = p < a.nparents ? a.child[p * 8 + ct] : -1;
   }
-  double acc[SYM_ACC];
-#pragma unroll
-  for (int j = 0; j < SYM_ACC; ++j) acc[j] = 0.0;
-  const int nout = SYM_T * nn;
+  constexpr int nout = T * nn;
+  for (int o = threadIdx.x; o < nout; o += blockDim.x) Lacc[o] = 0.0;
   for (int e = 0; e < 189; ++e) {
     __syncthreads();
     if (threadIdx.x == 0) any = 0;
     __syncthreads();
-    if (threadIdx.x < SYM_T) {
+    if (threadIdx.x < T) {
       const int tg = tgt[threadIdx.x];
       const int sc = tg >= 0 ? a.ilist[(long long)tg * 189 + e] : -1;
       src[threadIdx.x] = sc;
@@ -76,38 +78,47 @@ __global__ void __launch_bounds__(SYM_THREADS) m2l_sym_kernel(SymArgs a) {
       Ms[idx] = sc >= 0 ? a.M[((long long)sc * a.R + a.rhs) * nn + m] : 0.0;
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < SYM_T * r; idx += blockDim.x) {
-      const int q = idx / SYM_T, k = idx - q * SYM_T;  // lanes share the operator row q
-      const double *v = Vt + (long long)q * nn;
-      const double *mk = Ms + k * nn;
-      double s = 0.0;
-      if (src[k] >= 0)
-        for (int m = 0; m < nn; ++m) s += v[m] * mk[m];
-      Y[k * a.max_rank + q] = s;
+    // Y[k][q] and Y[k + T/2][q]: thread = (k < T/2, q)
+    for (int idx = threadIdx.x; idx < (T / 2) * r; idx += blockDim.x) {
+      const int k = idx % (T / 2), q = idx / (T / 2);
+      const double *m0 = Ms + k * nn, *m1 = Ms + (k + T / 2) * nn;
+      double s00 = 0.0, s01 = 0.0, s10 = 0.0, s11 = 0.0;
+      int m = 0;
+      for (; m + 1 < nn; m += 2) {
+        const double v0 = Vt[(long long)m * r + q], v1 = Vt[(long long)(m + 1) * r + q];
+        s00 += v0 * m0[m];
+        s01 += v1 * m0[m + 1];
+        s10 += v0 * m1[m];
+        s11 += v1 * m1[m + 1];
+      }
+      if (m < nn) {
+        const double v0 = Vt[(long long)m * r + q];
+        s00 += v0 * m0[m];
+        s10 += v0 * m1[m];
+      }
+      Y[k * a.max_rank + q] = s00 + s01;
+      Y[(k + T / 2) * a.max_rank + q] = s10 + s11;
     }
     __syncthreads();
-#pragma unroll
-    for (int j = 0; j < SYM_ACC; ++j) {
-      const int o = threadIdx.x + j * SYM_THREADS;
-      if (o < nout) {
-        const int k = o / nn, n = o - k * nn;
-        if (src[k] >= 0) {
-          const double *u = Ut + (long long)n * r;
-          const double *y = Y + k * a.max_rank;
-          double s = 0.0;
-          for (int q = 0; q < r; ++q) s += u[q] * y[q];
-          acc[j] += s;
-        }
+    for (int o = threadIdx.x; o < nout; o += blockDim.x) {
+      const int k = o / nn, n = o - k * nn;
+      if (src[k] < 0) continue;
+      const double *u = Ut + (long long)n * r;
+      const double *y = Y + k * a.max_rank;
+      double s0 = 0.0, s1 = 0.0;
+      int q = 0;
+      for (; q + 1 < r; q += 2) {
+        s0 += u[q] * y[q];
+        s1 += u[q + 1] * y[q + 1];
       }
+      if (q < r) s0 += u[q] * y[q];
+      Lacc[o] += s0 + s1;
     }
   }
-#pragma unroll
-  for (int j = 0; j < SYM_ACC; ++j) {
-    const int o = threadIdx.x + j * SYM_THREADS;
-    if (o < nout) {
-      const int k = o / nn, n = o - k * nn;
-      if (tgt[k] >= 0) a.L[((long long)tgt[k] * a.R + a.rhs) * nn + n] += a.scale * acc[j];
-    }
+  __syncthreads();
+  for (int o = threadIdx.x; o < nout; o += blockDim.x) {
+    const int k = o / nn, n = o - k * nn;
+    if (tgt[k] >= 0) a.L[((long long)tgt[k] * a.R + a.rhs) * nn + n] += a.scale * Lacc[o];
   }
 }
 
@@ -152,7 +163,6 @@ b200fmm_status run_m2l_fp64(Context &c, int level) {
   const double scale = 2.0 / (c.cfg.box_width / (double)(1LL << level));
   if (c.cfg.kernel == B200FMM_CHEB_SYM && c.cfg.precision == B200FMM_FP64) {
     SymArgs a;
-    a.nn = c.nn;
     a.R = c.R;
     a.scale = scale;
     a.nparents = c.lv[level - 1].n;
@@ -166,12 +176,22 @@ b200fmm_status run_m2l_fp64(Context &c, int level) {
     a.M = T.M;
     a.L = T.L;
     a.max_rank = c.max_rank;
-    const size_t sh = sizeof(double) * ((size_t)SYM_T * c.nn + (size_t)SYM_T * c.max_rank);
-    B200_CUDA(cudaFuncSetAttribute(m2l_sym_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
-    const dim3 grid((unsigned)((a.nparents + SYM_T - 1) / SYM_T), 8);
+    const int T = c.p >= 8 ? 16 : 32;
+    const size_t sh = sizeof(double) * (2 * (size_t)T * c.nn + (size_t)T * c.max_rank);
+    const dim3 grid((unsigned)((a.nparents + T - 1) / T), 8);
     for (int r = 0; r < c.R; ++r) {
       a.rhs = r;
-      m2l_sym_kernel<<<grid, SYM_THREADS, sh, c.stream>>>(a);
+      switch (c.p) {
+#define B200_SYM(PV)                                                                                        \
+  case PV:                                                                                                  \
+    B200_CUDA(cudaFuncSetAttribute(m2l_sym_kernel<PV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh)); \
+    m2l_sym_kernel<PV><<<grid, SYM_THREADS, sh, c.stream>>>(a);                                             \
+    break;
+        B200_SYM(3) B200_SYM(4) B200_SYM(5) B200_SYM(6) B200_SYM(7) B200_SYM(8)
+#undef B200_SYM
+        default:
+          return fail(B200FMM_ERR_UNSUPPORTED, "order not built");
+      }
       ++c.launches;
     }
   } else {

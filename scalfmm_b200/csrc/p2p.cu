@@ -7,7 +7,8 @@
 //
 //  * FP64 (parity form): one CTA per target leaf, source leaves staged through shared memory, the
 //    reference's arithmetic sequence (1/r^2, sqrt, products).
-//  * FP32 (mixed form): positions are stored relative to their own leaf centre as a float pair
+//  * FP32 (mixed form), two source particles per step with Blackwell's packed FP32x2 instructions
+//    (add/mul/fma.f32x2): positions are stored relative to their own leaf centre as a float pair
 //    (hi, lo) with hi + lo exact to ~2^-48 of the leaf width.  For each source leaf the target is moved into
 //    that leaf's frame in FP64 once and split again, so that per pair dx = (t_hi - s_hi) + (t_lo - s_lo):
 //    the first difference is exact for nearby particles (Sterbenz), which keeps the close pairs -- the ones
@@ -87,21 +88,60 @@ __global__ void p2p_fp64_kernel(int R, long long N, const long long *__restrict_
 }
 
 // ---- FP32 compensated ------------------------------------------------------------------------------
+//
+// Layout of the FP32 copies (one buffer, see p2p_fp32_layout):
+//   tgt_hi[R][N] float4 (x_hi, y_hi, z_hi, q) and tgt_lo[N] float4 (x_lo, y_lo, z_lo, 0): leaf-local position
+//     of every particle as a float pair, read by the lane that owns the particle as a target;
+//   src[R][npairs][4] float4: the same particles as sources, two per record and pre-negated so that packed
+//     FP32x2 instructions consume them directly: (-x0,-x1,-y0,-y1) (-z0,-z1,q0,q1) (-lx0,-lx1,-ly0,-ly1)
+//     (-lz0,-lz1,0,0).  Leaf L's records start at (leaf_start[L] + L) / 2; an odd leaf is padded with a
+//     zero-charge particle far away.
+constexpr double P2P32_PAD = 1.0e15;
+
+__host__ __device__ inline long long p2p_pairs_capacity(long long N) { return N + 2; }
 
 __global__ void pack_local32(long long N, int R, const long long *__restrict__ keys_leaf,
                              const long long *__restrict__ leaf_start, const double *__restrict__ x,
                              const double *__restrict__ y, const double *__restrict__ z, const double *__restrict__ q,
                              double cx0, double cy0, double cz0, double leaf_w, float4 *__restrict__ hi,
-                             float4 *__restrict__ lo) {
+                             float4 *__restrict__ lo, float4 *__restrict__ src) {
   const long long leaf = blockIdx.x;
   int ix, iy, iz;
   morton_decode3(keys_leaf[leaf], ix, iy, iz);
   const double c0 = cx0 + (ix + 0.5) * leaf_w, c1 = cy0 + (iy + 0.5) * leaf_w, c2 = cz0 + (iz + 0.5) * leaf_w;
-  for (long long i = leaf_start[leaf] + threadIdx.x; i < leaf_start[leaf + 1]; i += blockDim.x) {
+  const long long s0 = leaf_start[leaf], s1 = leaf_start[leaf + 1];
+  for (long long i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
     const double lx = x[i] - c0, ly = y[i] - c1, lz = z[i] - c2;
     const float hx = (float)lx, hy = (float)ly, hz = (float)lz;
     lo[i] = make_float4((float)(lx - (double)hx), (float)(ly - (double)hy), (float)(lz - (double)hz), 0.f);
     for (int r = 0; r < R; ++r) hi[(long long)r * N + i] = make_float4(hx, hy, hz, (float)q[(long long)r * N + i]);
+  }
+  const long long P = p2p_pairs_capacity(N);
+  const long long pofs = (s0 + leaf) >> 1;
+  const long long np = (s1 - s0 + 1) >> 1;
+  for (long long pp = threadIdx.x; pp < np; pp += blockDim.x) {
+    float h[2][3], l[2][3];
+    bool real[2];
+    for (int u = 0; u < 2; ++u) {
+      const long long j = s0 + 2 * pp + u;
+      real[u] = j < s1;
+      const double d[3] = {real[u] ? x[j] - c0 : P2P32_PAD, real[u] ? y[j] - c1 : P2P32_PAD,
+                           real[u] ? z[j] - c2 : P2P32_PAD};
+      for (int a = 0; a < 3; ++a) {
+        h[u][a] = (float)d[a];
+        l[u][a] = (float)(d[a] - (double)h[u][a]);
+      }
+    }
+    for (int r = 0; r < R; ++r) {
+      const long long j0 = s0 + 2 * pp;
+      const float q0 = (float)q[(long long)r * N + j0];
+      const float q1 = real[1] ? (float)q[(long long)r * N + j0 + 1] : 0.f;
+      float4 *rec = src + ((long long)r * P + pofs + pp) * 4;
+      rec[0] = make_float4(-h[0][0], -h[1][0], -h[0][1], -h[1][1]);
+      rec[1] = make_float4(-h[0][2], -h[1][2], q0, q1);
+      rec[2] = make_float4(-l[0][0], -l[1][0], -l[0][1], -l[1][1]);
+      rec[3] = make_float4(-l[0][2], -l[1][2], 0.f, 0.f);
+    }
   }
 }
 
@@ -114,7 +154,7 @@ __device__ __forceinline__ void two_sum(float &hi, float &lo, float v) {
 }
 
 constexpr int P2P32_WARPS = 4;        // target leaves per CTA (one warp each)
-constexpr int P2P32_STAGE = 128;      // source particles per bulk-copy stage
+constexpr int P2P32_STAGE = 64;       // source pair records (128 particles) per bulk-copy stage
 
 __device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -144,16 +184,16 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
                : "memory");
 }
 
-// One warp per target leaf.  The source ranges of the 27 neighbour slots are walked as a sequence of
-// stages of <= P2P32_STAGE particles, each copied by one bulk copy (16-byte float4 records, so address and
-// size are 16-byte multiples).  Two stage buffers per warp: the copy of stage k+1 overlaps the math of k.
+// One warp per target leaf, one target particle per lane, two source particles per packed FP32x2 step.
+// The sources of the <=27 neighbour slots are walked as stages of <= P2P32_STAGE pair records, each copied
+// by one bulk copy (64-byte records: 16-byte aligned addresses and sizes) into a double buffer, so the copy
+// of stage k+1 overlaps the math of stage k.
 __global__ void __launch_bounds__(P2P32_WARPS * 32) p2p_fp32_kernel(
     int R, long long N, long long nleaves, const long long *__restrict__ leaf_start, const int *__restrict__ nbr,
-    int variant, const float4 *__restrict__ pq, const float4 *__restrict__ plo, double leaf_w,
-    double *__restrict__ phi, double *__restrict__ fx, double *__restrict__ fy, double *__restrict__ fz,
-    int *__restrict__ status) {
-  __shared__ __align__(128) float4 buf[P2P32_WARPS][2][P2P32_STAGE];
-  __shared__ __align__(128) float4 blo[P2P32_WARPS][2][P2P32_STAGE];
+    int variant, const float4 *__restrict__ pq, const float4 *__restrict__ plo, const float4 *__restrict__ src,
+    double leaf_w, double *__restrict__ phi, double *__restrict__ fx, double *__restrict__ fy,
+    double *__restrict__ fz, int *__restrict__ status) {
+  __shared__ __align__(128) float4 buf[P2P32_WARPS][2][4 * P2P32_STAGE];
   __shared__ __align__(8) unsigned long long bar[P2P32_WARPS][2];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long leaf = (long long)blockIdx.x * P2P32_WARPS + w;
@@ -164,18 +204,23 @@ __global__ void __launch_bounds__(P2P32_WARPS * 32) p2p_fp32_kernel(
   }
   __syncwarp();
   if (leaf >= nleaves) return;
+  const long long P = p2p_pairs_capacity(N);
   const long long t0 = leaf_start[leaf], t1 = leaf_start[leaf + 1];
-  // the list of (slot, begin, end) stages
-  int slots[27];
+  int slots[27], sleaf[27];
   int ns = 0;
   for (int e = 0; e < 27; ++e) {
     if (variant == 1 && e == 13) continue;
     const int sl = nbr[leaf * 27 + e];
-    if (sl >= 0) slots[ns++] = e;
+    if (sl >= 0) {
+      slots[ns] = e;
+      sleaf[ns] = sl;
+      ++ns;
+    }
   }
   unsigned phase[2] = {0, 0};
   for (int r = 0; r < R; ++r) {
     const float4 *pr = pq + (long long)r * N;
+    const float4 *sr = src + (long long)r * P * 4;
     for (long long tb = t0; tb < t1; tb += 32) {
       const long long i = tb + lane;
       const bool active = i < t1;
@@ -183,98 +228,99 @@ __global__ void __launch_bounds__(P2P32_WARPS * 32) p2p_fp32_kernel(
       const float4 mel = active ? plo[i] : make_float4(0.f, 0.f, 0.f, 0.f);
       const double mx = (double)me.x + (double)mel.x, my = (double)me.y + (double)mel.y,
                    mz = (double)me.z + (double)mel.z;
+      const int self_local = (int)(i - t0);  // index of the target within its own leaf
       float ph_hi = 0.f, ph_lo = 0.f, gx_hi = 0.f, gx_lo = 0.f, gy_hi = 0.f, gy_lo = 0.f, gz_hi = 0.f, gz_lo = 0.f;
-      // stage iterator: (slot index e, begin b) -> next
-      int se = 0;
-      long long sb = ns > 0 ? leaf_start[nbr[leaf * 27 + slots[0]]] : 0;
-      auto stage_end = [&](int e) { return leaf_start[nbr[leaf * 27 + slots[e]] + 1]; };
-      // issue the first stage
-      int buf_id = 0;
-      long long cur_b = sb;
-      int cur_e = se;
-      int cur_n = 0;
+      // stage iterator over (slot e, first pair pb); pair counts per source leaf
+      auto pair_base = [&](int e) { return (leaf_start[sleaf[e]] + sleaf[e]) >> 1; };
+      auto pair_count = [&](int e) { return (leaf_start[sleaf[e] + 1] - leaf_start[sleaf[e]] + 1) >> 1; };
+      int buf_id = 0, cur_e = 0, cur_n = 0;
+      long long cur_p = 0;  // pair index within the source leaf
       if (ns > 0) {
-        const long long e1 = stage_end(0);
-        cur_n = (int)min((long long)P2P32_STAGE, e1 - sb);
+        cur_n = (int)min((long long)P2P32_STAGE, pair_count(0));
         if (lane == 0) {
-          mbar_expect_tx(&bar[w][0], cur_n * 32);
-          bulk_g2s(&buf[w][0][0], pr + sb, cur_n * 16, &bar[w][0]);
-          bulk_g2s(&blo[w][0][0], plo + sb, cur_n * 16, &bar[w][0]);
+          mbar_expect_tx(&bar[w][0], cur_n * 64);
+          bulk_g2s(&buf[w][0][0], sr + pair_base(0) * 4, cur_n * 64, &bar[w][0]);
         }
       }
       while (cur_n > 0) {
-        // next stage
-        long long nb = cur_b + cur_n;
         int ne = cur_e;
-        if (nb >= stage_end(ne)) {
+        long long np = cur_p + cur_n;
+        if (np >= pair_count(ne)) {
           ++ne;
-          if (ne < ns) nb = leaf_start[nbr[leaf * 27 + slots[ne]]];
+          np = 0;
         }
         int nxt_n = 0;
         if (ne < ns) {
-          nxt_n = (int)min((long long)P2P32_STAGE, stage_end(ne) - nb);
+          nxt_n = (int)min((long long)P2P32_STAGE, pair_count(ne) - np);
           if (lane == 0) {
-            mbar_expect_tx(&bar[w][buf_id ^ 1], nxt_n * 32);
-            bulk_g2s(&buf[w][buf_id ^ 1][0], pr + nb, nxt_n * 16, &bar[w][buf_id ^ 1]);
-            bulk_g2s(&blo[w][buf_id ^ 1][0], plo + nb, nxt_n * 16, &bar[w][buf_id ^ 1]);
+            mbar_expect_tx(&bar[w][buf_id ^ 1], nxt_n * 64);
+            bulk_g2s(&buf[w][buf_id ^ 1][0], sr + (pair_base(ne) + np) * 4, nxt_n * 64, &bar[w][buf_id ^ 1]);
           }
         }
-        // wait for the current stage
         if (!mbar_wait(&bar[w][buf_id], phase[buf_id])) {
           if (lane == 0) atomicExch(status, 1);
           return;
         }
         phase[buf_id] ^= 1;
         // the target moved into the source leaf's frame (FP64, exact multiples of the leaf width), split into
-        // a float pair
+        // a float pair and broadcast to both halves of the packed operands
         const int sl_pos = slots[cur_e];
         const double tdx = mx - (double)(sl_pos / 9 - 1) * leaf_w, tdy = my - (double)((sl_pos / 3) % 3 - 1) * leaf_w,
                      tdz = mz - (double)(sl_pos % 3 - 1) * leaf_w;
         const float thx = (float)tdx, thy = (float)tdy, thz = (float)tdz;
-        const float tlx = (float)(tdx - (double)thx), tly = (float)(tdy - (double)thy), tlz = (float)(tdz - (double)thz);
-        float pv = 0.f, ax = 0.f, ay = 0.f, az = 0.f;
+        const float2 th_x = make_float2(thx, thx), th_y = make_float2(thy, thy), th_z = make_float2(thz, thz);
+        const float tlx = (float)(tdx - (double)thx), tly = (float)(tdy - (double)thy),
+                    tlz = (float)(tdz - (double)thz);
+        const float2 tl_x = make_float2(tlx, tlx), tl_y = make_float2(tly, tly), tl_z = make_float2(tlz, tlz);
+        float2 pv = make_float2(0.f, 0.f), ax = pv, ay = pv, az = pv;
         const float4 *s = buf[w][buf_id];
-        const float4 *sl = blo[w][buf_id];
         if (sl_pos == 13) {
-          const int self = (int)(i - cur_b);
-#pragma unroll 4
+          const int self_pair = self_local - 2 * (int)cur_p;  // source index of the target within this stage
+#pragma unroll 2
           for (int k = 0; k < cur_n; ++k) {
-            const float4 v = s[k];
-            const float4 u = sl[k];
-            const float dx = (thx - v.x) + (tlx - u.x), dy = (thy - v.y) + (tly - u.y), dz = (thz - v.z) + (tlz - u.z);
-            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            const float inv = (k == self) ? 0.f : rsqrtf(r2);
-            const float qi = v.w * inv;
-            const float qi3 = qi * inv * inv;
-            pv += qi;
-            ax = fmaf(dx, qi3, ax);
-            ay = fmaf(dy, qi3, ay);
-            az = fmaf(dz, qi3, az);
+            const float4 A = s[4 * k], B = s[4 * k + 1], C = s[4 * k + 2], D = s[4 * k + 3];
+            const float2 dx = __fadd2_rn(__fadd2_rn(th_x, make_float2(A.x, A.y)), __fadd2_rn(tl_x, make_float2(C.x, C.y)));
+            const float2 dy = __fadd2_rn(__fadd2_rn(th_y, make_float2(A.z, A.w)), __fadd2_rn(tl_y, make_float2(C.z, C.w)));
+            const float2 dz = __fadd2_rn(__fadd2_rn(th_z, make_float2(B.x, B.y)), __fadd2_rn(tl_z, make_float2(D.x, D.y)));
+            float2 r2 = __fmul2_rn(dx, dx);
+            r2 = __ffma2_rn(dy, dy, r2);
+            r2 = __ffma2_rn(dz, dz, r2);
+            const float2 inv = make_float2(2 * k == self_pair ? 0.f : rsqrtf(r2.x),
+                                           2 * k + 1 == self_pair ? 0.f : rsqrtf(r2.y));
+            const float2 qi = __fmul2_rn(make_float2(B.z, B.w), inv);
+            const float2 qi3 = __fmul2_rn(qi, __fmul2_rn(inv, inv));
+            pv = __fadd2_rn(pv, qi);
+            ax = __ffma2_rn(dx, qi3, ax);
+            ay = __ffma2_rn(dy, qi3, ay);
+            az = __ffma2_rn(dz, qi3, az);
           }
         } else {
-#pragma unroll 8
+#pragma unroll 4
           for (int k = 0; k < cur_n; ++k) {
-            const float4 v = s[k];
-            const float4 u = sl[k];
-            const float dx = (thx - v.x) + (tlx - u.x), dy = (thy - v.y) + (tly - u.y), dz = (thz - v.z) + (tlz - u.z);
-            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            const float inv = rsqrtf(r2);
-            const float qi = v.w * inv;
-            const float qi3 = qi * inv * inv;
-            pv += qi;
-            ax = fmaf(dx, qi3, ax);
-            ay = fmaf(dy, qi3, ay);
-            az = fmaf(dz, qi3, az);
+            const float4 A = s[4 * k], B = s[4 * k + 1], C = s[4 * k + 2], D = s[4 * k + 3];
+            const float2 dx = __fadd2_rn(__fadd2_rn(th_x, make_float2(A.x, A.y)), __fadd2_rn(tl_x, make_float2(C.x, C.y)));
+            const float2 dy = __fadd2_rn(__fadd2_rn(th_y, make_float2(A.z, A.w)), __fadd2_rn(tl_y, make_float2(C.z, C.w)));
+            const float2 dz = __fadd2_rn(__fadd2_rn(th_z, make_float2(B.x, B.y)), __fadd2_rn(tl_z, make_float2(D.x, D.y)));
+            float2 r2 = __fmul2_rn(dx, dx);
+            r2 = __ffma2_rn(dy, dy, r2);
+            r2 = __ffma2_rn(dz, dz, r2);
+            const float2 inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+            const float2 qi = __fmul2_rn(make_float2(B.z, B.w), inv);
+            const float2 qi3 = __fmul2_rn(qi, __fmul2_rn(inv, inv));
+            pv = __fadd2_rn(pv, qi);
+            ax = __ffma2_rn(dx, qi3, ax);
+            ay = __ffma2_rn(dy, qi3, ay);
+            az = __ffma2_rn(dz, qi3, az);
           }
         }
-        two_sum(ph_hi, ph_lo, pv);
-        two_sum(gx_hi, gx_lo, ax);
-        two_sum(gy_hi, gy_lo, ay);
-        two_sum(gz_hi, gz_lo, az);
+        two_sum(ph_hi, ph_lo, pv.x + pv.y);
+        two_sum(gx_hi, gx_lo, ax.x + ax.y);
+        two_sum(gy_hi, gy_lo, ay.x + ay.y);
+        two_sum(gz_hi, gz_lo, az.x + az.y);
         __syncwarp();  // every lane is done with this buffer before it is refilled
         buf_id ^= 1;
-        cur_b = nb;
         cur_e = ne;
+        cur_p = np;
         cur_n = nxt_n;
       }
       if (active) {
@@ -296,21 +342,20 @@ b200fmm_status run_p2p(Context &c, int variant) {
   const Level &L = c.lv[LL];
   if (L.n == 0) return B200FMM_OK;
   if (c.cfg.precision == B200FMM_MIXED) {
+    float4 *hi = c.d_pq32, *lo = c.d_pq32 + c.N * c.R, *src = c.d_pq32 + c.N * (c.R + 1);
     if (!c.packed32) {
       c.packed32 = true;
       const double W = c.cfg.box_width;
       pack_local32<<<(unsigned)L.n, 64, 0, c.stream>>>(c.N, c.R, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q,
                                                        c.cfg.center[0] - W / 2, c.cfg.center[1] - W / 2,
-                                                       c.cfg.center[2] - W / 2, W / (double)(1 << LL), c.d_pq32,
-                                                       c.d_pq32 + c.N * c.R);
+                                                       c.cfg.center[2] - W / 2, W / (double)(1 << LL), hi, lo, src);
       ++c.launches;
     }
     int *status = c.d_status;
     const unsigned blocks = grid_for(L.n, P2P32_WARPS);
     B200_CUDA(cudaEventRecord(c.ev[10], c.stream));
     p2p_fp32_kernel<<<blocks, P2P32_WARPS * 32, 0, c.stream>>>(c.R, c.N, L.n, c.d_leaf_start, c.d_leaf_nbr, variant,
-                                                               c.d_pq32, c.d_pq32 + c.N * c.R,
-                                                               c.cfg.box_width / (double)(1 << LL), c.d_phi,
+                                                               hi, lo, src, c.cfg.box_width / (double)(1 << LL), c.d_phi,
                                                                c.d_fx, c.d_fy, c.d_fz, status);
     B200_CUDA(cudaEventRecord(c.ev[11], c.stream));
     ++c.launches;
@@ -329,10 +374,11 @@ b200fmm_status run_p2p(Context &c, int variant) {
 }  // namespace b200
 
 // ---- allocation-free entry point -------------------------------------------------------------------
-// Scratch of b200fmm_p2p_noalloc: the hi and lo FP32 leaf-local particle copies (2 x 2^18 float4 = 8 MiB)
-// and the status word of the kernel's bounded waits.  In host code these names are host-side stand-ins,
-// not device addresses: the host passes the addresses looked up with cudaGetSymbolAddress.
-static __device__ __align__(256) float4 g_noalloc_stage[2 * B200FMM_NOALLOC_MAX_PARTICLES];
+// Scratch of b200fmm_p2p_noalloc: the FP32 leaf-local copies of the particles -- targets (hi, lo) and
+// pair-packed sources, 6 float4 per particle plus 8 (24 MiB at 2^18 particles) -- and the status word of the
+// kernel's bounded waits.  In host code these names are host-side stand-ins, not device addresses: the host
+// passes the addresses looked up with cudaGetSymbolAddress.
+static __device__ __align__(256) float4 g_noalloc_stage[6 * B200FMM_NOALLOC_MAX_PARTICLES + 8];
 static __device__ __align__(256) int g_noalloc_status[4];
 
 namespace b200 {
@@ -385,9 +431,9 @@ extern "C" b200fmm_status b200fmm_p2p_noalloc(long long n, const double *x, cons
   B200_CUDA(cudaMemsetAsync(status, 0, sizeof(int) * 4, s));
   pack_local32<<<(unsigned)nleaves, 64, 0, s>>>(n, 1, leaf_keys, leaf_start, x, y, z, q, center[0] - box_width / 2,
                                                center[1] - box_width / 2, center[2] - box_width / 2, leaf_w, stage,
-                                               stage + n);
+                                               stage + n, stage + 2 * n);
   p2p_fp32_kernel<<<grid_for(nleaves, P2P32_WARPS), P2P32_WARPS * 32, 0, s>>>(
-      1, n, nleaves, leaf_start, leaf_nbr, variant, stage, stage + n, leaf_w, phi, fx, fy, fz, status);
+      1, n, nleaves, leaf_start, leaf_nbr, variant, stage, stage + n, stage + 2 * n, leaf_w, phi, fx, fy, fz, status);
   B200_CUDA(cudaGetLastError());
   int st = 0;
   B200_CUDA(cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -456,7 +456,7 @@ b200fmm_status upload_sym_operators(Context &c) {
     for (int n = 0; n < nn; ++n)
       for (int a = 0; a < r; ++a) {
         Ut[toff[t] + (size_t)n * r + a] = Uc[(size_t)a * nn + pv[n]];
-        Vt[toff[t] + (size_t)a * nn + n] = Vc[(size_t)a * nn + pv[n]];
+        Vt[toff[t] + (size_t)n * r + a] = Vc[(size_t)a * nn + pv[n]];
       }
   }
   B200_CUDA(cudaMalloc(&c.d_Ut, sizeof(double) * std::max<long long>(tot, 1)));

@@ -473,8 +473,9 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
     B200_CHECK(grow(c, *p, cr, (size_t)n * c.R));
   }
   {
-    size_t cp = c.cap_N * (c.R + 1);
-    B200_CHECK(grow(c, c.d_pq32, cp, (size_t)n * (c.R + 1)));
+    // FP32 P2P copies: target hi [R][N], target lo [N], pair-packed sources [R][N+2][4]
+    size_t cp = c.cap_N * (c.R + 1) + 4 * c.R * (c.cap_N + 2);
+    B200_CHECK(grow(c, c.d_pq32, cp, (size_t)n * (c.R + 1) + 4 * (size_t)c.R * (n + 2)));
   }
   c.cap_N = std::max(c.cap_N, (size_t)n);
   {
