@@ -32,20 +32,21 @@ struct SymArgs {
   int max_rank;
 };
 
-template <int P>
-__host__ __device__ constexpr int sym_targets() { return P >= 8 ? 16 : 32; }
+constexpr int SYM_T = 16;  // targets per CTA (children of one type of SYM_T consecutive parents)
 
-// One CTA: the T targets of child type blockIdx.y among T consecutive parents.  For each of the 189 transfer
-// vectors of that child type: gather the source multipoles, Y = V_t^T M (rank r), then L += U_t Y, with the
-// targets' local sums kept in shared memory across all transfer vectors (each owned by one thread).  Both
-// phases give every thread independent FMA chains (two targets x two partial sums).
+// One CTA: the SYM_T targets of child type blockIdx.y among SYM_T consecutive parents.  For each of the 189
+// transfer vectors of that child type: gather the source multipoles, stage V_t in shared memory (coalesced)
+// and form Y = V_t^T M (rank r); stage U_t in the same buffer and add U_t Y to the targets' local sums, which
+// stay in registers across all transfer vectors.
 template <int P>
 __global__ void __launch_bounds__(SYM_THREADS) m2l_sym_kernel(SymArgs a) {
-  constexpr int nn = P * P * P, T = sym_targets<P>();
+  constexpr int nn = P * P * P, T = SYM_T;
+  constexpr int nout = T * nn;
+  constexpr int NACC = (nout + SYM_THREADS - 1) / SYM_THREADS;
   extern __shared__ double sh[];
   double *Ms = sh;                        // [T][nn] gathered source multipoles
-  double *Lacc = Ms + T * nn;             // [T][nn] local sums
-  double *Y = Lacc + T * nn;              // [T][max_rank]
+  double *Y = Ms + T * nn;                // [T][max_rank]
+  double *Op = Y + T * a.max_rank;        // [nn][r] V_t, then U_t
   __shared__ int tgt[T], src[T];
   __shared__ int any;
   const int ct = blockIdx.y;
@@ -54,8 +55,9 @@ __global__ void __launch_bounds__(SYM_THREADS) m2l_sym_kernel(SymArgs a) {
     const long long p = p0 + threadIdx.x;
     tgt[threadIdx.x] = p < a.nparents ? a.child[p * 8 + ct] : -1;
   }
-  constexpr int nout = T * nn;
-  for (int o = threadIdx.x; o < nout; o += blockDim.x) Lacc[o] = 0.0;
+  double acc[NACC];
+#pragma unroll
+  for (int j = 0; j < NACC; ++j) acc[j] = 0.0;
   for (int e = 0; e < 189; ++e) {
     __syncthreads();
     if (threadIdx.x == 0) any = 0;
@@ -77,48 +79,50 @@ __global__ void __launch_bounds__(SYM_THREADS) m2l_sym_kernel(SymArgs a) {
       const int sc = src[k];
       Ms[idx] = sc >= 0 ? a.M[((long long)sc * a.R + a.rhs) * nn + m] : 0.0;
     }
+    for (int idx = threadIdx.x; idx < nn * r; idx += blockDim.x) Op[idx] = Vt[idx];
     __syncthreads();
-    // Y[k][q] and Y[k + T/2][q]: thread = (k < T/2, q)
-    for (int idx = threadIdx.x; idx < (T / 2) * r; idx += blockDim.x) {
-      const int k = idx % (T / 2), q = idx / (T / 2);
-      const double *m0 = Ms + k * nn, *m1 = Ms + (k + T / 2) * nn;
-      double s00 = 0.0, s01 = 0.0, s10 = 0.0, s11 = 0.0;
+    for (int idx = threadIdx.x; idx < T * r; idx += blockDim.x) {
+      const int k = idx / r, q = idx - k * r;
+      const double *mk = Ms + k * nn;
+      double s0 = 0.0, s1 = 0.0;
       int m = 0;
       for (; m + 1 < nn; m += 2) {
-        const double v0 = Vt[(long long)m * r + q], v1 = Vt[(long long)(m + 1) * r + q];
-        s00 += v0 * m0[m];
-        s01 += v1 * m0[m + 1];
-        s10 += v0 * m1[m];
-        s11 += v1 * m1[m + 1];
+        s0 += Op[m * r + q] * mk[m];
+        s1 += Op[(m + 1) * r + q] * mk[m + 1];
       }
-      if (m < nn) {
-        const double v0 = Vt[(long long)m * r + q];
-        s00 += v0 * m0[m];
-        s10 += v0 * m1[m];
-      }
-      Y[k * a.max_rank + q] = s00 + s01;
-      Y[(k + T / 2) * a.max_rank + q] = s10 + s11;
+      if (m < nn) s0 += Op[m * r + q] * mk[m];
+      Y[k * a.max_rank + q] = s0 + s1;
     }
     __syncthreads();
-    for (int o = threadIdx.x; o < nout; o += blockDim.x) {
-      const int k = o / nn, n = o - k * nn;
-      if (src[k] < 0) continue;
-      const double *u = Ut + (long long)n * r;
-      const double *y = Y + k * a.max_rank;
-      double s0 = 0.0, s1 = 0.0;
-      int q = 0;
-      for (; q + 1 < r; q += 2) {
-        s0 += u[q] * y[q];
-        s1 += u[q + 1] * y[q + 1];
+    for (int idx = threadIdx.x; idx < nn * r; idx += blockDim.x) Op[idx] = Ut[idx];
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < NACC; ++j) {
+      const int o = threadIdx.x + j * SYM_THREADS;
+      if (o < nout) {
+        const int k = o / nn, n = o - k * nn;
+        if (src[k] >= 0) {
+          const double *u = Op + n * r;
+          const double *y = Y + k * a.max_rank;
+          double s0 = 0.0, s1 = 0.0;
+          int q = 0;
+          for (; q + 1 < r; q += 2) {
+            s0 += u[q] * y[q];
+            s1 += u[q + 1] * y[q + 1];
+          }
+          if (q < r) s0 += u[q] * y[q];
+          acc[j] += s0 + s1;
+        }
       }
-      if (q < r) s0 += u[q] * y[q];
-      Lacc[o] += s0 + s1;
     }
   }
-  __syncthreads();
-  for (int o = threadIdx.x; o < nout; o += blockDim.x) {
-    const int k = o / nn, n = o - k * nn;
-    if (tgt[k] >= 0) a.L[((long long)tgt[k] * a.R + a.rhs) * nn + n] += a.scale * Lacc[o];
+#pragma unroll
+  for (int j = 0; j < NACC; ++j) {
+    const int o = threadIdx.x + j * SYM_THREADS;
+    if (o < nout) {
+      const int k = o / nn, n = o - k * nn;
+      if (tgt[k] >= 0) a.L[((long long)tgt[k] * a.R + a.rhs) * nn + n] += a.scale * acc[j];
+    }
   }
 }
 
@@ -176,8 +180,9 @@ b200fmm_status run_m2l_fp64(Context &c, int level) {
     a.M = T.M;
     a.L = T.L;
     a.max_rank = c.max_rank;
-    const int T = c.p >= 8 ? 16 : 32;
-    const size_t sh = sizeof(double) * (2 * (size_t)T * c.nn + (size_t)T * c.max_rank);
+    const int T = SYM_T;
+    const size_t sh = sizeof(double) * ((size_t)T * c.nn + (size_t)T * c.max_rank + (size_t)c.nn * c.max_rank);
+    if (sh > 227 * 1024) return fail(B200FMM_ERR_UNSUPPORTED, "compressed operators too large for the FP64 M2L kernel");
     const dim3 grid((unsigned)((a.nparents + T - 1) / T), 8);
     for (int r = 0; r < c.R; ++r) {
       a.rhs = r;

@@ -154,7 +154,7 @@ __device__ __forceinline__ void two_sum(float &hi, float &lo, float v) {
 }
 
 constexpr int P2P32_WARPS = 4;        // target leaves per CTA (one warp each)
-constexpr int P2P32_STAGE = 64;       // source pair records (128 particles) per bulk-copy stage
+constexpr int P2P32_STAGE = 48;       // source pair records (96 particles) per bulk-copy stage
 
 __device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -186,38 +186,54 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
 
 // One warp per target leaf, one target particle per lane, two source particles per packed FP32x2 step.
 // The sources of the <=27 neighbour slots are walked as stages of <= P2P32_STAGE pair records, each copied
-// by one bulk copy (64-byte records: 16-byte aligned addresses and sizes) into a double buffer, so the copy
-// of stage k+1 overlaps the math of stage k.
-__global__ void __launch_bounds__(P2P32_WARPS * 32) p2p_fp32_kernel(
+// by one bulk copy (64-byte records: 16-byte aligned addresses and sizes) into a ring of P2P32_NBUF buffers,
+// issued P2P32_NBUF - 1 stages ahead of the math.
+constexpr int P2P32_NBUF = 3;
+
+__device__ __forceinline__ void fast_two_sum_exact(float a, float b, float &s, float &e) {
+  s = a + b;
+  const float bp = s - a;
+  e = (a - (s - bp)) + (b - bp);
+}
+
+__global__ void __launch_bounds__(P2P32_WARPS * 32, 6) p2p_fp32_kernel(
     int R, long long N, long long nleaves, const long long *__restrict__ leaf_start, const int *__restrict__ nbr,
     int variant, const float4 *__restrict__ pq, const float4 *__restrict__ plo, const float4 *__restrict__ src,
     double leaf_w, double *__restrict__ phi, double *__restrict__ fx, double *__restrict__ fy,
     double *__restrict__ fz, int *__restrict__ status) {
-  __shared__ __align__(128) float4 buf[P2P32_WARPS][2][4 * P2P32_STAGE];
-  __shared__ __align__(8) unsigned long long bar[P2P32_WARPS][2];
+  __shared__ __align__(128) float4 buf[P2P32_WARPS][P2P32_NBUF][4 * P2P32_STAGE];
+  __shared__ __align__(8) unsigned long long bar[P2P32_WARPS][P2P32_NBUF];
+  __shared__ long long sbase[P2P32_WARPS][27];
+  __shared__ int scount[P2P32_WARPS][27];
+  __shared__ signed char spos[P2P32_WARPS][27];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long leaf = (long long)blockIdx.x * P2P32_WARPS + w;
   if (lane == 0) {
-    mbar_init(&bar[w][0], 1);
-    mbar_init(&bar[w][1], 1);
+    for (int b = 0; b < P2P32_NBUF; ++b) mbar_init(&bar[w][b], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncwarp();
   if (leaf >= nleaves) return;
   const long long P = p2p_pairs_capacity(N);
   const long long t0 = leaf_start[leaf], t1 = leaf_start[leaf + 1];
-  int slots[27], sleaf[27];
+  // the source slots of this leaf: pair-record base, pair count and neighbour position
   int ns = 0;
-  for (int e = 0; e < 27; ++e) {
-    if (variant == 1 && e == 13) continue;
-    const int sl = nbr[leaf * 27 + e];
+  {
+    const int e = lane < 27 ? lane : 0;
+    const int sl = (lane < 27 && !(variant == 1 && e == 13)) ? nbr[leaf * 27 + e] : -1;
+    const unsigned mask = __ballot_sync(0xffffffffu, sl >= 0);
     if (sl >= 0) {
-      slots[ns] = e;
-      sleaf[ns] = sl;
-      ++ns;
+      const int k = __popc(mask & ((1u << lane) - 1u));
+      const long long a0 = leaf_start[sl], a1 = leaf_start[sl + 1];
+      sbase[w][k] = (a0 + sl) >> 1;
+      scount[w][k] = (int)((a1 - a0 + 1) >> 1);
+      spos[w][k] = (signed char)e;
     }
+    ns = __popc(mask);
+    __syncwarp();
   }
-  unsigned phase[2] = {0, 0};
+  const float lw = (float)leaf_w;
+  unsigned phase_bits = 0;  // one parity bit per buffer
   for (int r = 0; r < R; ++r) {
     const float4 *pr = pq + (long long)r * N;
     const float4 *sr = src + (long long)r * P * 4;
@@ -226,58 +242,65 @@ __global__ void __launch_bounds__(P2P32_WARPS * 32) p2p_fp32_kernel(
       const bool active = i < t1;
       const float4 me = active ? pr[i] : make_float4(0.f, 0.f, 0.f, 0.f);
       const float4 mel = active ? plo[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-      const double mx = (double)me.x + (double)mel.x, my = (double)me.y + (double)mel.y,
-                   mz = (double)me.z + (double)mel.z;
       const int self_local = (int)(i - t0);  // index of the target within its own leaf
       float ph_hi = 0.f, ph_lo = 0.f, gx_hi = 0.f, gx_lo = 0.f, gy_hi = 0.f, gy_lo = 0.f, gz_hi = 0.f, gz_lo = 0.f;
-      // stage iterator over (slot e, first pair pb); pair counts per source leaf
-      auto pair_base = [&](int e) { return (leaf_start[sleaf[e]] + sleaf[e]) >> 1; };
-      auto pair_count = [&](int e) { return (leaf_start[sleaf[e] + 1] - leaf_start[sleaf[e]] + 1) >> 1; };
-      int buf_id = 0, cur_e = 0, cur_n = 0;
-      long long cur_p = 0;  // pair index within the source leaf
-      if (ns > 0) {
-        cur_n = (int)min((long long)P2P32_STAGE, pair_count(0));
+      // stage sequence: (slot e, first pair p, pair count n); issue up to NBUF-1 stages ahead
+      int ie = 0, ip = 0;       // next stage to issue
+      int ce = 0, cp = 0;       // stage being computed
+      int issued = 0, done = 0;
+      auto next_stage = [&](int &e, int &p0, int &n) -> bool {
+        while (e < ns && p0 >= scount[w][e]) {
+          ++e;
+          p0 = 0;
+        }
+        if (e >= ns) return false;
+        n = min(P2P32_STAGE, scount[w][e] - p0);
+        return true;
+      };
+      auto issue = [&]() {
+        int n;
+        if (!next_stage(ie, ip, n)) return false;
+        const int b = issued % P2P32_NBUF;
         if (lane == 0) {
-          mbar_expect_tx(&bar[w][0], cur_n * 64);
-          bulk_g2s(&buf[w][0][0], sr + pair_base(0) * 4, cur_n * 64, &bar[w][0]);
+          mbar_expect_tx(&bar[w][b], n * 64);
+          bulk_g2s(&buf[w][b][0], sr + (sbase[w][ie] + ip) * 4, n * 64, &bar[w][b]);
         }
-      }
-      while (cur_n > 0) {
-        int ne = cur_e;
-        long long np = cur_p + cur_n;
-        if (np >= pair_count(ne)) {
-          ++ne;
-          np = 0;
-        }
-        int nxt_n = 0;
-        if (ne < ns) {
-          nxt_n = (int)min((long long)P2P32_STAGE, pair_count(ne) - np);
-          if (lane == 0) {
-            mbar_expect_tx(&bar[w][buf_id ^ 1], nxt_n * 64);
-            bulk_g2s(&buf[w][buf_id ^ 1][0], sr + (pair_base(ne) + np) * 4, nxt_n * 64, &bar[w][buf_id ^ 1]);
-          }
-        }
-        if (!mbar_wait(&bar[w][buf_id], phase[buf_id])) {
+        ip += n;
+        ++issued;
+        return true;
+      };
+      for (int k = 0; k < P2P32_NBUF - 1; ++k)
+        if (!issue()) break;
+      while (done < issued) {
+        int cn;
+        next_stage(ce, cp, cn);
+        const int b = done % P2P32_NBUF;
+        if (!mbar_wait(&bar[w][b], (phase_bits >> b) & 1u)) {
           if (lane == 0) atomicExch(status, 1);
           return;
         }
-        phase[buf_id] ^= 1;
-        // the target moved into the source leaf's frame (FP64, exact multiples of the leaf width), split into
-        // a float pair and broadcast to both halves of the packed operands
-        const int sl_pos = slots[cur_e];
-        const double tdx = mx - (double)(sl_pos / 9 - 1) * leaf_w, tdy = my - (double)((sl_pos / 3) % 3 - 1) * leaf_w,
-                     tdz = mz - (double)(sl_pos % 3 - 1) * leaf_w;
-        const float thx = (float)tdx, thy = (float)tdy, thz = (float)tdz;
+        phase_bits ^= 1u << b;
+        // the target moved into the source leaf's frame: (hi - off) by an exact two-sum, the rounding error
+        // folded into lo (off is a small multiple of the leaf width)
+        const int sl_pos = spos[w][ce];
+        float thx, thy, thz, tlx, tly, tlz;
+        {
+          float e0;
+          fast_two_sum_exact(me.x, -(float)(sl_pos / 9 - 1) * lw, thx, e0);
+          tlx = mel.x + e0;
+          fast_two_sum_exact(me.y, -(float)((sl_pos / 3) % 3 - 1) * lw, thy, e0);
+          tly = mel.y + e0;
+          fast_two_sum_exact(me.z, -(float)(sl_pos % 3 - 1) * lw, thz, e0);
+          tlz = mel.z + e0;
+        }
         const float2 th_x = make_float2(thx, thx), th_y = make_float2(thy, thy), th_z = make_float2(thz, thz);
-        const float tlx = (float)(tdx - (double)thx), tly = (float)(tdy - (double)thy),
-                    tlz = (float)(tdz - (double)thz);
         const float2 tl_x = make_float2(tlx, tlx), tl_y = make_float2(tly, tly), tl_z = make_float2(tlz, tlz);
         float2 pv = make_float2(0.f, 0.f), ax = pv, ay = pv, az = pv;
-        const float4 *s = buf[w][buf_id];
+        const float4 *s = buf[w][b];
         if (sl_pos == 13) {
-          const int self_pair = self_local - 2 * (int)cur_p;  // source index of the target within this stage
+          const int self_pair = self_local - 2 * cp;  // source index of the target within this stage
 #pragma unroll 2
-          for (int k = 0; k < cur_n; ++k) {
+          for (int k = 0; k < cn; ++k) {
             const float4 A = s[4 * k], B = s[4 * k + 1], C = s[4 * k + 2], D = s[4 * k + 3];
             const float2 dx = __fadd2_rn(__fadd2_rn(th_x, make_float2(A.x, A.y)), __fadd2_rn(tl_x, make_float2(C.x, C.y)));
             const float2 dy = __fadd2_rn(__fadd2_rn(th_y, make_float2(A.z, A.w)), __fadd2_rn(tl_y, make_float2(C.z, C.w)));
@@ -296,7 +319,7 @@ __global__ void __launch_bounds__(P2P32_WARPS * 32) p2p_fp32_kernel(
           }
         } else {
 #pragma unroll 4
-          for (int k = 0; k < cur_n; ++k) {
+          for (int k = 0; k < cn; ++k) {
             const float4 A = s[4 * k], B = s[4 * k + 1], C = s[4 * k + 2], D = s[4 * k + 3];
             const float2 dx = __fadd2_rn(__fadd2_rn(th_x, make_float2(A.x, A.y)), __fadd2_rn(tl_x, make_float2(C.x, C.y)));
             const float2 dy = __fadd2_rn(__fadd2_rn(th_y, make_float2(A.z, A.w)), __fadd2_rn(tl_y, make_float2(C.z, C.w)));
@@ -317,11 +340,10 @@ __global__ void __launch_bounds__(P2P32_WARPS * 32) p2p_fp32_kernel(
         two_sum(gx_hi, gx_lo, ax.x + ax.y);
         two_sum(gy_hi, gy_lo, ay.x + ay.y);
         two_sum(gz_hi, gz_lo, az.x + az.y);
-        __syncwarp();  // every lane is done with this buffer before it is refilled
-        buf_id ^= 1;
-        cur_e = ne;
-        cur_p = np;
-        cur_n = nxt_n;
+        cp += cn;
+        ++done;
+        __syncwarp();  // every lane is done with buffer b before it is refilled
+        issue();
       }
       if (active) {
         const long long j = (long long)r * N + i;
