@@ -34,6 +34,50 @@ struct SymArgs {
 
 constexpr int SYM_T = 16;  // targets per CTA (children of one type of SYM_T consecutive parents)
 
+// Copies into shared memory with every load of a thread issued before its stores, so that the loads of one
+// staging step are in flight together instead of one L2 round trip after another.
+constexpr int STAGE_UNROLL = 16;
+
+__device__ __forceinline__ void stage_block(double *dst, const double *__restrict__ src, int count) {
+  for (int base = 0; base < count; base += STAGE_UNROLL * SYM_THREADS) {
+    double v[STAGE_UNROLL];
+#pragma unroll
+    for (int u = 0; u < STAGE_UNROLL; ++u) {
+      const int idx = base + u * SYM_THREADS + threadIdx.x;
+      v[u] = idx < count ? __ldg(src + idx) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < STAGE_UNROLL; ++u) {
+      const int idx = base + u * SYM_THREADS + threadIdx.x;
+      if (idx < count) dst[idx] = v[u];
+    }
+  }
+}
+
+// Ms[k][m] = M[src[k]][rhs][m] (0 for a missing source)
+template <int nn, int T>
+__device__ __forceinline__ void stage_rows(double *Ms, const double *__restrict__ M, const int *src, int R, int rhs) {
+  constexpr int count = T * nn;
+  for (int base = 0; base < count; base += STAGE_UNROLL * SYM_THREADS) {
+    double v[STAGE_UNROLL];
+#pragma unroll
+    for (int u = 0; u < STAGE_UNROLL; ++u) {
+      const int idx = base + u * SYM_THREADS + threadIdx.x;
+      v[u] = 0.0;
+      if (idx < count) {
+        const int k = idx / nn, m = idx - k * nn;
+        const int sc = src[k];
+        if (sc >= 0) v[u] = __ldg(M + ((long long)sc * R + rhs) * nn + m);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < STAGE_UNROLL; ++u) {
+      const int idx = base + u * SYM_THREADS + threadIdx.x;
+      if (idx < count) Ms[idx] = v[u];
+    }
+  }
+}
+
 // One CTA: the SYM_T targets of child type blockIdx.y among SYM_T consecutive parents.  For each of the 189
 // transfer vectors of that child type: gather the source multipoles, stage V_t in shared memory (coalesced)
 // and form Y = V_t^T M (rank r); stage U_t in the same buffer and add U_t Y to the targets' local sums, which
@@ -74,12 +118,8 @@ __global__ void __launch_bounds__(SYM_THREADS) m2l_sym_kernel(SymArgs a) {
     const int r = a.trank[t];
     const double *Ut = a.Ut + a.toff[t];
     const double *Vt = a.Vt + a.toff[t];
-    for (int idx = threadIdx.x; idx < nout; idx += blockDim.x) {
-      const int k = idx / nn, m = idx - k * nn;
-      const int sc = src[k];
-      Ms[idx] = sc >= 0 ? a.M[((long long)sc * a.R + a.rhs) * nn + m] : 0.0;
-    }
-    for (int idx = threadIdx.x; idx < nn * r; idx += blockDim.x) Op[idx] = Vt[idx];
+    stage_rows<nn, T>(Ms, a.M, src, a.R, a.rhs);
+    stage_block(Op, Vt, nn * r);
     __syncthreads();
     for (int idx = threadIdx.x; idx < T * r; idx += blockDim.x) {
       const int k = idx / r, q = idx - k * r;
@@ -94,7 +134,7 @@ __global__ void __launch_bounds__(SYM_THREADS) m2l_sym_kernel(SymArgs a) {
       Y[k * a.max_rank + q] = s0 + s1;
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < nn * r; idx += blockDim.x) Op[idx] = Ut[idx];
+    stage_block(Op, Ut, nn * r);
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < NACC; ++j) {
