@@ -69,6 +69,7 @@ struct __align__(64) TcParams {
   int item0, nitems;  // items [item0, item0 + nitems) of the list run in this launch
   int R, nn, KP, NP, NH, NHALF, NK, stages, ncols;
   int nseg;  // accumulator resets per transfer vector (the K chunks are split into nseg segments)
+  int nbuf;  // TMEM accumulators: 2 (alternating per segment) when 2 * NP columns fit, else 1
   int stage_bytes;
   signed char off[8][189][3];
   short slot[8][189];
@@ -134,21 +135,6 @@ __device__ __forceinline__ void mma_commit(unsigned long long *bar) {
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ void tmem_ld32(unsigned taddr, float *v) {
-  unsigned r[32];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
-        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
-        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
-}
-
 __device__ __forceinline__ void tmem_ld16(unsigned taddr, unsigned *r) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
@@ -158,16 +144,39 @@ __device__ __forceinline__ void tmem_ld16(unsigned taddr, unsigned *r) {
       : "r"(taddr));
 }
 
+// add N accumulator columns starting at TMEM address taddr (a multiple of 16 columns) into acc[0..N)
+template <int N>
+__device__ __forceinline__ void drain_cols(unsigned taddr, float *acc) {
+  static_assert(N % 16 == 0, "drained in groups of 16 columns");
+#pragma unroll
+  for (int c0 = 0; c0 < N; c0 += 16) {
+    unsigned r[16];
+    tmem_ld16(taddr + c0, r);
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) acc[c0 + i] += __uint_as_float(r[i]);
+  }
+}
+
 // ---- the kernel -------------------------------------------------------------------------------------
-// CW: accumulator columns owned by one epilogue thread (NP / 2), a compile-time constant so that the
-// running sums stay in registers.
-template <int CW>
+// CW: accumulator columns owned by one epilogue thread (NP / 2) and NHALF: MMA column halves, compile-time
+// constants so that the running sums stay in registers.  With one half a thread owns the columns
+// [ch*CW, (ch+1)*CW).  With two halves of NH = CW columns each, split at SPLIT = 16 * ceil(CW / 32) so that
+// every TMEM load starts on a multiple of 16 columns, the part-0 warps own [0, SPLIT) of half 0 and
+// [0, CW - SPLIT) of half 1, the part-1 warps [SPLIT, CW) of half 0 and [CW - SPLIT, CW) of half 1
+// (columns counted from the start of each half).
+//
+// Overlap of the segment drains with the MMAs: with two TMEM accumulators (orders <= 6) the MMA of segment
+// s+1 runs in the other accumulator while segment s drains.  With one (order 7: 352 of 512 columns) the
+// epilogue drains half 0 first and releases it, and the first chunk of the next segment issues all its
+// half-0 MMAs before waiting for half 1.
+template <int CW, int NHALF>
 __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_constant__ TcParams P) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1024-byte aligned stage buffers (the swizzle pattern repeats every 512 B)
   unsigned char *smem = (unsigned char *)(((unsigned long long)smem_raw + 1023) & ~1023ull);
   __shared__ __align__(8) unsigned long long full_bar[MAX_STAGES], empty_bar[MAX_STAGES];
-  __shared__ __align__(8) unsigned long long acc_full, acc_empty;
+  __shared__ __align__(8) unsigned long long acc_full[2], acc_empty[2][2];
   __shared__ unsigned tmem_base_sh;
   __shared__ volatile int abort_sh;
 
@@ -178,8 +187,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
       mbar_init(&full_bar[s], 1);
       mbar_init(&empty_bar[s], 1);
     }
-    mbar_init(&acc_full, 1);
-    mbar_init(&acc_empty, 8);  // one arrive per epilogue warp
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b][0], 8);  // one arrive per epilogue warp
+      mbar_init(&acc_empty[b][1], 8);
+    }
     abort_sh = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -240,21 +252,29 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
     if (lane == 0) {
       const unsigned idesc = (1u << 4) | ((unsigned)(P.NH >> 3) << 17) | ((unsigned)(128 >> 4) << 24);
       int stage = 0;
-      unsigned phase = 0, acc_phase = 0;
+      unsigned phase = 0;
+      unsigned empty_par = 0xFu;  // parity to wait for, per (buffer, half): starts at 1 (passes at once)
+      int seg = 0;
+      const bool defer = (P.nbuf == 1 && NHALF == 2);
       for (int it = blockIdx.x; it < P.nitems && !abort_sh; it += gridDim.x) {
         const TcItem w = P.items[P.item0 + it];
         for (int e = w.t0; e < w.t1 && !abort_sh; ++e) {
-          for (int sg = 0; sg < P.nseg && !abort_sh; ++sg) {
+          for (int sg = 0; sg < P.nseg && !abort_sh; ++sg, ++seg) {
             const int k0 = sg * P.NK / P.nseg, k1 = (sg + 1) * P.NK / P.nseg;
-            // the epilogue has drained the accumulator of the previous segment
-            if (!mbar_wait(&acc_empty, acc_phase ^ 1)) {
-              atomicExch(P.status + 1, 1);
-              abort_sh = 1;
-              break;
+            const int b = P.nbuf == 2 ? (seg & 1) : 0;
+            const unsigned dbase = tmem + (unsigned)(b * P.NP);
+            // the epilogue has drained this accumulator (both halves, or half 0 only when deferring half 1)
+            for (int h = 0; h < (defer ? 1 : NHALF); ++h) {
+              const int bit = b * 2 + h;
+              if (!mbar_wait(&acc_empty[b][h], (empty_par >> bit) & 1u)) {
+                atomicExch(P.status + 1, 1);
+                abort_sh = 1;
+                break;
+              }
+              empty_par ^= 1u << bit;
             }
-            acc_phase ^= 1;
+            if (abort_sh) break;
             tc_fence_after();
-            bool first = true;
             for (int kc = k0; kc < k1; ++kc) {
               if (!mbar_wait(&full_bar[stage], phase)) {
                 atomicExch(P.status + 1, 1);
@@ -265,61 +285,86 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
               const unsigned char *sbuf = smem + (size_t)stage * P.stage_bytes;
               const unsigned char *ahi = sbuf, *alo = sbuf + a_bytes;
               const unsigned char *bhi = sbuf + 2 * a_bytes, *blo = sbuf + 2 * a_bytes + b_bytes;
+              const bool firstc = (kc == k0);
 #pragma unroll
-              for (int ks = 0; ks < 2; ++ks) {
-                for (int h = 0; h < P.NHALF; ++h) {
-                  const unsigned d = tmem + h * P.NH;
+              for (int h = 0; h < NHALF; ++h) {
+                if (firstc && defer && h == 1) {
+                  if (!mbar_wait(&acc_empty[0][1], (empty_par >> 1) & 1u)) {
+                    atomicExch(P.status + 1, 1);
+                    abort_sh = 1;
+                    break;
+                  }
+                  empty_par ^= 2u;
+                  tc_fence_after();
+                }
+                const unsigned d = dbase + h * P.NH;
+#pragma unroll
+                for (int ks = 0; ks < 2; ++ks) {
                   const int bo = h * P.NH * 64 + ks * 32;
                   // the small cross terms first, the leading term last
-                  mma_f16(d, sdesc(ahi + ks * 32), sdesc(blo + bo), idesc, first ? 0u : 1u);
+                  mma_f16(d, sdesc(ahi + ks * 32), sdesc(blo + bo), idesc, (firstc && ks == 0) ? 0u : 1u);
                   mma_f16(d, sdesc(alo + ks * 32), sdesc(bhi + bo), idesc, 1u);
                   mma_f16(d, sdesc(ahi + ks * 32), sdesc(bhi + bo), idesc, 1u);
                 }
-                first = false;
               }
+              if (abort_sh) break;
               mma_commit(&empty_bar[stage]);  // frees the stage once these MMAs have read it
               if (++stage == S) {
                 stage = 0;
                 phase ^= 1;
               }
             }
-            mma_commit(&acc_full);  // segment accumulated
+            mma_commit(&acc_full[b]);  // segment accumulated
           }
         }
       }
     }
   } else {
     // ------------------------------------------------ epilogue (warps 2..9)
+    constexpr int SPLIT = 16 * ((CW + 31) / 32);
     const int q = warp & 3;              // TMEM lane quarter this warp may access
-    const int ch = (warp - 2) >> 2;      // column half
+    const int ch = (warp - 2) >> 2;      // which part of each half
     const int row = q * 32 + lane;       // target within the tile
-    const unsigned tbase = tmem + ((unsigned)(q * 32) << 16) + (unsigned)(ch * CW);
-    unsigned acc_phase = 0;
+    const unsigned tlane = tmem + ((unsigned)(q * 32) << 16);
+    unsigned full_par = 0;
+    int seg = 0;
     float acc[CW];
 #pragma unroll
     for (int i = 0; i < CW; ++i) acc[i] = 0.f;
     for (int it = blockIdx.x; it < P.nitems && !abort_sh; it += gridDim.x) {
       const TcItem w = P.items[P.item0 + it];
       const int nseg_item = (w.t1 - w.t0) * P.nseg;
-      for (int sgi = 0; sgi < nseg_item; ++sgi) {
-        if (!mbar_wait(&acc_full, acc_phase)) {
+      for (int sgi = 0; sgi < nseg_item; ++sgi, ++seg) {
+        const int b = P.nbuf == 2 ? (seg & 1) : 0;
+        if (!mbar_wait(&acc_full[b], (full_par >> b) & 1u)) {
           atomicExch(P.status + 1, 1);
           abort_sh = 1;
           break;
         }
-        acc_phase ^= 1;
+        full_par ^= 1u << b;
         tc_fence_after();
-#pragma unroll
-        for (int c0 = 0; c0 < CW; c0 += 16) {
-          unsigned r[16];
-          tmem_ld16(tbase + c0, r);
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-          for (int i = 0; i < 16; ++i) acc[c0 + i] += __uint_as_float(r[i]);
+        const unsigned tb = tlane + (unsigned)(b * P.NP);
+        if constexpr (NHALF == 1) {
+          drain_cols<CW>(tb + ch * CW, acc);
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acc_empty[b][0]);
+        } else {
+          // both parts drain G = CW - SPLIT columns of each half into acc[0, G) and acc[SPLIT, CW); the
+          // remaining 16-column group, acc[G, SPLIT), comes from half 0 for part 0 and half 1 for part 1
+          constexpr int G = CW - SPLIT;
+          static_assert(SPLIT - G == 16, "one extra group of 16 columns");
+          drain_cols<G>(tb + (ch == 0 ? 0 : SPLIT), acc);
+          if (ch == 0) drain_cols<16>(tb + G, acc + G);
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acc_empty[b][0]);
+          if (ch != 0) drain_cols<16>(tb + CW + G, acc + G);
+          drain_cols<G>(tb + CW + (ch == 0 ? 0 : SPLIT), acc + SPLIT);
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acc_empty[b][1]);
         }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&acc_empty);
       }
       if (abort_sh) break;
       // flush the item's sums into the FP64 locals
@@ -331,11 +376,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
       if (gx < Lv.side && gy < Lv.side && gz < Lv.side) cell = Lv.grid[((long long)gz * Lv.side + gy) * Lv.side + gx];
       if (cell >= 0) {
         const double sc = *Lv.scale_out;
-        double *Lrow = Lv.L + ((long long)cell * P.R + w.rhs) * P.nn + ch * CW;
-        const int lim = P.nn - ch * CW;
+        double *Lrow = Lv.L + ((long long)cell * P.R + w.rhs) * P.nn;
+        // first accumulator column of this thread's part in each half, and the part's width in half 0
+        const int n0 = NHALF == 1 ? ch * CW : (ch == 0 ? 0 : SPLIT);
+        const int w0 = NHALF == 1 ? CW : (ch == 0 ? SPLIT : CW - SPLIT);
+        const int n1 = NHALF == 1 ? 0 : (ch == 0 ? CW : 2 * CW - SPLIT);
 #pragma unroll
-        for (int i = 0; i < CW; ++i)
-          if (i < lim) atomicAdd(Lrow + i, (double)acc[i] * sc);
+        for (int i = 0; i < CW; ++i) {
+          const int n = i < w0 ? n0 + i : n1 + (i - w0);
+          if (n < P.nn) atomicAdd(Lrow + n, (double)acc[i] * sc);
+        }
       }
 #pragma unroll
       for (int i = 0; i < CW; ++i) acc[i] = 0.f;
@@ -424,7 +474,7 @@ EncodeTiledFn encode_fn() {
 }  // namespace
 
 struct DenseTC {
-  int KP = 0, NP = 0, NH = 0, NHALF = 0, NK = 0, stages = 0, ncols = 0, stage_bytes = 0;
+  int KP = 0, NP = 0, NH = 0, NHALF = 0, NK = 0, stages = 0, ncols = 0, stage_bytes = 0, nbuf = 1;
   __half *Bhi = nullptr, *Blo = nullptr;
   // per level
   __half *Ahi[kMaxHeight] = {}, *Alo[kMaxHeight] = {};
@@ -468,8 +518,9 @@ b200fmm_status tc_init(Context &c) {
   t->stage_bytes = 2 * (TILE_X * TILE_Y * TILE_Z * KCHUNK * 2) + 2 * t->NP * KCHUNK * 2;
   t->stages = std::min(MAX_STAGES, (220 * 1024) / t->stage_bytes);
   if (t->stages < 2) return fail(B200FMM_ERR_UNSUPPORTED, "stage buffers do not fit in shared memory");
+  t->nbuf = 2 * t->NP <= 512 ? 2 : 1;
   t->ncols = 32;
-  while (t->ncols < t->NP) t->ncols *= 2;
+  while (t->ncols < t->nbuf * t->NP) t->ncols *= 2;
   const size_t bsz = (size_t)343 * t->NP * t->KP;
   B200_CUDA(cudaMalloc(&t->Bhi, bsz * sizeof(__half)));
   B200_CUDA(cudaMalloc(&t->Blo, bsz * sizeof(__half)));
@@ -596,6 +647,7 @@ static b200fmm_status tc_prepare(Context &c) {
   P.stage_bytes = t->stage_bytes;
   // accumulator resets per transfer vector: 2 for p >= 6 keeps the M2L within ~1e-6 of FP64
   P.nseg = std::min(t->NK, c.p >= 6 ? 2 : 1);
+  P.nbuf = t->nbuf;
   if (const char *e = getenv("B200FMM_TC_SEGMENTS")) P.nseg = std::max(1, std::min(t->NK, atoi(e)));
   std::memcpy(P.off, c.itab.off, sizeof(P.off));
   std::memcpy(P.slot, c.itab.slot, sizeof(P.slot));
@@ -634,17 +686,17 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
   const size_t smem = (size_t)t->stages * t->stage_bytes + 1024;
   const int grid = std::min(t->grid, P.nitems);
   B200_CUDA(cudaEventRecord(c.ev[8], c.stream));
-  switch (t->NP / 2) {
-#define B200_TC_CASE(CWV)                                                                                      \
-  case CWV:                                                                                                    \
-    B200_CUDA(cudaFuncSetAttribute(m2l_tc_kernel<CWV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-    m2l_tc_kernel<CWV><<<grid, TC_THREADS, smem, c.stream>>>(P);                                               \
+  switch (t->NP) {
+#define B200_TC_CASE(NPV, CWV, NHV)                                                                              \
+  case NPV:                                                                                                        \
+    B200_CUDA(cudaFuncSetAttribute(m2l_tc_kernel<CWV, NHV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    m2l_tc_kernel<CWV, NHV><<<grid, TC_THREADS, smem, c.stream>>>(P);                                              \
     break;
-    B200_TC_CASE(16)
-    B200_TC_CASE(32)
-    B200_TC_CASE(64)
-    B200_TC_CASE(112)
-    B200_TC_CASE(176)
+    B200_TC_CASE(32, 16, 1)
+    B200_TC_CASE(64, 32, 1)
+    B200_TC_CASE(128, 64, 1)
+    B200_TC_CASE(224, 112, 1)
+    B200_TC_CASE(352, 176, 2)
 #undef B200_TC_CASE
     default:
       return fail(B200FMM_ERR_UNSUPPORTED, "no tensor-core M2L instance for this order");
