@@ -39,7 +39,7 @@ os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
 
 METRIC = "particles/s per FMM eval (1M uniform, Chebyshev p=7, height 6, mixed precision)"
 N_PART, ORDER, HEIGHT, SEED = 1_000_000, 7, 6, 42
-FLOPS_PER_P2P_PAIR = 20  # SURVEY 8(d) work unit
+FLOPS_PER_P2P_PAIR = 20  # 3 sub, 5 for r^2, rsqrt as 1, 3 for 1/r^3 and q scaling, 2 potential, 6 force
 
 
 def parse():
@@ -77,31 +77,42 @@ class ClockSampler:
               "clocks_event_reasons.hw_thermal_slowdown", "clocks_event_reasons.sw_thermal_slowdown",
               "clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index):
+    def __init__(self, index, period_ms=20):
         self.index = index
+        self.period_ms = period_ms
         self.samples = []
-        self._stop = threading.Event()
+        self.proc = None
         self._t = threading.Thread(target=self._run, daemon=True)
 
     def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + ",".join(self.FIELDS),
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                vals = [v.strip() for v in out.stdout.strip().split(",")]
+        # one long-lived nvidia-smi streaming a line every period_ms
+        try:
+            for line in self.proc.stdout:
+                vals = [v.strip() for v in line.strip().split(",")]
                 if len(vals) == len(self.FIELDS):
                     self.samples.append(vals)
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+        except Exception:
+            pass
 
     def __enter__(self):
-        self._t.start()
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + ",".join(self.FIELDS),
+                                          "--format=csv,noheader,nounits", "-lms", str(self.period_ms)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t.start()
+            time.sleep(0.3)  # let the first samples arrive before the timed region starts
+        except Exception:
+            self.proc = None
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        self._t.join(timeout=10)
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=10)
+            except Exception:
+                self.proc.kill()
+            self._t.join(timeout=10)
 
     def summary(self):
         if not self.samples:

@@ -111,6 +111,9 @@ B200FMM_API b200fmm_status b200fmm_execute(b200fmm_handle h, unsigned ops);
 /* Level-batched operators (FAbstractKernels).  They accumulate (+=) like the reference kernels.
  * m2m/l2l take the parent level; m2l the level of the target cells (2..height-1). */
 B200FMM_API b200fmm_status b200fmm_reset_expansions(b200fmm_handle h);
+/* Zero the potentials and forces only (the containers' resetToInitialState for the particle outputs,
+ * Src/Components/FBasicParticleContainer.hpp:449-460), keeping the expansions. */
+B200FMM_API b200fmm_status b200fmm_zero_results(b200fmm_handle h);
 B200FMM_API b200fmm_status b200fmm_p2m(b200fmm_handle h);
 B200FMM_API b200fmm_status b200fmm_m2m(b200fmm_handle h, int level);
 B200FMM_API b200fmm_status b200fmm_m2l(b200fmm_handle h, int level);

@@ -28,7 +28,7 @@ PRECISIONS = {"fp64": FP64, "mixed": MIXED}
 EXPORTS = (
     "b200fmm_create", "b200fmm_destroy", "b200fmm_last_error", "b200fmm_version", "b200fmm_set_sym_operators",
     "b200fmm_get_sym_operators", "b200fmm_set_particles", "b200fmm_set_charges", "b200fmm_execute",
-    "b200fmm_reset_expansions", "b200fmm_p2m", "b200fmm_m2m", "b200fmm_m2l", "b200fmm_l2l", "b200fmm_l2p",
+    "b200fmm_reset_expansions", "b200fmm_zero_results", "b200fmm_p2m", "b200fmm_m2m", "b200fmm_m2l", "b200fmm_l2l", "b200fmm_l2p",
     "b200fmm_p2p", "b200fmm_get_results", "b200fmm_synchronize", "b200fmm_tree_info", "b200fmm_get_cells",
     "b200fmm_get_permutation", "b200fmm_last_timings", "b200fmm_last_kernel_times", "b200fmm_tree_stats",
     "b200fmm_last_launch_count", "b200fmm_p2p_noalloc", "b200fmm_direct",
@@ -87,7 +87,8 @@ def lib():
         L.b200fmm_set_particles.argtypes = [ctypes.c_void_p, ctypes.c_longlong] + [ctypes.c_void_p] * 4 + [ctypes.c_int]
         L.b200fmm_set_charges.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
         L.b200fmm_execute.argtypes = [ctypes.c_void_p, ctypes.c_uint]
-        for n in ("b200fmm_reset_expansions", "b200fmm_p2m", "b200fmm_l2p", "b200fmm_synchronize"):
+        for n in ("b200fmm_reset_expansions", "b200fmm_zero_results", "b200fmm_p2m", "b200fmm_l2p",
+                  "b200fmm_synchronize"):
             getattr(L, n).argtypes = [ctypes.c_void_p]
         for n in ("b200fmm_m2m", "b200fmm_m2l", "b200fmm_l2l", "b200fmm_p2p"):
             getattr(L, n).argtypes = [ctypes.c_void_p, ctypes.c_int]
@@ -201,6 +202,9 @@ class FMM:
 
     def reset_expansions(self):
         _check(lib().b200fmm_reset_expansions(self._h), "reset_expansions")
+
+    def zero_results(self):
+        _check(lib().b200fmm_zero_results(self._h), "zero_results")
 
     def p2m(self):
         _check(lib().b200fmm_p2m(self._h), "p2m")

@@ -288,6 +288,16 @@ b200fmm_status b200fmm_reset_expansions(b200fmm_handle h) {
   return zero_state(c);
 }
 
+b200fmm_status b200fmm_zero_results(b200fmm_handle h) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  B200_CHECK(need_particles(c));
+  B200_CHECK(set_device(c));
+  const size_t pb = sizeof(double) * (size_t)c.N * c.R;
+  for (double *p : {c.d_phi, c.d_fx, c.d_fy, c.d_fz}) B200_CUDA(cudaMemsetAsync(p, 0, pb, c.stream));
+  return B200FMM_OK;
+}
+
 b200fmm_status b200fmm_execute(b200fmm_handle h, unsigned ops) {
   B200_CHECK(check_handle(h));
   Context &c = *h;
