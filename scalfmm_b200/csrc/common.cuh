@@ -104,7 +104,9 @@ struct Context {
   long long *d_perm = nullptr;                            // sorted -> original
   long long *d_leaf_start = nullptr;                      // [nleaves+1]
   int *d_leaf_nbr = nullptr;                              // [nleaves][27] (13 = self), -1 if empty
-  float4 *d_pq32 = nullptr;                               // [R][N] leaf-local FP32 (x,y,z,q) (MIXED)
+  float4 *d_pq32 = nullptr;                               // FP32 near-field copies (MIXED), see p2p.cu
+  int *d_leaf_rank = nullptr;      // [nleaves] position of each leaf in the column-major record order (MIXED P2P)
+  long long *d_rec_base = nullptr; // [nleaves+1] first source record of each leaf, in that order
   double *d_phi = nullptr, *d_fx = nullptr, *d_fy = nullptr, *d_fz = nullptr;  // [R][N] sorted results
   Level lv[kMaxHeight];
   bool has_particles = false;
@@ -161,6 +163,9 @@ b200fmm_status run_l2l(Context &c, int level);
 b200fmm_status run_l2p(Context &c);
 // p2p.cu
 b200fmm_status run_p2p(Context &c, int variant);
+// Orders the leaves by (x, y) column, z within a column (stable from Morton order), into d_leaf_rank, and
+// lays out the FP32 source records in that order (d_rec_base).  Uses the free tree-build scratch.
+b200fmm_status leaf_column_order(Context &c);
 // m2l_fp64.cu
 b200fmm_status run_m2l_fp64(Context &c, int level);
 // m2l_tc.cu

@@ -8,13 +8,12 @@
 //  * FP64 (parity form): one CTA per target leaf, source leaves staged through shared memory, the
 //    reference's arithmetic sequence (1/r^2, sqrt, products).
 //  * FP32 (mixed form), two source particles per step with Blackwell's packed FP32x2 instructions
-//    (add/mul/fma.f32x2): positions are stored relative to their own leaf centre as a float pair
-//    (hi, lo) with hi + lo exact to ~2^-48 of the leaf width.  For each source leaf the target is moved into
-//    that leaf's frame in FP64 once and split again, so that per pair dx = (t_hi - s_hi) + (t_lo - s_lo):
-//    the first difference is exact for nearby particles (Sterbenz), which keeps the close pairs -- the ones
-//    that dominate the forces -- accurate to a few ulp.  One warp per target leaf; the source leaves are
-//    copied into shared memory by the bulk-copy engine (cp.async.bulk + mbarrier, double buffered); rsqrt on
-//    the SFU; per-target compensated (two-sum) accumulation of the per-leaf partial sums; the result is added
+//    (add/mul/fma.f32x2): positions relative to the box corner as a float pair (hi, lo), so that per pair
+//    dx = (t_hi - s_hi) + (t_lo - s_lo) with the first difference exact for nearby particles (Sterbenz),
+//    which keeps the close pairs -- the ones that dominate the forces -- accurate to a few ulp.  One warp per
+//    target leaf; the neighbour leaves are walked as contiguous runs of records (one per neighbour column)
+//    copied into shared memory by the bulk-copy engine (cp.async.bulk + mbarrier, 3-deep ring); rsqrt on the
+//    SFU; per-target compensated (two-sum) accumulation of the per-stage partial sums; the result is added
 //    in FP64 to the far field.
 #include "common.cuh"
 
@@ -89,44 +88,57 @@ __global__ void p2p_fp64_kernel(int R, long long N, const long long *__restrict_
 
 // ---- FP32 compensated ------------------------------------------------------------------------------
 //
-// Layout of the FP32 copies (one buffer, see p2p_fp32_layout):
-//   tgt_hi[R][N] float4 (x_hi, y_hi, z_hi, q) and tgt_lo[N] float4 (x_lo, y_lo, z_lo, 0): leaf-local position
-//     of every particle as a float pair, read by the lane that owns the particle as a target;
-//   src[R][npairs][4] float4: the same particles as sources, two per record and pre-negated so that packed
-//     FP32x2 instructions consume them directly: (-x0,-x1,-y0,-y1) (-z0,-z1,q0,q1) (-lx0,-lx1,-ly0,-ly1)
-//     (-lz0,-lz1,0,0).  Leaf L's records start at (leaf_start[L] + L) / 2; an odd leaf is padded with a
-//     zero-charge particle far away.
+// Layout of the FP32 copies (one buffer, d_pq32):
+//   tgt_hi[R][N] float4 (x_hi, y_hi, z_hi, q) and tgt_lo[N] float4 (x_lo, y_lo, z_lo, 0): the position of every
+//     particle relative to the box corner as a float pair (hi = fl(x - x0), lo = fl(x - x0 - hi)), read by the
+//     lane that owns the particle as a target;
+//   src[R][N+2][4] float4: the same particles as sources, two per 64-byte record and pre-negated so that
+//     packed FP32x2 instructions consume them directly: (-x0,-x1,-y0,-y1) (-z0,-z1,q0,q1) (-lx0,-lx1,-ly0,-ly1)
+//     (-lz0,-lz1,0,0).  A leaf with an odd count is padded with a zero-charge particle far away.
+// Record order: the leaves in column order (x, y, then z; rank_of[leaf], first record rec_base[rank]), so that
+// the up to three z-neighbours of each of the 9 neighbour columns of a target leaf are one contiguous run of
+// records.  Without rank_of/rec_base (the allocation-free entry point) the leaves stay in Morton order with
+// leaf L's records starting at (leaf_start[L] + L) / 2 (gap records padded); only Morton-adjacent z-neighbours
+// then share a run.
+//
+// Because the coordinates are relative to the box corner (>= 0) and hi carries 24 bits, for close pairs
+// t_hi - s_hi is exact (Sterbenz), and dx = (t_hi - s_hi) + (t_lo - s_lo) is accurate to about one ulp of dx:
+// the close pairs, which dominate the forces, keep full FP32 relative accuracy.
 constexpr double P2P32_PAD = 1.0e15;
 
 __host__ __device__ inline long long p2p_pairs_capacity(long long N) { return N + 2; }
 
-__global__ void pack_local32(long long N, int R, const long long *__restrict__ keys_leaf,
-                             const long long *__restrict__ leaf_start, const double *__restrict__ x,
-                             const double *__restrict__ y, const double *__restrict__ z, const double *__restrict__ q,
-                             double cx0, double cy0, double cz0, double leaf_w, float4 *__restrict__ hi,
-                             float4 *__restrict__ lo, float4 *__restrict__ src) {
+// first source record of the leaf at position rank of the record order
+__device__ __forceinline__ long long rec_begin(const long long *__restrict__ rec_base,
+                                               const long long *__restrict__ leaf_start, long long rank) {
+  return rec_base ? rec_base[rank] : (leaf_start[rank] + rank) >> 1;
+}
+
+__global__ void pack_records32(long long N, int R, const long long *__restrict__ leaf_start,
+                               const int *__restrict__ rank_of, const long long *__restrict__ rec_base,
+                               const double *__restrict__ x, const double *__restrict__ y,
+                               const double *__restrict__ z, const double *__restrict__ q, double x0, double y0,
+                               double z0, float4 *__restrict__ hi, float4 *__restrict__ lo,
+                               float4 *__restrict__ src) {
   const long long leaf = blockIdx.x;
-  int ix, iy, iz;
-  morton_decode3(keys_leaf[leaf], ix, iy, iz);
-  const double c0 = cx0 + (ix + 0.5) * leaf_w, c1 = cy0 + (iy + 0.5) * leaf_w, c2 = cz0 + (iz + 0.5) * leaf_w;
   const long long s0 = leaf_start[leaf], s1 = leaf_start[leaf + 1];
+  const long long rank = rank_of ? rank_of[leaf] : leaf;
+  const long long b0 = rec_begin(rec_base, leaf_start, rank), b1 = rec_begin(rec_base, leaf_start, rank + 1);
   for (long long i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
-    const double lx = x[i] - c0, ly = y[i] - c1, lz = z[i] - c2;
+    const double lx = x[i] - x0, ly = y[i] - y0, lz = z[i] - z0;
     const float hx = (float)lx, hy = (float)ly, hz = (float)lz;
     lo[i] = make_float4((float)(lx - (double)hx), (float)(ly - (double)hy), (float)(lz - (double)hz), 0.f);
     for (int r = 0; r < R; ++r) hi[(long long)r * N + i] = make_float4(hx, hy, hz, (float)q[(long long)r * N + i]);
   }
   const long long P = p2p_pairs_capacity(N);
-  const long long pofs = (s0 + leaf) >> 1;
-  const long long np = (s1 - s0 + 1) >> 1;
-  for (long long pp = threadIdx.x; pp < np; pp += blockDim.x) {
+  for (long long pp = threadIdx.x; pp < b1 - b0; pp += blockDim.x) {
     float h[2][3], l[2][3];
     bool real[2];
     for (int u = 0; u < 2; ++u) {
       const long long j = s0 + 2 * pp + u;
       real[u] = j < s1;
-      const double d[3] = {real[u] ? x[j] - c0 : P2P32_PAD, real[u] ? y[j] - c1 : P2P32_PAD,
-                           real[u] ? z[j] - c2 : P2P32_PAD};
+      const double d[3] = {real[u] ? x[j] - x0 : P2P32_PAD, real[u] ? y[j] - y0 : P2P32_PAD,
+                           real[u] ? z[j] - z0 : P2P32_PAD};
       for (int a = 0; a < 3; ++a) {
         h[u][a] = (float)d[a];
         l[u][a] = (float)(d[a] - (double)h[u][a]);
@@ -134,9 +146,9 @@ __global__ void pack_local32(long long N, int R, const long long *__restrict__ k
     }
     for (int r = 0; r < R; ++r) {
       const long long j0 = s0 + 2 * pp;
-      const float q0 = (float)q[(long long)r * N + j0];
+      const float q0 = real[0] ? (float)q[(long long)r * N + j0] : 0.f;
       const float q1 = real[1] ? (float)q[(long long)r * N + j0 + 1] : 0.f;
-      float4 *rec = src + ((long long)r * P + pofs + pp) * 4;
+      float4 *rec = src + ((long long)r * P + b0 + pp) * 4;
       rec[0] = make_float4(-h[0][0], -h[1][0], -h[0][1], -h[1][1]);
       rec[1] = make_float4(-h[0][2], -h[1][2], q0, q1);
       rec[2] = make_float4(-l[0][0], -l[1][0], -l[0][1], -l[1][1]);
@@ -153,8 +165,9 @@ __device__ __forceinline__ void two_sum(float &hi, float &lo, float v) {
   lo += err;
 }
 
-constexpr int P2P32_WARPS = 4;        // target leaves per CTA (one warp each)
-constexpr int P2P32_STAGE = 48;       // source pair records (96 particles) per bulk-copy stage
+constexpr int P2P32_WARPS = 4;   // target leaves per CTA (one warp each)
+constexpr int P2P32_STAGE = 48;  // source records (96 particles) per bulk-copy stage
+constexpr int P2P32_NBUF = 3;    // stages in flight per warp
 
 __device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -184,28 +197,50 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
                : "memory");
 }
 
-// One warp per target leaf, one target particle per lane, two source particles per packed FP32x2 step.
-// The sources of the <=27 neighbour slots are walked as stages of <= P2P32_STAGE pair records, each copied
-// by one bulk copy (64-byte records: 16-byte aligned addresses and sizes) into a ring of P2P32_NBUF buffers,
-// issued P2P32_NBUF - 1 stages ahead of the math.
-constexpr int P2P32_NBUF = 3;
-
-__device__ __forceinline__ void fast_two_sum_exact(float a, float b, float &s, float &e) {
-  s = a + b;
-  const float bp = s - a;
-  e = (a - (s - bp)) + (b - bp);
+// One record (two sources) against the lane's target: packed FP32x2 difference, r^2, rsqrt on the SFU.
+template <bool SELF>
+__device__ __forceinline__ void p2p_record(const float4 *__restrict__ s, int k, int self_rel, float2 th_x,
+                                           float2 th_y, float2 th_z, float2 tl_x, float2 tl_y, float2 tl_z,
+                                           float2 &pv, float2 &ax, float2 &ay, float2 &az) {
+  const float4 A = s[4 * k], B = s[4 * k + 1], C = s[4 * k + 2], D = s[4 * k + 3];
+  const float2 dx = __fadd2_rn(__fadd2_rn(th_x, make_float2(A.x, A.y)), __fadd2_rn(tl_x, make_float2(C.x, C.y)));
+  const float2 dy = __fadd2_rn(__fadd2_rn(th_y, make_float2(A.z, A.w)), __fadd2_rn(tl_y, make_float2(C.z, C.w)));
+  const float2 dz = __fadd2_rn(__fadd2_rn(th_z, make_float2(B.x, B.y)), __fadd2_rn(tl_z, make_float2(D.x, D.y)));
+  float2 r2 = __fmul2_rn(dx, dx);
+  r2 = __ffma2_rn(dy, dy, r2);
+  r2 = __ffma2_rn(dz, dz, r2);
+  float2 inv;
+  if (SELF) {
+    inv = make_float2(2 * k == self_rel ? 0.f : rsqrtf(r2.x), 2 * k + 1 == self_rel ? 0.f : rsqrtf(r2.y));
+  } else {
+    inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+  }
+  const float2 qi = __fmul2_rn(make_float2(B.z, B.w), inv);
+  const float2 qi3 = __fmul2_rn(qi, __fmul2_rn(inv, inv));
+  pv = __fadd2_rn(pv, qi);
+  ax = __ffma2_rn(dx, qi3, ax);
+  ay = __ffma2_rn(dy, qi3, ay);
+  az = __ffma2_rn(dz, qi3, az);
 }
 
+// One warp per target leaf.  The target particles are taken 32 at a time; a chunk of m <= 16 (or <= 8)
+// targets is replicated over 2 (or 4) lane groups, each group walking every 2nd (4th) source record, and the
+// groups' sums are combined by shuffles at the end, so that small and ragged leaves keep the lanes busy.
+// The sources are walked as runs of contiguous records (one per neighbour column and z-adjacent group),
+// each split into stages of <= P2P32_STAGE records copied by one bulk copy into a ring of P2P32_NBUF buffers,
+// issued P2P32_NBUF - 1 stages ahead of the math.  Per stage the partial sums enter the target's (hi, lo)
+// accumulators by a two-sum.
 __global__ void __launch_bounds__(P2P32_WARPS * 32, 6) p2p_fp32_kernel(
     int R, long long N, long long nleaves, const long long *__restrict__ leaf_start, const int *__restrict__ nbr,
-    int variant, const float4 *__restrict__ pq, const float4 *__restrict__ plo, const float4 *__restrict__ src,
-    double leaf_w, double *__restrict__ phi, double *__restrict__ fx, double *__restrict__ fy,
-    double *__restrict__ fz, int *__restrict__ status) {
+    int variant, const int *__restrict__ rank_of, const long long *__restrict__ rec_base,
+    const float4 *__restrict__ pq, const float4 *__restrict__ plo, const float4 *__restrict__ src,
+    double *__restrict__ phi, double *__restrict__ fx, double *__restrict__ fy, double *__restrict__ fz,
+    int *__restrict__ status) {
   __shared__ __align__(128) float4 buf[P2P32_WARPS][P2P32_NBUF][4 * P2P32_STAGE];
   __shared__ __align__(8) unsigned long long bar[P2P32_WARPS][P2P32_NBUF];
-  __shared__ long long sbase[P2P32_WARPS][27];
-  __shared__ int scount[P2P32_WARPS][27];
-  __shared__ signed char spos[P2P32_WARPS][27];
+  __shared__ long long rbase[P2P32_WARPS][27];
+  __shared__ int rcount[P2P32_WARPS][27];
+  __shared__ unsigned char rself[P2P32_WARPS][27];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long leaf = (long long)blockIdx.x * P2P32_WARPS + w;
   if (lane == 0) {
@@ -216,45 +251,64 @@ __global__ void __launch_bounds__(P2P32_WARPS * 32, 6) p2p_fp32_kernel(
   if (leaf >= nleaves) return;
   const long long P = p2p_pairs_capacity(N);
   const long long t0 = leaf_start[leaf], t1 = leaf_start[leaf + 1];
-  // the source slots of this leaf: pair-record base, pair count and neighbour position
-  int ns = 0;
+  const int my_rank = rank_of ? rank_of[leaf] : (int)leaf;
+  const long long self_rec = rec_begin(rec_base, leaf_start, my_rank);
+  // the runs of this leaf: lane e < 27 looks at neighbour position e = ((dx+1)*3 + dy+1)*3 + dz+1
+  int nr = 0;
   {
-    const int e = lane < 27 ? lane : 0;
-    const int sl = (lane < 27 && !(variant == 1 && e == 13)) ? nbr[leaf * 27 + e] : -1;
-    const unsigned mask = __ballot_sync(0xffffffffu, sl >= 0);
-    if (sl >= 0) {
-      const int k = __popc(mask & ((1u << lane) - 1u));
-      const long long a0 = leaf_start[sl], a1 = leaf_start[sl + 1];
-      sbase[w][k] = (a0 + sl) >> 1;
-      scount[w][k] = (int)((a1 - a0 + 1) >> 1);
-      spos[w][k] = (signed char)e;
+    const int e = lane < 27 ? lane : 26;
+    int nb = lane < 27 ? nbr[leaf * 27 + e] : -1;
+    if (variant == 1 && e == 13) nb = -1;
+    const int rk = nb >= 0 ? (rank_of ? rank_of[nb] : nb) : -1;
+    const int dz = e % 3;
+    const int rk_prev = __shfl_up_sync(0xffffffffu, rk, 1);
+    const int rk_next = __shfl_down_sync(0xffffffffu, rk, 1);
+    const int rk_next2 = __shfl_down_sync(0xffffffffu, rk, 2);
+    const bool start = lane < 27 && rk >= 0 && !(dz > 0 && rk_prev >= 0 && rk_prev + 1 == rk);
+    int last = rk;
+    if (dz < 2 && rk_next >= 0 && rk_next == last + 1) {
+      last = rk_next;
+      if (dz == 0 && rk_next2 >= 0 && rk_next2 == last + 1) last = rk_next2;
     }
-    ns = __popc(mask);
+    const unsigned mask = __ballot_sync(0xffffffffu, start);
+    if (start) {
+      const int k = __popc(mask & ((1u << lane) - 1u));
+      const long long b0 = rec_begin(rec_base, leaf_start, rk), b1 = rec_begin(rec_base, leaf_start, last + 1);
+      rbase[w][k] = b0;
+      rcount[w][k] = (int)(b1 - b0);
+      rself[w][k] = (variant == 0 && e / 3 == 4 && rk <= my_rank && my_rank <= last) ? 1 : 0;
+    }
+    nr = __popc(mask);
     __syncwarp();
   }
-  const float lw = (float)leaf_w;
   unsigned phase_bits = 0;  // one parity bit per buffer
   for (int r = 0; r < R; ++r) {
     const float4 *pr = pq + (long long)r * N;
     const float4 *sr = src + (long long)r * P * 4;
     for (long long tb = t0; tb < t1; tb += 32) {
-      const long long i = tb + lane;
-      const bool active = i < t1;
+      const int m = (int)min(32LL, t1 - tb);
+      const int T = m <= 8 ? 8 : (m <= 16 ? 16 : 32);  // targets per lane group
+      const int G = 32 / T;                             // lane groups, each on every G-th record
+      const int tl = lane & (T - 1), g = lane / T;
+      const long long i = tb + tl;
+      const bool active = tl < m;
       const float4 me = active ? pr[i] : make_float4(0.f, 0.f, 0.f, 0.f);
       const float4 mel = active ? plo[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-      const int self_local = (int)(i - t0);  // index of the target within its own leaf
+      const long long self_slot = 2 * self_rec + (i - t0);  // the target's own slot in the record numbering
+      const float2 th_x = make_float2(me.x, me.x), th_y = make_float2(me.y, me.y), th_z = make_float2(me.z, me.z);
+      const float2 tl_x = make_float2(mel.x, mel.x), tl_y = make_float2(mel.y, mel.y), tl_z = make_float2(mel.z, mel.z);
       float ph_hi = 0.f, ph_lo = 0.f, gx_hi = 0.f, gx_lo = 0.f, gy_hi = 0.f, gy_lo = 0.f, gz_hi = 0.f, gz_lo = 0.f;
-      // stage sequence: (slot e, first pair p, pair count n); issue up to NBUF-1 stages ahead
-      int ie = 0, ip = 0;       // next stage to issue
-      int ce = 0, cp = 0;       // stage being computed
+      // stage sequence: (run e, first record p, record count n); issue up to NBUF-1 stages ahead
+      int ie = 0, ip = 0;  // next stage to issue
+      int ce = 0, cp = 0;  // stage being computed
       int issued = 0, done = 0;
       auto next_stage = [&](int &e, int &p0, int &n) -> bool {
-        while (e < ns && p0 >= scount[w][e]) {
+        while (e < nr && p0 >= rcount[w][e]) {
           ++e;
           p0 = 0;
         }
-        if (e >= ns) return false;
-        n = min(P2P32_STAGE, scount[w][e] - p0);
+        if (e >= nr) return false;
+        n = min(P2P32_STAGE, rcount[w][e] - p0);
         return true;
       };
       auto issue = [&]() {
@@ -263,7 +317,7 @@ __global__ void __launch_bounds__(P2P32_WARPS * 32, 6) p2p_fp32_kernel(
         const int b = issued % P2P32_NBUF;
         if (lane == 0) {
           mbar_expect_tx(&bar[w][b], n * 64);
-          bulk_g2s(&buf[w][b][0], sr + (sbase[w][ie] + ip) * 4, n * 64, &bar[w][b]);
+          bulk_g2s(&buf[w][b][0], sr + (rbase[w][ie] + ip) * 4, n * 64, &bar[w][b]);
         }
         ip += n;
         ++issued;
@@ -280,61 +334,17 @@ __global__ void __launch_bounds__(P2P32_WARPS * 32, 6) p2p_fp32_kernel(
           return;
         }
         phase_bits ^= 1u << b;
-        // the target moved into the source leaf's frame: (hi - off) by an exact two-sum, the rounding error
-        // folded into lo (off is a small multiple of the leaf width)
-        const int sl_pos = spos[w][ce];
-        float thx, thy, thz, tlx, tly, tlz;
-        {
-          float e0;
-          fast_two_sum_exact(me.x, -(float)(sl_pos / 9 - 1) * lw, thx, e0);
-          tlx = mel.x + e0;
-          fast_two_sum_exact(me.y, -(float)((sl_pos / 3) % 3 - 1) * lw, thy, e0);
-          tly = mel.y + e0;
-          fast_two_sum_exact(me.z, -(float)(sl_pos % 3 - 1) * lw, thz, e0);
-          tlz = mel.z + e0;
-        }
-        const float2 th_x = make_float2(thx, thx), th_y = make_float2(thy, thy), th_z = make_float2(thz, thz);
-        const float2 tl_x = make_float2(tlx, tlx), tl_y = make_float2(tly, tly), tl_z = make_float2(tlz, tlz);
         float2 pv = make_float2(0.f, 0.f), ax = pv, ay = pv, az = pv;
         const float4 *s = buf[w][b];
-        if (sl_pos == 13) {
-          const int self_pair = self_local - 2 * cp;  // source index of the target within this stage
+        if (rself[w][ce]) {
+          const int self_rel = (int)(self_slot - 2 * (rbase[w][ce] + cp));  // the target's slot in this stage
 #pragma unroll 2
-          for (int k = 0; k < cn; ++k) {
-            const float4 A = s[4 * k], B = s[4 * k + 1], C = s[4 * k + 2], D = s[4 * k + 3];
-            const float2 dx = __fadd2_rn(__fadd2_rn(th_x, make_float2(A.x, A.y)), __fadd2_rn(tl_x, make_float2(C.x, C.y)));
-            const float2 dy = __fadd2_rn(__fadd2_rn(th_y, make_float2(A.z, A.w)), __fadd2_rn(tl_y, make_float2(C.z, C.w)));
-            const float2 dz = __fadd2_rn(__fadd2_rn(th_z, make_float2(B.x, B.y)), __fadd2_rn(tl_z, make_float2(D.x, D.y)));
-            float2 r2 = __fmul2_rn(dx, dx);
-            r2 = __ffma2_rn(dy, dy, r2);
-            r2 = __ffma2_rn(dz, dz, r2);
-            const float2 inv = make_float2(2 * k == self_pair ? 0.f : rsqrtf(r2.x),
-                                           2 * k + 1 == self_pair ? 0.f : rsqrtf(r2.y));
-            const float2 qi = __fmul2_rn(make_float2(B.z, B.w), inv);
-            const float2 qi3 = __fmul2_rn(qi, __fmul2_rn(inv, inv));
-            pv = __fadd2_rn(pv, qi);
-            ax = __ffma2_rn(dx, qi3, ax);
-            ay = __ffma2_rn(dy, qi3, ay);
-            az = __ffma2_rn(dz, qi3, az);
-          }
+          for (int k = g; k < cn; k += G)
+            p2p_record<true>(s, k, self_rel, th_x, th_y, th_z, tl_x, tl_y, tl_z, pv, ax, ay, az);
         } else {
 #pragma unroll 4
-          for (int k = 0; k < cn; ++k) {
-            const float4 A = s[4 * k], B = s[4 * k + 1], C = s[4 * k + 2], D = s[4 * k + 3];
-            const float2 dx = __fadd2_rn(__fadd2_rn(th_x, make_float2(A.x, A.y)), __fadd2_rn(tl_x, make_float2(C.x, C.y)));
-            const float2 dy = __fadd2_rn(__fadd2_rn(th_y, make_float2(A.z, A.w)), __fadd2_rn(tl_y, make_float2(C.z, C.w)));
-            const float2 dz = __fadd2_rn(__fadd2_rn(th_z, make_float2(B.x, B.y)), __fadd2_rn(tl_z, make_float2(D.x, D.y)));
-            float2 r2 = __fmul2_rn(dx, dx);
-            r2 = __ffma2_rn(dy, dy, r2);
-            r2 = __ffma2_rn(dz, dz, r2);
-            const float2 inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
-            const float2 qi = __fmul2_rn(make_float2(B.z, B.w), inv);
-            const float2 qi3 = __fmul2_rn(qi, __fmul2_rn(inv, inv));
-            pv = __fadd2_rn(pv, qi);
-            ax = __ffma2_rn(dx, qi3, ax);
-            ay = __ffma2_rn(dy, qi3, ay);
-            az = __ffma2_rn(dz, qi3, az);
-          }
+          for (int k = g; k < cn; k += G)
+            p2p_record<false>(s, k, 0, th_x, th_y, th_z, tl_x, tl_y, tl_z, pv, ax, ay, az);
         }
         two_sum(ph_hi, ph_lo, pv.x + pv.y);
         two_sum(gx_hi, gx_lo, ax.x + ax.y);
@@ -345,7 +355,25 @@ __global__ void __launch_bounds__(P2P32_WARPS * 32, 6) p2p_fp32_kernel(
         __syncwarp();  // every lane is done with buffer b before it is refilled
         issue();
       }
-      if (active) {
+      // combine the lane groups that shared this chunk's targets
+      for (int off = T; off < 32; off <<= 1) {
+        float oh = __shfl_xor_sync(0xffffffffu, ph_hi, off), ol = __shfl_xor_sync(0xffffffffu, ph_lo, off);
+        two_sum(ph_hi, ph_lo, oh);
+        ph_lo += ol;
+        oh = __shfl_xor_sync(0xffffffffu, gx_hi, off);
+        ol = __shfl_xor_sync(0xffffffffu, gx_lo, off);
+        two_sum(gx_hi, gx_lo, oh);
+        gx_lo += ol;
+        oh = __shfl_xor_sync(0xffffffffu, gy_hi, off);
+        ol = __shfl_xor_sync(0xffffffffu, gy_lo, off);
+        two_sum(gy_hi, gy_lo, oh);
+        gy_lo += ol;
+        oh = __shfl_xor_sync(0xffffffffu, gz_hi, off);
+        ol = __shfl_xor_sync(0xffffffffu, gz_lo, off);
+        two_sum(gz_hi, gz_lo, oh);
+        gz_lo += ol;
+      }
+      if (active && g == 0) {
         const long long j = (long long)r * N + i;
         const double tq = -(double)me.w;
         phi[j] += (double)ph_hi + (double)ph_lo;
@@ -367,17 +395,18 @@ b200fmm_status run_p2p(Context &c, int variant) {
     float4 *hi = c.d_pq32, *lo = c.d_pq32 + c.N * c.R, *src = c.d_pq32 + c.N * (c.R + 1);
     if (!c.packed32) {
       c.packed32 = true;
+      B200_CHECK(leaf_column_order(c));
       const double W = c.cfg.box_width;
-      pack_local32<<<(unsigned)L.n, 64, 0, c.stream>>>(c.N, c.R, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q,
-                                                       c.cfg.center[0] - W / 2, c.cfg.center[1] - W / 2,
-                                                       c.cfg.center[2] - W / 2, W / (double)(1 << LL), hi, lo, src);
+      pack_records32<<<(unsigned)L.n, 64, 0, c.stream>>>(c.N, c.R, c.d_leaf_start, c.d_leaf_rank, c.d_rec_base, c.d_x,
+                                                         c.d_y, c.d_z, c.d_q, c.cfg.center[0] - W / 2,
+                                                         c.cfg.center[1] - W / 2, c.cfg.center[2] - W / 2, hi, lo, src);
       ++c.launches;
     }
     int *status = c.d_status;
     const unsigned blocks = grid_for(L.n, P2P32_WARPS);
     B200_CUDA(cudaEventRecord(c.ev[10], c.stream));
     p2p_fp32_kernel<<<blocks, P2P32_WARPS * 32, 0, c.stream>>>(c.R, c.N, L.n, c.d_leaf_start, c.d_leaf_nbr, variant,
-                                                               hi, lo, src, c.cfg.box_width / (double)(1 << LL), c.d_phi,
+                                                               c.d_leaf_rank, c.d_rec_base, hi, lo, src, c.d_phi,
                                                                c.d_fx, c.d_fy, c.d_fz, status);
     B200_CUDA(cudaEventRecord(c.ev[11], c.stream));
     ++c.launches;
@@ -396,7 +425,7 @@ b200fmm_status run_p2p(Context &c, int variant) {
 }  // namespace b200
 
 // ---- allocation-free entry point -------------------------------------------------------------------
-// Scratch of b200fmm_p2p_noalloc: the FP32 leaf-local copies of the particles -- targets (hi, lo) and
+// Scratch of b200fmm_p2p_noalloc: the FP32 copies of the particles -- targets (hi, lo) and
 // pair-packed sources, 6 float4 per particle plus 8 (24 MiB at 2^18 particles) -- and the status word of the
 // kernel's bounded waits.  In host code these names are host-side stand-ins, not device addresses: the host
 // passes the addresses looked up with cudaGetSymbolAddress.
@@ -448,14 +477,13 @@ extern "C" b200fmm_status b200fmm_p2p_noalloc(long long n, const double *x, cons
   int *status = nullptr;
   B200_CHECK(noalloc_addresses(&stage, &status));
   cudaStream_t s = (cudaStream_t)stream;
-  const int LL = height - 1;
-  const double leaf_w = box_width / (double)(1 << LL);
   B200_CUDA(cudaMemsetAsync(status, 0, sizeof(int) * 4, s));
-  pack_local32<<<(unsigned)nleaves, 64, 0, s>>>(n, 1, leaf_keys, leaf_start, x, y, z, q, center[0] - box_width / 2,
-                                               center[1] - box_width / 2, center[2] - box_width / 2, leaf_w, stage,
-                                               stage + n, stage + 2 * n);
+  pack_records32<<<(unsigned)nleaves, 64, 0, s>>>(n, 1, leaf_start, nullptr, nullptr, x, y, z, q,
+                                                 center[0] - box_width / 2, center[1] - box_width / 2,
+                                                 center[2] - box_width / 2, stage, stage + n, stage + 2 * n);
   p2p_fp32_kernel<<<grid_for(nleaves, P2P32_WARPS), P2P32_WARPS * 32, 0, s>>>(
-      1, n, nleaves, leaf_start, leaf_nbr, variant, stage, stage + n, stage + 2 * n, leaf_w, phi, fx, fy, fz, status);
+      1, n, nleaves, leaf_start, leaf_nbr, variant, nullptr, nullptr, stage, stage + n, stage + 2 * n, phi, fx, fy, fz,
+      status);
   B200_CUDA(cudaGetLastError());
   int st = 0;
   B200_CUDA(cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -69,7 +69,6 @@ __global__ void rs_hist(const unsigned long long *__restrict__ keys, long long n
 // Exclusive scan of an unsigned array in tiles of 1024 (one block per tile), block sums out.
 __global__ void scan_tiles_u32(const unsigned *__restrict__ in, unsigned *__restrict__ out, long long n,
                                unsigned *__restrict__ sums) {
-  __shared__ unsigned s[1024];
   __shared__ unsigned wsum[32];
   const long long i = (long long)blockIdx.x * 1024 + threadIdx.x;
   const unsigned v = i < n ? in[i] : 0u;
@@ -96,7 +95,6 @@ __global__ void scan_tiles_u32(const unsigned *__restrict__ in, unsigned *__rest
   const unsigned incl = x + (w > 0 ? wsum[w - 1] : 0u);
   if (i < n) out[i] = incl - v;
   if (threadIdx.x == 1023 && sums) sums[blockIdx.x] = incl;
-  (void)s;
 }
 
 __global__ void add_tile_offsets_u32(unsigned *__restrict__ out, long long n, const unsigned *__restrict__ offs) {
@@ -320,6 +318,32 @@ __global__ void fill_int(long long n, int *p, int v) {
   if (i < n) p[i] = v;
 }
 
+// column key of a leaf: (x, y) of its cell; a stable sort by it from Morton order (monotone in z inside a
+// column) puts the three z-neighbours of every column next to each other
+__global__ void leaf_column_keys(long long nleaves, const long long *__restrict__ keys, int LL,
+                                 unsigned long long *__restrict__ k, int *__restrict__ v) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= nleaves) return;
+  int ix, iy, iz;
+  morton_decode3(keys[i], ix, iy, iz);
+  k[i] = ((unsigned long long)ix << LL) | (unsigned long long)iy;
+  v[i] = (int)i;
+}
+
+__global__ void leaf_rank_kernel(long long nleaves, const int *__restrict__ order,
+                                 const long long *__restrict__ leaf_start, int *__restrict__ rank_of,
+                                 long long *__restrict__ nrec) {
+  const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (r >= nleaves) return;
+  const int leaf = order[r];
+  rank_of[leaf] = (int)r;
+  nrec[r] = (leaf_start[leaf + 1] - leaf_start[leaf] + 1) >> 1;  // two particles per record
+}
+
+__global__ void rec_total_kernel(long long nleaves, const long long *__restrict__ nrec, long long *__restrict__ base) {
+  base[nleaves] = base[nleaves - 1] + nrec[nleaves - 1];
+}
+
 // grow-only device buffer: reallocates (and bumps the tree generation) only when n exceeds the capacity
 template <class T>
 b200fmm_status grow(Context &c, T *&p, size_t &cap, size_t n) {
@@ -383,6 +407,8 @@ void free_tree(Context &c) {
   dfree(c.d_perm);
   dfree(c.d_leaf_start);
   dfree(c.d_leaf_nbr);
+  dfree(c.d_leaf_rank);
+  dfree(c.d_rec_base);
   dfree(c.d_pq32);
   dfree(c.d_phi);
   dfree(c.d_fx);
@@ -544,6 +570,10 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
     B200_CHECK(grow(c, c.d_leaf_start, cl, (size_t)nleaves + 1));
     cl = c.cap_leaf * 27;
     B200_CHECK(grow(c, c.d_leaf_nbr, cl, (size_t)(nleaves + 1) * 27));
+    cl = c.cap_leaf;
+    B200_CHECK(grow(c, c.d_leaf_rank, cl, (size_t)nleaves + 1));
+    cl = c.cap_leaf;
+    B200_CHECK(grow(c, c.d_rec_base, cl, (size_t)nleaves + 1));
     c.cap_leaf = std::max(c.cap_leaf, (size_t)nleaves + 1);
   }
   compact_leaves<<<grid_for(n, 256), 256, 0, s>>>(n, k0, flags, idx, leaf.keys, c.d_leaf_start);
@@ -584,6 +614,38 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
       c.tree_launches += 2;
     }
   }
+  B200_CUDA(cudaGetLastError());
+  return B200FMM_OK;
+}
+
+}  // namespace b200
+
+namespace b200 {
+
+b200fmm_status leaf_column_order(Context &c) {
+  const int LL = c.H - 1;
+  const long long nl = c.lv[LL].n;
+  cudaStream_t s = c.stream;
+  // the particle sort's buffers are free after the tree build and hold 2(N+1) >= 2 nleaves entries
+  unsigned long long *k0 = c.d_sortk, *k1 = c.d_sortk + nl;
+  int *v0 = c.d_sortv, *v1 = c.d_sortv + nl;
+  const long long nb = (nl + RS_TILE - 1) / RS_TILE;
+  unsigned *cnt = c.d_cnt, *off = c.d_cnt + RS_BINS * nb;
+  leaf_column_keys<<<grid_for(nl, 256), 256, 0, s>>>(nl, c.lv[LL].keys, LL, k0, v0);
+  ++c.launches;
+  for (int sh = 0; sh < 2 * LL; sh += 4) {
+    rs_hist<<<(unsigned)nb, RS_THREADS, 0, s>>>(k0, nl, sh, (int)nb, cnt);
+    B200_CHECK(scan_u32(c, cnt, off, RS_BINS * nb, (unsigned *)c.d_scan));
+    rs_scatter<<<(unsigned)nb, RS_THREADS, 0, s>>>(k0, v0, k1, v1, nl, sh, (int)nb, off);
+    c.launches += 2;
+    std::swap(k0, k1);
+    std::swap(v0, v1);
+  }
+  long long *nrec = c.d_flags;
+  leaf_rank_kernel<<<grid_for(nl, 256), 256, 0, s>>>(nl, v0, c.d_leaf_start, c.d_leaf_rank, nrec);
+  B200_CHECK(scan_i64(c, nrec, c.d_rec_base, nl, (long long *)c.d_scan));
+  rec_total_kernel<<<1, 1, 0, s>>>(nl, nrec, c.d_rec_base);
+  c.launches += 2;
   B200_CUDA(cudaGetLastError());
   return B200FMM_OK;
 }

@@ -6,6 +6,12 @@ to its own pool -- so this entry point keeps its scratch in a fixed device array
 test calls it through the C ABI twice in a row on caller-owned device buffers and compares each result with
 the regular handle-based b200fmm_p2p on the same particles.  This file is named so that pytest collects it
 last.
+
+Tolerance: the two calls in a row agree exactly.  Against the handle's P2P the same FP32 arithmetic runs, but
+the handle walks the source leaves in column order (one run per neighbour column) while the allocation-free
+entry point, which cannot sort, keeps Morton order (runs of Morton-adjacent leaves): the per-stage partial
+sums are grouped differently, so the two agree to the FP32 path's accuracy (compensated sums: 1e-6 relative),
+not bit for bit.
 """
 import ctypes
 
@@ -72,7 +78,12 @@ def test_p2p_noalloc_matches_handle_p2p(variant):
         got = [o.cpu().numpy() for o in out]
         for k, g in zip(("phi", "fx", "fy", "fz"), got):
             want = ref[k][order]
-            assert S.rel_l2(g, want) < 1e-12, (call, k, S.rel_l2(g, want))
+            assert S.rel_l2(g, want) < 1e-6, (call, k, S.rel_l2(g, want))
+        if call == 0:
+            first = got
+        else:
+            for a, b in zip(first, got):
+                assert np.array_equal(a, b)
 
 
 def test_p2p_noalloc_rejects_oversized_input():
