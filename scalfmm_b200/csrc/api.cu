@@ -262,6 +262,8 @@ b200fmm_status b200fmm_set_particles(b200fmm_handle h, long long n, const double
   B200_CUDA(cudaEventRecord(c.ev[14], c.stream));
   b200fmm_status st = build_tree(c, x, y, z, q, on_device != 0);
   if (st != B200FMM_OK) return st;
+  B200_CHECK(zero_state(c));  // a new tree starts from zero expansions and results
+  c.state_zero = true;
   B200_CUDA(cudaEventRecord(c.ev[15], c.stream));
   B200_CUDA(cudaEventSynchronize(c.ev[15]));
   float ms = 0;
@@ -285,7 +287,9 @@ b200fmm_status b200fmm_reset_expansions(b200fmm_handle h) {
   Context &c = *h;
   B200_CHECK(need_particles(c));
   B200_CHECK(set_device(c));
-  return zero_state(c);
+  B200_CHECK(zero_state(c));
+  c.state_zero = true;
+  return B200FMM_OK;
 }
 
 b200fmm_status b200fmm_zero_results(b200fmm_handle h) {
@@ -306,7 +310,8 @@ b200fmm_status b200fmm_execute(b200fmm_handle h, unsigned ops) {
   c.launches = 0;
   const int LL = c.H - 1;
   B200_CHECK(record(c, 0));
-  B200_CHECK(zero_state(c));
+  if (!c.state_zero) B200_CHECK(zero_state(c));  // skipped right after set_particles, which zeroed them
+  c.state_zero = false;
   B200_CHECK(record(c, 1));
   if (ops & B200FMM_P2M) B200_CHECK(run_p2m(c));
   B200_CHECK(record(c, 2));
@@ -332,6 +337,7 @@ b200fmm_status b200fmm_execute(b200fmm_handle h, unsigned ops) {
 
 b200fmm_status b200fmm_p2m(b200fmm_handle h) {
   B200_CHECK(check_handle(h));
+  h->state_zero = false;
   B200_CHECK(need_particles(*h));
   B200_CHECK(set_device(*h));
   return run_p2m(*h);
@@ -339,6 +345,7 @@ b200fmm_status b200fmm_p2m(b200fmm_handle h) {
 
 b200fmm_status b200fmm_m2m(b200fmm_handle h, int level) {
   B200_CHECK(check_handle(h));
+  h->state_zero = false;
   B200_CHECK(need_particles(*h));
   B200_CHECK(set_device(*h));
   return run_m2m(*h, level);
@@ -346,6 +353,7 @@ b200fmm_status b200fmm_m2m(b200fmm_handle h, int level) {
 
 b200fmm_status b200fmm_m2l(b200fmm_handle h, int level) {
   B200_CHECK(check_handle(h));
+  h->state_zero = false;
   B200_CHECK(need_particles(*h));
   B200_CHECK(set_device(*h));
   if (level < 2 || level > h->H - 1) return fail(B200FMM_ERR_INVALID, "m2l: level must be in [2, height-1]");
@@ -354,6 +362,7 @@ b200fmm_status b200fmm_m2l(b200fmm_handle h, int level) {
 
 b200fmm_status b200fmm_l2l(b200fmm_handle h, int level) {
   B200_CHECK(check_handle(h));
+  h->state_zero = false;
   B200_CHECK(need_particles(*h));
   B200_CHECK(set_device(*h));
   return run_l2l(*h, level);
@@ -361,6 +370,7 @@ b200fmm_status b200fmm_l2l(b200fmm_handle h, int level) {
 
 b200fmm_status b200fmm_l2p(b200fmm_handle h) {
   B200_CHECK(check_handle(h));
+  h->state_zero = false;
   B200_CHECK(need_particles(*h));
   B200_CHECK(set_device(*h));
   return run_l2p(*h);
@@ -368,6 +378,7 @@ b200fmm_status b200fmm_l2p(b200fmm_handle h) {
 
 b200fmm_status b200fmm_p2p(b200fmm_handle h, int variant) {
   B200_CHECK(check_handle(h));
+  h->state_zero = false;
   B200_CHECK(need_particles(*h));
   if (variant != 0 && variant != 1) return fail(B200FMM_ERR_INVALID, "p2p variant must be 0 or 1");
   B200_CHECK(set_device(*h));

@@ -111,6 +111,7 @@ struct Context {
   Level lv[kMaxHeight];
   bool has_particles = false;
   bool packed32 = false;      // d_pq32 holds the current particles
+  bool state_zero = false;    // expansions and results are all zero (nothing ran since they were reset)
 
   // grow-only buffers of the tree build (capacities in elements)
   size_t cap_N = 0, cap_leaf = 0, cap_sort = 0, cap_cnt = 0, cap_stage = 0, cap_scan = 0;
