@@ -5,7 +5,9 @@
 // the timed CPU baseline, never part of the product path.
 //
 // What each entry point runs (paths relative to the reference project root):
-//   ref_fmm            Examples/ChebyshevInterpolationFMM.cpp:103-140 (tree insert + execute)
+//   ref_fmm            Examples/ChebyshevInterpolationFMM.cpp:103-140 (tree insert + execute); kind 0
+//                      FChebSymKernel, 1 FChebDenseKernel, 2 FUnifKernel (Lagrange, FFT-based M2L,
+//                      Src/Kernels/Uniform/FUnifKernel.hpp)
 //   ref_sym_operators  Src/Kernels/Chebyshev/FChebSymM2LHandler.hpp:303-344 (SymmetryHandler)
 //   ref_expansions     same run as ref_fmm, then FOctree::forEachCellWithLevel (FOctree.hpp:1713)
 //   ref_direct         Examples/DirectComputation.cpp:104-142 (NonMutualParticles loop)
@@ -24,6 +26,8 @@
 #include "Kernels/Chebyshev/FChebCell.hpp"
 #include "Kernels/Chebyshev/FChebSymKernel.hpp"
 #include "Kernels/Chebyshev/FChebDenseKernel.hpp"
+#include "Kernels/Uniform/FUnifCell.hpp"
+#include "Kernels/Uniform/FUnifKernel.hpp"
 #include "Kernels/Interpolation/FInterpMatrixKernel.hpp"
 #include "Kernels/P2P/FP2PParticleContainerIndexed.hpp"
 #include "Kernels/P2P/FP2PR.hpp"
@@ -62,18 +66,34 @@ struct Outputs {
   double *multipoles, *locals;  // [cap][nvals][nnodes]
 };
 
+// The Chebyshev kernels take the compression accuracy; the Lagrange kernel has no compression
+// (FUnifKernel.hpp:57-67).
+template <class KernelClass, int KIND, class MK>
+KernelClass make_kernel(int height, double width, const FPoint<double> &center, const MK *mk, double eps) {
+  if constexpr (KIND == 2) {
+    (void)eps;
+    return KernelClass(height, width, center, mk);
+  } else {
+    return KernelClass(height, width, center, mk, eps);
+  }
+}
+
 template <int ORDER, int NVALS, int KIND>
 int run_fmm(const Problem &p, Outputs &o) {
   typedef double FReal;
   constexpr int nnodes = ORDER * ORDER * ORDER;
   typedef FP2PParticleContainerIndexed<FReal, 1, 1, NVALS> ContainerClass;
   typedef FSimpleLeaf<FReal, ContainerClass> LeafClass;
-  typedef FChebCell<FReal, ORDER, 1, 1, NVALS> CellClass;
+  typedef typename std::conditional<KIND == 2, FUnifCell<FReal, ORDER, 1, 1, NVALS>,
+                                    FChebCell<FReal, ORDER, 1, 1, NVALS>>::type CellClass;
   typedef FOctree<FReal, CellClass, ContainerClass, LeafClass> OctreeClass;
   typedef FInterpMatrixKernelR<FReal> MatrixKernelClass;
   typedef typename std::conditional<
       KIND == 0, FChebSymKernel<FReal, CellClass, ContainerClass, MatrixKernelClass, ORDER, NVALS>,
-      FChebDenseKernel<FReal, CellClass, ContainerClass, MatrixKernelClass, ORDER, NVALS>>::type KernelClass;
+      typename std::conditional<KIND == 1,
+                                FChebDenseKernel<FReal, CellClass, ContainerClass, MatrixKernelClass, ORDER, NVALS>,
+                                FUnifKernel<FReal, CellClass, ContainerClass, MatrixKernelClass, ORDER, NVALS>>::type>::type
+      KernelClass;
 
   omp_set_num_threads(p.nthreads);
   const MatrixKernelClass MatrixKernel;
@@ -90,7 +110,7 @@ int run_fmm(const Problem &p, Outputs &o) {
   const double t_insert = seconds_since(t0);
 
   t0 = Clock::now();
-  KernelClass kernels(p.height, p.box_width, center, &MatrixKernel, p.eps);
+  KernelClass kernels = make_kernel<KernelClass, KIND>(p.height, p.box_width, center, &MatrixKernel, p.eps);
   const double t_kernel = seconds_since(t0);
 
   t0 = Clock::now();
@@ -147,7 +167,8 @@ int run_fmm(const Problem &p, Outputs &o) {
 
 template <int ORDER>
 int dispatch_nvals(int kind, int nvals, const Problem &p, Outputs &o) {
-  if (nvals == 1) return kind == 0 ? run_fmm<ORDER, 1, 0>(p, o) : run_fmm<ORDER, 1, 1>(p, o);
+  if (nvals == 1)
+    return kind == 0 ? run_fmm<ORDER, 1, 0>(p, o) : kind == 1 ? run_fmm<ORDER, 1, 1>(p, o) : run_fmm<ORDER, 1, 2>(p, o);
   if (nvals == 16 && kind == 0) return run_fmm<ORDER, 16, 0>(p, o);
   return -2;
 }

@@ -48,8 +48,14 @@ def fmm_cases():
         ("dense_p4_h4_n2000", O.CHEB_DENSE, 4, 4, 2000, 15, 1),
         ("dense_p5_h3_n1000", O.CHEB_DENSE, 5, 3, 1000, 16, 1),
         ("sym_p5_h4_n1500_rhs16", O.CHEB_SYM, 5, 4, 1500, 17, 16),
+        # the reference's FUnifKernel: its M2L runs in Fourier space (FFTW calls served by oracle/ref/fftw)
+        ("lagrange_p4_h4_n2000", O.LAGRANGE, 4, 4, 2000, 18, 1),
+        ("lagrange_p6_h3_n1000", O.LAGRANGE, 6, 3, 1000, 19, 1),
     ]
+    only = set(sys.argv[1:])  # optional case names: regenerate just those
     for name, kind, order, height, n, seed, nrhs in cases:
+        if only and name not in only:
+            continue
         pos, q = particles(n, seed, nrhs)
         r = O.ref_fmm(kind, order, height, 1.0, CENTER, pos[0], pos[1], pos[2], q)
         np.savez_compressed(OUT / f"fmm_{name}.npz", kind=kind, order=order, height=height, x=pos[0], y=pos[1],
@@ -75,9 +81,12 @@ def direct_case():
 if __name__ == "__main__":
     if not O.ref_available():
         sys.exit("oracle/_ref/libscalfmm_ref.so is missing: run `make -C oracle ref` where the reference exists")
-    sym_ops()
-    fmm_cases()
-    expansion_case()
-    direct_case()
+    if len(sys.argv) > 1:
+        fmm_cases()
+    else:
+        sym_ops()
+        fmm_cases()
+        expansion_case()
+        direct_case()
     for f in sorted(OUT.glob("*.npz")):
         print(f.name, f.stat().st_size)

@@ -232,6 +232,17 @@ def test_mixed_close_to_fp64(kernel):
         assert S.rel_l2(out["mixed"][k], out["fp64"][k]) < 2e-6, (k, S.rel_l2(out["mixed"][k], out["fp64"][k]))
 
 
+@pytest.mark.parametrize("name", ["lagrange_p4_h4_n2000", "lagrange_p6_h3_n1000"])
+def test_lagrange_matches_reference(golden, name):
+    """The reference's FUnifKernel (Fourier-space M2L) against the dense Lagrange M2L here: FP64 to 1e-12,
+    MIXED (tensor-core M2L, FP32 P2P) to 2e-6."""
+    g = golden(f"fmm_{name}.npz")
+    for prec, tol in (("fp64", 1e-12), ("mixed", 2e-6)):
+        r = run(g, kernel="lagrange", precision=prec)
+        for k in FIELDS:
+            assert S.rel_l2(r[k], g[k]) < tol, (prec, k, S.rel_l2(r[k], g[k]))
+
+
 def test_lagrange_fp64_matches_oracle():
     rng = np.random.default_rng(4)
     n = 2000
