@@ -278,3 +278,79 @@ def test_mixed_m2l_locals_match_fp64_dense(order, height):
     for lvl in range(2, height):
         err = S.rel_l2(loc["mixed"][lvl], loc["fp64"][lvl])
         assert err < 2e-6, (lvl, err)
+
+
+def _fp64_and_mixed(kernel, order, height, x, y, z, q, nrhs=1):
+    out = {}
+    for prec in ("fp64", "mixed"):
+        f = S.FMM(kernel, order, height, nrhs=nrhs, precision=prec)
+        if prec == "fp64":
+            out["ops"] = f.get_sym_operators() if kernel == "cheb_sym" else None
+        f.set_particles(x, y, z, q)
+        f.execute()
+        out[prec] = f.results()
+        f.close()
+    return out
+
+
+def test_ellipsoid_surface_lagrange_p6():
+    """The uneven-surface workload's shape (points on an ellipsoid surface, Lagrange order 6) on a deep tree
+    whose leaves are mostly empty: FP64 against the CPU restatement to 1e-12, MIXED against FP64 to 2e-6."""
+    from distributions import ellipsoid_surface
+
+    n, height = 12000, 6
+    x, y, z = ellipsoid_surface(n, seed=21)
+    q = np.random.default_rng(22).uniform(0.0, 1.0, n)
+    out = _fp64_and_mixed("lagrange", 6, height, x, y, z, q)
+    o = O.fmm(O.LAGRANGE, 6, height, 1.0, CENTER, x, y, z, q)
+    for k in FIELDS:
+        assert S.rel_l2(out["fp64"][k], o[k]) < 1e-12, k
+        assert S.rel_l2(out["mixed"][k], out["fp64"][k]) < 2e-6, k
+
+
+def test_plummer_cheb_sym():
+    """The batch workload's Plummer-sphere particles (strongly clustered centre): FP64 ChebSym against the
+    CPU restatement with the library's own operators to 1e-12, MIXED against FP64 to 2e-6."""
+    from distributions import plummer
+
+    n, height = 15000, 6
+    x, y, z = plummer(n, seed=23)
+    q = np.random.default_rng(24).uniform(-1.0, 1.0, n)
+    out = _fp64_and_mixed("cheb_sym", 5, height, x, y, z, q)
+    ranks, uv = out["ops"]
+    o = O.fmm(O.CHEB_SYM, 5, height, 1.0, CENTER, x, y, z, q, sym_ranks=ranks, sym_uv=uv)
+    for k in FIELDS:
+        assert S.rel_l2(out["fp64"][k], o[k]) < 1e-12, k
+    # the sym FP64 form carries the 10^-5 compression; MIXED runs the uncompressed operators
+    f = S.FMM("cheb_dense", 5, height)
+    f.set_particles(x, y, z, q)
+    f.execute()
+    dense = f.results()
+    f.close()
+    for k in FIELDS:
+        assert S.rel_l2(out["mixed"][k], dense[k]) < 2e-6, k
+
+
+def test_multi_rhs_mixed_matches_single_rhs():
+    """Sixteen charge vectors on one tree (the multi-RHS workload's shape, order 7): each RHS of the MIXED
+    multi-RHS evaluation equals a single-RHS MIXED evaluation of that charge vector (same FP32 and
+    tensor-core arithmetic per RHS; the per-level power-of-two operand scale is taken over all RHS, which
+    can only move values near the bottom of the FP16 range), to 1e-8."""
+    rng = np.random.default_rng(25)
+    n, height, nrhs = 20000, 5, 16
+    x, y, z = rng.random((3, n))
+    q = rng.uniform(-1.0, 1.0, (nrhs, n))
+    f = S.FMM("cheb_sym", 7, height, nrhs=nrhs, precision="mixed")
+    f.set_particles(x, y, z, q.ravel())
+    f.execute()
+    multi = f.results()
+    f.close()
+    for r in (0, 7, 15):
+        g = S.FMM("cheb_sym", 7, height, precision="mixed")
+        g.set_particles(x, y, z, q[r])
+        g.execute()
+        single = g.results()
+        g.close()
+        for k in FIELDS:
+            m = np.asarray(multi[k]).reshape(nrhs, n)[r]
+            assert S.rel_l2(m, single[k]) < 1e-8, (r, k)
