@@ -121,7 +121,7 @@ struct Context {
   unsigned *d_cnt = nullptr;              // radix histograms and offsets
   double *d_stage = nullptr;              // host input staged on the device
   long long *d_scan = nullptr;            // scan block sums
-  int *d_err = nullptr;                   // domain error flag
+  int *d_err = nullptr;                   // domain error flag; from byte 16 the cell count of each level
   long long *h_pinned = nullptr;          // small pinned host buffer for counts
   int tree_gen = 0;                       // bumped whenever a tree buffer moves
 

@@ -238,6 +238,19 @@ __global__ void head_flags(long long n, const unsigned long long *__restrict__ k
   flags[i] = (i == 0 || (keys[i] >> shift) != (keys[i - 1] >> shift)) ? 1 : 0;
 }
 
+// cells of every level 0..LL: one per change of the sorted particle key above that level's bits
+__global__ void level_counts_kernel(long long n, const unsigned long long *__restrict__ keys, int LL,
+                                    unsigned long long *__restrict__ counts) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  for (int l = 0; l <= LL; ++l) {
+    const int shift = 3 * (LL - l);
+    const bool head = i < n && (i == 0 || (keys[i] >> shift) != (keys[i - 1] >> shift));
+    const unsigned m = __ballot_sync(0xffffffffu, head);
+    if (lane == 0 && m) atomicAdd(counts + l, (unsigned long long)__popc(m));
+  }
+}
+
 __global__ void head_flags_i64(long long n, const long long *__restrict__ keys, long long *__restrict__ flags) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -518,7 +531,8 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
   B200_CHECK(grow(c, c.d_cnt, c.cap_cnt, (size_t)2 * RS_BINS * nb));
   B200_CHECK(grow(c, c.d_scan, c.cap_scan,
                   std::max(scan_tmp_elems<long long>(n + 1), scan_tmp_elems<unsigned>(RS_BINS * nb))));
-  if (!c.d_err) B200_CUDA(cudaMalloc(&c.d_err, sizeof(int)));
+  // the domain error flag (int) followed, 16 bytes in, by the per-level cell counts
+  if (!c.d_err) B200_CUDA(cudaMalloc(&c.d_err, 32 + sizeof(unsigned long long) * kMaxHeight));
   // inputs on the device
   const double *dx = x, *dy = y, *dz = z, *dq = q;
   if (!on_device) {
@@ -556,13 +570,16 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
   head_flags<<<grid_for(n, 256), 256, 0, s>>>(n, k0, 0, flags);
   c.tree_launches += 2;
   B200_CHECK(scan_i64(c, flags, idx, n, (long long *)c.d_scan));
-  // one synchronisation: the leaf count and the domain error flag
-  B200_CUDA(cudaMemcpyAsync(c.h_pinned, idx + n - 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
-  B200_CUDA(cudaMemcpyAsync(c.h_pinned + 1, flags + n - 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  // the cell count of every level at once, then the build's one synchronisation
+  unsigned long long *counts = (unsigned long long *)(c.d_err + 4);
+  B200_CUDA(cudaMemsetAsync(counts, 0, sizeof(unsigned long long) * kMaxHeight, s));
+  level_counts_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, k0, LL, counts);
+  ++c.tree_launches;
   B200_CUDA(cudaMemcpyAsync(c.h_pinned + 2, c.d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  B200_CUDA(cudaMemcpyAsync(c.h_pinned + 8, counts, sizeof(long long) * (LL + 1), cudaMemcpyDeviceToHost, s));
   B200_CUDA(cudaStreamSynchronize(s));
   if ((int)c.h_pinned[2]) return fail(B200FMM_ERR_DOMAIN, "a particle lies outside the box or has a non-finite coordinate");
-  const long long nleaves = c.h_pinned[0] + c.h_pinned[1];
+  const long long nleaves = c.h_pinned[8 + LL];
   Level &leaf = c.lv[LL];
   B200_CHECK(level_storage(c, leaf, nleaves));
   {
@@ -588,10 +605,7 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
     head_flags_i64<<<grid_for(nc, 256), 256, 0, s>>>(nc, ch.keys, flags);
     ++c.tree_launches;
     B200_CHECK(scan_i64(c, flags, idx, nc, (long long *)c.d_scan));
-    B200_CUDA(cudaMemcpyAsync(c.h_pinned + 4, idx + nc - 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
-    B200_CUDA(cudaMemcpyAsync(c.h_pinned + 5, flags + nc - 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
-    B200_CUDA(cudaStreamSynchronize(s));
-    B200_CHECK(level_storage(c, pa, c.h_pinned[4] + c.h_pinned[5]));
+    B200_CHECK(level_storage(c, pa, c.h_pinned[8 + l]));  // counted before the synchronisation
     fill_int<<<grid_for(pa.n * 8, 256), 256, 0, s>>>(pa.n * 8, pa.child, -1);
     compact_parents<<<grid_for(nc, 256), 256, 0, s>>>(nc, ch.keys, flags, idx, pa.keys, ch.parent, pa.child);
     c.tree_launches += 2;
