@@ -105,7 +105,10 @@ B200FMM_API b200fmm_status b200fmm_set_particles(b200fmm_handle h, long long n, 
 B200FMM_API b200fmm_status b200fmm_set_charges(b200fmm_handle h, const double *q, int on_device);
 
 /* Whole evaluation (FFmmAlgorithmThread::executeCore, FFmmAlgorithmThread.hpp:118-159): zeroes the
- * expansions and results, then runs the passes selected by ops. */
+ * expansions and results, then runs the passes selected by ops.  The second execute() with the same ops on
+ * one tree (after set_charges(), say) captures the passes into a CUDA graph, and later ones replay it with
+ * a single launch; set_particles() drops it.  Environment B200FMM_GRAPHS=0 keeps every call on plain
+ * launches.  A stream that the caller is capturing always gets plain launches. */
 B200FMM_API b200fmm_status b200fmm_execute(b200fmm_handle h, unsigned ops);
 
 /* Level-batched operators (FAbstractKernels).  They accumulate (+=) like the reference kernels.
@@ -137,10 +140,12 @@ B200FMM_API b200fmm_status b200fmm_get_cells(b200fmm_handle h, int level, long l
 B200FMM_API b200fmm_status b200fmm_get_permutation(b200fmm_handle h, long long *perm);
 
 /* Device time of the passes of the last execute(), milliseconds:
- * [0] tree build (last set_particles), [1] P2M, [2] M2M, [3] M2L, [4] L2L, [5] L2P, [6] P2P, [7] total. */
+ * [0] tree build (last set_particles), [1] P2M, [2] M2M, [3] M2L, [4] L2L, [5] L2P, [6] P2P, [7] total.
+ * After an execute() that replayed a CUDA graph only [0] and [7] are measured; [1]..[6] are 0. */
 B200FMM_API b200fmm_status b200fmm_last_timings(b200fmm_handle h, double *ms8);
 /* Device time of single kernels of the last execute(), milliseconds: [0] the M2L kernel (the tensor-core
- * kernel alone in MIXED, the whole M2L pass in FP64), [1] the P2P kernel, [2] P2M, [3] L2P. */
+ * kernel alone in MIXED, the whole M2L pass in FP64), [1] the P2P kernel, [2] P2M, [3] L2P (all 0 after a
+ * graph replay). */
 B200FMM_API b200fmm_status b200fmm_last_kernel_times(b200fmm_handle h, double *ms4);
 /* Work counts of the current tree: M2L (target, source) pairs over levels 2..height-1 and ordered P2P
  * particle pairs (i != j) over each leaf and its neighbours. */

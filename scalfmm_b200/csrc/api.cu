@@ -6,6 +6,7 @@
 #include "common.cuh"
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 
@@ -110,8 +111,14 @@ b200fmm_status zero_state(Context &c) {
 }
 
 b200fmm_status record(Context &c, int k) {
-  B200_CUDA(cudaEventRecord(c.ev[k], c.stream));
+  B200_CUDA(record_event(c, k));
   return B200FMM_OK;
+}
+
+void drop_graph(Context &c) {
+  if (c.graph) cudaGraphExecDestroy(c.graph);
+  c.graph = nullptr;
+  c.graph_serial = -1;
 }
 
 b200fmm_status run_m2l(Context &c, int level) {
@@ -122,6 +129,7 @@ b200fmm_status run_m2l(Context &c, int level) {
 void destroy_context(b200fmm_context *c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  drop_graph(*c);
   free_tree(*c);
   tc_free(*c);
   for (void *p : {(void *)c->d_roots, (void *)c->d_Troots, (void *)c->d_S, (void *)c->d_pindices, (void *)c->d_pvec,
@@ -220,6 +228,8 @@ b200fmm_status b200fmm_set_sym_operators(b200fmm_handle h, const int *ranks, con
   Context &c = *h;
   if (c.cfg.kernel != B200FMM_CHEB_SYM || c.cfg.precision != B200FMM_FP64)
     return fail(B200FMM_ERR_STATE, "symmetric operators apply to the FP64 CHEB_SYM kernel only");
+  drop_graph(c);  // a captured execute() holds the old operator buffers
+  c.eager_serial = -1;
   if (!ranks || !uv) return fail(B200FMM_ERR_INVALID, "null argument");
   long long need = 0;
   int nclass = 0;
@@ -259,6 +269,8 @@ b200fmm_status b200fmm_set_particles(b200fmm_handle h, long long n, const double
   B200_CHECK(set_device(c));
   c.has_particles = false;
   c.N = n;
+  ++c.tree_serial;
+  drop_graph(c);
   B200_CUDA(cudaEventRecord(c.ev[14], c.stream));
   b200fmm_status st = build_tree(c, x, y, z, q, on_device != 0);
   if (st != B200FMM_OK) return st;
@@ -302,15 +314,13 @@ b200fmm_status b200fmm_zero_results(b200fmm_handle h) {
   return B200FMM_OK;
 }
 
-b200fmm_status b200fmm_execute(b200fmm_handle h, unsigned ops) {
-  B200_CHECK(check_handle(h));
-  Context &c = *h;
-  B200_CHECK(need_particles(c));
-  B200_CHECK(set_device(c));
+// The passes of execute(), in the reference's order (FFmmAlgorithmThread::executeCore).
+static b200fmm_status execute_body(Context &c, unsigned ops) {
   c.launches = 0;
   const int LL = c.H - 1;
   B200_CHECK(record(c, 0));
-  if (!c.state_zero) B200_CHECK(zero_state(c));  // skipped right after set_particles, which zeroed them
+  // skipped right after set_particles, which zeroed them; always part of a captured graph
+  if (!c.state_zero || c.capturing) B200_CHECK(zero_state(c));
   c.state_zero = false;
   B200_CHECK(record(c, 1));
   if (ops & B200FMM_P2M) B200_CHECK(run_p2m(c));
@@ -332,6 +342,70 @@ b200fmm_status b200fmm_execute(b200fmm_handle h, unsigned ops) {
   B200_CHECK(record(c, 6));
   if (ops & B200FMM_P2P) B200_CHECK(run_p2p(c, 0));
   B200_CHECK(record(c, 7));
+  return B200FMM_OK;
+}
+
+static bool graphs_enabled() {
+  const char *e = std::getenv("B200FMM_GRAPHS");
+  return !(e && e[0] == '0');
+}
+
+// Capture execute_body into c.graph.  On any failure the capture is discarded, the error cleared and the
+// tree stays on the eager path.
+static void capture_graph(Context &c, unsigned ops) {
+  drop_graph(c);
+  c.packed32 = false;  // the graph repacks the FP32 near-field copies, which carry the charges
+  if (cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    c.eager_ops = ~0u;
+    return;
+  }
+  c.capturing = true;
+  const b200fmm_status st = execute_body(c, ops);
+  c.capturing = false;
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(c.stream, &g);
+  cudaGraphExec_t x = nullptr;
+  if (st == B200FMM_OK && e == cudaSuccess && g && cudaGraphInstantiate(&x, g, 0) == cudaSuccess) {
+    c.graph = x;
+    c.graph_serial = c.tree_serial;
+    c.graph_ops = ops;
+    c.graph_launches = c.launches;
+  } else {
+    c.eager_ops = ~0u;  // not again for this tree
+  }
+  if (g) cudaGraphDestroy(g);
+  cudaGetLastError();
+}
+
+b200fmm_status b200fmm_execute(b200fmm_handle h, unsigned ops) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  B200_CHECK(need_particles(c));
+  B200_CHECK(set_device(c));
+  // a caller that is itself capturing this stream gets the plain launches in its own graph
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  B200_CUDA(cudaStreamIsCapturing(c.stream, &cs));
+  if (graphs_enabled() && cs == cudaStreamCaptureStatusNone && c.eager_serial == c.tree_serial &&
+      c.eager_ops == ops) {
+    if (!c.graph || c.graph_serial != c.tree_serial || c.graph_ops != ops) capture_graph(c, ops);
+    if (c.graph) {
+      B200_CUDA(cudaEventRecord(c.ev[0], c.stream));
+      B200_CUDA(cudaGraphLaunch(c.graph, c.stream));
+      B200_CUDA(cudaEventRecord(c.ev[7], c.stream));
+      c.packed32 = true;
+      c.state_zero = false;
+      c.last_was_graph = true;
+      c.launches = c.graph_launches;
+      return B200FMM_OK;
+    }
+  }
+  c.last_was_graph = false;
+  B200_CHECK(execute_body(c, ops));
+  if (c.eager_ops != ~0u || c.eager_serial != c.tree_serial) {
+    c.eager_serial = c.tree_serial;
+    c.eager_ops = ops;
+  }
   return B200FMM_OK;
 }
 
@@ -469,7 +543,7 @@ b200fmm_status b200fmm_last_timings(b200fmm_handle h, double *ms8) {
   ms8[0] = c.ms[0];
   for (int k = 1; k <= 6; ++k) {
     float t = 0;
-    if (cudaEventElapsedTime(&t, c.ev[k], c.ev[k + 1]) != cudaSuccess) t = 0;
+    if (c.last_was_graph || cudaEventElapsedTime(&t, c.ev[k], c.ev[k + 1]) != cudaSuccess) t = 0;
     ms8[k] = t;
   }
   float tot = 0;
@@ -484,6 +558,10 @@ b200fmm_status b200fmm_last_kernel_times(b200fmm_handle h, double *ms4) {
   if (!ms4) return fail(B200FMM_ERR_INVALID, "null argument");
   B200_CHECK(set_device(c));
   B200_CUDA(cudaEventSynchronize(c.ev[7]));
+  if (c.last_was_graph) {
+    for (int k = 0; k < 4; ++k) ms4[k] = 0;
+    return B200FMM_OK;
+  }
   float t = 0;
   if (c.cfg.precision == B200FMM_MIXED && cudaEventElapsedTime(&t, c.ev[8], c.ev[9]) == cudaSuccess)
     ms4[0] = t;

@@ -112,6 +112,16 @@ struct Context {
   bool has_particles = false;
   bool packed32 = false;      // d_pq32 holds the current particles
   bool state_zero = false;    // expansions and results are all zero (nothing ran since they were reset)
+  // CUDA graph of execute(): captured on the second execute() of one tree with the same operations and
+  // replayed from then on (set_charges() keeps the tree; set_particles() starts a new one)
+  long long tree_serial = 0;              // bumped by every set_particles()
+  long long column_serial = -1;           // tree whose leaves are in the FP32 P2P column order
+  long long eager_serial = -1, graph_serial = -1;
+  unsigned eager_ops = 0, graph_ops = 0;
+  cudaGraphExec_t graph = nullptr;
+  long long graph_launches = 0;           // kernels in the graph
+  bool capturing = false;                 // inside the capture: no timing events
+  bool last_was_graph = false;            // the last execute() replayed the graph (only its total is timed)
 
   // grow-only buffers of the tree build (capacities in elements)
   size_t cap_N = 0, cap_leaf = 0, cap_sort = 0, cap_cnt = 0, cap_stage = 0, cap_scan = 0;
@@ -214,6 +224,11 @@ __device__ inline int find_key(const long long *keys, long long n, long long key
       hi = mid;
   }
   return (lo < n && keys[lo] == key) ? (int)lo : -1;
+}
+
+// Timing event k on the handle's stream, except while execute() is being captured into a CUDA graph.
+inline cudaError_t record_event(Context &c, int k) {
+  return c.capturing ? cudaSuccess : cudaEventRecord(c.ev[k], c.stream);
 }
 
 inline unsigned grid_for(long long n, int block) {

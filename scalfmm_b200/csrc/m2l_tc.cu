@@ -685,7 +685,7 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
   if (P.nitems <= 0) return B200FMM_OK;
   const size_t smem = (size_t)t->stages * t->stage_bytes + 1024;
   const int grid = std::min(t->grid, P.nitems);
-  B200_CUDA(cudaEventRecord(c.ev[8], c.stream));
+  B200_CUDA(record_event(c, 8));
   switch (t->NP) {
 #define B200_TC_CASE(NPV, CWV, NHV)                                                                              \
   case NPV:                                                                                                        \
@@ -701,7 +701,7 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
     default:
       return fail(B200FMM_ERR_UNSUPPORTED, "no tensor-core M2L instance for this order");
   }
-  B200_CUDA(cudaEventRecord(c.ev[9], c.stream));
+  B200_CUDA(record_event(c, 9));
   ++c.launches;
   B200_CUDA(cudaGetLastError());
   return B200FMM_OK;

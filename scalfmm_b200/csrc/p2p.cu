@@ -342,9 +342,19 @@ __global__ void __launch_bounds__(P2P32_WARPS * 32, 6) p2p_fp32_kernel(
           for (int k = g; k < cn; k += G)
             p2p_record<true>(s, k, self_rel, th_x, th_y, th_z, tl_x, tl_y, tl_z, pv, ax, ay, az);
         } else {
-#pragma unroll 4
-          for (int k = g; k < cn; k += G)
+          // two independent accumulator sets, so that consecutive records do not wait on each other's sums
+          float2 pv2 = make_float2(0.f, 0.f), ax2 = pv2, ay2 = pv2, az2 = pv2;
+          int k = g;
+#pragma unroll 2
+          for (; k + G < cn; k += 2 * G) {
             p2p_record<false>(s, k, 0, th_x, th_y, th_z, tl_x, tl_y, tl_z, pv, ax, ay, az);
+            p2p_record<false>(s, k + G, 0, th_x, th_y, th_z, tl_x, tl_y, tl_z, pv2, ax2, ay2, az2);
+          }
+          if (k < cn) p2p_record<false>(s, k, 0, th_x, th_y, th_z, tl_x, tl_y, tl_z, pv, ax, ay, az);
+          pv = __fadd2_rn(pv, pv2);
+          ax = __fadd2_rn(ax, ax2);
+          ay = __fadd2_rn(ay, ay2);
+          az = __fadd2_rn(az, az2);
         }
         two_sum(ph_hi, ph_lo, pv.x + pv.y);
         two_sum(gx_hi, gx_lo, ax.x + ax.y);
@@ -395,7 +405,10 @@ b200fmm_status run_p2p(Context &c, int variant) {
     float4 *hi = c.d_pq32, *lo = c.d_pq32 + c.N * c.R, *src = c.d_pq32 + c.N * (c.R + 1);
     if (!c.packed32) {
       c.packed32 = true;
-      B200_CHECK(leaf_column_order(c));
+      if (c.column_serial != c.tree_serial) {
+        B200_CHECK(leaf_column_order(c));
+        c.column_serial = c.tree_serial;
+      }
       const double W = c.cfg.box_width;
       pack_records32<<<(unsigned)L.n, 64, 0, c.stream>>>(c.N, c.R, c.d_leaf_start, c.d_leaf_rank, c.d_rec_base, c.d_x,
                                                          c.d_y, c.d_z, c.d_q, c.cfg.center[0] - W / 2,
@@ -404,18 +417,18 @@ b200fmm_status run_p2p(Context &c, int variant) {
     }
     int *status = c.d_status;
     const unsigned blocks = grid_for(L.n, P2P32_WARPS);
-    B200_CUDA(cudaEventRecord(c.ev[10], c.stream));
+    B200_CUDA(record_event(c, 10));
     p2p_fp32_kernel<<<blocks, P2P32_WARPS * 32, 0, c.stream>>>(c.R, c.N, L.n, c.d_leaf_start, c.d_leaf_nbr, variant,
                                                                c.d_leaf_rank, c.d_rec_base, hi, lo, src, c.d_phi,
                                                                c.d_fx, c.d_fy, c.d_fz, status);
-    B200_CUDA(cudaEventRecord(c.ev[11], c.stream));
+    B200_CUDA(record_event(c, 11));
     ++c.launches;
   } else {
-    B200_CUDA(cudaEventRecord(c.ev[10], c.stream));
+    B200_CUDA(record_event(c, 10));
     p2p_fp64_kernel<<<(unsigned)L.n, P2P64_THREADS, 0, c.stream>>>(c.R, c.N, c.d_leaf_start, c.d_leaf_nbr, variant,
                                                                    c.d_x, c.d_y, c.d_z, c.d_q, c.d_phi, c.d_fx,
                                                                    c.d_fy, c.d_fz);
-    B200_CUDA(cudaEventRecord(c.ev[11], c.stream));
+    B200_CUDA(record_event(c, 11));
     ++c.launches;
   }
   B200_CUDA(cudaGetLastError());

@@ -354,3 +354,37 @@ def test_multi_rhs_mixed_matches_single_rhs():
         for k in FIELDS:
             m = np.asarray(multi[k]).reshape(nrhs, n)[r]
             assert S.rel_l2(m, single[k]) < 1e-8, (r, k)
+
+
+@pytest.mark.parametrize("kernel,precision", [("cheb_sym", "fp64"), ("cheb_sym", "mixed"), ("lagrange", "mixed")])
+def test_repeated_execute_replays_a_graph(kernel, precision):
+    """New charges on one tree (an iterative solver's pattern): the second execute() captures the passes into
+    a CUDA graph and later ones replay it.  Each replay must equal a fresh handle's plain evaluation of the
+    same charges (1e-12: only the order of FP64 atomic additions may differ), and only the total time is
+    reported for a replay."""
+    rng = np.random.default_rng(31)
+    n, order, height = 6000, 5, 5
+    x, y, z = rng.random((3, n))
+    qs = [rng.uniform(-1, 1, n) for _ in range(4)]
+    f = S.FMM(kernel, order, height, precision=precision)
+    f.set_particles(x, y, z, qs[0])
+    f.execute()
+    assert f.timings()["p2m"] > 0  # plain launches: per-pass times
+    for q in qs[1:]:
+        f.set_charges(q)
+        f.execute()
+        got = f.results()
+        t = f.timings()
+        assert t["p2m"] == 0 and t["total"] > 0
+        g = S.FMM(kernel, order, height, precision=precision)
+        g.set_particles(x, y, z, q)
+        g.execute()
+        want = g.results()
+        g.close()
+        for k in FIELDS:
+            assert S.rel_l2(got[k], want[k]) < 1e-12, k
+    # a new tree goes back to plain launches
+    f.set_particles(y, z, x, qs[0])
+    f.execute()
+    assert f.timings()["p2m"] > 0
+    f.close()
