@@ -17,24 +17,30 @@ namespace {
 
 
 // S_j(x) and dS_j/dx for j < p.  Chebyshev: 1/p + 2/p sum_o T_o(x) T_o(xbar_j), dT_o = o U_{o-1}.
-template <int P>
-__device__ __forceinline__ void basis_eval(int kernel, double x, const double *__restrict__ roots,
+// Lagrange (equispaced nodes): prod_{m != j} (x - x_m) / (x_j - x_m) and its derivative.  Compile-time order
+// and basis, every loop unrolled, so that S and dS stay in registers.
+template <int P, bool LAGR>
+__device__ __forceinline__ void basis_eval(double x, const double *__restrict__ roots,
                                            const double *__restrict__ Tr, double *S, double *dS) {
   constexpr int p = P;
-  if (kernel == B200FMM_LAGRANGE) {
+  if constexpr (LAGR) {
     if (x > 1.0) x = 1.0;
     if (x < -1.0) x = -1.0;
+#pragma unroll
     for (int j = 0; j < p; ++j) {
       double num = 1.0, den = 1.0, dsum = 0.0;
+#pragma unroll
       for (int m = 0; m < p; ++m) {
         if (m == j) continue;
         den *= roots[j] - roots[m];
         num *= x - roots[m];
       }
       if (dS) {
+#pragma unroll
         for (int k = 0; k < p; ++k) {
           if (k == j) continue;
           double t = 1.0;
+#pragma unroll
           for (int m = 0; m < p; ++m)
             if (m != j && m != k) t *= x - roots[m];
           dsum += t;
@@ -43,133 +49,153 @@ __device__ __forceinline__ void basis_eval(int kernel, double x, const double *_
       }
       S[j] = num / den;
     }
-    return;
-  }
-  double T[P], U[P];
-  T[0] = 1.0;
-  T[1] = x;
-  U[0] = 1.0;
-  U[1] = 2.0 * x;
+  } else {
+    double T[P], U[P];
+    T[0] = 1.0;
+    T[1] = x;
+    U[0] = 1.0;
+    U[1] = 2.0 * x;
 #pragma unroll
-  for (int o = 2; o < p; ++o) {
-    T[o] = 2.0 * x * T[o - 1] - T[o - 2];
-    U[o] = 2.0 * x * U[o - 1] - U[o - 2];
-  }
-  const double ip = 1.0 / p;
-#pragma unroll
-  for (int j = 0; j < p; ++j) {
-    double s = ip, ds = 0.0;
-#pragma unroll
-    for (int o = 1; o < p; ++o) {
-      const double t = 2.0 * ip * Tr[o * p + j];
-      s += T[o] * t;
-      ds += (double)o * U[o - 1] * t;
+    for (int o = 2; o < p; ++o) {
+      T[o] = 2.0 * x * T[o - 1] - T[o - 2];
+      U[o] = 2.0 * x * U[o - 1] - U[o - 2];
     }
-    S[j] = s;
-    if (dS) dS[j] = ds;
+    const double ip = 1.0 / p;
+#pragma unroll
+    for (int j = 0; j < p; ++j) {
+      double s = ip, ds = 0.0;
+#pragma unroll
+      for (int o = 1; o < p; ++o) {
+        const double t = 2.0 * ip * Tr[o * p + j];
+        s += T[o] * t;
+        ds += (double)o * U[o - 1] * t;
+      }
+      S[j] = s;
+      if (dS) dS[j] = ds;
+    }
   }
 }
 
-// ---- P2M: one warp per leaf ------------------------------------------------------------------------
-// The lanes first evaluate the 1-D weights of 32 particles (one particle each) into shared memory; then each
-// lane owns nodes n = lane, lane+32, ... and sums q * wx * wy * wz over those particles.
-constexpr int LEAF_WARPS = 4;
+// ---- P2M: one 64-thread block per leaf -------------------------------------------------------------
+// M[nx,ny,nz] = sum_j q_j Sx_j[nx] Sy_j[ny] Sz_j[nz].  The threads first evaluate the 1-D weights of up to 64
+// particles (one each) into shared memory; then thread t < p^2 owns the node line (ny, nz) = (t % p, t / p)
+// and keeps its p sums over nx in registers: per particle one product q Sy Sz and p FMAs with the
+// broadcast Sx row, instead of three shared-memory reads per node and particle.
+constexpr int P2M_THREADS = 64;
+constexpr int LEAF_WARPS = 4;  // L2P: leaves per CTA, one warp each
 
-template <int P>
-__global__ void __launch_bounds__(LEAF_WARPS * 32) p2m_kernel(
-    int kernel, int R, long long N, long long nleaves, const long long *__restrict__ keys,
+template <int P, bool LAGR>
+__global__ void __launch_bounds__(P2M_THREADS, 8) p2m_kernel(
+    int R, long long N, long long nleaves, const long long *__restrict__ keys,
     const long long *__restrict__ leaf_start, const double *__restrict__ x, const double *__restrict__ y,
     const double *__restrict__ z, const double *__restrict__ q, double cx0, double cy0, double cz0, double leaf_w,
     const double *__restrict__ roots, const double *__restrict__ Tr, double *__restrict__ M) {
-  constexpr int p = P, nn = P * P * P, NK = (nn + 31) / 32;
-  __shared__ double W[LEAF_WARPS][32][3][P];
-  __shared__ double Q[LEAF_WARPS][32];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long long leaf = (long long)blockIdx.x * LEAF_WARPS + w;
-  if (leaf >= nleaves) return;
+  constexpr int p = P, nn = P * P * P, PX = (P + 1) & ~1;  // Sx rows padded to 16 bytes
+  __shared__ __align__(16) double Wx[P2M_THREADS][PX];
+  __shared__ double Wy[P2M_THREADS][P], Wz[P2M_THREADS][P], Q[P2M_THREADS];
+  const int t = threadIdx.x;
+  const long long leaf = blockIdx.x;
   int ix, iy, iz;
   morton_decode3(keys[leaf], ix, iy, iz);
   const double ctr[3] = {cx0 + (ix + 0.5) * leaf_w, cy0 + (iy + 0.5) * leaf_w, cz0 + (iz + 0.5) * leaf_w};
   const long long s0 = leaf_start[leaf], s1 = leaf_start[leaf + 1];
+  const int ny = t % p, nz = t / p;
+  const bool owner = t < p * p;
   for (int r = 0; r < R; ++r) {
-    double acc[NK];
+    double acc[P];
 #pragma unroll
-    for (int k = 0; k < NK; ++k) acc[k] = 0.0;
-    for (long long b = s0; b < s1; b += 32) {
-      const int cnt = (int)min((long long)32, s1 - b);
-      __syncwarp();
-      if (lane < cnt) {
-        const long long i = b + lane;
+    for (int k = 0; k < p; ++k) acc[k] = 0.0;
+    for (long long b = s0; b < s1; b += P2M_THREADS) {
+      const int cnt = (int)min((long long)P2M_THREADS, s1 - b);
+      __syncthreads();
+      if (t < cnt) {
+        const long long i = b + t;
         const double pos[3] = {x[i], y[i], z[i]};
+        double wv[P];
+#pragma unroll
         for (int d = 0; d < 3; ++d) {
           const double a = ctr[d] - leaf_w / 2, bb = ctr[d] + leaf_w / 2;
-          double wv[P];
-          basis_eval<P>(kernel, (2.0 * pos[d] - bb - a) / (bb - a), roots, Tr, wv, nullptr);
+          basis_eval<P, LAGR>((2.0 * pos[d] - bb - a) / (bb - a), roots, Tr, wv, nullptr);
+          double *dst = d == 0 ? Wx[t] : (d == 1 ? Wy[t] : Wz[t]);
 #pragma unroll
-          for (int k = 0; k < p; ++k) W[w][lane][d][k] = wv[k];
+          for (int k = 0; k < p; ++k) dst[k] = wv[k];
         }
-        Q[w][lane] = q[(long long)r * N + i];
+        Q[t] = q[(long long)r * N + i];
       }
-      __syncwarp();
+      __syncthreads();
+      if (owner) {
+        for (int j = 0; j < cnt; ++j) {
+          const double w = Q[j] * Wy[j][ny] * Wz[j][nz];
 #pragma unroll
-      for (int k = 0; k < NK; ++k) {
-        const int n = lane + 32 * k;
-        if (n < nn) {
-          const int nx = n % p, ny = (n / p) % p, nz = n / (p * p);
-          double a = acc[k];
-          for (int j = 0; j < cnt; ++j) a += Q[w][j] * W[w][j][0][nx] * W[w][j][1][ny] * W[w][j][2][nz];
-          acc[k] = a;
+          for (int k = 0; k < p; ++k) acc[k] += w * Wx[j][k];
         }
       }
     }
+    if (owner) {
+      double *out = M + (leaf * R + r) * nn + (nz * p + ny) * p;
 #pragma unroll
-    for (int k = 0; k < NK; ++k) {
-      const int n = lane + 32 * k;
-      if (n < nn) M[(leaf * R + r) * nn + n] += acc[k];
+      for (int k = 0; k < p; ++k) out[k] += acc[k];
     }
   }
 }
 
 // ---- M2M / L2L: one warp per child ------------------------------------------------------------------
 // Each warp applies the child's three 1-D interpolators, one axis at a time, in its own shared-memory
-// buffers.  M2M: the 8 children's contributions to the parent are then added in child order (deterministic).
-__device__ inline void warp_contract(int p, int d, const double *__restrict__ A, const double *in, double *out,
-                                     bool transpose, int lane) {
-  const int nn = p * p * p;
+// buffers.  A lane owns whole lines along the axis: it loads the line's p values into registers and writes
+// the p results, with the p x p interpolator in registers.  M2M: the 8 children's contributions to the
+// parent are then added in child order (deterministic).
+template <int P, bool TRANSPOSE>
+__device__ __forceinline__ void warp_lines(const double *__restrict__ A, int d, const double *in, double *out,
+                                           int lane) {
+  constexpr int p = P, nl = P * P;
+  double a[P][P];
+#pragma unroll
+  for (int i = 0; i < p; ++i)
+#pragma unroll
+    for (int m = 0; m < p; ++m) a[i][m] = TRANSPOSE ? A[m * p + i] : A[i * p + m];
   const int stride = d == 0 ? 1 : (d == 1 ? p : p * p);
-  for (int e = lane; e < nn; e += 32) {
-    const int nd = (e / stride) % p;
-    const int base = e - nd * stride;
-    double s = 0.0;
-    for (int m = 0; m < p; ++m) s += (transpose ? A[m * p + nd] : A[nd * p + m]) * in[base + m * stride];
-    out[e] = s;
+  for (int l = lane; l < nl; l += 32) {
+    // first element of line l: the two other indices of the line, in increasing axis order
+    const int base = d == 0 ? l * p : (d == 1 ? (l % p) + (l / p) * p * p : l);
+    double v[P];
+#pragma unroll
+    for (int m = 0; m < p; ++m) v[m] = in[base + m * stride];
+#pragma unroll
+    for (int i = 0; i < p; ++i) {
+      double s = 0.0;
+#pragma unroll
+      for (int m = 0; m < p; ++m) s += a[i][m] * v[m];
+      out[base + i * stride] = s;
+    }
   }
 }
 
-__global__ void __launch_bounds__(256) m2m_kernel(int p, int R, long long nparents, const int *__restrict__ child,
+template <int P>
+__global__ void __launch_bounds__(256) m2m_kernel(int R, long long nparents, const int *__restrict__ child,
                                                   const double *__restrict__ S, const double *__restrict__ Mc,
                                                   double *__restrict__ Mp) {
+  constexpr int p = P, nn = P * P * P;
   extern __shared__ double sh[];
-  const int nn = p * p * p;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double *b0 = sh + (size_t)w * 2 * nn, *b1 = b0 + nn;  // per-warp buffers; b0 ends with the contribution
+  double *b0 = sh + (size_t)w * 2 * nn, *b1 = b0 + nn;  // per-warp buffers; b1 ends with the contribution
   const long long pc = blockIdx.x;
   const int ci = child[pc * 8 + w];
   for (int r = 0; r < R; ++r) {
     if (ci >= 0) {
       for (int e = lane; e < nn; e += 32) b0[e] = Mc[((long long)ci * R + r) * nn + e];
       __syncwarp();
-      warp_contract(p, 0, S + (w * 3 + 0) * p * p, b0, b1, false, lane);
+      warp_lines<P, false>(S + (w * 3 + 0) * p * p, 0, b0, b1, lane);
       __syncwarp();
-      warp_contract(p, 1, S + (w * 3 + 1) * p * p, b1, b0, false, lane);
+      warp_lines<P, false>(S + (w * 3 + 1) * p * p, 1, b1, b0, lane);
       __syncwarp();
-      warp_contract(p, 2, S + (w * 3 + 2) * p * p, b0, b1, false, lane);
+      warp_lines<P, false>(S + (w * 3 + 2) * p * p, 2, b0, b1, lane);
     } else {
       for (int e = lane; e < nn; e += 32) b1[e] = 0.0;
     }
     __syncthreads();
     for (int e = threadIdx.x; e < nn; e += blockDim.x) {
       double s = 0.0;
+#pragma unroll
       for (int k = 0; k < 8; ++k) s += sh[(size_t)k * 2 * nn + nn + e];
       Mp[(pc * R + r) * nn + e] += s;
     }
@@ -177,13 +203,14 @@ __global__ void __launch_bounds__(256) m2m_kernel(int p, int R, long long nparen
   }
 }
 
-__global__ void __launch_bounds__(256) l2l_kernel(int p, int R, long long nparents, const int *__restrict__ child,
+template <int P>
+__global__ void __launch_bounds__(256) l2l_kernel(int R, long long nparents, const int *__restrict__ child,
                                                   const double *__restrict__ S, const double *__restrict__ Lp,
                                                   double *__restrict__ Lc) {
+  constexpr int p = P, nn = P * P * P;
   extern __shared__ double sh[];
-  const int nn = p * p * p;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double *par = sh;                                   // parent local
+  double *par = sh;  // parent local
   double *b0 = sh + nn + (size_t)w * 2 * nn, *b1 = b0 + nn;
   const long long pc = blockIdx.x;
   const int ci = child[pc * 8 + w];
@@ -192,37 +219,38 @@ __global__ void __launch_bounds__(256) l2l_kernel(int p, int R, long long nparen
     for (int e = threadIdx.x; e < nn; e += blockDim.x) par[e] = Lp[(pc * R + r) * nn + e];
     __syncthreads();
     if (ci < 0) continue;
-    warp_contract(p, 0, S + (w * 3 + 0) * p * p, par, b0, true, lane);
+    warp_lines<P, true>(S + (w * 3 + 0) * p * p, 0, par, b0, lane);
     __syncwarp();
-    warp_contract(p, 1, S + (w * 3 + 1) * p * p, b0, b1, true, lane);
+    warp_lines<P, true>(S + (w * 3 + 1) * p * p, 1, b0, b1, lane);
     __syncwarp();
-    const double *A = S + (w * 3 + 2) * p * p;
-    for (int e = lane; e < nn; e += 32) {
-      const int nz = e / (p * p), base = e - nz * p * p;
-      double s = 0.0;
-      for (int m = 0; m < p; ++m) s += A[m * p + nz] * b1[base + m * p * p];
-      Lc[((long long)ci * R + r) * nn + e] += s;
-    }
+    warp_lines<P, true>(S + (w * 3 + 2) * p * p, 2, b1, b0, lane);
+    __syncwarp();
+    double *out = Lc + ((long long)ci * R + r) * nn;
+    for (int e = lane; e < nn; e += 32) out[e] += b0[e];
   }
 }
 
 // ---- L2P: one warp per leaf, one particle per lane ----------------------------------------------------
-template <int P>
-__global__ void __launch_bounds__(LEAF_WARPS * 32) l2p_kernel(
-    int kernel, int R, long long N, long long nleaves, const long long *__restrict__ keys,
+// The leaf's local expansion sits in shared memory; each lane contracts it with its particle's weights one
+// axis at a time (x in registers, then y, then z whose weights sit in the lane's shared-memory row).
+template <int P, bool LAGR>
+__global__ void __launch_bounds__(LEAF_WARPS * 32, 3) l2p_kernel(
+    int R, long long N, long long nleaves, const long long *__restrict__ keys,
     const long long *__restrict__ leaf_start, const double *__restrict__ x, const double *__restrict__ y,
     const double *__restrict__ z, const double *__restrict__ q, double cx0, double cy0, double cz0, double leaf_w,
     const double *__restrict__ roots, const double *__restrict__ Tr, const double *__restrict__ L,
     double *__restrict__ phi, double *__restrict__ fx, double *__restrict__ fy, double *__restrict__ fz) {
   constexpr int p = P, nn = P * P * P;
   __shared__ double sL[LEAF_WARPS][nn];
+  __shared__ double sWz[LEAF_WARPS][32][2 * P + 1];  // z weights and derivatives of each lane's particle
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long leaf = (long long)blockIdx.x * LEAF_WARPS + w;
   if (leaf >= nleaves) return;
   double *Lw = sL[w];
+  double *wz = sWz[w][lane], *dwz = wz + P;
   int ix, iy, iz;
   morton_decode3(keys[leaf], ix, iy, iz);
-  const double ctr[3] = {cx0 + (ix + 0.5) * leaf_w, cy0 + (iy + 0.5) * leaf_w, cz0 + (iz + 0.5) * leaf_w};
+  const double cx = cx0 + (ix + 0.5) * leaf_w, cy = cy0 + (iy + 0.5) * leaf_w, cz = cz0 + (iz + 0.5) * leaf_w;
   const double jac = 2.0 / leaf_w;
   const long long s0 = leaf_start[leaf], s1 = leaf_start[leaf + 1];
   for (int r = 0; r < R; ++r) {
@@ -230,12 +258,17 @@ __global__ void __launch_bounds__(LEAF_WARPS * 32) l2p_kernel(
     for (int e = lane; e < nn; e += 32) Lw[e] = L[(leaf * R + r) * nn + e];
     __syncwarp();
     for (long long i = s0 + lane; i < s1; i += 32) {
-      const double pos[3] = {x[i], y[i], z[i]};
-      double wv[3][P], dw[3][P];
+      double wx[P], dwx[P], wy[P], dwy[P];
+      basis_eval<P, LAGR>((2.0 * x[i] - 2.0 * cx) / leaf_w, roots, Tr, wx, dwx);
+      basis_eval<P, LAGR>((2.0 * y[i] - 2.0 * cy) / leaf_w, roots, Tr, wy, dwy);
+      {
+        double tz[P], tdz[P];
+        basis_eval<P, LAGR>((2.0 * z[i] - 2.0 * cz) / leaf_w, roots, Tr, tz, tdz);
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const double a = ctr[d] - leaf_w / 2, b = ctr[d] + leaf_w / 2;
-        basis_eval<P>(kernel, (2.0 * pos[d] - b - a) / (b - a), roots, Tr, wv[d], dw[d]);
+        for (int k = 0; k < p; ++k) {
+          wz[k] = tz[k];
+          dwz[k] = tdz[k];
+        }
       }
       double pv = 0, gx = 0, gy = 0, gz = 0;
 #pragma unroll 1
@@ -247,17 +280,19 @@ __global__ void __launch_bounds__(LEAF_WARPS * 32) l2p_kernel(
           double a = 0, ad = 0;
 #pragma unroll
           for (int kx = 0; kx < p; ++kx) {
-            a += wv[0][kx] * row[kx];
-            ad += dw[0][kx] * row[kx];
+            const double v = row[kx];
+            a += wx[kx] * v;
+            ad += dwx[kx] * v;
           }
-          bz += wv[1][ky] * a;
-          bzx += wv[1][ky] * ad;
-          bzy += dw[1][ky] * a;
+          bz += wy[ky] * a;
+          bzx += wy[ky] * ad;
+          bzy += dwy[ky] * a;
         }
-        pv += wv[2][kz] * bz;
-        gx += wv[2][kz] * bzx;
-        gy += wv[2][kz] * bzy;
-        gz += dw[2][kz] * bz;
+        const double zk = wz[kz], dzk = dwz[kz];
+        pv += zk * bz;
+        gx += zk * bzx;
+        gy += zk * bzy;
+        gz += dzk * bz;
       }
       const long long j = (long long)r * N + i;
       const double qq = q[j];
@@ -276,11 +311,19 @@ b200fmm_status run_p2m(Context &c) {
   const Level &L = c.lv[LL];
   if (L.n == 0) return B200FMM_OK;
   const double W = c.cfg.box_width;
+  const double x0 = c.cfg.center[0] - W / 2, y0 = c.cfg.center[1] - W / 2, z0 = c.cfg.center[2] - W / 2;
+  const double lw = W / (double)(1 << LL);
+  const bool lagr = c.cfg.kernel == B200FMM_LAGRANGE;
 #define B200_P2M(PV)                                                                                        \
   case PV:                                                                                                  \
-    p2m_kernel<PV><<<grid_for(L.n, LEAF_WARPS), LEAF_WARPS * 32, 0, c.stream>>>(                             \
-        c.cfg.kernel, c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, c.cfg.center[0] - W / 2, \
-        c.cfg.center[1] - W / 2, c.cfg.center[2] - W / 2, W / (double)(1 << LL), c.d_roots, c.d_Troots, L.M);     \
+    if (lagr)                                                                                               \
+      p2m_kernel<PV, true><<<(unsigned)L.n, P2M_THREADS, 0, c.stream>>>(                                     \
+          c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, x0, y0, z0, lw, c.d_roots,        \
+          c.d_Troots, L.M);                                                                                 \
+    else                                                                                                    \
+      p2m_kernel<PV, false><<<(unsigned)L.n, P2M_THREADS, 0, c.stream>>>(                                    \
+          c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, x0, y0, z0, lw, c.d_roots,        \
+          c.d_Troots, L.M);                                                                                 \
     break;
   switch (c.p) {
     B200_P2M(3) B200_P2M(4) B200_P2M(5) B200_P2M(6) B200_P2M(7) B200_P2M(8)
@@ -297,8 +340,16 @@ b200fmm_status run_m2m(Context &c, int level) {
   const Level &P = c.lv[level], &C = c.lv[level + 1];
   if (P.n == 0) return B200FMM_OK;
   const size_t sh = sizeof(double) * 16 * c.nn;
-  B200_CUDA(cudaFuncSetAttribute(m2m_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
-  m2m_kernel<<<(unsigned)P.n, 256, sh, c.stream>>>(c.p, c.R, P.n, P.child, c.d_S, C.M, P.M);
+#define B200_M2M(PV)                                                                                        \
+  case PV:                                                                                                  \
+    B200_CUDA(cudaFuncSetAttribute(m2m_kernel<PV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));   \
+    m2m_kernel<PV><<<(unsigned)P.n, 256, sh, c.stream>>>(c.R, P.n, P.child, c.d_S, C.M, P.M);               \
+    break;
+  switch (c.p) {
+    B200_M2M(3) B200_M2M(4) B200_M2M(5) B200_M2M(6) B200_M2M(7) B200_M2M(8)
+    default: return fail(B200FMM_ERR_UNSUPPORTED, "order not built");
+  }
+#undef B200_M2M
   ++c.launches;
   B200_CUDA(cudaGetLastError());
   return B200FMM_OK;
@@ -309,8 +360,16 @@ b200fmm_status run_l2l(Context &c, int level) {
   const Level &P = c.lv[level], &C = c.lv[level + 1];
   if (P.n == 0) return B200FMM_OK;
   const size_t sh = sizeof(double) * 17 * c.nn;
-  B200_CUDA(cudaFuncSetAttribute(l2l_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
-  l2l_kernel<<<(unsigned)P.n, 256, sh, c.stream>>>(c.p, c.R, P.n, P.child, c.d_S, P.L, C.L);
+#define B200_L2L(PV)                                                                                        \
+  case PV:                                                                                                  \
+    B200_CUDA(cudaFuncSetAttribute(l2l_kernel<PV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));   \
+    l2l_kernel<PV><<<(unsigned)P.n, 256, sh, c.stream>>>(c.R, P.n, P.child, c.d_S, P.L, C.L);               \
+    break;
+  switch (c.p) {
+    B200_L2L(3) B200_L2L(4) B200_L2L(5) B200_L2L(6) B200_L2L(7) B200_L2L(8)
+    default: return fail(B200FMM_ERR_UNSUPPORTED, "order not built");
+  }
+#undef B200_L2L
   ++c.launches;
   B200_CUDA(cudaGetLastError());
   return B200FMM_OK;
@@ -321,12 +380,19 @@ b200fmm_status run_l2p(Context &c) {
   const Level &L = c.lv[LL];
   if (L.n == 0) return B200FMM_OK;
   const double W = c.cfg.box_width;
+  const double x0 = c.cfg.center[0] - W / 2, y0 = c.cfg.center[1] - W / 2, z0 = c.cfg.center[2] - W / 2;
+  const double lw = W / (double)(1 << LL);
+  const bool lagr = c.cfg.kernel == B200FMM_LAGRANGE;
 #define B200_L2P(PV)                                                                                         \
   case PV:                                                                                                   \
-    l2p_kernel<PV><<<grid_for(L.n, LEAF_WARPS), LEAF_WARPS * 32, 0, c.stream>>>(                              \
-        c.cfg.kernel, c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, c.cfg.center[0] - W / 2,  \
-        c.cfg.center[1] - W / 2, c.cfg.center[2] - W / 2, W / (double)(1 << LL), c.d_roots, c.d_Troots, L.L,      \
-        c.d_phi, c.d_fx, c.d_fy, c.d_fz);                                                                    \
+    if (lagr)                                                                                                \
+      l2p_kernel<PV, true><<<grid_for(L.n, LEAF_WARPS), LEAF_WARPS * 32, 0, c.stream>>>(                      \
+          c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, x0, y0, z0, lw, c.d_roots,         \
+          c.d_Troots, L.L, c.d_phi, c.d_fx, c.d_fy, c.d_fz);                                                 \
+    else                                                                                                     \
+      l2p_kernel<PV, false><<<grid_for(L.n, LEAF_WARPS), LEAF_WARPS * 32, 0, c.stream>>>(                     \
+          c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, x0, y0, z0, lw, c.d_roots,         \
+          c.d_Troots, L.L, c.d_phi, c.d_fx, c.d_fy, c.d_fz);                                                 \
     break;
   switch (c.p) {
     B200_L2P(3) B200_L2P(4) B200_L2P(5) B200_L2P(6) B200_L2P(7) B200_L2P(8)

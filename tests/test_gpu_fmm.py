@@ -333,9 +333,9 @@ def test_plummer_cheb_sym():
 
 def test_multi_rhs_mixed_matches_single_rhs():
     """Sixteen charge vectors on one tree (the multi-RHS workload's shape, order 7): each RHS of the MIXED
-    multi-RHS evaluation equals a single-RHS MIXED evaluation of that charge vector (same FP32 and
-    tensor-core arithmetic per RHS; the per-level power-of-two operand scale is taken over all RHS, which
-    can only move values near the bottom of the FP16 range), to 1e-8."""
+    multi-RHS evaluation is within the MIXED tolerance (2e-6) of a single-RHS FP64 evaluation of that charge
+    vector with the same (dense) operators, and within 1e-6 of a single-RHS MIXED evaluation (the work items
+    of the tensor-core M2L are split differently with 16 RHS, so the FP32 partial sums group differently)."""
     rng = np.random.default_rng(25)
     n, height, nrhs = 20000, 5, 16
     x, y, z = rng.random((3, n))
@@ -346,14 +346,17 @@ def test_multi_rhs_mixed_matches_single_rhs():
     multi = f.results()
     f.close()
     for r in (0, 7, 15):
-        g = S.FMM("cheb_sym", 7, height, precision="mixed")
-        g.set_particles(x, y, z, q[r])
-        g.execute()
-        single = g.results()
-        g.close()
+        single = {}
+        for kernel, prec in (("cheb_dense", "fp64"), ("cheb_sym", "mixed")):
+            g = S.FMM(kernel, 7, height, precision=prec)
+            g.set_particles(x, y, z, q[r])
+            g.execute()
+            single[prec] = g.results()
+            g.close()
         for k in FIELDS:
             m = np.asarray(multi[k]).reshape(nrhs, n)[r]
-            assert S.rel_l2(m, single[k]) < 1e-8, (r, k)
+            assert S.rel_l2(m, single["fp64"][k]) < 2e-6, (r, k)
+            assert S.rel_l2(m, single["mixed"][k]) < 1e-6, (r, k)
 
 
 @pytest.mark.parametrize("kernel,precision", [("cheb_sym", "fp64"), ("cheb_sym", "mixed"), ("lagrange", "mixed")])
