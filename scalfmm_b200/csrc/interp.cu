@@ -232,9 +232,10 @@ __global__ void __launch_bounds__(256) l2l_kernel(int R, long long nparents, con
 
 // ---- L2P: one warp per leaf, one particle per lane ----------------------------------------------------
 // The leaf's local expansion sits in shared memory; each lane contracts it with its particle's weights one
-// axis at a time (x in registers, then y, then z whose weights sit in the lane's shared-memory row).
+// axis at a time: the x weights in registers, the y and z weights (and derivatives) in the lane's own
+// shared-memory row, so that the loops over y and z need no register indexing and the kernel stays small.
 template <int P, bool LAGR>
-__global__ void __launch_bounds__(LEAF_WARPS * 32, 3) l2p_kernel(
+__global__ void __launch_bounds__(LEAF_WARPS * 32) l2p_kernel(
     int R, long long N, long long nleaves, const long long *__restrict__ keys,
     const long long *__restrict__ leaf_start, const double *__restrict__ x, const double *__restrict__ y,
     const double *__restrict__ z, const double *__restrict__ q, double cx0, double cy0, double cz0, double leaf_w,
@@ -242,12 +243,12 @@ __global__ void __launch_bounds__(LEAF_WARPS * 32, 3) l2p_kernel(
     double *__restrict__ phi, double *__restrict__ fx, double *__restrict__ fy, double *__restrict__ fz) {
   constexpr int p = P, nn = P * P * P;
   __shared__ double sL[LEAF_WARPS][nn];
-  __shared__ double sWz[LEAF_WARPS][32][2 * P + 1];  // z weights and derivatives of each lane's particle
+  __shared__ double sW[LEAF_WARPS][32][4 * P + 1];  // wy, dwy, wz, dwz of each lane's particle (+1: banks)
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long leaf = (long long)blockIdx.x * LEAF_WARPS + w;
   if (leaf >= nleaves) return;
   double *Lw = sL[w];
-  double *wz = sWz[w][lane], *dwz = wz + P;
+  double *wy = sW[w][lane], *dwy = wy + P, *wz = wy + 2 * P, *dwz = wy + 3 * P;
   int ix, iy, iz;
   morton_decode3(keys[leaf], ix, iy, iz);
   const double cx = cx0 + (ix + 0.5) * leaf_w, cy = cy0 + (iy + 0.5) * leaf_w, cz = cz0 + (iz + 0.5) * leaf_w;
@@ -258,23 +259,28 @@ __global__ void __launch_bounds__(LEAF_WARPS * 32, 3) l2p_kernel(
     for (int e = lane; e < nn; e += 32) Lw[e] = L[(leaf * R + r) * nn + e];
     __syncwarp();
     for (long long i = s0 + lane; i < s1; i += 32) {
-      double wx[P], dwx[P], wy[P], dwy[P];
-      basis_eval<P, LAGR>((2.0 * x[i] - 2.0 * cx) / leaf_w, roots, Tr, wx, dwx);
-      basis_eval<P, LAGR>((2.0 * y[i] - 2.0 * cy) / leaf_w, roots, Tr, wy, dwy);
+      double wx[P], dwx[P];
       {
-        double tz[P], tdz[P];
-        basis_eval<P, LAGR>((2.0 * z[i] - 2.0 * cz) / leaf_w, roots, Tr, tz, tdz);
+        double t[P], dt[P];
+        basis_eval<P, LAGR>((2.0 * y[i] - 2.0 * cy) / leaf_w, roots, Tr, t, dt);
 #pragma unroll
         for (int k = 0; k < p; ++k) {
-          wz[k] = tz[k];
-          dwz[k] = tdz[k];
+          wy[k] = t[k];
+          dwy[k] = dt[k];
+        }
+        basis_eval<P, LAGR>((2.0 * z[i] - 2.0 * cz) / leaf_w, roots, Tr, t, dt);
+#pragma unroll
+        for (int k = 0; k < p; ++k) {
+          wz[k] = t[k];
+          dwz[k] = dt[k];
         }
       }
+      basis_eval<P, LAGR>((2.0 * x[i] - 2.0 * cx) / leaf_w, roots, Tr, wx, dwx);
       double pv = 0, gx = 0, gy = 0, gz = 0;
 #pragma unroll 1
       for (int kz = 0; kz < p; ++kz) {
         double bz = 0, bzx = 0, bzy = 0;
-#pragma unroll
+#pragma unroll 1
         for (int ky = 0; ky < p; ++ky) {
           const double *row = Lw + (kz * p + ky) * p;
           double a = 0, ad = 0;
@@ -284,15 +290,16 @@ __global__ void __launch_bounds__(LEAF_WARPS * 32, 3) l2p_kernel(
             a += wx[kx] * v;
             ad += dwx[kx] * v;
           }
-          bz += wy[ky] * a;
-          bzx += wy[ky] * ad;
+          const double yk = wy[ky];
+          bz += yk * a;
+          bzx += yk * ad;
           bzy += dwy[ky] * a;
         }
-        const double zk = wz[kz], dzk = dwz[kz];
+        const double zk = wz[kz];
         pv += zk * bz;
         gx += zk * bzx;
         gy += zk * bzy;
-        gz += dzk * bz;
+        gz += dwz[kz] * bz;
       }
       const long long j = (long long)r * N + i;
       const double qq = q[j];
