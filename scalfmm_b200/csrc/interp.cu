@@ -82,7 +82,7 @@ __device__ __forceinline__ void basis_eval(double x, const double *__restrict__ 
 // and keeps its p sums over nx in registers: per particle one product q Sy Sz and p FMAs with the
 // broadcast Sx row, instead of three shared-memory reads per node and particle.
 constexpr int P2M_THREADS = 64;
-constexpr int LEAF_WARPS = 4;  // L2P: leaves per CTA, one warp each
+constexpr int L2P_WARPS = 2;  // L2P: leaves per CTA, one warp each (static shared memory <= 48 KB at order 8)
 
 template <int P, bool LAGR>
 __global__ void __launch_bounds__(P2M_THREADS, 8) p2m_kernel(
@@ -235,17 +235,17 @@ __global__ void __launch_bounds__(256) l2l_kernel(int R, long long nparents, con
 // axis at a time: the x weights in registers, the y and z weights (and derivatives) in the lane's own
 // shared-memory row, so that the loops over y and z need no register indexing and the kernel stays small.
 template <int P, bool LAGR>
-__global__ void __launch_bounds__(LEAF_WARPS * 32) l2p_kernel(
+__global__ void __launch_bounds__(L2P_WARPS * 32) l2p_kernel(
     int R, long long N, long long nleaves, const long long *__restrict__ keys,
     const long long *__restrict__ leaf_start, const double *__restrict__ x, const double *__restrict__ y,
     const double *__restrict__ z, const double *__restrict__ q, double cx0, double cy0, double cz0, double leaf_w,
     const double *__restrict__ roots, const double *__restrict__ Tr, const double *__restrict__ L,
     double *__restrict__ phi, double *__restrict__ fx, double *__restrict__ fy, double *__restrict__ fz) {
   constexpr int p = P, nn = P * P * P;
-  __shared__ double sL[LEAF_WARPS][nn];
-  __shared__ double sW[LEAF_WARPS][32][4 * P + 1];  // wy, dwy, wz, dwz of each lane's particle (+1: banks)
+  __shared__ double sL[L2P_WARPS][nn];
+  __shared__ double sW[L2P_WARPS][32][4 * P + 1];  // wy, dwy, wz, dwz of each lane's particle (+1: banks)
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long long leaf = (long long)blockIdx.x * LEAF_WARPS + w;
+  const long long leaf = (long long)blockIdx.x * L2P_WARPS + w;
   if (leaf >= nleaves) return;
   double *Lw = sL[w];
   double *wy = sW[w][lane], *dwy = wy + P, *wz = wy + 2 * P, *dwz = wy + 3 * P;
@@ -393,11 +393,11 @@ b200fmm_status run_l2p(Context &c) {
 #define B200_L2P(PV)                                                                                         \
   case PV:                                                                                                   \
     if (lagr)                                                                                                \
-      l2p_kernel<PV, true><<<grid_for(L.n, LEAF_WARPS), LEAF_WARPS * 32, 0, c.stream>>>(                      \
+      l2p_kernel<PV, true><<<grid_for(L.n, L2P_WARPS), L2P_WARPS * 32, 0, c.stream>>>(                      \
           c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, x0, y0, z0, lw, c.d_roots,         \
           c.d_Troots, L.L, c.d_phi, c.d_fx, c.d_fy, c.d_fz);                                                 \
     else                                                                                                     \
-      l2p_kernel<PV, false><<<grid_for(L.n, LEAF_WARPS), LEAF_WARPS * 32, 0, c.stream>>>(                     \
+      l2p_kernel<PV, false><<<grid_for(L.n, L2P_WARPS), L2P_WARPS * 32, 0, c.stream>>>(                     \
           c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, x0, y0, z0, lw, c.d_roots,         \
           c.d_Troots, L.L, c.d_phi, c.d_fx, c.d_fy, c.d_fz);                                                 \
     break;
