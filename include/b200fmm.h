@@ -175,6 +175,27 @@ B200FMM_API b200fmm_status b200fmm_p2p_noalloc(long long n, const double *x, con
                                                double box_width, const double *center, int variant, double *phi,
                                                double *fx, double *fy, double *fz, void *stream);
 
+/* Batches of independent problems of uneven size, each with its own order, height and box (the reference
+ * runs one FFmmAlgorithm per problem).  The problems are spread over nstreams worker streams, each driven by
+ * its own host thread, largest first, so that one problem's tree build overlaps other problems' passes;
+ * every worker keeps one handle per (order, height, box) it has met, so operators are computed once and
+ * device buffers are reused by later calls.  Host memory in and out; nrhs = 1.  execute() returns when
+ * every problem's results are written, or the first failure (its message names the problem). */
+typedef struct {
+  long long n;                  /* particles */
+  const double *x, *y, *z, *q;  /* n each */
+  double *phi, *fx, *fy, *fz;   /* n each, written (not accumulated), caller's particle order */
+  int order, height;
+  double box_width, center[3];
+} b200fmm_problem;
+typedef struct b200fmm_batch_context *b200fmm_batch;
+B200FMM_API b200fmm_status b200fmm_batch_create(int kernel, int precision, int nstreams, int device,
+                                                b200fmm_batch *out);
+B200FMM_API b200fmm_status b200fmm_batch_execute(b200fmm_batch b, int nproblems, const b200fmm_problem *problems);
+/* Host wall time of the last batch_execute(), milliseconds. */
+B200FMM_API b200fmm_status b200fmm_batch_last_time(b200fmm_batch b, double *ms);
+B200FMM_API b200fmm_status b200fmm_batch_destroy(b200fmm_batch b);
+
 /* FP64 direct sum on the GPU (Examples/DirectComputation.cpp:104-142) for the listed targets (all if
  * ntargets < 0).  Host pointers; outputs have ntargets (or n) entries. */
 B200FMM_API b200fmm_status b200fmm_direct(long long n, const double *x, const double *y, const double *z, const double *q,

@@ -31,7 +31,8 @@ EXPORTS = (
     "b200fmm_reset_expansions", "b200fmm_zero_results", "b200fmm_p2m", "b200fmm_m2m", "b200fmm_m2l", "b200fmm_l2l", "b200fmm_l2p",
     "b200fmm_p2p", "b200fmm_get_results", "b200fmm_synchronize", "b200fmm_tree_info", "b200fmm_get_cells",
     "b200fmm_get_permutation", "b200fmm_last_timings", "b200fmm_last_kernel_times", "b200fmm_tree_stats",
-    "b200fmm_last_launch_count", "b200fmm_p2p_noalloc", "b200fmm_direct",
+    "b200fmm_last_launch_count", "b200fmm_p2p_noalloc", "b200fmm_batch_create", "b200fmm_batch_execute",
+    "b200fmm_batch_last_time", "b200fmm_batch_destroy", "b200fmm_direct",
 )
 NOALLOC_MAX_PARTICLES = 262144
 
@@ -42,6 +43,14 @@ _lp = ctypes.POINTER(ctypes.c_longlong)
 
 class B200FmmError(RuntimeError):
     pass
+
+
+class Problem(ctypes.Structure):
+    """b200fmm_problem: one problem of a batch (host arrays)."""
+    _fields_ = [("n", ctypes.c_longlong), ("x", ctypes.c_void_p), ("y", ctypes.c_void_p), ("z", ctypes.c_void_p),
+                ("q", ctypes.c_void_p), ("phi", ctypes.c_void_p), ("fx", ctypes.c_void_p), ("fy", ctypes.c_void_p),
+                ("fz", ctypes.c_void_p), ("order", ctypes.c_int), ("height", ctypes.c_int),
+                ("box_width", ctypes.c_double), ("center", ctypes.c_double * 3)]
 
 
 class Config(ctypes.Structure):
@@ -103,6 +112,11 @@ def lib():
         L.b200fmm_p2p_noalloc.argtypes = ([ctypes.c_longlong] + [ctypes.c_void_p] * 4 + [ctypes.c_longlong]
                                           + [ctypes.c_void_p] * 3 + [ctypes.c_int, ctypes.c_double, _dp, ctypes.c_int]
                                           + [ctypes.c_void_p] * 5)
+        L.b200fmm_batch_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_void_p)]
+        L.b200fmm_batch_execute.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.b200fmm_batch_last_time.argtypes = [ctypes.c_void_p, _dp]
+        L.b200fmm_batch_destroy.argtypes = [ctypes.c_void_p]
         L.b200fmm_direct.argtypes = [ctypes.c_longlong, _dp, _dp, _dp, _dp, ctypes.c_longlong, _lp, _dp, _dp, _dp, _dp]
         _lib = L
     return _lib
@@ -282,6 +296,51 @@ class FMM:
         c = ctypes.c_longlong()
         _check(lib().b200fmm_last_launch_count(self._h, ctypes.byref(c)), "last_launch_count")
         return c.value
+
+
+class Batch:
+    """Many independent problems of uneven size, spread over worker streams (b200fmm_batch_*).
+
+    run(problems) takes a list of dicts with x, y, z, q (numpy), order, height and optionally box_width and
+    center, and returns one dict of phi, fx, fy, fz per problem."""
+
+    def __init__(self, kernel="cheb_sym", precision="mixed", nstreams=4, device=-1):
+        h = ctypes.c_void_p()
+        _check(lib().b200fmm_batch_create(KERNELS[kernel], PRECISIONS[precision], nstreams, device, ctypes.byref(h)),
+               "batch_create")
+        self._h = h
+
+    def run(self, problems):
+        keep, arr = [], (Problem * len(problems))()
+        outs = []
+        for k, pr in enumerate(problems):
+            x, y, z, q = (_f64(pr[a]) for a in ("x", "y", "z", "q"))
+            out = {f: np.zeros(x.size) for f in ("phi", "fx", "fy", "fz")}
+            keep += [x, y, z, q]
+            outs.append(out)
+            c = pr.get("center", (0.5, 0.5, 0.5))
+            arr[k] = Problem(x.size, x.ctypes.data, y.ctypes.data, z.ctypes.data, q.ctypes.data,
+                             out["phi"].ctypes.data, out["fx"].ctypes.data, out["fy"].ctypes.data,
+                             out["fz"].ctypes.data, int(pr["order"]), int(pr["height"]),
+                             float(pr.get("box_width", 1.0)), (ctypes.c_double * 3)(*c))
+        _check(lib().b200fmm_batch_execute(self._h, len(problems), arr), "batch_execute")
+        return outs
+
+    def last_time_ms(self):
+        ms = ctypes.c_double()
+        _check(lib().b200fmm_batch_last_time(self._h, ctypes.byref(ms)), "batch_last_time")
+        return ms.value
+
+    def close(self):
+        if self._h:
+            lib().b200fmm_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def direct(x, y, z, q, targets=None):

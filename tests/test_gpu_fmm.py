@@ -392,3 +392,34 @@ def test_repeated_execute_replays_a_graph(kernel, precision):
     f.execute()
     assert f.timings()["p2m"] > 0
     f.close()
+
+
+@pytest.mark.parametrize("kernel,precision,tol", [("cheb_sym", "fp64", 1e-12), ("cheb_sym", "mixed", 1e-10),
+                                                  ("lagrange", "mixed", 1e-10)])
+def test_batch_matches_single_problems(kernel, precision, tol):
+    """A batch of problems of uneven size, order and height (the batch workload's shape: Plummer positions,
+    orders 4..6, heights for about 30 particles per leaf) run over 3 worker streams equals each problem run
+    on its own handle (same arithmetic; only the order of FP64 atomic additions may differ); the batch is
+    run twice so that the second call reuses the workers' handles."""
+    from distributions import plummer
+
+    rng = np.random.default_rng(41)
+    problems = []
+    for k in range(9):
+        n = int(np.exp(rng.uniform(np.log(1500), np.log(40000))))
+        x, y, z = plummer(n, seed=100 + k)
+        height = int(min(6, max(3, np.ceil(np.log(max(n / 30, 1)) / np.log(8)) + 1)))
+        problems.append(dict(x=x, y=y, z=z, q=rng.uniform(-1, 1, n), order=4 + k % 3, height=height))
+    b = S.Batch(kernel, precision, nstreams=3, device=0)
+    for _ in range(2):
+        outs = b.run(problems)
+        assert b.last_time_ms() > 0
+        for pr, out in zip(problems, outs):
+            f = S.FMM(kernel, pr["order"], pr["height"], precision=precision)
+            f.set_particles(pr["x"], pr["y"], pr["z"], pr["q"])
+            f.execute()
+            want = f.results()
+            f.close()
+            for k in FIELDS:
+                assert S.rel_l2(out[k], want[k]) < tol, (pr["order"], pr["height"], k)
+    b.close()
