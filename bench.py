@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--height", type=int, default=HEIGHT, help="octree height (profiling of small cases only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batch-of-problems measurement")
     return ap.parse_args()
 
 
@@ -60,6 +61,53 @@ def particles(n, seed=SEED):
     pos = rng.random((3, n))
     q = rng.uniform(-1.0, 1.0, n)
     return pos[0].copy(), pos[1].copy(), pos[2].copy(), q
+
+
+def plummer(n, rng, scale=0.1):
+    """Plummer sphere (scale radius 0.1) centred in the unit cube, points outside the cube rejected."""
+    out, have = [], 0
+    while have < n:
+        m = 2 * n
+        r = scale / np.sqrt(rng.random(m) ** (-2.0 / 3.0) - 1.0)
+        d = rng.standard_normal((3, m))
+        d /= np.linalg.norm(d, axis=0)
+        pnt = d * r + 0.5
+        keep = np.all((pnt >= 0.0) & (pnt < 1.0), axis=0)
+        out.append(pnt[:, keep])
+        have += int(keep.sum())
+    pnt = np.concatenate(out, axis=1)[:, :n]
+    return pnt[0].copy(), pnt[1].copy(), pnt[2].copy()
+
+
+def batch_workload(seed=5):
+    """64 independent problems, sizes log-uniform in 10,000..500,000, Plummer positions, charges U[-1,1],
+    Chebyshev order 5..7 per problem, height chosen for about 30 particles per leaf."""
+    rng = np.random.default_rng(seed)
+    problems = []
+    for k in range(64):
+        n = int(np.exp(rng.uniform(np.log(1e4), np.log(5e5))))
+        x, y, z = plummer(n, rng)
+        height = int(min(7, max(4, round(np.log(n / 30.0) / np.log(8.0)) + 1)))
+        problems.append(dict(x=x, y=y, z=z, q=rng.uniform(-1.0, 1.0, n), order=5 + k % 3, height=height))
+    return problems
+
+
+def batch_measure(S, device):
+    problems = batch_workload()
+    total = sum(p["x"].size for p in problems)
+    b = S.Batch("cheb_sym", "mixed", nstreams=4, device=device)
+    b.run(problems)  # handles, operators and buffers of every (order, height)
+    ms = []
+    for _ in range(3):
+        b.run(problems)
+        ms.append(b.last_time_ms())
+    b.close()
+    best = min(ms)
+    return {"problems": len(problems), "particles": total, "ms": best, "particles_per_s": total / (best * 1e-3),
+            "workload": "64 problems, n log-uniform in [1e4, 5e5], Plummer (a = 0.1) truncated to the unit cube, "
+                        "Chebyshev order 5..7, height for ~30 particles/leaf, MIXED, 4 worker streams",
+            "timing": "host wall time of b200fmm_batch_execute (host arrays in and out, tree builds included), "
+                      "best of 3 after one untimed run"}
 
 
 def workload_config(n, height=HEIGHT):
@@ -326,6 +374,8 @@ def run_gpu(args):
 
     if rank == 0 and not args.no_accuracy:
         line["accuracy"] = accuracy(S, torch, dev, stream, x, y, z, q, line)
+    if rank == 0 and not args.no_batch:
+        line["batch"] = batch_measure(S, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             times, kind, cores, sample = cpu_eval(x, y, z, q, steps=1)
