@@ -79,16 +79,29 @@ def plummer(n, rng, scale=0.1):
     return pnt[0].copy(), pnt[1].copy(), pnt[2].copy()
 
 
+def leaf_height(x, y, z, target=30.0, lo=4, hi=7):
+    """Smallest height in [lo, hi] whose leaves hold about `target` particles as a particle sees them (the
+    particle-weighted mean occupancy, sum n_leaf^2 / N, at most 2 x target); the Plummer core is far denser
+    than the average, so the plain mean N / leaves would leave thousands of particles in the core leaves."""
+    for h in range(lo, hi + 1):
+        side = 1 << (h - 1)
+        c = np.minimum((np.stack([x, y, z]) * side).astype(np.int64), side - 1)
+        _, cnt = np.unique((c[0] * side + c[1]) * side + c[2], return_counts=True)
+        if (cnt.astype(float) ** 2).sum() / x.size <= 2.0 * target:
+            return h
+    return hi
+
+
 def batch_workload(seed=5):
     """64 independent problems, sizes log-uniform in 10,000..500,000, Plummer positions, charges U[-1,1],
-    Chebyshev order 5..7 per problem, height chosen for about 30 particles per leaf."""
+    Chebyshev order 5..7 per problem, height in 4..7 chosen for about 30 particles per leaf."""
     rng = np.random.default_rng(seed)
     problems = []
     for k in range(64):
         n = int(np.exp(rng.uniform(np.log(1e4), np.log(5e5))))
         x, y, z = plummer(n, rng)
-        height = int(min(7, max(4, round(np.log(n / 30.0) / np.log(8.0)) + 1)))
-        problems.append(dict(x=x, y=y, z=z, q=rng.uniform(-1.0, 1.0, n), order=5 + k % 3, height=height))
+        problems.append(dict(x=x, y=y, z=z, q=rng.uniform(-1.0, 1.0, n), order=5 + k % 3,
+                             height=leaf_height(x, y, z)))
     return problems
 
 
@@ -105,7 +118,8 @@ def batch_measure(S, device):
     best = min(ms)
     return {"problems": len(problems), "particles": total, "ms": best, "particles_per_s": total / (best * 1e-3),
             "workload": "64 problems, n log-uniform in [1e4, 5e5], Plummer (a = 0.1) truncated to the unit cube, "
-                        "Chebyshev order 5..7, height for ~30 particles/leaf, MIXED, 4 worker streams",
+                        "Chebyshev order 5..7, height 4..7 for ~30 particles per leaf as a particle sees it, MIXED, "
+                        "4 worker streams",
             "timing": "host wall time of b200fmm_batch_execute (host arrays in and out, tree builds included), "
                       "best of 3 after one untimed run"}
 

@@ -57,7 +57,22 @@ struct TcLevel {
   int *grid;           // [side^3] cell index or -1
   double *L;           // locals of the level
   double *scale_out;   // device scalar: scale_l * 2^-(sA + SB)
+  const int *sat;      // [8][HZ+1][HY+1][HX+1] occupied cells of each parity grid below (x, y, z), exclusive
 };
+
+// Occupied cells of parity grid `par` in the box [x0, x0+nx) x [y0, y0+ny) x [z0, z0+nz) (clipped).
+__device__ __forceinline__ int box_count(const TcLevel &L, int par, int x0, int y0, int z0, int nx, int ny, int nz) {
+  const int x1 = min(x0 + nx, L.HX), y1 = min(y0 + ny, L.HY), z1 = min(z0 + nz, L.HZ);
+  x0 = max(x0, 0);
+  y0 = max(y0, 0);
+  z0 = max(z0, 0);
+  if (x0 >= x1 || y0 >= y1 || z0 >= z1) return 0;
+  const int SX = L.HX + 1, SY = L.HY + 1;
+  const int *s = L.sat + (size_t)par * SX * SY * (L.HZ + 1);
+  auto at = [&](int x, int y, int z) { return s[((size_t)z * SY + y) * SX + x]; };
+  return at(x1, y1, z1) - at(x0, y1, z1) - at(x1, y0, z1) - at(x1, y1, z0) + at(x0, y0, z1) + at(x0, y1, z0) +
+         at(x1, y0, z0) - at(x0, y0, z0);
+}
 
 struct __align__(64) TcParams {
   CUtensorMap mapA_hi[kMaxHeight];
@@ -158,6 +173,32 @@ __device__ __forceinline__ void drain_cols(unsigned taddr, float *acc) {
   }
 }
 
+// The source box of transfer vector e for an item: parity grid sp, half-grid origin (ox, oy, oz), operator
+// slot.  Every warp role derives the same box, and skips the transfer vectors whose source box is empty
+// (those A tiles are all zero) and the items whose target tile is empty, so that sparse trees (surface or
+// clustered distributions) cost only their occupied tiles.
+struct SrcBox {
+  int sp, ox, oy, oz, slot;
+};
+__device__ __forceinline__ SrcBox src_box(const TcParams &P, const TcItem &w, int e) {
+  const int c = w.parity;
+  const int cx = (c >> 2) & 1, cy = (c >> 1) & 1, cz = c & 1;
+  const int dx = P.off[c][e][0], dy = P.off[c][e][1], dz = P.off[c][e][2];
+  SrcBox b;
+  b.sp = (((cx + dx) & 1) << 2) | (((cy + dy) & 1) << 1) | ((cz + dz) & 1);
+  b.ox = w.bx * TILE_X + ((cx + dx) >> 1);
+  b.oy = w.by * TILE_Y + ((cy + dy) >> 1);
+  b.oz = w.bz * TILE_Z + ((cz + dz) >> 1);
+  b.slot = P.slot[c][e];
+  return b;
+}
+__device__ __forceinline__ bool tile_busy(const TcParams &P, const TcItem &w) {
+  return box_count(P.lv[w.level], w.parity, w.bx * TILE_X, w.by * TILE_Y, w.bz * TILE_Z, TILE_X, TILE_Y, TILE_Z) > 0;
+}
+__device__ __forceinline__ bool src_busy(const TcParams &P, const TcItem &w, const SrcBox &b) {
+  return box_count(P.lv[w.level], b.sp, b.ox, b.oy, b.oz, TILE_X, TILE_Y, TILE_Z) > 0;
+}
+
 // ---- the kernel -------------------------------------------------------------------------------------
 // CW: accumulator columns owned by one epilogue thread (NP / 2) and NHALF: MMA column halves, compile-time
 // constants so that the running sums stay in registers.  With one half a thread owns the columns
@@ -215,14 +256,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
       unsigned phase = 0;
       for (int it = blockIdx.x; it < P.nitems && !abort_sh; it += gridDim.x) {
         const TcItem w = P.items[P.item0 + it];
-        const int c = w.parity;
-        const int cx = (c >> 2) & 1, cy = (c >> 1) & 1, cz = c & 1;
+        if (!tile_busy(P, w)) continue;
         for (int e = w.t0; e < w.t1 && !abort_sh; ++e) {
-          const int dx = P.off[c][e][0], dy = P.off[c][e][1], dz = P.off[c][e][2];
-          const int sp = (((cx + dx) & 1) << 2) | (((cy + dy) & 1) << 1) | ((cz + dz) & 1);
-          const int ox = w.bx * TILE_X + ((cx + dx) >> 1), oy = w.by * TILE_Y + ((cy + dy) >> 1),
-                    oz = w.bz * TILE_Z + ((cz + dz) >> 1);
-          const int slot = P.slot[c][e];
+          const SrcBox sb = src_box(P, w, e);
+          if (!src_busy(P, w, sb)) continue;
+          const int sp = sb.sp, ox = sb.ox, oy = sb.oy, oz = sb.oz, slot = sb.slot;
           for (int kc = 0; kc < P.NK; ++kc) {
             if (!mbar_wait(&empty_bar[stage], phase ^ 1)) {
               atomicExch(P.status + 1, 1);
@@ -258,7 +296,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
       const bool defer = (P.nbuf == 1 && NHALF == 2);
       for (int it = blockIdx.x; it < P.nitems && !abort_sh; it += gridDim.x) {
         const TcItem w = P.items[P.item0 + it];
+        if (!tile_busy(P, w)) continue;
         for (int e = w.t0; e < w.t1 && !abort_sh; ++e) {
+          if (!src_busy(P, w, src_box(P, w, e))) continue;
           for (int sg = 0; sg < P.nseg && !abort_sh; ++sg, ++seg) {
             const int k0 = sg * P.NK / P.nseg, k1 = (sg + 1) * P.NK / P.nseg;
             const int b = P.nbuf == 2 ? (seg & 1) : 0;
@@ -333,7 +373,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
     for (int i = 0; i < CW; ++i) acc[i] = 0.f;
     for (int it = blockIdx.x; it < P.nitems && !abort_sh; it += gridDim.x) {
       const TcItem w = P.items[P.item0 + it];
-      const int nseg_item = (w.t1 - w.t0) * P.nseg;
+      int nbusy = 0;  // transfer vectors of this item that the MMA warp runs
+      if (tile_busy(P, w))
+        for (int e = w.t0; e < w.t1; ++e) nbusy += src_busy(P, w, src_box(P, w, e)) ? 1 : 0;
+      if (nbusy == 0) continue;  // nothing accumulated: no flush
+      const int nseg_item = nbusy * P.nseg;
       for (int sgi = 0; sgi < nseg_item; ++sgi, ++seg) {
         const int b = P.nbuf == 2 ? (seg & 1) : 0;
         if (!mbar_wait(&acc_full[b], (full_par >> b) & 1u)) {
@@ -400,6 +444,47 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
 }
 
 // ---- conversion kernels -----------------------------------------------------------------------------
+
+// occupancy of each parity grid, stored one cell up/right so that three prefix passes give the exclusive
+// summed-area table that box_count reads
+__global__ void occ_mark_kernel(long long n, const long long *__restrict__ keys, int HX, int HY, int HZ,
+                                int *__restrict__ sat) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int ix, iy, iz;
+  morton_decode3(keys[i], ix, iy, iz);
+  const int c = ((ix & 1) << 2) | ((iy & 1) << 1) | (iz & 1);
+  const size_t SX = HX + 1, SY = HY + 1, SZ = HZ + 1;
+  sat[(((size_t)c * SZ + (iz >> 1) + 1) * SY + (iy >> 1) + 1) * SX + (ix >> 1) + 1] = 1;
+}
+
+__global__ void sat_pass_kernel(int *__restrict__ sat, int HX, int HY, int HZ, int axis) {
+  const long long SX = HX + 1, SY = HY + 1, SZ = HZ + 1;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long base, stride, len, nlines;
+  if (axis == 0) {
+    nlines = 8 * SZ * SY;
+    base = t * SX;
+    stride = 1;
+    len = SX;
+  } else if (axis == 1) {
+    nlines = 8 * SZ * SX;
+    base = (t / SX) * SY * SX + t % SX;
+    stride = SX;
+    len = SY;
+  } else {
+    nlines = 8 * SY * SX;
+    base = (t / (SY * SX)) * SZ * SY * SX + t % (SY * SX);
+    stride = SY * SX;
+    len = SZ;
+  }
+  if (t >= nlines) return;
+  int acc = 0;
+  for (long long k = 0; k < len; ++k) {
+    acc += sat[base + k * stride];
+    sat[base + k * stride] = acc;
+  }
+}
 
 // max |M| of a level -> bit pattern (non-negative doubles order like their bit patterns)
 __global__ void absmax_kernel(long long n, const double *__restrict__ v, unsigned long long *__restrict__ out) {
@@ -484,6 +569,9 @@ struct DenseTC {
   unsigned long long *amax = nullptr;     // [kMaxHeight]
   TcItem *items = nullptr;
   int nitems = 0;
+  int *sat[kMaxHeight] = {};              // occupancy summed-area tables, per level
+  size_t satn[kMaxHeight] = {};
+  long long sat_serial = -1;              // tree the tables describe
   int lvl_begin[kMaxHeight] = {}, lvl_end[kMaxHeight] = {};
   long long built_for_N = -1;             // tree the per-level buffers were sized for
   int built_for_gen = -1;                 // tree generation the tensor maps / pointers belong to
@@ -554,6 +642,7 @@ void tc_free(Context &c) {
   for (int l = 0; l < kMaxHeight; ++l) {
     if (t->Ahi[l]) cudaFree(t->Ahi[l]);
     if (t->Alo[l]) cudaFree(t->Alo[l]);
+    if (t->sat[l]) cudaFree(t->sat[l]);
   }
   delete t->params;
   delete t;
@@ -595,6 +684,14 @@ static b200fmm_status tc_prepare(Context &c) {
     P.lv[l].grid = c.lv[l].grid;
     P.lv[l].L = c.lv[l].L;
     P.lv[l].scale_out = t->scal + 2 * l + 1;
+    const size_t sn = (size_t)8 * (t->HX[l] + 1) * (t->HY[l] + 1) * (t->HZ[l] + 1);
+    if (t->satn[l] != sn) {
+      if (t->sat[l]) cudaFree(t->sat[l]);
+      B200_CUDA(cudaMalloc(&t->sat[l], sn * sizeof(int)));
+      t->satn[l] = sn;
+    }
+    P.lv[l].sat = t->sat[l];
+    t->sat_serial = -1;
     ntiles += (long long)c.R * 8 * (t->HX[l] / TILE_X) * (t->HY[l] / TILE_Y) * (t->HZ[l] / TILE_Z);
   }
   // split the 189 transfer vectors of each tile so that the items fill the SMs evenly
@@ -663,6 +760,23 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
   const int LL = c.H - 1;
   if (level != -1 && (level < 2 || level > LL)) return fail(B200FMM_ERR_INVALID, "m2l: level out of range");
   if (t->built_for_gen != c.tree_gen) B200_CHECK(tc_prepare(c));
+  if (t->sat_serial != c.tree_serial) {
+    // which cells of each level are occupied: lets the kernel skip empty target tiles and source boxes
+    for (int l = 2; l <= LL; ++l) {
+      const int HX = t->HX[l], HY = t->HY[l], HZ = t->HZ[l];
+      B200_CUDA(cudaMemsetAsync(t->sat[l], 0, t->satn[l] * sizeof(int), c.stream));
+      if (c.lv[l].n) {
+        occ_mark_kernel<<<grid_for(c.lv[l].n, 256), 256, 0, c.stream>>>(c.lv[l].n, c.lv[l].keys, HX, HY, HZ, t->sat[l]);
+        ++c.launches;
+      }
+      const long long lines[3] = {8LL * (HZ + 1) * (HY + 1), 8LL * (HZ + 1) * (HX + 1), 8LL * (HY + 1) * (HX + 1)};
+      for (int a = 0; a < 3; ++a) {
+        sat_pass_kernel<<<grid_for(lines[a], 128), 128, 0, c.stream>>>(t->sat[l], HX, HY, HZ, a);
+        ++c.launches;
+      }
+    }
+    t->sat_serial = c.tree_serial;
+  }
   const int l0 = level == -1 ? 2 : level, l1 = level == -1 ? LL : level;
   for (int l = l0; l <= l1; ++l) {
     const Level &Lv = c.lv[l];
