@@ -58,6 +58,7 @@ struct TcLevel {
   double *L;           // locals of the level
   double *scale_out;   // device scalar: scale_l * 2^-(sA + SB)
   const int *sat;      // [8][HZ+1][HY+1][HX+1] occupied cells of each parity grid below (x, y, z), exclusive
+  int tile0;           // first tile of this level in the busy masks
 };
 
 // Occupied cells of parity grid `par` in the box [x0, x0+nx) x [y0, y0+ny) x [z0, z0+nz) (clipped).
@@ -89,6 +90,9 @@ struct __align__(64) TcParams {
   signed char off[8][189][3];
   short slot[8][189];
   int *status;
+  // per tile (level, parity, bz, by, bx): 6 words, bit e set when transfer vector e has an occupied source
+  // box; bit 31 of word 5 set when the tile has an occupied target cell
+  const unsigned *busy;
 };
 
 // ---- PTX helpers ----------------------------------------------------------------------------------
@@ -192,11 +196,23 @@ __device__ __forceinline__ SrcBox src_box(const TcParams &P, const TcItem &w, in
   b.slot = P.slot[c][e];
   return b;
 }
-__device__ __forceinline__ bool tile_busy(const TcParams &P, const TcItem &w) {
-  return box_count(P.lv[w.level], w.parity, w.bx * TILE_X, w.by * TILE_Y, w.bz * TILE_Z, TILE_X, TILE_Y, TILE_Z) > 0;
+__device__ __forceinline__ long long tile_id(const TcParams &P, int level, int parity, int bx, int by, int bz) {
+  const TcLevel &L = P.lv[level];
+  const int TX = L.HX / TILE_X, TY = L.HY / TILE_Y, TZ = L.HZ / TILE_Z;
+  return L.tile0 + (((long long)parity * TZ + bz) * TY + by) * TX + bx;
 }
-__device__ __forceinline__ bool src_busy(const TcParams &P, const TcItem &w, const SrcBox &b) {
-  return box_count(P.lv[w.level], b.sp, b.ox, b.oy, b.oz, TILE_X, TILE_Y, TILE_Z) > 0;
+// the busy mask of an item's tile, read once per item by every role
+struct BusyMask {
+  unsigned w[6];
+  __device__ __forceinline__ bool tile() const { return (w[5] >> 31) & 1u; }
+  __device__ __forceinline__ bool src(int e) const { return (w[e >> 5] >> (e & 31)) & 1u; }
+};
+__device__ __forceinline__ BusyMask busy_mask(const TcParams &P, const TcItem &w) {
+  const unsigned *m = P.busy + 6 * tile_id(P, w.level, w.parity, w.bx, w.by, w.bz);
+  BusyMask b;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) b.w[k] = m[k];
+  return b;
 }
 
 // ---- the kernel -------------------------------------------------------------------------------------
@@ -256,10 +272,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
       unsigned phase = 0;
       for (int it = blockIdx.x; it < P.nitems && !abort_sh; it += gridDim.x) {
         const TcItem w = P.items[P.item0 + it];
-        if (!tile_busy(P, w)) continue;
+        const BusyMask bm = busy_mask(P, w);
+        if (!bm.tile()) continue;
         for (int e = w.t0; e < w.t1 && !abort_sh; ++e) {
+          if (!bm.src(e)) continue;
           const SrcBox sb = src_box(P, w, e);
-          if (!src_busy(P, w, sb)) continue;
           const int sp = sb.sp, ox = sb.ox, oy = sb.oy, oz = sb.oz, slot = sb.slot;
           for (int kc = 0; kc < P.NK; ++kc) {
             if (!mbar_wait(&empty_bar[stage], phase ^ 1)) {
@@ -296,9 +313,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
       const bool defer = (P.nbuf == 1 && NHALF == 2);
       for (int it = blockIdx.x; it < P.nitems && !abort_sh; it += gridDim.x) {
         const TcItem w = P.items[P.item0 + it];
-        if (!tile_busy(P, w)) continue;
+        const BusyMask bm = busy_mask(P, w);
+        if (!bm.tile()) continue;
         for (int e = w.t0; e < w.t1 && !abort_sh; ++e) {
-          if (!src_busy(P, w, src_box(P, w, e))) continue;
+          if (!bm.src(e)) continue;
           for (int sg = 0; sg < P.nseg && !abort_sh; ++sg, ++seg) {
             const int k0 = sg * P.NK / P.nseg, k1 = (sg + 1) * P.NK / P.nseg;
             const int b = P.nbuf == 2 ? (seg & 1) : 0;
@@ -374,8 +392,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
     for (int it = blockIdx.x; it < P.nitems && !abort_sh; it += gridDim.x) {
       const TcItem w = P.items[P.item0 + it];
       int nbusy = 0;  // transfer vectors of this item that the MMA warp runs
-      if (tile_busy(P, w))
-        for (int e = w.t0; e < w.t1; ++e) nbusy += src_busy(P, w, src_box(P, w, e)) ? 1 : 0;
+      const BusyMask bm = busy_mask(P, w);
+      if (bm.tile())
+        for (int e = w.t0; e < w.t1; ++e) nbusy += bm.src(e) ? 1 : 0;
       if (nbusy == 0) continue;  // nothing accumulated: no flush
       const int nseg_item = nbusy * P.nseg;
       for (int sgi = 0; sgi < nseg_item; ++sgi, ++seg) {
@@ -486,6 +505,28 @@ __global__ void sat_pass_kernel(int *__restrict__ sat, int HX, int HY, int HZ, i
   }
 }
 
+// busy masks of one level: one thread per (tile, transfer vector)
+__global__ void busy_mask_kernel(const __grid_constant__ TcParams P, int level, long long ntiles,
+                                 unsigned *__restrict__ busy) {
+  const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (g >= ntiles * 189) return;
+  const long long tl = g / 189;
+  const int e = (int)(g % 189);
+  const TcLevel &L = P.lv[level];
+  const int TX = L.HX / TILE_X, TY = L.HY / TILE_Y, TZ = L.HZ / TILE_Z;
+  TcItem w;
+  w.level = (short)level;
+  w.bx = (short)(tl % TX);
+  w.by = (short)((tl / TX) % TY);
+  w.bz = (short)((tl / ((long long)TX * TY)) % TZ);
+  w.parity = (short)(tl / ((long long)TX * TY * TZ));
+  unsigned *m = busy + 6 * (L.tile0 + tl);
+  const SrcBox b = src_box(P, w, e);
+  if (box_count(L, b.sp, b.ox, b.oy, b.oz, TILE_X, TILE_Y, TILE_Z) > 0) atomicOr(m + (e >> 5), 1u << (e & 31));
+  if (e == 0 && box_count(L, w.parity, w.bx * TILE_X, w.by * TILE_Y, w.bz * TILE_Z, TILE_X, TILE_Y, TILE_Z) > 0)
+    atomicOr(m + 5, 1u << 31);
+}
+
 // max |M| of a level -> bit pattern (non-negative doubles order like their bit patterns)
 __global__ void absmax_kernel(long long n, const double *__restrict__ v, unsigned long long *__restrict__ out) {
   double m = 0.0;
@@ -572,6 +613,8 @@ struct DenseTC {
   int *sat[kMaxHeight] = {};              // occupancy summed-area tables, per level
   size_t satn[kMaxHeight] = {};
   long long sat_serial = -1;              // tree the tables describe
+  unsigned *busy = nullptr;               // busy masks of every tile of every level
+  long long ntiles_all = 0;
   int lvl_begin[kMaxHeight] = {}, lvl_end[kMaxHeight] = {};
   long long built_for_N = -1;             // tree the per-level buffers were sized for
   int built_for_gen = -1;                 // tree generation the tensor maps / pointers belong to
@@ -637,7 +680,7 @@ b200fmm_status tc_init(Context &c) {
 void tc_free(Context &c) {
   DenseTC *t = c.tc;
   if (!t) return;
-  for (void *p : {(void *)t->Bhi, (void *)t->Blo, (void *)t->scal, (void *)t->amax, (void *)t->items})
+  for (void *p : {(void *)t->Bhi, (void *)t->Blo, (void *)t->scal, (void *)t->amax, (void *)t->items, (void *)t->busy})
     if (p) cudaFree(p);
   for (int l = 0; l < kMaxHeight; ++l) {
     if (t->Ahi[l]) cudaFree(t->Ahi[l]);
@@ -656,6 +699,7 @@ static b200fmm_status tc_prepare(Context &c) {
   const int LL = c.H - 1;
   std::vector<TcItem> items;
   long long ntiles = 0;
+  t->ntiles_all = 0;
   for (int l = 2; l <= LL; ++l) {
     const int h = 1 << (l - 1);
     t->HX[l] = std::max(h, TILE_X);
@@ -691,6 +735,8 @@ static b200fmm_status tc_prepare(Context &c) {
       t->satn[l] = sn;
     }
     P.lv[l].sat = t->sat[l];
+    P.lv[l].tile0 = (int)t->ntiles_all;
+    t->ntiles_all += 8LL * (t->HX[l] / TILE_X) * (t->HY[l] / TILE_Y) * (t->HZ[l] / TILE_Z);
     t->sat_serial = -1;
     ntiles += (long long)c.R * 8 * (t->HX[l] / TILE_X) * (t->HY[l] / TILE_Y) * (t->HZ[l] / TILE_Z);
   }
@@ -725,6 +771,9 @@ static b200fmm_status tc_prepare(Context &c) {
               }
     t->lvl_end[l] = (int)items.size();
   }
+  if (t->busy) cudaFree(t->busy);
+  B200_CUDA(cudaMalloc(&t->busy, sizeof(unsigned) * 6 * std::max<long long>(t->ntiles_all, 1)));
+  P.busy = t->busy;
   if (t->items) cudaFree(t->items);
   B200_CUDA(cudaMalloc(&t->items, sizeof(TcItem) * items.size()));
   B200_CUDA(cudaMemcpy(t->items, items.data(), sizeof(TcItem) * items.size(), cudaMemcpyHostToDevice));
@@ -774,6 +823,12 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
         sat_pass_kernel<<<grid_for(lines[a], 128), 128, 0, c.stream>>>(t->sat[l], HX, HY, HZ, a);
         ++c.launches;
       }
+    }
+    B200_CUDA(cudaMemsetAsync(t->busy, 0, sizeof(unsigned) * 6 * t->ntiles_all, c.stream));
+    for (int l = 2; l <= LL; ++l) {
+      const long long nt = 8LL * (t->HX[l] / TILE_X) * (t->HY[l] / TILE_Y) * (t->HZ[l] / TILE_Z);
+      busy_mask_kernel<<<grid_for(nt * 189, 256), 256, 0, c.stream>>>(*t->params, l, nt, t->busy);
+      ++c.launches;
     }
     t->sat_serial = c.tree_serial;
   }
