@@ -205,7 +205,10 @@ __device__ __forceinline__ long long tile_id(const TcParams &P, int level, int p
 struct BusyMask {
   unsigned w[6];
   __device__ __forceinline__ bool tile() const { return (w[5] >> 31) & 1u; }
-  __device__ __forceinline__ bool src(int e) const { return (w[e >> 5] >> (e & 31)) & 1u; }
+  __device__ __forceinline__ unsigned word(int k) const {
+    return k == 0 ? w[0] : k == 1 ? w[1] : k == 2 ? w[2] : k == 3 ? w[3] : k == 4 ? w[4] : w[5];
+  }
+  __device__ __forceinline__ bool src(int e) const { return (word(e >> 5) >> (e & 31)) & 1u; }
 };
 __device__ __forceinline__ BusyMask busy_mask(const TcParams &P, const TcItem &w) {
   const unsigned *m = P.busy + 6 * tile_id(P, w.level, w.parity, w.bx, w.by, w.bz);
@@ -464,40 +467,58 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
 
 // ---- conversion kernels -----------------------------------------------------------------------------
 
-// occupancy of each parity grid, stored one cell up/right so that three prefix passes give the exclusive
-// summed-area table that box_count reads
-__global__ void occ_mark_kernel(long long n, const long long *__restrict__ keys, int HX, int HY, int HZ,
-                                int *__restrict__ sat) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= n) return;
+// Occupied cells of every level's parity grids, then their summed-area tables, for all levels in one launch
+// each.  The cell marks are stored one cell up/right so that three prefix passes give the exclusive table
+// that box_count reads.
+struct LevelCells {
+  const long long *keys[kMaxHeight];
+  long long start[kMaxHeight + 1];  // concatenated numbering of the cells of levels 2..LL
+  long long lines[3][kMaxHeight + 1];  // the same for the lines of each prefix pass
+  int l0, l1;
+};
+
+__device__ __forceinline__ int level_of(const long long *start, int l0, int l1, long long g) {
+  int l = l0;
+  while (l < l1 && g >= start[l + 1]) ++l;
+  return l;
+}
+
+__global__ void occ_mark_kernel(const __grid_constant__ TcParams P, const __grid_constant__ LevelCells C) {
+  const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (g >= C.start[C.l1 + 1]) return;
+  const int l = level_of(C.start, C.l0, C.l1, g);
+  const TcLevel &L = P.lv[l];
   int ix, iy, iz;
-  morton_decode3(keys[i], ix, iy, iz);
+  morton_decode3(C.keys[l][g - C.start[l]], ix, iy, iz);
   const int c = ((ix & 1) << 2) | ((iy & 1) << 1) | (iz & 1);
-  const size_t SX = HX + 1, SY = HY + 1, SZ = HZ + 1;
+  const size_t SX = L.HX + 1, SY = L.HY + 1, SZ = L.HZ + 1;
+  int *sat = const_cast<int *>(L.sat);
   sat[(((size_t)c * SZ + (iz >> 1) + 1) * SY + (iy >> 1) + 1) * SX + (ix >> 1) + 1] = 1;
 }
 
-__global__ void sat_pass_kernel(int *__restrict__ sat, int HX, int HY, int HZ, int axis) {
-  const long long SX = HX + 1, SY = HY + 1, SZ = HZ + 1;
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  long long base, stride, len, nlines;
+__global__ void sat_pass_kernel(const __grid_constant__ TcParams P, const __grid_constant__ LevelCells C, int axis) {
+  const long long *ls = C.lines[axis];
+  const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (g >= ls[C.l1 + 1]) return;
+  const int l = level_of(ls, C.l0, C.l1, g);
+  const long long t = g - ls[l];
+  const TcLevel &L = P.lv[l];
+  const long long SX = L.HX + 1, SY = L.HY + 1, SZ = L.HZ + 1;
+  long long base, stride, len;
   if (axis == 0) {
-    nlines = 8 * SZ * SY;
     base = t * SX;
     stride = 1;
     len = SX;
   } else if (axis == 1) {
-    nlines = 8 * SZ * SX;
     base = (t / SX) * SY * SX + t % SX;
     stride = SX;
     len = SY;
   } else {
-    nlines = 8 * SY * SX;
     base = (t / (SY * SX)) * SZ * SY * SX + t % (SY * SX);
     stride = SY * SX;
     len = SZ;
   }
-  if (t >= nlines) return;
+  int *sat = const_cast<int *>(L.sat);
   int acc = 0;
   for (long long k = 0; k < len; ++k) {
     acc += sat[base + k * stride];
@@ -505,14 +526,17 @@ __global__ void sat_pass_kernel(int *__restrict__ sat, int HX, int HY, int HZ, i
   }
 }
 
-// busy masks of one level: one thread per (tile, transfer vector)
-__global__ void busy_mask_kernel(const __grid_constant__ TcParams P, int level, long long ntiles,
+// busy masks of every level: one thread per (tile, transfer vector); tiles are numbered across levels
+__global__ void busy_mask_kernel(const __grid_constant__ TcParams P, int l0, int l1, long long ntiles,
                                  unsigned *__restrict__ busy) {
   const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (g >= ntiles * 189) return;
-  const long long tl = g / 189;
+  const long long tg = g / 189;
   const int e = (int)(g % 189);
+  int level = l0;
+  while (level < l1 && tg >= P.lv[level + 1].tile0) ++level;
   const TcLevel &L = P.lv[level];
+  const long long tl = tg - L.tile0;
   const int TX = L.HX / TILE_X, TY = L.HY / TILE_Y, TZ = L.HZ / TILE_Z;
   TcItem w;
   w.level = (short)level;
@@ -520,7 +544,7 @@ __global__ void busy_mask_kernel(const __grid_constant__ TcParams P, int level, 
   w.by = (short)((tl / TX) % TY);
   w.bz = (short)((tl / ((long long)TX * TY)) % TZ);
   w.parity = (short)(tl / ((long long)TX * TY * TZ));
-  unsigned *m = busy + 6 * (L.tile0 + tl);
+  unsigned *m = busy + 6 * tg;
   const SrcBox b = src_box(P, w, e);
   if (box_count(L, b.sp, b.ox, b.oy, b.oz, TILE_X, TILE_Y, TILE_Z) > 0) atomicOr(m + (e >> 5), 1u << (e & 31));
   if (e == 0 && box_count(L, w.parity, w.bx * TILE_X, w.by * TILE_Y, w.bz * TILE_Z, TILE_X, TILE_Y, TILE_Z) > 0)
@@ -610,8 +634,8 @@ struct DenseTC {
   unsigned long long *amax = nullptr;     // [kMaxHeight]
   TcItem *items = nullptr;
   int nitems = 0;
-  int *sat[kMaxHeight] = {};              // occupancy summed-area tables, per level
-  size_t satn[kMaxHeight] = {};
+  int *sat = nullptr;                     // occupancy summed-area tables of all levels
+  size_t satn = 0, sat_off[kMaxHeight] = {};
   long long sat_serial = -1;              // tree the tables describe
   unsigned *busy = nullptr;               // busy masks of every tile of every level
   long long ntiles_all = 0;
@@ -685,8 +709,8 @@ void tc_free(Context &c) {
   for (int l = 0; l < kMaxHeight; ++l) {
     if (t->Ahi[l]) cudaFree(t->Ahi[l]);
     if (t->Alo[l]) cudaFree(t->Alo[l]);
-    if (t->sat[l]) cudaFree(t->sat[l]);
   }
+  if (t->sat) cudaFree(t->sat);
   delete t->params;
   delete t;
   c.tc = nullptr;
@@ -700,6 +724,7 @@ static b200fmm_status tc_prepare(Context &c) {
   std::vector<TcItem> items;
   long long ntiles = 0;
   t->ntiles_all = 0;
+  size_t sat_total = 0;
   for (int l = 2; l <= LL; ++l) {
     const int h = 1 << (l - 1);
     t->HX[l] = std::max(h, TILE_X);
@@ -728,13 +753,8 @@ static b200fmm_status tc_prepare(Context &c) {
     P.lv[l].grid = c.lv[l].grid;
     P.lv[l].L = c.lv[l].L;
     P.lv[l].scale_out = t->scal + 2 * l + 1;
-    const size_t sn = (size_t)8 * (t->HX[l] + 1) * (t->HY[l] + 1) * (t->HZ[l] + 1);
-    if (t->satn[l] != sn) {
-      if (t->sat[l]) cudaFree(t->sat[l]);
-      B200_CUDA(cudaMalloc(&t->sat[l], sn * sizeof(int)));
-      t->satn[l] = sn;
-    }
-    P.lv[l].sat = t->sat[l];
+    t->sat_off[l] = sat_total;
+    sat_total += (size_t)8 * (t->HX[l] + 1) * (t->HY[l] + 1) * (t->HZ[l] + 1);
     P.lv[l].tile0 = (int)t->ntiles_all;
     t->ntiles_all += 8LL * (t->HX[l] / TILE_X) * (t->HY[l] / TILE_Y) * (t->HZ[l] / TILE_Z);
     t->sat_serial = -1;
@@ -771,6 +791,12 @@ static b200fmm_status tc_prepare(Context &c) {
               }
     t->lvl_end[l] = (int)items.size();
   }
+  if (t->satn != sat_total) {
+    if (t->sat) cudaFree(t->sat);
+    B200_CUDA(cudaMalloc(&t->sat, std::max<size_t>(sat_total, 1) * sizeof(int)));
+    t->satn = sat_total;
+  }
+  for (int l = 2; l <= LL; ++l) P.lv[l].sat = t->sat + t->sat_off[l];
   if (t->busy) cudaFree(t->busy);
   B200_CUDA(cudaMalloc(&t->busy, sizeof(unsigned) * 6 * std::max<long long>(t->ntiles_all, 1)));
   P.busy = t->busy;
@@ -811,25 +837,32 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
   if (t->built_for_gen != c.tree_gen) B200_CHECK(tc_prepare(c));
   if (t->sat_serial != c.tree_serial) {
     // which cells of each level are occupied: lets the kernel skip empty target tiles and source boxes
+    LevelCells C{};
+    C.l0 = 2;
+    C.l1 = LL;
+    C.start[2] = 0;
+    for (int a = 0; a < 3; ++a) C.lines[a][2] = 0;
     for (int l = 2; l <= LL; ++l) {
-      const int HX = t->HX[l], HY = t->HY[l], HZ = t->HZ[l];
-      B200_CUDA(cudaMemsetAsync(t->sat[l], 0, t->satn[l] * sizeof(int), c.stream));
-      if (c.lv[l].n) {
-        occ_mark_kernel<<<grid_for(c.lv[l].n, 256), 256, 0, c.stream>>>(c.lv[l].n, c.lv[l].keys, HX, HY, HZ, t->sat[l]);
-        ++c.launches;
-      }
-      const long long lines[3] = {8LL * (HZ + 1) * (HY + 1), 8LL * (HZ + 1) * (HX + 1), 8LL * (HY + 1) * (HX + 1)};
-      for (int a = 0; a < 3; ++a) {
-        sat_pass_kernel<<<grid_for(lines[a], 128), 128, 0, c.stream>>>(t->sat[l], HX, HY, HZ, a);
-        ++c.launches;
-      }
+      const long long HX = t->HX[l], HY = t->HY[l], HZ = t->HZ[l];
+      C.keys[l] = c.lv[l].keys;
+      C.start[l + 1] = C.start[l] + c.lv[l].n;
+      C.lines[0][l + 1] = C.lines[0][l] + 8 * (HZ + 1) * (HY + 1);
+      C.lines[1][l + 1] = C.lines[1][l] + 8 * (HZ + 1) * (HX + 1);
+      C.lines[2][l + 1] = C.lines[2][l] + 8 * (HY + 1) * (HX + 1);
     }
+    const TcParams &P0 = *t->params;
+    B200_CUDA(cudaMemsetAsync(t->sat, 0, t->satn * sizeof(int), c.stream));
     B200_CUDA(cudaMemsetAsync(t->busy, 0, sizeof(unsigned) * 6 * t->ntiles_all, c.stream));
-    for (int l = 2; l <= LL; ++l) {
-      const long long nt = 8LL * (t->HX[l] / TILE_X) * (t->HY[l] / TILE_Y) * (t->HZ[l] / TILE_Z);
-      busy_mask_kernel<<<grid_for(nt * 189, 256), 256, 0, c.stream>>>(*t->params, l, nt, t->busy);
+    if (C.start[LL + 1] > 0) {
+      occ_mark_kernel<<<grid_for(C.start[LL + 1], 256), 256, 0, c.stream>>>(P0, C);
       ++c.launches;
     }
+    for (int a = 0; a < 3; ++a) {
+      sat_pass_kernel<<<grid_for(C.lines[a][LL + 1], 128), 128, 0, c.stream>>>(P0, C, a);
+      ++c.launches;
+    }
+    busy_mask_kernel<<<grid_for(t->ntiles_all * 189, 256), 256, 0, c.stream>>>(P0, 2, LL, t->ntiles_all, t->busy);
+    ++c.launches;
     t->sat_serial = c.tree_serial;
   }
   const int l0 = level == -1 ? 2 : level, l1 = level == -1 ? LL : level;
