@@ -139,6 +139,25 @@ __global__ void __launch_bounds__(P2M_THREADS, 8) p2m_kernel(
   }
 }
 
+// Copy NN doubles with T threads, all loads issued before the first store (one memory latency per copy
+// instead of one per element); ADD adds into dst instead of overwriting.
+template <int NN, int T, bool ADD = false>
+__device__ __forceinline__ void copy_block(double *dst, const double *__restrict__ src, int tid) {
+  constexpr int K = (NN + T - 1) / T;
+  double v[K], d[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int e = tid + k * T;
+    v[k] = e < NN ? src[e] : 0.0;
+    if (ADD) d[k] = e < NN ? dst[e] : 0.0;
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int e = tid + k * T;
+    if (e < NN) dst[e] = ADD ? d[k] + v[k] : v[k];
+  }
+}
+
 // ---- M2M / L2L: one warp per child ------------------------------------------------------------------
 // Each warp applies the child's three 1-D interpolators, one axis at a time, in its own shared-memory
 // buffers.  A lane owns whole lines along the axis: it loads the line's p values into registers and writes
@@ -182,7 +201,7 @@ __global__ void __launch_bounds__(256) m2m_kernel(int R, long long nparents, con
   const int ci = child[pc * 8 + w];
   for (int r = 0; r < R; ++r) {
     if (ci >= 0) {
-      for (int e = lane; e < nn; e += 32) b0[e] = Mc[((long long)ci * R + r) * nn + e];
+      copy_block<nn, 32>(b0, Mc + ((long long)ci * R + r) * nn, lane);
       __syncwarp();
       warp_lines<P, false>(S + (w * 3 + 0) * p * p, 0, b0, b1, lane);
       __syncwarp();
@@ -216,7 +235,7 @@ __global__ void __launch_bounds__(256) l2l_kernel(int R, long long nparents, con
   const int ci = child[pc * 8 + w];
   for (int r = 0; r < R; ++r) {
     __syncthreads();
-    for (int e = threadIdx.x; e < nn; e += blockDim.x) par[e] = Lp[(pc * R + r) * nn + e];
+    copy_block<nn, 256>(par, Lp + (pc * R + r) * nn, threadIdx.x);
     __syncthreads();
     if (ci < 0) continue;
     warp_lines<P, true>(S + (w * 3 + 0) * p * p, 0, par, b0, lane);
@@ -226,7 +245,7 @@ __global__ void __launch_bounds__(256) l2l_kernel(int R, long long nparents, con
     warp_lines<P, true>(S + (w * 3 + 2) * p * p, 2, b1, b0, lane);
     __syncwarp();
     double *out = Lc + ((long long)ci * R + r) * nn;
-    for (int e = lane; e < nn; e += 32) out[e] += b0[e];
+    copy_block<nn, 32, true>(out, b0, lane);
   }
 }
 
@@ -256,7 +275,7 @@ __global__ void __launch_bounds__(L2P_WARPS * 32) l2p_kernel(
   const long long s0 = leaf_start[leaf], s1 = leaf_start[leaf + 1];
   for (int r = 0; r < R; ++r) {
     __syncwarp();
-    for (int e = lane; e < nn; e += 32) Lw[e] = L[(leaf * R + r) * nn + e];
+    copy_block<nn, 32>(Lw, L + (leaf * R + r) * nn, lane);
     __syncwarp();
     for (long long i = s0 + lane; i < s1; i += 32) {
       double wx[P], dwx[P];
