@@ -111,6 +111,13 @@ B200FMM_API b200fmm_status b200fmm_set_charges(b200fmm_handle h, const double *q
  * launches.  A stream that the caller is capturing always gets plain launches. */
 B200FMM_API b200fmm_status b200fmm_execute(b200fmm_handle h, unsigned ops);
 
+/* Tile autotuner (MIXED): times the tensor-core M2L of the current tree with the 189 transfer vectors of
+ * each tile split into 1, 2, 3, 4, 6, 8 and 12 work items, keeps the fastest for this handle, and returns it
+ * with its kernel time (ms); the automatic choice fills the SMs by count.  It runs the M2L several times and
+ * leaves the expansions undefined: call execute() afterwards.  A no-op (splits = 0) in FP64.  The split
+ * changes how the FP32 partial sums are grouped, so results move within the MIXED tolerance. */
+B200FMM_API b200fmm_status b200fmm_autotune(b200fmm_handle h, int *splits, double *ms);
+
 /* Level-batched operators (FAbstractKernels).  They accumulate (+=) like the reference kernels.
  * m2m/l2l take the parent level; m2l the level of the target cells (2..height-1). */
 B200FMM_API b200fmm_status b200fmm_reset_expansions(b200fmm_handle h);

@@ -31,7 +31,7 @@ EXPORTS = (
     "b200fmm_reset_expansions", "b200fmm_zero_results", "b200fmm_p2m", "b200fmm_m2m", "b200fmm_m2l", "b200fmm_l2l", "b200fmm_l2p",
     "b200fmm_p2p", "b200fmm_get_results", "b200fmm_synchronize", "b200fmm_tree_info", "b200fmm_get_cells",
     "b200fmm_get_permutation", "b200fmm_last_timings", "b200fmm_last_kernel_times", "b200fmm_tree_stats",
-    "b200fmm_last_launch_count", "b200fmm_p2p_noalloc", "b200fmm_batch_create", "b200fmm_batch_execute",
+    "b200fmm_last_launch_count", "b200fmm_autotune", "b200fmm_p2p_noalloc", "b200fmm_batch_create", "b200fmm_batch_execute",
     "b200fmm_batch_last_time", "b200fmm_batch_destroy", "b200fmm_direct",
 )
 NOALLOC_MAX_PARTICLES = 262144
@@ -112,6 +112,7 @@ def lib():
         L.b200fmm_p2p_noalloc.argtypes = ([ctypes.c_longlong] + [ctypes.c_void_p] * 4 + [ctypes.c_longlong]
                                           + [ctypes.c_void_p] * 3 + [ctypes.c_int, ctypes.c_double, _dp, ctypes.c_int]
                                           + [ctypes.c_void_p] * 5)
+        L.b200fmm_autotune.argtypes = [ctypes.c_void_p, _ip, _dp]
         L.b200fmm_batch_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                            ctypes.POINTER(ctypes.c_void_p)]
         L.b200fmm_batch_execute.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
@@ -216,6 +217,12 @@ class FMM:
 
     def reset_expansions(self):
         _check(lib().b200fmm_reset_expansions(self._h), "reset_expansions")
+
+    def autotune(self):
+        """Pick the tensor-core M2L work split for the current tree (MIXED); returns (splits, kernel ms)."""
+        k, ms = ctypes.c_int(), ctypes.c_double()
+        _check(lib().b200fmm_autotune(self._h, ctypes.byref(k), ctypes.byref(ms)), "autotune")
+        return k.value, ms.value
 
     def zero_results(self):
         _check(lib().b200fmm_zero_results(self._h), "zero_results")

@@ -409,6 +409,43 @@ b200fmm_status b200fmm_execute(b200fmm_handle h, unsigned ops) {
   return B200FMM_OK;
 }
 
+b200fmm_status b200fmm_autotune(b200fmm_handle h, int *splits, double *ms) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  B200_CHECK(need_particles(c));
+  B200_CHECK(set_device(c));
+  if (splits) *splits = 0;
+  if (ms) *ms = 0;
+  if (c.cfg.precision != B200FMM_MIXED || !c.tc) return B200FMM_OK;  // nothing to tune
+  drop_graph(c);
+  c.eager_serial = -1;
+  const int cand[] = {1, 2, 3, 4, 6, 8, 12};
+  int best = 0;
+  float best_ms = 0.f;
+  for (int k : cand) {
+    tc_set_splits(c, k);
+    float t = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {  // the first run rebuilds the work items
+      B200_CHECK(execute_body(c, B200FMM_P2M | B200FMM_M2M | B200FMM_M2L));
+      B200_CUDA(cudaEventSynchronize(c.ev[7]));
+      B200_CHECK(check_status(c));
+      if (cudaEventElapsedTime(&t, c.ev[8], c.ev[9]) != cudaSuccess) {
+        cudaGetLastError();
+        t = 1e30f;
+      }
+    }
+    if (best == 0 || t < best_ms) {
+      best = k;
+      best_ms = t;
+    }
+  }
+  tc_set_splits(c, best);
+  c.state_zero = false;
+  if (splits) *splits = best;
+  if (ms) *ms = best_ms;
+  return B200FMM_OK;
+}
+
 b200fmm_status b200fmm_p2m(b200fmm_handle h) {
   B200_CHECK(check_handle(h));
   h->state_zero = false;

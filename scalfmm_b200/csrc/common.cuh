@@ -183,6 +183,8 @@ b200fmm_status run_m2l_fp64(Context &c, int level);
 b200fmm_status tc_init(Context &c);
 void tc_free(Context &c);
 b200fmm_status run_m2l_tc(Context &c, int level);
+void tc_set_splits(Context &c, int splits);
+int tc_splits_used(const Context &c);
 // direct.cu
 b200fmm_status run_direct(long long n, const double *x, const double *y, const double *z, const double *q,
                           long long nt, const long long *targets, double *phi, double *fx, double *fy, double *fz,

@@ -641,6 +641,8 @@ struct DenseTC {
   long long ntiles_all = 0;
   int lvl_begin[kMaxHeight] = {}, lvl_end[kMaxHeight] = {};
   long long built_for_N = -1;             // tree the per-level buffers were sized for
+  int splits = 0;                         // transfer-vector splits per tile: 0 = by SM fill, else fixed
+  int splits_used = 0;
   int built_for_gen = -1;                 // tree generation the tensor maps / pointers belong to
   TcParams *params = nullptr;             // host copy
   int grid = 0;
@@ -768,7 +770,9 @@ static b200fmm_status tc_prepare(Context &c) {
     ns = k;
     if ((double)n / (double)(rounds * t->grid) >= 0.9) break;
   }
+  if (t->splits > 0) ns = t->splits;  // chosen by b200fmm_autotune
   if (const char *e = getenv("B200FMM_TC_SPLITS")) ns = std::max(1, std::min(189, atoi(e)));
+  t->splits_used = ns;
   for (int l = LL; l >= 2; --l) {
     t->lvl_begin[l] = (int)items.size();
     for (int r = 0; r < c.R; ++r)
@@ -908,5 +912,17 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
   B200_CUDA(cudaGetLastError());
   return B200FMM_OK;
 }
+
+}  // namespace b200
+
+namespace b200 {
+
+// Splits of the 189 transfer vectors of each tile into work items: set (0 = automatic) and read back.
+void tc_set_splits(Context &c, int splits) {
+  if (!c.tc) return;
+  c.tc->splits = splits;
+  c.tc->built_for_gen = -1;  // the item list is rebuilt by the next run
+}
+int tc_splits_used(const Context &c) { return c.tc ? c.tc->splits_used : 0; }
 
 }  // namespace b200

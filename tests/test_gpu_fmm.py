@@ -423,3 +423,26 @@ def test_batch_matches_single_problems(kernel, precision, tol):
             for k in FIELDS:
                 assert S.rel_l2(out[k], want[k]) < tol, (pr["order"], pr["height"], k)
     b.close()
+
+
+def test_autotune_keeps_mixed_accuracy():
+    """The split autotuner picks one of its candidates, reports a kernel time, and the evaluation after it
+    stays within the MIXED tolerance of FP64 (the split only regroups FP32 partial sums)."""
+    rng = np.random.default_rng(51)
+    n, height = 30000, 5
+    x, y, z = rng.random((3, n))
+    q = rng.uniform(-1, 1, n)
+    f = S.FMM("cheb_sym", 6, height, precision="mixed")
+    f.set_particles(x, y, z, q)
+    k, ms = f.autotune()
+    assert k in (1, 2, 3, 4, 6, 8, 12) and ms > 0
+    f.execute()
+    got = f.results()
+    f.close()
+    g = S.FMM("cheb_dense", 6, height)
+    g.set_particles(x, y, z, q)
+    g.execute()
+    want = g.results()
+    g.close()
+    for key in FIELDS:
+        assert S.rel_l2(got[key], want[key]) < 2e-6, key
