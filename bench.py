@@ -314,6 +314,7 @@ def run_gpu(args):
         f.results_into(*out_h)
 
     step_device()
+    tuned_splits, _ = f.autotune()  # tensor-core M2L work split for this tree shape, kept by the handle
     for _ in range(args.warmup):
         step_device()
         step_e2e()
@@ -382,6 +383,7 @@ def run_gpu(args):
                 "tflops_at_20_per_pair": p2p_tflops, "frac_fp32_peak": p2p_tflops / fp32_peak,
                 "fp32_peak_note": "148 SMs x 128 FP32 lanes x 2 x 1965 MHz (nominal)"},
         "pass_ms": f.timings(),
+        "autotuned_m2l_splits": tuned_splits,
         "clocks": clk.summary(),
     }
     f.close()
