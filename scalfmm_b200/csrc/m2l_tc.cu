@@ -42,14 +42,13 @@ constexpr int TC_THREADS = 320;
 constexpr int TILE_X = 8, TILE_Y = 4, TILE_Z = 4;  // 128 targets
 constexpr int KCHUNK = 32;                          // fp16 elements per 64-byte swizzle row
 constexpr int SB = 15;                              // operator pre-scale 2^15
-constexpr int MAX_STAGES = 6;
+constexpr int MAX_STAGES = 4;
 constexpr long long WAIT_LIMIT = 1LL << 22;
 
 struct TcItem {
   short level, rhs, parity, split;
   short bx, by, bz;
   short t0, t1;
-  short half;  // column half of the operator rows (orders whose p^3 exceeds one 256-wide MMA)
 };
 
 struct TcLevel {
@@ -87,7 +86,6 @@ struct __align__(64) TcParams {
   int R, nn, KP, NP, NH, NHALF, NK, stages, ncols;
   int nseg;  // accumulator resets per transfer vector (the K chunks are split into nseg segments)
   int nbuf;  // TMEM accumulators: 2 (alternating per segment) when 2 * NP columns fit, else 1
-  int colsplit;  // column halves run as separate items (1, or 2 when p^3 > 256); NP is one half
   int stage_bytes;
   signed char off[8][189][3];
   short slot[8][189];
@@ -295,10 +293,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
             tma_load_5d(sbuf + a_bytes, &P.mapA_lo[w.level], &full_bar[stage], kc * KCHUNK, ox, oy, oz,
                         w.rhs * 8 + sp);
             for (int h = 0; h < P.NHALF; ++h) {
-              const int row = (w.half * P.NHALF + h) * P.NH;  // operator rows of this item's column half
-              tma_load_3d(sbuf + 2 * a_bytes + h * P.NH * 64, &P.mapB_hi, &full_bar[stage], kc * KCHUNK, row, slot);
+              tma_load_3d(sbuf + 2 * a_bytes + h * P.NH * 64, &P.mapB_hi, &full_bar[stage], kc * KCHUNK, h * P.NH, slot);
               tma_load_3d(sbuf + 2 * a_bytes + b_bytes + h * P.NH * 64, &P.mapB_lo, &full_bar[stage], kc * KCHUNK,
-                          row, slot);
+                          h * P.NH, slot);
             }
             if (++stage == S) {
               stage = 0;
@@ -392,13 +389,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
     const unsigned tlane = tmem + ((unsigned)(q * 32) << 16);
     unsigned full_par = 0;
     int seg = 0;
-    // one column half: part 0 owns columns [0, PA), part 1 [PA, 2 CW), PA a multiple of 16 so that every
-    // TMEM load starts on a 16-column boundary (for 2 CW = 176: 96 and 80)
-    constexpr int PA = NHALF == 1 ? 16 * ((CW + 15) / 16) : CW, PB = NHALF == 1 ? 2 * CW - PA : CW;
-    constexpr int NACC = PA > CW ? PA : CW;
-    float acc[NACC];
+    float acc[CW];
 #pragma unroll
-    for (int i = 0; i < NACC; ++i) acc[i] = 0.f;
+    for (int i = 0; i < CW; ++i) acc[i] = 0.f;
     for (int it = blockIdx.x; it < P.nitems && !abort_sh; it += gridDim.x) {
       const TcItem w = P.items[P.item0 + it];
       int nbusy = 0;  // transfer vectors of this item that the MMA warp runs
@@ -418,13 +411,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
         tc_fence_after();
         const unsigned tb = tlane + (unsigned)(b * P.NP);
         if constexpr (NHALF == 1) {
-          if constexpr (PA == PB) {
-            drain_cols<PA>(tb + ch * PA, acc);
-          } else {
-            // both parts drain PB columns with the same code; part 0 then drains its extra PA - PB
-            drain_cols<PB>(tb + (ch == 0 ? 0 : PA), acc);
-            if (ch == 0) drain_cols<PA - PB>(tb + PB, acc + PB);
-          }
+          drain_cols<CW>(tb + ch * CW, acc);
           tc_fence_before();
           __syncwarp();
           if (lane == 0) mbar_arrive(&acc_empty[b][0]);
@@ -457,25 +444,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
         const double sc = *Lv.scale_out;
         double *Lrow = Lv.L + ((long long)cell * P.R + w.rhs) * P.nn;
         // first accumulator column of this thread's part in each half, and the part's width in half 0
-        const int n0 = w.half * P.NP + (NHALF == 1 ? (ch == 0 ? 0 : PA) : (ch == 0 ? 0 : SPLIT));
-        const int w0 = NHALF == 1 ? (ch == 0 ? PA : PB) : (ch == 0 ? SPLIT : CW - SPLIT);
-        const int n1 = w.half * P.NP + (NHALF == 1 ? 0 : (ch == 0 ? CW : 2 * CW - SPLIT));
-        const int wtot = NHALF == 1 ? w0 : CW;  // accumulators this thread holds
-        // one column at a time: the volatile statements keep each conversion next to its reduction, so the
-        // compiler does not hoist all of them (which would need twice the accumulators' registers)
+        const int n0 = NHALF == 1 ? ch * CW : (ch == 0 ? 0 : SPLIT);
+        const int w0 = NHALF == 1 ? CW : (ch == 0 ? SPLIT : CW - SPLIT);
+        const int n1 = NHALF == 1 ? 0 : (ch == 0 ? CW : 2 * CW - SPLIT);
 #pragma unroll
-        for (int i = 0; i < NACC; ++i) {
-          float v = acc[i];
-          asm volatile("" : "+f"(v));
+        for (int i = 0; i < CW; ++i) {
           const int n = i < w0 ? n0 + i : n1 + (i - w0);
-          if (i < wtot && n < P.nn) {
-            const double d = (double)v * sc;
-            asm volatile("red.global.add.f64 [%0], %1;" ::"l"(Lrow + n), "d"(d) : "memory");
-          }
+          if (n < P.nn) atomicAdd(Lrow + n, (double)acc[i] * sc);
         }
       }
 #pragma unroll
-      for (int i = 0; i < NACC; ++i) acc[i] = 0.f;
+      for (int i = 0; i < CW; ++i) acc[i] = 0.f;
     }
   }
   __syncthreads();
@@ -646,7 +625,6 @@ EncodeTiledFn encode_fn() {
 
 struct DenseTC {
   int KP = 0, NP = 0, NH = 0, NHALF = 0, NK = 0, stages = 0, ncols = 0, stage_bytes = 0, nbuf = 1;
-  int NROWS = 0, colsplit = 1;  // operator rows (padded p^3) and the column halves they run in
   __half *Bhi = nullptr, *Blo = nullptr;
   // per level
   __half *Ahi[kMaxHeight] = {}, *Alo[kMaxHeight] = {};
@@ -688,16 +666,11 @@ b200fmm_status tc_init(Context &c) {
   c.tc = t;
   const int nn = c.nn;
   t->KP = (nn + KCHUNK - 1) / KCHUNK * KCHUNK;
-  // operator rows: when p^3 exceeds one 256-wide MMA the rows are split into two column halves that run
-  // as separate work items, so that an item's accumulator (and each epilogue thread's share) is half as
-  // wide: two TMEM buffers fit, the running sums stay in registers and the stages are smaller
-  t->NROWS = t->KP;
-  t->colsplit = t->NROWS > 256 ? 2 : 1;
-  t->NP = t->NROWS / t->colsplit;  // accumulator width of one item
-  t->NHALF = 1;
-  t->NH = t->NP;
+  t->NP = t->KP;
+  t->NHALF = t->NP > 256 ? 2 : 1;
+  t->NH = t->NP / t->NHALF;
   if (t->NH % 16 != 0 || t->NH > 256) return fail(B200FMM_ERR_UNSUPPORTED, "unsupported node count for the MMA tile");
-  if (t->NROWS > 352) return fail(B200FMM_ERR_UNSUPPORTED, "the tensor-core M2L supports orders up to 7");
+  if (t->NP > 352) return fail(B200FMM_ERR_UNSUPPORTED, "the tensor-core M2L supports orders up to 7");
   t->NK = t->KP / KCHUNK;
   t->stage_bytes = 2 * (TILE_X * TILE_Y * TILE_Z * KCHUNK * 2) + 2 * t->NP * KCHUNK * 2;
   t->stages = std::min(MAX_STAGES, (220 * 1024) / t->stage_bytes);
@@ -705,11 +678,11 @@ b200fmm_status tc_init(Context &c) {
   t->nbuf = 2 * t->NP <= 512 ? 2 : 1;
   t->ncols = 32;
   while (t->ncols < t->nbuf * t->NP) t->ncols *= 2;
-  const size_t bsz = (size_t)343 * t->NROWS * t->KP;
+  const size_t bsz = (size_t)343 * t->NP * t->KP;
   B200_CUDA(cudaMalloc(&t->Bhi, bsz * sizeof(__half)));
   B200_CUDA(cudaMalloc(&t->Blo, bsz * sizeof(__half)));
-  pack_operators<<<dim3(grid_for((long long)t->NROWS * t->KP, 256), 343), 256>>>(nn, t->KP, t->NROWS, c.d_dense,
-                                                                               t->Bhi, t->Blo);
+  pack_operators<<<dim3(grid_for((long long)t->NP * t->KP, 256), 343), 256>>>(nn, t->KP, t->NP, c.d_dense, t->Bhi,
+                                                                            t->Blo);
   B200_CUDA(cudaGetLastError());
   B200_CUDA(cudaDeviceSynchronize());
   // the FP64 dense operators are not needed by the mixed path after packing
@@ -719,8 +692,8 @@ b200fmm_status tc_init(Context &c) {
   B200_CUDA(cudaMalloc(&t->amax, sizeof(unsigned long long) * kMaxHeight));
   t->params = new TcParams();
   std::memset(t->params, 0, sizeof(TcParams));
-  cuuint64_t dims[3] = {(cuuint64_t)t->KP, (cuuint64_t)t->NROWS, 343};
-  cuuint64_t strides[2] = {(cuuint64_t)t->KP * 2, (cuuint64_t)t->KP * 2 * t->NROWS};
+  cuuint64_t dims[3] = {(cuuint64_t)t->KP, (cuuint64_t)t->NP, 343};
+  cuuint64_t strides[2] = {(cuuint64_t)t->KP * 2, (cuuint64_t)t->KP * 2 * t->NP};
   cuuint32_t box[3] = {KCHUNK, (cuuint32_t)t->NH, 1};
   B200_CHECK(encode(&t->params->mapB_hi, t->Bhi, 3, dims, strides, box));
   B200_CHECK(encode(&t->params->mapB_lo, t->Blo, 3, dims, strides, box));
@@ -792,7 +765,7 @@ static b200fmm_status tc_prepare(Context &c) {
   // split the 189 transfer vectors of each tile so that the items fill the SMs evenly
   int ns = 1;
   for (int k = 1; k <= 8; ++k) {
-    const long long n = ntiles * t->colsplit * k;
+    const long long n = ntiles * k;
     const long long rounds = (n + t->grid - 1) / t->grid;
     ns = k;
     if ((double)n / (double)(rounds * t->grid) >= 0.9) break;
@@ -807,10 +780,8 @@ static b200fmm_status tc_prepare(Context &c) {
         for (int bz = 0; bz < t->HZ[l] / TILE_Z; ++bz)
           for (int by = 0; by < t->HY[l] / TILE_Y; ++by)
             for (int bx = 0; bx < t->HX[l] / TILE_X; ++bx)
-              for (int s = 0; s < ns; ++s)
-                for (int hh = 0; hh < t->colsplit; ++hh) {
+              for (int s = 0; s < ns; ++s) {
                 TcItem w;
-                w.half = (short)hh;
                 w.level = (short)l;
                 w.rhs = (short)r;
                 w.parity = (short)par;
@@ -853,7 +824,6 @@ static b200fmm_status tc_prepare(Context &c) {
   // accumulator resets per transfer vector: 2 for p >= 6 keeps the M2L within ~1e-6 of FP64
   P.nseg = std::min(t->NK, c.p >= 6 ? 2 : 1);
   P.nbuf = t->nbuf;
-  P.colsplit = t->colsplit;
   if (const char *e = getenv("B200FMM_TC_SEGMENTS")) P.nseg = std::max(1, std::min(t->NK, atoi(e)));
   std::memcpy(P.off, c.itab.off, sizeof(P.off));
   std::memcpy(P.slot, c.itab.slot, sizeof(P.slot));
@@ -932,7 +902,7 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
     B200_TC_CASE(64, 32, 1)
     B200_TC_CASE(128, 64, 1)
     B200_TC_CASE(224, 112, 1)
-    B200_TC_CASE(176, 88, 1)
+    B200_TC_CASE(352, 176, 2)
 #undef B200_TC_CASE
     default:
       return fail(B200FMM_ERR_UNSUPPORTED, "no tensor-core M2L instance for this order");
