@@ -39,7 +39,6 @@ namespace b200 {
 namespace {
 
 constexpr int TC_THREADS = 320;
-constexpr int TC_THREADS_PAIR = 352;  // + one warp that forwards this CTA's operator half to the peer CTA
 constexpr int TILE_X = 8, TILE_Y = 4, TILE_Z = 4;  // 128 targets
 constexpr int KCHUNK = 32;                          // fp16 elements per 64-byte swizzle row
 constexpr int SB = 15;                              // operator pre-scale 2^15
@@ -87,7 +86,6 @@ struct __align__(64) TcParams {
   int R, nn, KP, NP, NH, NHALF, NK, stages, ncols;
   int nseg;  // accumulator resets per transfer vector (the K chunks are split into nseg segments)
   int nbuf;  // TMEM accumulators: 2 (alternating per segment) when 2 * NP columns fit, else 1
-  int NBH;   // CTA-pair mode: operator rows each CTA of the pair loads (NP / 2); 0 without pairs
   int stage_bytes;
   signed char off[8][189][3];
   short slot[8][189];
@@ -151,34 +149,6 @@ __device__ __forceinline__ void mma_f16(unsigned d_tmem, unsigned long long da, 
 }
 __device__ __forceinline__ void mma_commit(unsigned long long *bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar))
-               : "memory");
-}
-// CTA pairs (clusters of two CTAs whose target tiles share every operator chunk)
-__device__ __forceinline__ unsigned cluster_rank() {
-  unsigned r;
-  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ void cluster_sync() {
-  asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-// address of the same shared-memory object in CTA `rank` of the cluster
-__device__ __forceinline__ unsigned mapa(unsigned a, unsigned rank) {
-  unsigned d;
-  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(rank));
-  return d;
-}
-// bulk copy of this CTA's shared memory into another CTA's, completing on that CTA's mbarrier
-__device__ __forceinline__ void bulk_to_peer(unsigned dst, unsigned src, unsigned bytes, unsigned bar) {
-  asm volatile("cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-               "r"(src), "r"(bytes), "r"(bar)
-               : "memory");
-}
-// commit whose arrival goes to the same mbarrier in every CTA of ctamask
-__device__ __forceinline__ void mma_commit_mc(unsigned long long *bar, unsigned short ctamask) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
-                   su32(bar)),
-               "h"(ctamask)
                : "memory");
 }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -248,26 +218,6 @@ __device__ __forceinline__ BusyMask busy_mask(const TcParams &P, const TcItem &w
   return b;
 }
 
-// The work item of this CTA and the busy mask that decides which transfer vectors run.  With CTA pairs an
-// item covers two z-adjacent tiles, one per CTA (rank r takes tile 2 bz + r), and both CTAs run the union
-// of the two tiles' masks so that they walk the same operator chunks.
-template <bool PAIR>
-__device__ __forceinline__ void load_item(const TcParams &P, int it, unsigned rank, TcItem &own, BusyMask &bm) {
-  const TcItem w = P.items[P.item0 + it];
-  own = w;
-  if (PAIR) {
-    own.bz = (short)(2 * w.bz + rank);
-    TcItem a = w, b = w;
-    a.bz = (short)(2 * w.bz);
-    b.bz = (short)(2 * w.bz + 1);
-    const BusyMask m0 = busy_mask(P, a), m1 = busy_mask(P, b);
-#pragma unroll
-    for (int k = 0; k < 6; ++k) bm.w[k] = m0.w[k] | m1.w[k];
-  } else {
-    bm = busy_mask(P, w);
-  }
-}
-
 // ---- the kernel -------------------------------------------------------------------------------------
 // CW: accumulator columns owned by one epilogue thread (NP / 2) and NHALF: MMA column halves, compile-time
 // constants so that the running sums stay in registers.  With one half a thread owns the columns
@@ -280,35 +230,22 @@ __device__ __forceinline__ void load_item(const TcParams &P, int it, unsigned ra
 // s+1 runs in the other accumulator while segment s drains.  With one (order 7: 352 of 512 columns) the
 // epilogue drains half 0 first and releases it, and the first chunk of the next segment issues all its
 // half-0 MMAs before waiting for half 1.
-//
-// PAIR: the grid is made of clusters of two CTAs that take z-adjacent target tiles with the same transfer
-// vectors, so every operator chunk is needed by both.  Each CTA loads one half of the operator rows from
-// L2 and a forwarding warp copies that half into the peer CTA's stage over the cluster's shared-memory
-// network; each stage's slot is freed only when both CTAs' MMAs have read it.  This halves the operator
-// traffic from L2, which bounds the kernel.
-template <int CW, int NHALF, bool PAIR>
-__global__ void __launch_bounds__(PAIR ? TC_THREADS_PAIR : TC_THREADS, 1) m2l_tc_kernel(const __grid_constant__ TcParams P) {
+template <int CW, int NHALF>
+__global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_constant__ TcParams P) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1024-byte aligned stage buffers (the swizzle pattern repeats every 512 B)
   unsigned char *smem = (unsigned char *)(((unsigned long long)smem_raw + 1023) & ~1023ull);
-  __shared__ __align__(8) unsigned long long full_bar[MAX_STAGES], empty_bar[MAX_STAGES], half_bar[MAX_STAGES];
+  __shared__ __align__(8) unsigned long long full_bar[MAX_STAGES], empty_bar[MAX_STAGES];
   __shared__ __align__(8) unsigned long long acc_full[2], acc_empty[2][2];
   __shared__ unsigned tmem_base_sh;
   __shared__ volatile int abort_sh;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int S = P.stages;
-  const unsigned crank = PAIR ? cluster_rank() : 0u;
-  const int first = PAIR ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
-  const int step = PAIR ? (int)(gridDim.x >> 1) : (int)gridDim.x;
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
-      // PAIR: a stage is full when the local producer and forwarder have arrived and A, the own operator
-      // half (forwarder's arrival) and the peer's half (its bulk copy) have landed; it is empty when both
-      // CTAs' MMAs have read it
-      mbar_init(&full_bar[s], PAIR ? 2 : 1);
-      mbar_init(&empty_bar[s], PAIR ? 2 : 1);
-      mbar_init(&half_bar[s], 1);
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&acc_full[b], 1);
@@ -325,7 +262,6 @@ __global__ void __launch_bounds__(PAIR ? TC_THREADS_PAIR : TC_THREADS, 1) m2l_tc
   }
   tc_fence_before();
   __syncthreads();
-  if (PAIR) cluster_sync();  // both CTAs' barriers exist before any cross-CTA arrival
   tc_fence_after();
   const unsigned tmem = tmem_base_sh;
 
@@ -337,10 +273,9 @@ __global__ void __launch_bounds__(PAIR ? TC_THREADS_PAIR : TC_THREADS, 1) m2l_tc
     if (lane == 0) {
       int stage = 0;
       unsigned phase = 0;
-      for (int it = first; it < P.nitems && !abort_sh; it += step) {
-        TcItem w;
-        BusyMask bm;
-        load_item<PAIR>(P, it, crank, w, bm);
+      for (int it = blockIdx.x; it < P.nitems && !abort_sh; it += gridDim.x) {
+        const TcItem w = P.items[P.item0 + it];
+        const BusyMask bm = busy_mask(P, w);
         if (!bm.tile()) continue;
         for (int e = w.t0; e < w.t1 && !abort_sh; ++e) {
           if (!bm.src(e)) continue;
@@ -353,23 +288,6 @@ __global__ void __launch_bounds__(PAIR ? TC_THREADS_PAIR : TC_THREADS, 1) m2l_tc
               break;
             }
             unsigned char *sbuf = smem + (size_t)stage * P.stage_bytes;
-            if (PAIR) {
-              const int rows = P.NBH;
-              mbar_expect_tx(&full_bar[stage], 2 * a_bytes + 2 * rows * 64);  // A and the peer's half
-              mbar_expect_tx(&half_bar[stage], 2 * rows * 64);                 // this CTA's half
-              tma_load_5d(sbuf, &P.mapA_hi[w.level], &full_bar[stage], kc * KCHUNK, ox, oy, oz, w.rhs * 8 + sp);
-              tma_load_5d(sbuf + a_bytes, &P.mapA_lo[w.level], &full_bar[stage], kc * KCHUNK, ox, oy, oz,
-                          w.rhs * 8 + sp);
-              tma_load_3d(sbuf + 2 * a_bytes + crank * rows * 64, &P.mapB_hi, &half_bar[stage], kc * KCHUNK,
-                          (int)crank * rows, slot);
-              tma_load_3d(sbuf + 2 * a_bytes + b_bytes + crank * rows * 64, &P.mapB_lo, &half_bar[stage], kc * KCHUNK,
-                          (int)crank * rows, slot);
-              if (++stage == S) {
-                stage = 0;
-                phase ^= 1;
-              }
-              continue;
-            }
             mbar_expect_tx(&full_bar[stage], 2 * a_bytes + 2 * b_bytes);
             tma_load_5d(sbuf, &P.mapA_hi[w.level], &full_bar[stage], kc * KCHUNK, ox, oy, oz, w.rhs * 8 + sp);
             tma_load_5d(sbuf + a_bytes, &P.mapA_lo[w.level], &full_bar[stage], kc * KCHUNK, ox, oy, oz,
@@ -396,10 +314,9 @@ __global__ void __launch_bounds__(PAIR ? TC_THREADS_PAIR : TC_THREADS, 1) m2l_tc
       unsigned empty_par = 0xFu;  // parity to wait for, per (buffer, half): starts at 1 (passes at once)
       int seg = 0;
       const bool defer = (P.nbuf == 1 && NHALF == 2);
-      for (int it = first; it < P.nitems && !abort_sh; it += step) {
-        TcItem w;
-        BusyMask bm;
-        load_item<PAIR>(P, it, crank, w, bm);
+      for (int it = blockIdx.x; it < P.nitems && !abort_sh; it += gridDim.x) {
+        const TcItem w = P.items[P.item0 + it];
+        const BusyMask bm = busy_mask(P, w);
         if (!bm.tile()) continue;
         for (int e = w.t0; e < w.t1 && !abort_sh; ++e) {
           if (!bm.src(e)) continue;
@@ -452,51 +369,13 @@ __global__ void __launch_bounds__(PAIR ? TC_THREADS_PAIR : TC_THREADS, 1) m2l_tc
                 }
               }
               if (abort_sh) break;
-              // frees the stage once these MMAs have read it (PAIR: in both CTAs, which share its operator)
-              if (PAIR)
-                mma_commit_mc(&empty_bar[stage], (unsigned short)0x3);
-              else
-                mma_commit(&empty_bar[stage]);
+              mma_commit(&empty_bar[stage]);  // frees the stage once these MMAs have read it
               if (++stage == S) {
                 stage = 0;
                 phase ^= 1;
               }
             }
             mma_commit(&acc_full[b]);  // segment accumulated
-          }
-        }
-      }
-    }
-  } else if (PAIR && warp == TC_THREADS / 32) {
-    // ------------------------------------------------ forwarder (CTA pairs): this CTA's operator half to the peer
-    if (lane == 0) {
-      const unsigned peer = crank ^ 1u;
-      const int rows = P.NBH;
-      int stage = 0;
-      unsigned phase = 0;
-      for (int it = first; it < P.nitems && !abort_sh; it += step) {
-        TcItem w;
-        BusyMask bm;
-        load_item<PAIR>(P, it, crank, w, bm);
-        if (!bm.tile()) continue;
-        for (int e = w.t0; e < w.t1 && !abort_sh; ++e) {
-          if (!bm.src(e)) continue;
-          for (int kc = 0; kc < P.NK; ++kc) {
-            if (!mbar_wait(&half_bar[stage], phase)) {  // this CTA's half has landed
-              atomicExch(P.status + 1, 1);
-              abort_sh = 1;
-              break;
-            }
-            const unsigned char *sbuf = smem + (size_t)stage * P.stage_bytes;
-            const unsigned src_hi = su32(sbuf + 2 * a_bytes + crank * rows * 64), src_lo = src_hi + b_bytes;
-            const unsigned rbar = mapa(su32(&full_bar[stage]), peer);
-            bulk_to_peer(mapa(src_hi, peer), src_hi, rows * 64, rbar);
-            bulk_to_peer(mapa(src_lo, peer), src_lo, rows * 64, rbar);
-            mbar_arrive(&full_bar[stage]);  // and is present here
-            if (++stage == S) {
-              stage = 0;
-              phase ^= 1;
-            }
           }
         }
       }
@@ -513,11 +392,10 @@ __global__ void __launch_bounds__(PAIR ? TC_THREADS_PAIR : TC_THREADS, 1) m2l_tc
     float acc[CW];
 #pragma unroll
     for (int i = 0; i < CW; ++i) acc[i] = 0.f;
-    for (int it = first; it < P.nitems && !abort_sh; it += step) {
-      TcItem w;
-      BusyMask bm;
-      load_item<PAIR>(P, it, crank, w, bm);
+    for (int it = blockIdx.x; it < P.nitems && !abort_sh; it += gridDim.x) {
+      const TcItem w = P.items[P.item0 + it];
       int nbusy = 0;  // transfer vectors of this item that the MMA warp runs
+      const BusyMask bm = busy_mask(P, w);
       if (bm.tile())
         for (int e = w.t0; e < w.t1; ++e) nbusy += bm.src(e) ? 1 : 0;
       if (nbusy == 0) continue;  // nothing accumulated: no flush
@@ -585,8 +463,6 @@ __global__ void __launch_bounds__(PAIR ? TC_THREADS_PAIR : TC_THREADS, 1) m2l_tc
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P.ncols));
   }
-  // PAIR: neither CTA leaves while the other may still read its shared memory or arrive on its barriers
-  if (PAIR) cluster_sync();
 }
 
 // ---- conversion kernels -----------------------------------------------------------------------------
@@ -749,8 +625,6 @@ EncodeTiledFn encode_fn() {
 
 struct DenseTC {
   int KP = 0, NP = 0, NH = 0, NHALF = 0, NK = 0, stages = 0, ncols = 0, stage_bytes = 0, nbuf = 1;
-  bool pair = false;  // CTA pairs sharing each operator chunk (B200FMM_TC_PAIR=0 turns them off)
-  int NBH = 0;        // operator rows each CTA of a pair loads
   __half *Bhi = nullptr, *Blo = nullptr;
   // per level
   __half *Ahi[kMaxHeight] = {}, *Alo[kMaxHeight] = {};
@@ -804,11 +678,6 @@ b200fmm_status tc_init(Context &c) {
   t->nbuf = 2 * t->NP <= 512 ? 2 : 1;
   t->ncols = 32;
   while (t->ncols < t->nbuf * t->NP) t->ncols *= 2;
-  {
-    const char *e = getenv("B200FMM_TC_PAIR");
-    t->pair = !(e && e[0] == '0');
-  }
-  t->NBH = t->NP / 2;  // a multiple of 16 rows: the 512-byte swizzle atoms of the two halves line up
   const size_t bsz = (size_t)343 * t->NP * t->KP;
   B200_CUDA(cudaMalloc(&t->Bhi, bsz * sizeof(__half)));
   B200_CUDA(cudaMalloc(&t->Blo, bsz * sizeof(__half)));
@@ -825,7 +694,7 @@ b200fmm_status tc_init(Context &c) {
   std::memset(t->params, 0, sizeof(TcParams));
   cuuint64_t dims[3] = {(cuuint64_t)t->KP, (cuuint64_t)t->NP, 343};
   cuuint64_t strides[2] = {(cuuint64_t)t->KP * 2, (cuuint64_t)t->KP * 2 * t->NP};
-  cuuint32_t box[3] = {KCHUNK, (cuuint32_t)(t->pair ? t->NBH : t->NH), 1};
+  cuuint32_t box[3] = {KCHUNK, (cuuint32_t)t->NH, 1};
   B200_CHECK(encode(&t->params->mapB_hi, t->Bhi, 3, dims, strides, box));
   B200_CHECK(encode(&t->params->mapB_lo, t->Blo, 3, dims, strides, box));
   int dev_sms = 148;
@@ -862,7 +731,7 @@ static b200fmm_status tc_prepare(Context &c) {
     const int h = 1 << (l - 1);
     t->HX[l] = std::max(h, TILE_X);
     t->HY[l] = std::max(h, TILE_Y);
-    t->HZ[l] = std::max(h, t->pair ? 2 * TILE_Z : TILE_Z);  // pairs take two z-adjacent tiles
+    t->HZ[l] = std::max(h, TILE_Z);
     const size_t elems = (size_t)c.R * 8 * t->HZ[l] * t->HY[l] * t->HX[l] * t->KP;
     if (t->Abytes[l] != elems * sizeof(__half)) {
       if (t->Ahi[l]) cudaFree(t->Ahi[l]);
@@ -895,13 +764,11 @@ static b200fmm_status tc_prepare(Context &c) {
   }
   // split the 189 transfer vectors of each tile so that the items fill the SMs evenly
   int ns = 1;
-  const long long units = t->pair ? t->grid / 2 : t->grid;  // CTA pairs or CTAs
-  const long long tiles_items = t->pair ? ntiles / 2 : ntiles;
   for (int k = 1; k <= 8; ++k) {
-    const long long n = tiles_items * k;
-    const long long rounds = (n + units - 1) / units;
+    const long long n = ntiles * k;
+    const long long rounds = (n + t->grid - 1) / t->grid;
     ns = k;
-    if ((double)n / (double)(rounds * units) >= 0.9) break;
+    if ((double)n / (double)(rounds * t->grid) >= 0.9) break;
   }
   if (t->splits > 0) ns = t->splits;  // chosen by b200fmm_autotune
   if (const char *e = getenv("B200FMM_TC_SPLITS")) ns = std::max(1, std::min(189, atoi(e)));
@@ -910,7 +777,7 @@ static b200fmm_status tc_prepare(Context &c) {
     t->lvl_begin[l] = (int)items.size();
     for (int r = 0; r < c.R; ++r)
       for (int par = 0; par < 8; ++par)
-        for (int bz = 0; bz < t->HZ[l] / TILE_Z / (t->pair ? 2 : 1); ++bz)
+        for (int bz = 0; bz < t->HZ[l] / TILE_Z; ++bz)
           for (int by = 0; by < t->HY[l] / TILE_Y; ++by)
             for (int bx = 0; bx < t->HX[l] / TILE_X; ++bx)
               for (int s = 0; s < ns; ++s) {
@@ -957,7 +824,6 @@ static b200fmm_status tc_prepare(Context &c) {
   // accumulator resets per transfer vector: 2 for p >= 6 keeps the M2L within ~1e-6 of FP64
   P.nseg = std::min(t->NK, c.p >= 6 ? 2 : 1);
   P.nbuf = t->nbuf;
-  P.NBH = t->pair ? t->NBH : 0;
   if (const char *e = getenv("B200FMM_TC_SEGMENTS")) P.nseg = std::max(1, std::min(t->NK, atoi(e)));
   std::memcpy(P.off, c.itab.off, sizeof(P.off));
   std::memcpy(P.slot, c.itab.slot, sizeof(P.slot));
@@ -1024,35 +890,13 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
   P.nitems = t->lvl_end[l0] - t->lvl_begin[l1];
   if (P.nitems <= 0) return B200FMM_OK;
   const size_t smem = (size_t)t->stages * t->stage_bytes + 1024;
-  int grid = std::min(t->grid, t->pair ? 2 * P.nitems : P.nitems);
-  if (t->pair) grid = std::max(2, grid & ~1);
+  const int grid = std::min(t->grid, P.nitems);
   B200_CUDA(record_event(c, 8));
-  cudaLaunchConfig_t cfg = {};
-  cudaLaunchAttribute attr[1];
-  cfg.gridDim = dim3((unsigned)grid, 1, 1);
-  cfg.blockDim = dim3(t->pair ? TC_THREADS_PAIR : TC_THREADS, 1, 1);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = c.stream;
-  if (t->pair) {
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = 2;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-  }
   switch (t->NP) {
 #define B200_TC_CASE(NPV, CWV, NHV)                                                                              \
   case NPV:                                                                                                        \
-    if (t->pair) {                                                                                                 \
-      B200_CUDA(cudaFuncSetAttribute(m2l_tc_kernel<CWV, NHV, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
-                                     (int)smem));                                                                  \
-      B200_CUDA(cudaLaunchKernelEx(&cfg, m2l_tc_kernel<CWV, NHV, true>, P));                                       \
-    } else {                                                                                                       \
-      B200_CUDA(cudaFuncSetAttribute(m2l_tc_kernel<CWV, NHV, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
-                                     (int)smem));                                                                  \
-      B200_CUDA(cudaLaunchKernelEx(&cfg, m2l_tc_kernel<CWV, NHV, false>, P));                                      \
-    }                                                                                                              \
+    B200_CUDA(cudaFuncSetAttribute(m2l_tc_kernel<CWV, NHV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    m2l_tc_kernel<CWV, NHV><<<grid, TC_THREADS, smem, c.stream>>>(P);                                              \
     break;
     B200_TC_CASE(32, 16, 1)
     B200_TC_CASE(64, 32, 1)
