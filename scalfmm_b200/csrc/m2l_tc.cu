@@ -40,14 +40,9 @@ namespace {
 
 constexpr int TC_THREADS = 320;
 constexpr int TILE_X = 8, TILE_Y = 4, TILE_Z = 4;  // 128 targets
-// K extent of one pipeline stage: 16 FP16 (one MMA K step) in 32-byte swizzled rows.  Small stages let more
-// of the shared memory hold loads in flight (S - 1 of S stages), which is what bounds the kernel: the
-// operator and multipole stream from L2 is latency-bound at the shared-memory depth.
-constexpr int KCHUNK = 16;
-constexpr int ROWB = KCHUNK * 2;    // bytes per stage row
-constexpr int KSTEPS = KCHUNK / 16; // MMA K steps per stage
+constexpr int KCHUNK = 32;                          // fp16 elements per 64-byte swizzle row
 constexpr int SB = 15;                              // operator pre-scale 2^15
-constexpr int MAX_STAGES = 8;
+constexpr int MAX_STAGES = 4;
 constexpr long long WAIT_LIMIT = 1LL << 22;
 
 struct TcItem {
@@ -140,12 +135,10 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
       "l"(map), "r"(su32(bar)), "r"(c0), "r"(c1), "r"(c2)
       : "memory");
 }
-// UMMA shared-memory descriptor: K-major, rows of ROWB bytes swizzled in 8-row groups (8 ROWB apart);
-// layout type 6 = 32-byte swizzle, 4 = 64-byte swizzle.
+// UMMA shared-memory descriptor: K-major, 64-byte swizzle, rows of 64 B in 8-row groups 512 B apart.
 __device__ __forceinline__ unsigned long long sdesc(const void *p) {
   const unsigned long long a = su32(p);
-  constexpr unsigned long long sbo = (8ull * ROWB) >> 4, layout = ROWB == 64 ? 4ull : 6ull;
-  return ((a >> 4) & 0x3FFFull) | (1ull << 16) | (sbo << 32) | (1ull << 46) | (layout << 61);
+  return ((a >> 4) & 0x3FFFull) | (1ull << 16) | (32ull << 32) | (1ull << 46) | (4ull << 61);
 }
 __device__ __forceinline__ void mma_f16(unsigned d_tmem, unsigned long long da, unsigned long long db, unsigned idesc,
                                         unsigned accumulate) {
@@ -300,9 +293,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
             tma_load_5d(sbuf + a_bytes, &P.mapA_lo[w.level], &full_bar[stage], kc * KCHUNK, ox, oy, oz,
                         w.rhs * 8 + sp);
             for (int h = 0; h < P.NHALF; ++h) {
-              tma_load_3d(sbuf + 2 * a_bytes + h * P.NH * ROWB, &P.mapB_hi, &full_bar[stage], kc * KCHUNK, h * P.NH,
-                          slot);
-              tma_load_3d(sbuf + 2 * a_bytes + b_bytes + h * P.NH * ROWB, &P.mapB_lo, &full_bar[stage], kc * KCHUNK,
+              tma_load_3d(sbuf + 2 * a_bytes + h * P.NH * 64, &P.mapB_hi, &full_bar[stage], kc * KCHUNK, h * P.NH, slot);
+              tma_load_3d(sbuf + 2 * a_bytes + b_bytes + h * P.NH * 64, &P.mapB_lo, &full_bar[stage], kc * KCHUNK,
                           h * P.NH, slot);
             }
             if (++stage == S) {
@@ -368,8 +360,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
                 }
                 const unsigned d = dbase + h * P.NH;
 #pragma unroll
-                for (int ks = 0; ks < KSTEPS; ++ks) {
-                  const int bo = h * P.NH * ROWB + ks * 32;
+                for (int ks = 0; ks < 2; ++ks) {
+                  const int bo = h * P.NH * 64 + ks * 32;
                   // the small cross terms first, the leading term last
                   mma_f16(d, sdesc(ahi + ks * 32), sdesc(blo + bo), idesc, (firstc && ks == 0) ? 0u : 1u);
                   mma_f16(d, sdesc(alo + ks * 32), sdesc(bhi + bo), idesc, 1u);
@@ -662,8 +654,7 @@ static b200fmm_status encode(CUtensorMap *map, void *base, int rank, const cuuin
   if (!fn) return fail(B200FMM_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is not available");
   cuuint32_t es[5] = {1, 1, 1, 1, 1};
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, (cuuint32_t)rank, base, dims, strides, box, es,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, ROWB == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B,
-                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(B200FMM_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
   return B200FMM_OK;
