@@ -251,12 +251,6 @@ __global__ void level_counts_kernel(long long n, const unsigned long long *__res
   }
 }
 
-__global__ void head_flags_i64(long long n, const long long *__restrict__ keys, long long *__restrict__ flags) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  flags[i] = (i == 0 || (keys[i] >> 3) != (keys[i - 1] >> 3)) ? 1 : 0;
-}
-
 __global__ void compact_leaves(long long n, const unsigned long long *__restrict__ keys,
                                const long long *__restrict__ flags, const long long *__restrict__ idx,
                                long long *__restrict__ leaf_keys, long long *__restrict__ leaf_start) {
@@ -268,15 +262,111 @@ __global__ void compact_leaves(long long n, const unsigned long long *__restrict
   }
 }
 
-__global__ void compact_parents(long long n, const long long *__restrict__ ckeys, const long long *__restrict__ flags,
-                                const long long *__restrict__ idx, long long *__restrict__ pkeys,
-                                int *__restrict__ parent, int *__restrict__ pchild) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const long long pi = idx[i] + flags[i] - 1;  // inclusive index of this child's parent
-  if (flags[i]) pkeys[pi] = ckeys[i] >> 3;
-  parent[i] = (int)pi;
-  pchild[pi * 8 + (ckeys[i] & 7)] = (int)i;
+// ---- upper levels of the tree, all at once from the sorted leaf keys ---------------------------------
+// Cell c of level l < LL starts at the first leaf whose key >> 3(LL - l) differs from its predecessor's;
+// a leaf's cell index at level l is the number of such starts up to it, minus one.  Three launches for
+// all levels: per-block start counts, their exclusive scans, then keys and parent/child links.
+constexpr int ML_T = 1024;
+struct LevelLinks {
+  long long *keys[kMaxHeight];
+  int *parent[kMaxHeight];
+  int *child[kMaxHeight];
+};
+
+__device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned *ws, unsigned &total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  unsigned x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) ws[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    unsigned t = lane < (int)(blockDim.x >> 5) ? ws[lane] : 0u, u = t;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xffffffffu, u, o);
+      if (lane >= o) u += y;
+    }
+    ws[lane] = u - t;
+    if (lane == 31) ws[32] = u;
+  }
+  __syncthreads();
+  const unsigned r = ws[w] + x - v;
+  total = ws[32];
+  __syncthreads();
+  return r;
+}
+
+__global__ void ml_count_kernel(long long nl, const long long *__restrict__ K, int LL, unsigned *__restrict__ bcount,
+                                int nblk) {
+  __shared__ unsigned ws[33];
+  const long long i = (long long)blockIdx.x * ML_T + threadIdx.x;
+  const long long k = i < nl ? K[i] : 0, kp = (i > 0 && i < nl) ? K[i - 1] : 0;
+  for (int l = 0; l < LL; ++l) {
+    const int sh = 3 * (LL - l);
+    const bool head = i < nl && (i == 0 || (k >> sh) != (kp >> sh));
+    unsigned total;
+    block_exclusive_scan(head ? 1u : 0u, ws, total);
+    if (threadIdx.x == 0) bcount[(long long)l * nblk + blockIdx.x] = total;
+  }
+}
+
+__global__ void ml_scan_kernel(unsigned *__restrict__ bcount, int nblk) {
+  __shared__ unsigned ws[33];
+  unsigned *b = bcount + (long long)blockIdx.x * nblk;
+  unsigned carry = 0;
+  for (int base = 0; base < nblk; base += ML_T) {
+    const int j = base + threadIdx.x;
+    const unsigned v = j < nblk ? b[j] : 0u;
+    unsigned total;
+    const unsigned ex = block_exclusive_scan(v, ws, total);
+    if (j < nblk) b[j] = carry + ex;
+    carry += total;
+  }
+}
+
+__global__ void ml_build_kernel(long long nl, const long long *__restrict__ K, int LL,
+                                const unsigned *__restrict__ boff, int nblk, LevelLinks P) {
+  __shared__ unsigned ws[33];
+  const long long i = (long long)blockIdx.x * ML_T + threadIdx.x;
+  const long long k = i < nl ? K[i] : 0, kp = (i > 0 && i < nl) ? K[i - 1] : 0;
+  int idx_next = (int)i;  // this leaf's cell at level l + 1 (at LL: the leaf itself)
+  bool head_next = true;  // the leaf starts that cell
+  for (int l = LL - 1; l >= 0; --l) {
+    const int sh = 3 * (LL - l);
+    const bool head = i < nl && (i == 0 || (k >> sh) != (kp >> sh));
+    unsigned total;
+    const unsigned ex = block_exclusive_scan(head ? 1u : 0u, ws, total);
+    const int idx = (int)(boff[(long long)l * nblk + blockIdx.x] + ex) + (head ? 1 : 0) - 1;
+    if (i < nl) {
+      if (head) P.keys[l][idx] = k >> sh;
+      if (head_next) {
+        P.parent[l + 1][idx_next] = idx;
+        P.child[l][(long long)idx * 8 + ((k >> (sh - 3)) & 7)] = idx_next;
+      }
+    }
+    idx_next = idx;
+    head_next = head;
+  }
+}
+
+// interaction lists and dense grids of every level in one launch each: block b serves cell b of the
+// concatenated levels 2..LL
+struct LevelCellsT {
+  const long long *keys[kMaxHeight];
+  int *ilist[kMaxHeight];
+  int *grid[kMaxHeight];
+  long long start[kMaxHeight + 1];
+  int l0, l1;
+};
+
+__device__ __forceinline__ int level_at(const LevelCellsT &C, long long g) {
+  int l = C.l0;
+  while (l < C.l1 && g >= C.start[l + 1]) ++l;
+  return l;
 }
 
 __global__ void leaf_neighbors_kernel(long long nleaves, const long long *__restrict__ keys, int height,
@@ -298,10 +388,12 @@ __global__ void leaf_neighbors_kernel(long long nleaves, const long long *__rest
   }
 }
 
-__global__ void ilist_kernel(long long ncells, const long long *__restrict__ keys, int level,
-                             const IListTable *__restrict__ tab, int *__restrict__ ilist) {
-  const long long c = blockIdx.x;
-  if (c >= ncells) return;
+__global__ void ilist_kernel(const __grid_constant__ LevelCellsT C, const IListTable *__restrict__ tab) {
+  const int level = level_at(C, blockIdx.x);
+  const long long c = blockIdx.x - C.start[level];
+  const long long ncells = C.start[level + 1] - C.start[level];
+  const long long *__restrict__ keys = C.keys[level];
+  int *__restrict__ ilist = C.ilist[level];
   int ix, iy, iz;
   const long long key = keys[c];
   morton_decode3(key, ix, iy, iz);
@@ -316,19 +408,17 @@ __global__ void ilist_kernel(long long ncells, const long long *__restrict__ key
   }
 }
 
-__global__ void grid_index_kernel(long long ncells, const long long *__restrict__ keys, int level,
-                                  int *__restrict__ grid) {
-  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (c >= ncells) return;
+__global__ void grid_index_kernel(const __grid_constant__ LevelCellsT C) {
+  const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (g >= C.start[C.l1 + 1]) return;
+  const int level = level_at(C, g);
+  const long long c = g - C.start[level];
+  const long long *__restrict__ keys = C.keys[level];
+  int *__restrict__ grid = C.grid[level];
   int ix, iy, iz;
   morton_decode3(keys[c], ix, iy, iz);
   const long long side = 1LL << level;
   grid[((long long)iz * side + iy) * side + ix] = (int)c;
-}
-
-__global__ void fill_int(long long n, int *p, int v) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i < n) p[i] = v;
 }
 
 // column key of a leaf: (x, y) of its cell; a stable sort by it from Morton order (monotone in z inside a
@@ -597,35 +687,57 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
   ++c.tree_launches;
   c.h_pinned[3] = c.N;
   B200_CUDA(cudaMemcpyAsync(c.d_leaf_start + nleaves, c.h_pinned + 3, sizeof(long long), cudaMemcpyHostToDevice, s));
-  // upper levels
+  // upper levels: storage from the counts taken before the synchronisation, then keys and links of every
+  // level from the leaf keys in three launches
+  LevelLinks links{};
   for (int l = LL - 1; l >= 0; --l) {
-    Level &ch = c.lv[l + 1];
     Level &pa = c.lv[l];
-    const long long nc = ch.n;
-    head_flags_i64<<<grid_for(nc, 256), 256, 0, s>>>(nc, ch.keys, flags);
-    ++c.tree_launches;
-    B200_CHECK(scan_i64(c, flags, idx, nc, (long long *)c.d_scan));
-    B200_CHECK(level_storage(c, pa, c.h_pinned[8 + l]));  // counted before the synchronisation
-    fill_int<<<grid_for(pa.n * 8, 256), 256, 0, s>>>(pa.n * 8, pa.child, -1);
-    compact_parents<<<grid_for(nc, 256), 256, 0, s>>>(nc, ch.keys, flags, idx, pa.keys, ch.parent, pa.child);
-    c.tree_launches += 2;
+    B200_CHECK(level_storage(c, pa, c.h_pinned[8 + l]));
+    B200_CUDA(cudaMemsetAsync(pa.child, 0xFF, sizeof(int) * 8 * (size_t)pa.n, s));  // -1: no child
+    links.keys[l] = pa.keys;
+    links.parent[l] = pa.parent;
+    links.child[l] = pa.child;
   }
-  // neighbour and interaction lists
+  links.parent[LL] = leaf.parent;
+  if (LL > 0) {
+    const int nblk = (int)((nleaves + ML_T - 1) / ML_T);
+    unsigned *bcount = (unsigned *)c.d_flags;  // LL * nblk entries; the flag scratch is free now
+    ml_count_kernel<<<nblk, ML_T, 0, s>>>(nleaves, leaf.keys, LL, bcount, nblk);
+    ml_scan_kernel<<<LL, ML_T, 0, s>>>(bcount, nblk);
+    ml_build_kernel<<<nblk, ML_T, 0, s>>>(nleaves, leaf.keys, LL, bcount, nblk, links);
+    c.tree_launches += 3;
+  }
+  // neighbour and interaction lists, dense grids
   leaf_neighbors_kernel<<<grid_for(nleaves, 128), 128, 0, s>>>(nleaves, leaf.keys, H, c.d_leaf_nbr);
   ++c.tree_launches;
-  for (int l = 2; l <= LL; ++l) {
-    Level &L = c.lv[l];
-    ilist_kernel<<<(unsigned)L.n, 192, 0, s>>>(L.n, L.keys, l, c.d_itab, L.ilist);
-    ++c.tree_launches;
-    if (c.cfg.precision == B200FMM_MIXED) {
-      const long long side = 1LL << l;
-      if (!L.grid) {
-        B200_CUDA(cudaMalloc(&L.grid, sizeof(int) * side * side * side));
-        ++c.tree_gen;
+  if (LL >= 2) {
+    LevelCellsT C{};
+    C.l0 = 2;
+    C.l1 = LL;
+    C.start[2] = 0;
+    for (int l = 2; l <= LL; ++l) {
+      Level &L = c.lv[l];
+      C.keys[l] = L.keys;
+      C.ilist[l] = L.ilist;
+      C.start[l + 1] = C.start[l] + L.n;
+      if (c.cfg.precision == B200FMM_MIXED) {
+        const long long side = 1LL << l;
+        if (!L.grid) {
+          B200_CUDA(cudaMalloc(&L.grid, sizeof(int) * side * side * side));
+          ++c.tree_gen;
+        }
+        B200_CUDA(cudaMemsetAsync(L.grid, 0xFF, sizeof(int) * side * side * side, s));  // -1: empty
+        C.grid[l] = L.grid;
       }
-      fill_int<<<grid_for(side * side * side, 256), 256, 0, s>>>(side * side * side, L.grid, -1);
-      grid_index_kernel<<<grid_for(L.n, 256), 256, 0, s>>>(L.n, L.keys, l, L.grid);
-      c.tree_launches += 2;
+    }
+    const long long total = C.start[LL + 1];
+    if (total > 0) {
+      ilist_kernel<<<(unsigned)total, 192, 0, s>>>(C, c.d_itab);
+      ++c.tree_launches;
+      if (c.cfg.precision == B200FMM_MIXED) {
+        grid_index_kernel<<<grid_for(total, 256), 256, 0, s>>>(C);
+        ++c.tree_launches;
+      }
     }
   }
   B200_CUDA(cudaGetLastError());
