@@ -419,13 +419,13 @@ b200fmm_status b200fmm_autotune(b200fmm_handle h, int *splits, double *ms) {
   if (c.cfg.precision != B200FMM_MIXED || !c.tc) return B200FMM_OK;  // nothing to tune
   drop_graph(c);
   c.eager_serial = -1;
-  const int cand[] = {1, 2, 3, 4, 6, 8, 12};
+  const int cand[] = {1, 2, 3, 4};  // work ranges per CTA (pair) of the tensor-core M2L
   int best = 0;
   float best_ms = 0.f;
   for (int k : cand) {
     tc_set_splits(c, k);
     float t = 0.f;
-    for (int rep = 0; rep < 2; ++rep) {  // the first run rebuilds the work items
+    for (int rep = 0; rep < 2; ++rep) {  // the first run rebuilds the work units
       B200_CHECK(execute_body(c, B200FMM_P2M | B200FMM_M2M | B200FMM_M2L));
       B200_CUDA(cudaEventSynchronize(c.ev[7]));
       B200_CHECK(check_status(c));

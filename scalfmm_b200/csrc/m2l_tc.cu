@@ -22,7 +22,8 @@
 //     scale * 2^-(sA+sB) * sum into the FP64 locals (atomic adds: several items of the same tile contribute).
 //
 // Roles: warp 0 = TMA producer (one elected thread), warp 1 = MMA issuer (one thread) and TMEM owner,
-// warps 2..9 = epilogue (TMEM lane quarter = warp % 4, column half = (warp - 2) / 4).  Shared memory: STAGES x {A_hi, A_lo, B_hi, B_lo}
+// warps 2..9 = epilogue (TMEM lane quarter = warp % 4, column half = (warp - 2) / 4), warp 10 = issuer of the
+// second column half at order 7, warp 11 idle (blocks are sized in whole groups of four warps).  Shared memory: STAGES x {A_hi, A_lo, B_hi, B_lo}
 // K-chunks with the 64-byte swizzle the UMMA descriptors describe.  Every mbarrier wait is bounded; a wait
 // that runs out sets a device status word, the CTA abandons its work, frees its TMEM and returns.
 #include "common.cuh"
@@ -38,17 +39,19 @@ namespace b200 {
 
 namespace {
 
-constexpr int TC_THREADS = 320;
+constexpr int TC_THREADS = 384;  // 12 warps: TMA, MMA, 8 epilogue, second MMA issuer, spare
 constexpr int TILE_X = 8, TILE_Y = 4, TILE_Z = 4;  // 128 targets
 constexpr int KCHUNK = 32;                          // fp16 elements per 64-byte swizzle row
 constexpr int SB = 15;                              // operator pre-scale 2^15
-constexpr int MAX_STAGES = 4;
+constexpr int MAX_STAGES = 8;         // stage barriers allocated
+constexpr int MAX_STAGES_SINGLE = 4;  // stages used by single CTAs
 constexpr long long WAIT_LIMIT = 1LL << 22;
 
+// A work unit: one target tile (CTA pairs: the z-adjacent tiles bz, bz + 1) of one level and right-hand side,
+// with the 189 transfer vectors of its parity.  Its work is the number of those whose source box is occupied.
 struct TcItem {
-  short level, rhs, parity, split;
-  short bx, by, bz;
-  short t0, t1;
+  int level, rhs, parity;
+  int bx, by, bz;
 };
 
 struct TcLevel {
@@ -59,6 +62,8 @@ struct TcLevel {
   double *scale_out;   // device scalar: scale_l * 2^-(sA + SB)
   const int *sat;      // [8][HZ+1][HY+1][HX+1] occupied cells of each parity grid below (x, y, z), exclusive
   int tile0;           // first tile of this level in the busy masks
+  int unit0, nunits;   // work units of this level: [unit0, unit0 + nunits), ordered rhs, parity, z, y, x
+  int TZu;             // units along z: tiles, or pairs of tiles
 };
 
 // Occupied cells of parity grid `par` in the box [x0, x0+nx) x [y0, y0+ny) x [z0, z0+nz) (clipped).
@@ -81,8 +86,12 @@ struct __align__(64) TcParams {
   CUtensorMap mapB_hi;
   CUtensorMap mapB_lo;
   TcLevel lv[kMaxHeight];
-  const TcItem *items;
-  int item0, nitems;  // items [item0, item0 + nitems) of the list run in this launch
+  // exclusive prefix sums of the work of all units (finest level first); this launch runs the units
+  // [u_begin, u_end), split into ranges of equal work: CTA (pair) g takes ranges g, g + G, ... of G * nranges
+  const int *prefix;
+  int u_begin, u_end, ranges_per_cta;
+  int l0, l1;  // levels of the units [u_begin, u_end)
+  int pair;    // units are pairs of z-adjacent tiles
   int R, nn, KP, NP, NH, NHALF, NK, stages, ncols;
   int nseg;  // accumulator resets per transfer vector (the K chunks are split into nseg segments)
   int nbuf;  // TMEM accumulators: 2 (alternating per segment) when 2 * NP columns fit, else 1
@@ -151,6 +160,65 @@ __device__ __forceinline__ void mma_commit(unsigned long long *bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar))
                : "memory");
 }
+// ---- CTA-pair forms (cta_group::2): the even CTA of a cluster pair issues M = 256 MMAs whose A rows
+// 0..127 and B columns [0, N/2) come from its own shared memory and A rows 128..255 and B columns [N/2, N)
+// from its peer's, at the same offsets; each CTA's TMEM receives its own 128 rows of D.
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// shared::cluster address of the variable at shared::cta address `a` in cluster CTA `rank`
+__device__ __forceinline__ unsigned mapa_shared(unsigned a, unsigned rank) {
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// arrive on a barrier of another CTA of the cluster.  The only data handed over this way is TMEM, which the
+// arriving warp has finished reading (tcgen05.wait::ld) before it arrives, so CTA-scope release suffices.
+__device__ __forceinline__ void mbar_arrive_cluster(unsigned cluster_addr) {
+  asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+// tile loads into this CTA's shared memory whose completion is counted on the even CTA's barrier
+__device__ __forceinline__ void tma_load_5d_pair(void *dst, const CUtensorMap *map, unsigned bar_cluster, int c0, int c1,
+                                                 int c2, int c3, int c4) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, "
+      "%5, %6, %7}], [%2];" ::"r"(su32(dst)),
+      "l"(map), "r"(bar_cluster), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4)
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_3d_pair(void *dst, const CUtensorMap *map, unsigned bar_cluster, int c0, int c1,
+                                                 int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, "
+      "%5}], [%2];" ::"r"(su32(dst)),
+      "l"(map), "r"(bar_cluster), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+__device__ __forceinline__ void mma_f16_pair(unsigned d_tmem, unsigned long long da, unsigned long long db,
+                                             unsigned idesc, unsigned accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+          d_tmem),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+}
+// arrive on the barrier at this shared::cta offset in both CTAs of the pair once the issued MMAs complete
+__device__ __forceinline__ void mma_commit_pair_both(unsigned long long *bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+          su32(bar)),
+      "h"((unsigned short)3)
+      : "memory");
+}
+__device__ __forceinline__ void mma_commit_pair_local(unsigned long long *bar) {
+  asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar))
+               : "memory");
+}
+
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 
@@ -184,7 +252,8 @@ __device__ __forceinline__ void drain_cols(unsigned taddr, float *acc) {
 struct SrcBox {
   int sp, ox, oy, oz, slot;
 };
-__device__ __forceinline__ SrcBox src_box(const TcParams &P, const TcItem &w, int e) {
+// bz: the target tile's z index (an item's tile, or in CTA pairs the item's tile + the CTA's rank)
+__device__ __forceinline__ SrcBox src_box(const TcParams &P, const TcItem &w, int bz, int e) {
   const int c = w.parity;
   const int cx = (c >> 2) & 1, cy = (c >> 1) & 1, cz = c & 1;
   const int dx = P.off[c][e][0], dy = P.off[c][e][1], dz = P.off[c][e][2];
@@ -192,7 +261,7 @@ __device__ __forceinline__ SrcBox src_box(const TcParams &P, const TcItem &w, in
   b.sp = (((cx + dx) & 1) << 2) | (((cy + dy) & 1) << 1) | ((cz + dz) & 1);
   b.ox = w.bx * TILE_X + ((cx + dx) >> 1);
   b.oy = w.by * TILE_Y + ((cy + dy) >> 1);
-  b.oz = w.bz * TILE_Z + ((cz + dz) >> 1);
+  b.oz = bz * TILE_Z + ((cz + dz) >> 1);
   b.slot = P.slot[c][e];
   return b;
 }
@@ -217,6 +286,66 @@ __device__ __forceinline__ BusyMask busy_mask(const TcParams &P, const TcItem &w
   for (int k = 0; k < 6; ++k) b.w[k] = m[k];
   return b;
 }
+// CTA pairs work on the z-adjacent tiles bz and bz + 1 (bz even) with the same transfer vectors: a pair skips
+// a transfer vector (or the item) only when it is idle for both tiles.  A level with an odd number of z tiles
+// has no tile bz + 1 in its last pair; that tile's A boxes lie outside the grid (zero-filled loads) and its
+// rows map to no cell.
+__device__ __forceinline__ BusyMask busy_mask_pair(const TcParams &P, const TcItem &w) {
+  BusyMask b = busy_mask(P, w);
+  if (w.bz + 1 < P.lv[w.level].HZ / TILE_Z) {
+    const unsigned *m = P.busy + 6 * tile_id(P, w.level, w.parity, w.bx, w.by, w.bz + 1);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) b.w[k] |= m[k];
+  }
+  return b;
+}
+
+__device__ __forceinline__ TcItem decode_unit(const TcParams &P, int u) {
+  int level = P.l1;
+  while (level > P.l0 && u >= P.lv[level].unit0 + P.lv[level].nunits) --level;
+  const TcLevel &L = P.lv[level];
+  const int TX = L.HX / TILE_X, TY = L.HY / TILE_Y;
+  int r = u - L.unit0;
+  TcItem w;
+  w.level = level;
+  w.bx = r % TX;
+  r /= TX;
+  w.by = r % TY;
+  r /= TY;
+  w.bz = (r % L.TZu) * (P.pair ? 2 : 1);
+  r /= L.TZu;
+  w.parity = r & 7;
+  w.rhs = r >> 3;
+  return w;
+}
+// the largest unit u in [u_begin, u_end) whose work starts at or before lo
+__device__ __forceinline__ int first_unit(const TcParams &P, long long lo) {
+  int a = P.u_begin, b = P.u_end;
+  while (b - a > 1) {
+    const int m = (a + b) >> 1;
+    if (P.prefix[m] <= lo) a = m; else b = m;
+  }
+  return a;
+}
+// Every role walks the same sequence: for each of its ranges, the units the range overlaps and, in each, the
+// busy transfer vectors of ranks [r0, r1).  f(w, bm, r0, r1) handles one unit fragment; it returns false to stop.
+template <class F>
+__device__ __forceinline__ void for_each_fragment(const TcParams &P, int g, int G, F &&f) {
+  const long long base = P.prefix[P.u_begin], W = (long long)P.prefix[P.u_end] - base;
+  const int nr = G * P.ranges_per_cta;
+  for (int m = 0; m < P.ranges_per_cta; ++m) {
+    const int j = g + m * G;
+    const long long lo = base + W * j / nr, hi = base + W * (j + 1) / nr;
+    if (lo >= hi) continue;
+    for (int u = first_unit(P, lo); u < P.u_end; ++u) {
+      const long long p0 = P.prefix[u], p1 = P.prefix[u + 1];
+      if (p0 >= hi) break;
+      const int r0 = (int)(max(lo, p0) - p0), r1 = (int)(min(hi, p1) - p0);
+      if (r1 <= r0) continue;
+      if (!f(decode_unit(P, u), r0, r1)) return;
+    }
+  }
+}
 
 // ---- the kernel -------------------------------------------------------------------------------------
 // CW: accumulator columns owned by one epilogue thread (NP / 2) and NHALF: MMA column halves, compile-time
@@ -230,72 +359,125 @@ __device__ __forceinline__ BusyMask busy_mask(const TcParams &P, const TcItem &w
 // s+1 runs in the other accumulator while segment s drains.  With one (order 7: 352 of 512 columns) the
 // epilogue drains half 0 first and releases it, and the first chunk of the next segment issues all its
 // half-0 MMAs before waiting for half 1.
-template <int CW, int NHALF>
+//
+// PAIR: clusters of two CTAs on the z-adjacent tiles (bz, bz + 1) of an item share each operator chunk
+// through cta_group::2 MMAs (M = 256).  Each CTA loads its own A tile and half of the chunk's B rows, so a
+// CTA reads 16 KB of A and NP / 2 rows of B per K chunk instead of all NP rows.  The even CTA's producer
+// expects both CTAs' bytes on its full barrier, its MMA warp issues all MMAs, and the commits arrive on the
+// stage and accumulator barriers of both CTAs; the epilogue warps of both CTAs release the accumulator on
+// the even CTA's barriers (16 arrivals).
+template <int CW, int NHALF, bool PAIR>
 __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_constant__ TcParams P) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1024-byte aligned stage buffers (the swizzle pattern repeats every 512 B)
   unsigned char *smem = (unsigned char *)(((unsigned long long)smem_raw + 1023) & ~1023ull);
   __shared__ __align__(8) unsigned long long full_bar[MAX_STAGES], empty_bar[MAX_STAGES];
-  __shared__ __align__(8) unsigned long long acc_full[2], acc_empty[2][2];
+  __shared__ __align__(8) unsigned long long acc_full[2][2], acc_empty[2][2], done_bar;
   __shared__ unsigned tmem_base_sh;
   __shared__ volatile int abort_sh;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int S = P.stages;
+  const unsigned rank = PAIR ? cluster_rank() : 0u;
+  const bool leader = rank == 0;
+  // the work ranges of this CTA, or of this CTA pair
+  const int g_id = PAIR ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
+  const int g_count = PAIR ? (int)(gridDim.x >> 1) : (int)gridDim.x;
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(&full_bar[s], 1);
-      mbar_init(&empty_bar[s], 1);
+      mbar_init(&empty_bar[s], NHALF);  // one commit per MMA issuer
     }
     for (int b = 0; b < 2; ++b) {
-      mbar_init(&acc_full[b], 1);
-      mbar_init(&acc_empty[b][0], 8);  // one arrive per epilogue warp
-      mbar_init(&acc_empty[b][1], 8);
+      mbar_init(&acc_full[b][0], 1);
+      mbar_init(&acc_full[b][1], 1);
+      mbar_init(&acc_empty[b][0], PAIR ? 16 : 8);  // one arrive per epilogue warp (of both CTAs)
+      mbar_init(&acc_empty[b][1], PAIR ? 16 : 8);
     }
+    mbar_init(&done_bar, NHALF);
     abort_sh = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_base_sh)),
-                 "r"(P.ncols));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    if constexpr (PAIR) {
+      // both CTAs' warp 1 allocate together; the same columns are allocated in each CTA's TMEM
+      asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_base_sh)),
+                   "r"(P.ncols));
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    } else {
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_base_sh)),
+                   "r"(P.ncols));
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
   }
   tc_fence_before();
   __syncthreads();
+  if constexpr (PAIR) cluster_sync_all();  // the peer's barriers are initialised before any remote arrival
   tc_fence_after();
   const unsigned tmem = tmem_base_sh;
+  // a role that gives up marks the status word and stops both CTAs of a pair
+  auto give_up = [&]() {
+    atomicExch(P.status + 1, 1);
+    abort_sh = 1;
+    if constexpr (PAIR)
+      asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(mapa_shared(su32((const void *)&abort_sh), rank ^ 1u)),
+                   "r"(1)
+                   : "memory");
+  };
+  auto wait_bar = [&](unsigned long long *b, unsigned parity) -> bool { return mbar_wait(b, parity); };
+  auto item_mask = [&](const TcItem &w) -> BusyMask {
+    if constexpr (PAIR) return busy_mask_pair(P, w);
+    return busy_mask(P, w);
+  };
 
   const int a_bytes = TILE_X * TILE_Y * TILE_Z * KCHUNK * 2;  // 8 KB
-  const int b_bytes = P.NP * KCHUNK * 2;
+  const int nb_rows = PAIR ? P.NH / 2 : P.NH;                 // B rows of one column half in this CTA
+  const int b_bytes = NHALF * nb_rows * KCHUNK * 2;
 
   if (warp == 0) {
-    // ------------------------------------------------ TMA producer
+    // ------------------------------------------------ TMA producer (both CTAs of a pair)
     if (lane == 0) {
       int stage = 0;
       unsigned phase = 0;
-      for (int it = blockIdx.x; it < P.nitems && !abort_sh; it += gridDim.x) {
-        const TcItem w = P.items[P.item0 + it];
-        const BusyMask bm = busy_mask(P, w);
-        if (!bm.tile()) continue;
-        for (int e = w.t0; e < w.t1 && !abort_sh; ++e) {
+      // the barrier that counts this stage's bytes: this CTA's, or the even CTA's in a pair
+      const unsigned full0 = PAIR ? mapa_shared(su32(&full_bar[0]), 0u) : su32(&full_bar[0]);
+      const int stage_tx = (PAIR ? 2 : 1) * (2 * a_bytes + 2 * b_bytes);
+      for_each_fragment(P, g_id, g_count, [&](const TcItem &w, int r0, int r1) -> bool {
+        const BusyMask bm = item_mask(w);
+        const int bz = w.bz + (int)rank;
+        int rank_e = 0;
+        for (int e = 0; e < 189 && rank_e < r1 && !abort_sh; ++e) {
           if (!bm.src(e)) continue;
-          const SrcBox sb = src_box(P, w, e);
+          if (rank_e++ < r0) continue;
+          const SrcBox sb = src_box(P, w, bz, e);
           const int sp = sb.sp, ox = sb.ox, oy = sb.oy, oz = sb.oz, slot = sb.slot;
           for (int kc = 0; kc < P.NK; ++kc) {
-            if (!mbar_wait(&empty_bar[stage], phase ^ 1)) {
-              atomicExch(P.status + 1, 1);
-              abort_sh = 1;
+            if (!wait_bar(&empty_bar[stage], phase ^ 1)) {
+              give_up();
               break;
             }
             unsigned char *sbuf = smem + (size_t)stage * P.stage_bytes;
-            mbar_expect_tx(&full_bar[stage], 2 * a_bytes + 2 * b_bytes);
-            tma_load_5d(sbuf, &P.mapA_hi[w.level], &full_bar[stage], kc * KCHUNK, ox, oy, oz, w.rhs * 8 + sp);
-            tma_load_5d(sbuf + a_bytes, &P.mapA_lo[w.level], &full_bar[stage], kc * KCHUNK, ox, oy, oz,
-                        w.rhs * 8 + sp);
-            for (int h = 0; h < P.NHALF; ++h) {
-              tma_load_3d(sbuf + 2 * a_bytes + h * P.NH * 64, &P.mapB_hi, &full_bar[stage], kc * KCHUNK, h * P.NH, slot);
-              tma_load_3d(sbuf + 2 * a_bytes + b_bytes + h * P.NH * 64, &P.mapB_lo, &full_bar[stage], kc * KCHUNK,
-                          h * P.NH, slot);
+            if (leader) mbar_expect_tx(&full_bar[stage], stage_tx);
+            const int c4 = w.rhs * 8 + sp;
+            if constexpr (PAIR) {
+              const unsigned fb = full0 + 8u * (unsigned)stage;
+              tma_load_5d_pair(sbuf, &P.mapA_hi[w.level], fb, kc * KCHUNK, ox, oy, oz, c4);
+              tma_load_5d_pair(sbuf + a_bytes, &P.mapA_lo[w.level], fb, kc * KCHUNK, ox, oy, oz, c4);
+              for (int h = 0; h < NHALF; ++h) {
+                const int row0 = h * P.NH + (int)rank * nb_rows;
+                tma_load_3d_pair(sbuf + 2 * a_bytes + h * nb_rows * 64, &P.mapB_hi, fb, kc * KCHUNK, row0, slot);
+                tma_load_3d_pair(sbuf + 2 * a_bytes + b_bytes + h * nb_rows * 64, &P.mapB_lo, fb, kc * KCHUNK, row0,
+                                 slot);
+              }
+            } else {
+              tma_load_5d(sbuf, &P.mapA_hi[w.level], &full_bar[stage], kc * KCHUNK, ox, oy, oz, c4);
+              tma_load_5d(sbuf + a_bytes, &P.mapA_lo[w.level], &full_bar[stage], kc * KCHUNK, ox, oy, oz, c4);
+              for (int h = 0; h < NHALF; ++h) {
+                tma_load_3d(sbuf + 2 * a_bytes + h * nb_rows * 64, &P.mapB_hi, &full_bar[stage], kc * KCHUNK,
+                            h * P.NH, slot);
+                tma_load_3d(sbuf + 2 * a_bytes + b_bytes + h * nb_rows * 64, &P.mapB_lo, &full_bar[stage],
+                            kc * KCHUNK, h * P.NH, slot);
+              }
             }
             if (++stage == S) {
               stage = 0;
@@ -303,140 +485,183 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
             }
           }
         }
-      }
+        return !abort_sh;
+      });
     }
-  } else if (warp == 1) {
-    // ------------------------------------------------ MMA issuer
-    if (lane == 0) {
-      const unsigned idesc = (1u << 4) | ((unsigned)(P.NH >> 3) << 17) | ((unsigned)(128 >> 4) << 24);
+  } else if (warp == 1 || (NHALF == 2 && warp == 10)) {
+    // ------------------------------------------------ MMA issuers (the even CTA of a pair)
+    // With two column halves each half has its own issuing thread (warp 1: half 0, warp 10: half 1), so
+    // that each thread issues 6 MMAs per K chunk and each half drains while the other half's MMAs run.
+    const int hh = warp == 1 ? 0 : 1;
+    if (lane == 0 && leader) {
+      const unsigned idesc =
+          (1u << 4) | ((unsigned)(P.NH >> 3) << 17) | ((unsigned)((PAIR ? 256 : 128) >> 4) << 24);
+      // descriptors of stage 0's operands: another stage, K step or column half adds (byte offset >> 4) to
+      // the 14-bit start-address field, which never carries (shared addresses stay below 2^18 bytes)
+      const unsigned long long dA_hi = sdesc(smem), dA_lo = dA_hi + (unsigned)(a_bytes >> 4);
+      const unsigned long long dB_hi = dA_hi + (unsigned)((2 * a_bytes) >> 4), dB_lo = dB_hi + (unsigned)(b_bytes >> 4);
+      const unsigned stage_step = (unsigned)P.stage_bytes >> 4;
+      const unsigned half_step = (unsigned)(nb_rows * 64) >> 4;
       int stage = 0;
       unsigned phase = 0;
-      unsigned empty_par = 0xFu;  // parity to wait for, per (buffer, half): starts at 1 (passes at once)
-      int seg = 0;
-      const bool defer = (P.nbuf == 1 && NHALF == 2);
-      for (int it = blockIdx.x; it < P.nitems && !abort_sh; it += gridDim.x) {
-        const TcItem w = P.items[P.item0 + it];
-        const BusyMask bm = busy_mask(P, w);
-        if (!bm.tile()) continue;
-        for (int e = w.t0; e < w.t1 && !abort_sh; ++e) {
-          if (!bm.src(e)) continue;
-          for (int sg = 0; sg < P.nseg && !abort_sh; ++sg, ++seg) {
-            const int k0 = sg * P.NK / P.nseg, k1 = (sg + 1) * P.NK / P.nseg;
-            const int b = P.nbuf == 2 ? (seg & 1) : 0;
-            const unsigned dbase = tmem + (unsigned)(b * P.NP);
-            // the epilogue has drained this accumulator (both halves, or half 0 only when deferring half 1)
-            for (int h = 0; h < (defer ? 1 : NHALF); ++h) {
-              const int bit = b * 2 + h;
-              if (!mbar_wait(&acc_empty[b][h], (empty_par >> bit) & 1u)) {
-                atomicExch(P.status + 1, 1);
-                abort_sh = 1;
-                break;
-              }
-              empty_par ^= 1u << bit;
-            }
-            if (abort_sh) break;
-            tc_fence_after();
-            for (int kc = k0; kc < k1; ++kc) {
-              if (!mbar_wait(&full_bar[stage], phase)) {
-                atomicExch(P.status + 1, 1);
-                abort_sh = 1;
-                break;
-              }
-              tc_fence_after();
-              const unsigned char *sbuf = smem + (size_t)stage * P.stage_bytes;
-              const unsigned char *ahi = sbuf, *alo = sbuf + a_bytes;
-              const unsigned char *bhi = sbuf + 2 * a_bytes, *blo = sbuf + 2 * a_bytes + b_bytes;
-              const bool firstc = (kc == k0);
+      auto commit = [&](unsigned long long *bar) {
+        if constexpr (PAIR)
+          mma_commit_pair_both(bar);
+        else
+          mma_commit(bar);
+      };
+      // the 6 MMAs of one column half of the K chunk in stage st: D += A_hi B_lo + A_lo B_hi + A_hi B_hi
+      // (the small cross terms first, the leading term last); `first` starts a new accumulation
+      auto issue_half = [&](int st, int h, unsigned d, bool first) {
+        const unsigned so = (unsigned)st * stage_step;
+        const unsigned bo = so + (unsigned)h * half_step;
 #pragma unroll
-              for (int h = 0; h < NHALF; ++h) {
-                if (firstc && defer && h == 1) {
-                  if (!mbar_wait(&acc_empty[0][1], (empty_par >> 1) & 1u)) {
-                    atomicExch(P.status + 1, 1);
-                    abort_sh = 1;
-                    break;
-                  }
-                  empty_par ^= 2u;
-                  tc_fence_after();
-                }
-                const unsigned d = dbase + h * P.NH;
-#pragma unroll
-                for (int ks = 0; ks < 2; ++ks) {
-                  const int bo = h * P.NH * 64 + ks * 32;
-                  // the small cross terms first, the leading term last
-                  mma_f16(d, sdesc(ahi + ks * 32), sdesc(blo + bo), idesc, (firstc && ks == 0) ? 0u : 1u);
-                  mma_f16(d, sdesc(alo + ks * 32), sdesc(bhi + bo), idesc, 1u);
-                  mma_f16(d, sdesc(ahi + ks * 32), sdesc(bhi + bo), idesc, 1u);
-                }
-              }
-              if (abort_sh) break;
-              mma_commit(&empty_bar[stage]);  // frees the stage once these MMAs have read it
-              if (++stage == S) {
-                stage = 0;
-                phase ^= 1;
-              }
-            }
-            mma_commit(&acc_full[b]);  // segment accumulated
+        for (int ks = 0; ks < 2; ++ks) {
+          const unsigned k2 = 2u * ks;  // 16 fp16 = 32 bytes of K
+          if constexpr (PAIR) {
+            mma_f16_pair(d, dA_hi + so + k2, dB_lo + bo + k2, idesc, (first && ks == 0) ? 0u : 1u);
+            mma_f16_pair(d, dA_lo + so + k2, dB_hi + bo + k2, idesc, 1u);
+            mma_f16_pair(d, dA_hi + so + k2, dB_hi + bo + k2, idesc, 1u);
+          } else {
+            mma_f16(d, dA_hi + so + k2, dB_lo + bo + k2, idesc, (first && ks == 0) ? 0u : 1u);
+            mma_f16(d, dA_lo + so + k2, dB_hi + bo + k2, idesc, 1u);
+            mma_f16(d, dA_hi + so + k2, dB_hi + bo + k2, idesc, 1u);
           }
         }
-      }
+      };
+      // the next stage in order once its operands have landed, or -1
+      auto next_full = [&]() -> int {
+        if (!wait_bar(&full_bar[stage], phase)) {
+          give_up();
+          return -1;
+        }
+        const int st = stage;
+        if (++stage == S) {
+          stage = 0;
+          phase ^= 1;
+        }
+        return st;
+      };
+      unsigned empty_par = 0xFu;  // parity to wait for, per (buffer, half): starts at 1 (passes at once)
+      int seg = 0;
+      for_each_fragment(P, g_id, g_count, [&](const TcItem &w, int r0, int r1) -> bool {
+        // every MMA of a fragment runs the same schedule: only the count of transfer vectors matters here
+        (void)w;
+        for (int ev = r0; ev < r1 && !abort_sh; ++ev) {
+          for (int sg = 0; sg < P.nseg && !abort_sh; ++sg, ++seg) {
+            const int k0 = sg * P.NK / P.nseg, k1 = (sg + 1) * P.NK / P.nseg;
+            if constexpr (NHALF == 1) {
+              // one accumulator per segment, alternating between two when they fit
+              const int b = P.nbuf == 2 ? (seg & 1) : 0;
+              if (!wait_bar(&acc_empty[b][0], (empty_par >> (2 * b)) & 1u)) {
+                give_up();
+                break;
+              }
+              empty_par ^= 1u << (2 * b);
+              tc_fence_after();
+              for (int kc = k0; kc < k1; ++kc) {
+                const int st = next_full();
+                if (st < 0) break;
+                issue_half(st, 0, tmem + (unsigned)(b * P.NP), kc == k0);
+                commit(&empty_bar[st]);  // frees the stage (in both CTAs) once these MMAs have read it
+              }
+              commit(&acc_full[b][0]);  // segment accumulated
+            } else {
+              // one accumulator of two column halves (order 7): this thread's half
+              if (!wait_bar(&acc_empty[0][hh], (empty_par >> hh) & 1u)) {
+                give_up();
+                break;
+              }
+              empty_par ^= 1u << hh;
+              tc_fence_after();
+              for (int kc = k0; kc < k1; ++kc) {
+                const int st = next_full();
+                if (st < 0) break;
+                issue_half(st, hh, tmem + (unsigned)(hh * P.NH), kc == k0);
+                commit(&empty_bar[st]);
+              }
+              commit(&acc_full[0][hh]);
+            }
+          }
+        }
+        return !abort_sh;
+      });
+      // every MMA issued here has completed before the CTAs (and their TMEM) are released
+      if constexpr (PAIR)
+        mma_commit_pair_local(&done_bar);
+      else
+        mma_commit(&done_bar);
+      if (!wait_bar(&done_bar, 0)) give_up();
     }
-  } else {
-    // ------------------------------------------------ epilogue (warps 2..9)
+  } else if (warp >= 2 && warp <= 9) {
+    // ------------------------------------------------ epilogue (warps 2..9 of both CTAs)
     constexpr int SPLIT = 16 * ((CW + 31) / 32);
     const int q = warp & 3;              // TMEM lane quarter this warp may access
     const int ch = (warp - 2) >> 2;      // which part of each half
     const int row = q * 32 + lane;       // target within the tile
     const unsigned tlane = tmem + ((unsigned)(q * 32) << 16);
+    // the accumulator is released on the even CTA's barriers
+    const unsigned empty0 = PAIR ? mapa_shared(su32(&acc_empty[0][0]), 0u) : 0u;
+    auto release = [&](int b, int h) {
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) {
+        if constexpr (PAIR)
+          mbar_arrive_cluster(empty0 + 8u * (unsigned)(b * 2 + h));
+        else
+          mbar_arrive(&acc_empty[b][h]);
+      }
+    };
     unsigned full_par = 0;
     int seg = 0;
     float acc[CW];
 #pragma unroll
     for (int i = 0; i < CW; ++i) acc[i] = 0.f;
-    for (int it = blockIdx.x; it < P.nitems && !abort_sh; it += gridDim.x) {
-      const TcItem w = P.items[P.item0 + it];
-      int nbusy = 0;  // transfer vectors of this item that the MMA warp runs
-      const BusyMask bm = busy_mask(P, w);
-      if (bm.tile())
-        for (int e = w.t0; e < w.t1; ++e) nbusy += bm.src(e) ? 1 : 0;
-      if (nbusy == 0) continue;  // nothing accumulated: no flush
-      const int nseg_item = nbusy * P.nseg;
+    for_each_fragment(P, g_id, g_count, [&](const TcItem &w, int r0, int r1) -> bool {
+      const int nseg_item = (r1 - r0) * P.nseg;  // accumulator segments of this fragment
       for (int sgi = 0; sgi < nseg_item; ++sgi, ++seg) {
-        const int b = P.nbuf == 2 ? (seg & 1) : 0;
-        if (!mbar_wait(&acc_full[b], (full_par >> b) & 1u)) {
-          atomicExch(P.status + 1, 1);
-          abort_sh = 1;
-          break;
-        }
-        full_par ^= 1u << b;
-        tc_fence_after();
-        const unsigned tb = tlane + (unsigned)(b * P.NP);
         if constexpr (NHALF == 1) {
-          drain_cols<CW>(tb + ch * CW, acc);
-          tc_fence_before();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&acc_empty[b][0]);
+          const int b = P.nbuf == 2 ? (seg & 1) : 0;
+          if (!wait_bar(&acc_full[b][0], (full_par >> b) & 1u)) {
+            give_up();
+            break;
+          }
+          full_par ^= 1u << b;
+          tc_fence_after();
+          drain_cols<CW>(tlane + (unsigned)(b * P.NP) + ch * CW, acc);
+          release(b, 0);
         } else {
-          // both parts drain G = CW - SPLIT columns of each half into acc[0, G) and acc[SPLIT, CW); the
-          // remaining 16-column group, acc[G, SPLIT), comes from half 0 for part 0 and half 1 for part 1
+          // each half is committed on its own barrier.  Both parts drain G = CW - SPLIT columns of each
+          // half into acc[0, G) and acc[SPLIT, CW); the remaining 16-column group, acc[G, SPLIT), comes from
+          // half 0 for part 0 and half 1 for part 1
           constexpr int G = CW - SPLIT;
           static_assert(SPLIT - G == 16, "one extra group of 16 columns");
-          drain_cols<G>(tb + (ch == 0 ? 0 : SPLIT), acc);
-          if (ch == 0) drain_cols<16>(tb + G, acc + G);
-          tc_fence_before();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&acc_empty[b][0]);
-          if (ch != 0) drain_cols<16>(tb + CW + G, acc + G);
-          drain_cols<G>(tb + CW + (ch == 0 ? 0 : SPLIT), acc + SPLIT);
-          tc_fence_before();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&acc_empty[b][1]);
+          if (!wait_bar(&acc_full[0][0], full_par & 1u)) {
+            give_up();
+            break;
+          }
+          full_par ^= 1u;
+          tc_fence_after();
+          drain_cols<G>(tlane + (ch == 0 ? 0 : SPLIT), acc);
+          if (ch == 0) drain_cols<16>(tlane + G, acc + G);
+          release(0, 0);
+          if (!wait_bar(&acc_full[0][1], (full_par >> 1) & 1u)) {
+            give_up();
+            break;
+          }
+          full_par ^= 2u;
+          tc_fence_after();
+          if (ch != 0) drain_cols<16>(tlane + CW + G, acc + G);
+          drain_cols<G>(tlane + CW + (ch == 0 ? 0 : SPLIT), acc + SPLIT);
+          release(0, 1);
         }
       }
-      if (abort_sh) break;
-      // flush the item's sums into the FP64 locals
+      if (abort_sh) return false;
+      // flush the fragment's sums into the FP64 locals
       const TcLevel &Lv = P.lv[w.level];
       const int c = w.parity;
-      const int hx = w.bx * TILE_X + (row & 7), hy = w.by * TILE_Y + ((row >> 3) & 3), hz = w.bz * TILE_Z + (row >> 5);
+      const int bz = w.bz + (int)rank;
+      const int hx = w.bx * TILE_X + (row & 7), hy = w.by * TILE_Y + ((row >> 3) & 3), hz = bz * TILE_Z + (row >> 5);
       const int gx = 2 * hx + ((c >> 2) & 1), gy = 2 * hy + ((c >> 1) & 1), gz = 2 * hz + (c & 1);
       int cell = -1;
       if (gx < Lv.side && gy < Lv.side && gz < Lv.side) cell = Lv.grid[((long long)gz * Lv.side + gy) * Lv.side + gx];
@@ -455,13 +680,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
       }
 #pragma unroll
       for (int i = 0; i < CW; ++i) acc[i] = 0.f;
-    }
+      return true;
+    });
   }
+  tc_fence_before();
   __syncthreads();
+  // neither CTA of a pair releases its TMEM or exits while the other may still use it
+  if constexpr (PAIR) cluster_sync_all();
   if (warp == 1) {
     __syncwarp();
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P.ncols));
+    if constexpr (PAIR)
+      asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P.ncols));
+    else
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P.ncols));
   }
 }
 
@@ -545,10 +777,52 @@ __global__ void busy_mask_kernel(const __grid_constant__ TcParams P, int l0, int
   w.bz = (short)((tl / ((long long)TX * TY)) % TZ);
   w.parity = (short)(tl / ((long long)TX * TY * TZ));
   unsigned *m = busy + 6 * tg;
-  const SrcBox b = src_box(P, w, e);
+  const SrcBox b = src_box(P, w, w.bz, e);
   if (box_count(L, b.sp, b.ox, b.oy, b.oz, TILE_X, TILE_Y, TILE_Z) > 0) atomicOr(m + (e >> 5), 1u << (e & 31));
   if (e == 0 && box_count(L, w.parity, w.bx * TILE_X, w.by * TILE_Y, w.bz * TILE_Z, TILE_X, TILE_Y, TILE_Z) > 0)
     atomicOr(m + 5, 1u << 31);
+}
+
+// Work of every unit of levels [P.l0, P.l1]: the number of transfer vectors with an occupied source box when
+// the unit's target tile (either tile of a pair) is occupied, else 0.  Written to prefix[u], which the scan
+// below turns into exclusive prefix sums.
+__global__ void unit_work_kernel(const __grid_constant__ TcParams P, int nunits, int *__restrict__ prefix) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= nunits) return;
+  const TcItem w = decode_unit(P, u);
+  const BusyMask b = P.pair ? busy_mask_pair(P, w) : busy_mask(P, w);
+  int n = 0;
+  if (b.tile()) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) n += __popc(b.w[k]);
+    n += __popc(b.w[5] & ((1u << (189 - 160)) - 1u));
+  }
+  prefix[u] = n;
+}
+
+// In-place exclusive prefix sums of prefix[0, n) with the total in prefix[n] (one block of 1024 threads).
+__global__ void __launch_bounds__(1024) unit_scan_kernel(int n, int *__restrict__ prefix) {
+  __shared__ int part[1024];
+  const int t = threadIdx.x;
+  const int chunk = (n + 1023) / 1024;
+  const int a = min(n, t * chunk), b = min(n, a + chunk);
+  int sum = 0;
+  for (int i = a; i < b; ++i) sum += prefix[i];
+  part[t] = sum;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {
+    const int v = t >= off ? part[t - off] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int run = part[t] - sum;  // exclusive start of this thread's chunk
+  for (int i = a; i < b; ++i) {
+    const int v = prefix[i];
+    prefix[i] = run;
+    run += v;
+  }
+  if (t == 1023) prefix[n] = part[1023];
 }
 
 // max |M| of a level -> bit pattern (non-negative doubles order like their bit patterns)
@@ -625,6 +899,7 @@ EncodeTiledFn encode_fn() {
 
 struct DenseTC {
   int KP = 0, NP = 0, NH = 0, NHALF = 0, NK = 0, stages = 0, ncols = 0, stage_bytes = 0, nbuf = 1;
+  bool pair = false;  // CTA pairs with cta_group::2 MMAs (B200FMM_TC_PAIR=0 keeps single CTAs)
   __half *Bhi = nullptr, *Blo = nullptr;
   // per level
   __half *Ahi[kMaxHeight] = {}, *Alo[kMaxHeight] = {};
@@ -632,16 +907,15 @@ struct DenseTC {
   int HX[kMaxHeight] = {}, HY[kMaxHeight] = {}, HZ[kMaxHeight] = {};
   double *scal = nullptr;                 // [kMaxHeight][2]: pre, post
   unsigned long long *amax = nullptr;     // [kMaxHeight]
-  TcItem *items = nullptr;
-  int nitems = 0;
+ int *prefix = nullptr;                  // work units of all levels: work, then exclusive prefix sums
+  int nunits_all = 0;
   int *sat = nullptr;                     // occupancy summed-area tables of all levels
   size_t satn = 0, sat_off[kMaxHeight] = {};
   long long sat_serial = -1;              // tree the tables describe
   unsigned *busy = nullptr;               // busy masks of every tile of every level
   long long ntiles_all = 0;
-  int lvl_begin[kMaxHeight] = {}, lvl_end[kMaxHeight] = {};
   long long built_for_N = -1;             // tree the per-level buffers were sized for
-  int splits = 0;                         // transfer-vector splits per tile: 0 = by SM fill, else fixed
+  int splits = 0;                         // work ranges per CTA (pair): 0 = default (1), else fixed
   int splits_used = 0;
   int built_for_gen = -1;                 // tree generation the tensor maps / pointers belong to
   TcParams *params = nullptr;             // host copy
@@ -672,8 +946,12 @@ b200fmm_status tc_init(Context &c) {
   if (t->NH % 16 != 0 || t->NH > 256) return fail(B200FMM_ERR_UNSUPPORTED, "unsupported node count for the MMA tile");
   if (t->NP > 352) return fail(B200FMM_ERR_UNSUPPORTED, "the tensor-core M2L supports orders up to 7");
   t->NK = t->KP / KCHUNK;
-  t->stage_bytes = 2 * (TILE_X * TILE_Y * TILE_Z * KCHUNK * 2) + 2 * t->NP * KCHUNK * 2;
-  t->stages = std::min(MAX_STAGES, (220 * 1024) / t->stage_bytes);
+  t->pair = true;
+  if (const char *e = getenv("B200FMM_TC_PAIR")) t->pair = atoi(e) != 0;
+  // a CTA of a pair holds NP / 2 rows of each operator chunk: NH / 2 rows of each column half
+  const int b_rows = t->pair ? t->NP / 2 : t->NP;
+  t->stage_bytes = 2 * (TILE_X * TILE_Y * TILE_Z * KCHUNK * 2) + 2 * b_rows * KCHUNK * 2;
+  t->stages = std::min(t->pair ? MAX_STAGES : MAX_STAGES_SINGLE, (220 * 1024) / t->stage_bytes);
   if (t->stages < 2) return fail(B200FMM_ERR_UNSUPPORTED, "stage buffers do not fit in shared memory");
   t->nbuf = 2 * t->NP <= 512 ? 2 : 1;
   t->ncols = 32;
@@ -694,19 +972,57 @@ b200fmm_status tc_init(Context &c) {
   std::memset(t->params, 0, sizeof(TcParams));
   cuuint64_t dims[3] = {(cuuint64_t)t->KP, (cuuint64_t)t->NP, 343};
   cuuint64_t strides[2] = {(cuuint64_t)t->KP * 2, (cuuint64_t)t->KP * 2 * t->NP};
-  cuuint32_t box[3] = {KCHUNK, (cuuint32_t)t->NH, 1};
+  cuuint32_t box[3] = {KCHUNK, (cuuint32_t)(t->pair ? t->NH / 2 : t->NH), 1};
   B200_CHECK(encode(&t->params->mapB_hi, t->Bhi, 3, dims, strides, box));
   B200_CHECK(encode(&t->params->mapB_lo, t->Blo, 3, dims, strides, box));
   int dev_sms = 148;
   cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c.device);
   t->grid = dev_sms;
+  if (t->pair) {
+    // persistent grid of CTA pairs: as many as can be resident at once
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 2;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    const size_t smem = (size_t)t->stages * t->stage_bytes + 1024;
+    cfg.gridDim = dim3(dev_sms & ~1);
+    cfg.blockDim = dim3(TC_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    cudaError_t err = cudaSuccess;
+    switch (t->NP) {
+#define B200_TC_OCC(NPV, CWV, NHV)                                                                               \
+  case NPV:                                                                                                        \
+    err = cudaFuncSetAttribute(m2l_tc_kernel<CWV, NHV, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+    if (err == cudaSuccess) err = cudaOccupancyMaxActiveClusters(&nclusters, m2l_tc_kernel<CWV, NHV, true>, &cfg);      \
+    break;
+      B200_TC_OCC(32, 16, 1)
+      B200_TC_OCC(64, 32, 1)
+      B200_TC_OCC(128, 64, 1)
+      B200_TC_OCC(224, 112, 1)
+      B200_TC_OCC(352, 176, 2)
+#undef B200_TC_OCC
+      default:
+        break;
+    }
+    if (err != cudaSuccess || nclusters < 1) {
+      cudaGetLastError();
+      return fail(B200FMM_ERR_CUDA, "tensor-core M2L: no CTA pair can be resident (" +
+                                        std::string(cudaGetErrorString(err)) + ")");
+    }
+    t->grid = 2 * std::min(nclusters, dev_sms / 2);
+  }
   return B200FMM_OK;
 }
 
 void tc_free(Context &c) {
   DenseTC *t = c.tc;
   if (!t) return;
-  for (void *p : {(void *)t->Bhi, (void *)t->Blo, (void *)t->scal, (void *)t->amax, (void *)t->items, (void *)t->busy})
+  for (void *p : {(void *)t->Bhi, (void *)t->Blo, (void *)t->scal, (void *)t->amax, (void *)t->prefix, (void *)t->busy})
     if (p) cudaFree(p);
   for (int l = 0; l < kMaxHeight; ++l) {
     if (t->Ahi[l]) cudaFree(t->Ahi[l]);
@@ -723,8 +1039,6 @@ static b200fmm_status tc_prepare(Context &c) {
   DenseTC *t = c.tc;
   TcParams &P = *t->params;
   const int LL = c.H - 1;
-  std::vector<TcItem> items;
-  long long ntiles = 0;
   t->ntiles_all = 0;
   size_t sat_total = 0;
   for (int l = 2; l <= LL; ++l) {
@@ -760,41 +1074,20 @@ static b200fmm_status tc_prepare(Context &c) {
     P.lv[l].tile0 = (int)t->ntiles_all;
     t->ntiles_all += 8LL * (t->HX[l] / TILE_X) * (t->HY[l] / TILE_Y) * (t->HZ[l] / TILE_Z);
     t->sat_serial = -1;
-    ntiles += (long long)c.R * 8 * (t->HX[l] / TILE_X) * (t->HY[l] / TILE_Y) * (t->HZ[l] / TILE_Z);
   }
-  // split the 189 transfer vectors of each tile so that the items fill the SMs evenly
-  int ns = 1;
-  for (int k = 1; k <= 8; ++k) {
-    const long long n = ntiles * k;
-    const long long rounds = (n + t->grid - 1) / t->grid;
-    ns = k;
-    if ((double)n / (double)(rounds * t->grid) >= 0.9) break;
-  }
-  if (t->splits > 0) ns = t->splits;  // chosen by b200fmm_autotune
-  if (const char *e = getenv("B200FMM_TC_SPLITS")) ns = std::max(1, std::min(189, atoi(e)));
-  t->splits_used = ns;
+  // work units, finest level first: every tile (or pair of z-adjacent tiles) of every right-hand side
+  int nunits = 0;
   for (int l = LL; l >= 2; --l) {
-    t->lvl_begin[l] = (int)items.size();
-    for (int r = 0; r < c.R; ++r)
-      for (int par = 0; par < 8; ++par)
-        for (int bz = 0; bz < t->HZ[l] / TILE_Z; ++bz)
-          for (int by = 0; by < t->HY[l] / TILE_Y; ++by)
-            for (int bx = 0; bx < t->HX[l] / TILE_X; ++bx)
-              for (int s = 0; s < ns; ++s) {
-                TcItem w;
-                w.level = (short)l;
-                w.rhs = (short)r;
-                w.parity = (short)par;
-                w.split = (short)s;
-                w.bx = (short)bx;
-                w.by = (short)by;
-                w.bz = (short)bz;
-                w.t0 = (short)(189 * s / ns);
-                w.t1 = (short)(189 * (s + 1) / ns);
-                items.push_back(w);
-              }
-    t->lvl_end[l] = (int)items.size();
+    const int TZ = t->HZ[l] / TILE_Z;
+    P.lv[l].TZu = t->pair ? (TZ + 1) / 2 : TZ;
+    P.lv[l].unit0 = nunits;
+    P.lv[l].nunits = c.R * 8 * P.lv[l].TZu * (t->HY[l] / TILE_Y) * (t->HX[l] / TILE_X);
+    nunits += P.lv[l].nunits;
   }
+  t->nunits_all = nunits;
+  int ns = t->splits > 0 ? t->splits : 1;  // work ranges per CTA (pair), chosen by b200fmm_autotune
+  if (const char *e = getenv("B200FMM_TC_SPLITS")) ns = std::max(1, std::min(64, atoi(e)));
+  t->splits_used = ns;
   if (t->satn != sat_total) {
     if (t->sat) cudaFree(t->sat);
     B200_CUDA(cudaMalloc(&t->sat, std::max<size_t>(sat_total, 1) * sizeof(int)));
@@ -804,13 +1097,11 @@ static b200fmm_status tc_prepare(Context &c) {
   if (t->busy) cudaFree(t->busy);
   B200_CUDA(cudaMalloc(&t->busy, sizeof(unsigned) * 6 * std::max<long long>(t->ntiles_all, 1)));
   P.busy = t->busy;
-  if (t->items) cudaFree(t->items);
-  B200_CUDA(cudaMalloc(&t->items, sizeof(TcItem) * items.size()));
-  B200_CUDA(cudaMemcpy(t->items, items.data(), sizeof(TcItem) * items.size(), cudaMemcpyHostToDevice));
-  t->nitems = (int)items.size();
-  P.items = t->items;
-  P.item0 = 0;
-  P.nitems = t->nitems;
+  if (t->prefix) cudaFree(t->prefix);
+  B200_CUDA(cudaMalloc(&t->prefix, sizeof(int) * (nunits + 1)));
+  P.prefix = t->prefix;
+  P.ranges_per_cta = ns;
+  P.pair = t->pair ? 1 : 0;
   P.R = c.R;
   P.nn = c.nn;
   P.KP = t->KP;
@@ -824,6 +1115,7 @@ static b200fmm_status tc_prepare(Context &c) {
   // accumulator resets per transfer vector: 2 for p >= 6 keeps the M2L within ~1e-6 of FP64
   P.nseg = std::min(t->NK, c.p >= 6 ? 2 : 1);
   P.nbuf = t->nbuf;
+  // a group of two chunks holds two stages while the producer fills the next ones: only with 5 or more
   if (const char *e = getenv("B200FMM_TC_SEGMENTS")) P.nseg = std::max(1, std::min(t->NK, atoi(e)));
   std::memcpy(P.off, c.itab.off, sizeof(P.off));
   std::memcpy(P.slot, c.itab.slot, sizeof(P.slot));
@@ -866,7 +1158,14 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
       ++c.launches;
     }
     busy_mask_kernel<<<grid_for(t->ntiles_all * 189, 256), 256, 0, c.stream>>>(P0, 2, LL, t->ntiles_all, t->busy);
-    ++c.launches;
+    // the work of every unit of every level and its prefix sums, from which each launch splits its units
+    // into ranges of equal work
+    TcParams Pw = P0;
+    Pw.l0 = 2;
+    Pw.l1 = LL;
+    unit_work_kernel<<<grid_for(t->nunits_all, 256), 256, 0, c.stream>>>(Pw, t->nunits_all, t->prefix);
+    unit_scan_kernel<<<1, 1024, 0, c.stream>>>(t->nunits_all, t->prefix);
+    c.launches += 3;
     t->sat_serial = c.tree_serial;
   }
   const int l0 = level == -1 ? 2 : level, l1 = level == -1 ? LL : level;
@@ -884,19 +1183,40 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
                                                           Lv.keys, Lv.M, t->scal + 2 * l, t->Ahi[l], t->Alo[l]);
     c.launches += 3;
   }
-  // items are ordered by level, finest first: levels [l0, l1] are one contiguous range
+  // units are ordered by level, finest first: levels [l0, l1] are one contiguous range
   TcParams &P = *t->params;
-  P.item0 = t->lvl_begin[l1];
-  P.nitems = t->lvl_end[l0] - t->lvl_begin[l1];
-  if (P.nitems <= 0) return B200FMM_OK;
+  P.l0 = l0;
+  P.l1 = l1;
+  P.u_begin = P.lv[l1].unit0;
+  P.u_end = P.lv[l0].unit0 + P.lv[l0].nunits;
+  if (P.u_end <= P.u_begin) return B200FMM_OK;
   const size_t smem = (size_t)t->stages * t->stage_bytes + 1024;
-  const int grid = std::min(t->grid, P.nitems);
+  const int grid = t->grid;  // persistent: one CTA (pair) per SM (pair of SMs)
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = t->pair ? 2 : 1;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(TC_THREADS);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = c.stream;
+  cfg.attrs = at;
+  cfg.numAttrs = t->pair ? 1 : 0;
   B200_CUDA(record_event(c, 8));
   switch (t->NP) {
-#define B200_TC_CASE(NPV, CWV, NHV)                                                                              \
-  case NPV:                                                                                                        \
-    B200_CUDA(cudaFuncSetAttribute(m2l_tc_kernel<CWV, NHV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-    m2l_tc_kernel<CWV, NHV><<<grid, TC_THREADS, smem, c.stream>>>(P);                                              \
+#define B200_TC_CASE(NPV, CWV, NHV)                                                                                 \
+  case NPV:                                                                                                           \
+    if (t->pair) {                                                                                                    \
+      B200_CUDA(cudaFuncSetAttribute(m2l_tc_kernel<CWV, NHV, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,      \
+                                     (int)smem));                                                                     \
+      B200_CUDA(cudaLaunchKernelEx(&cfg, m2l_tc_kernel<CWV, NHV, true>, P));                                          \
+    } else {                                                                                                          \
+      B200_CUDA(cudaFuncSetAttribute(m2l_tc_kernel<CWV, NHV, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
+                                     (int)smem));                                                                     \
+      B200_CUDA(cudaLaunchKernelEx(&cfg, m2l_tc_kernel<CWV, NHV, false>, P));                                         \
+    }                                                                                                                 \
     break;
     B200_TC_CASE(32, 16, 1)
     B200_TC_CASE(64, 32, 1)

@@ -280,6 +280,33 @@ def test_mixed_m2l_locals_match_fp64_dense(order, height):
         assert err < 2e-6, (lvl, err)
 
 
+@pytest.mark.parametrize("order,height", [(3, 5), (6, 4), (7, 5)])
+def test_cta_pair_m2l_matches_single_cta(order, height, monkeypatch):
+    """The tensor-core M2L on CTA pairs (cta_group::2, M = 256, each CTA holding half of every operator
+    chunk) against single CTAs (B200FMM_TC_PAIR=0): both within 2e-6 of the FP64 dense M2L, and of each
+    other (their work ranges, hence their FP32 partial sums, differ).  Levels 2 and 3 have one tile in z, so
+    their pairs run with a missing second tile; 3 work ranges per CTA exercise fragments that start and
+    end inside a tile's transfer vectors."""
+    rng = np.random.default_rng(order * 100 + height)
+    n = 20000
+    x, y, z = rng.random((3, n))
+    q = rng.uniform(-1, 1, n)
+    ops = S.P2M | S.M2M | S.M2L
+    monkeypatch.setenv("B200FMM_TC_SPLITS", "3")
+    loc = {}
+    for mode, prec, pair in (("fp64", "fp64", "1"), ("pair", "mixed", "1"), ("single", "mixed", "0")):
+        monkeypatch.setenv("B200FMM_TC_PAIR", pair)
+        f = S.FMM("cheb_dense", order, height, precision=prec)
+        f.set_particles(x, y, z, q)
+        f.execute(ops)
+        loc[mode] = {lvl: f.cells(lvl)[2] for lvl in range(2, height)}
+        f.close()
+    for lvl in range(2, height):
+        assert S.rel_l2(loc["pair"][lvl], loc["single"][lvl]) < 2e-6, lvl
+        assert S.rel_l2(loc["pair"][lvl], loc["fp64"][lvl]) < 2e-6, lvl
+        assert S.rel_l2(loc["single"][lvl], loc["fp64"][lvl]) < 2e-6, lvl
+
+
 def _fp64_and_mixed(kernel, order, height, x, y, z, q, nrhs=1):
     out = {}
     for prec in ("fp64", "mixed"):
