@@ -318,32 +318,48 @@ __device__ __forceinline__ TcItem decode_unit(const TcParams &P, int u) {
   w.rhs = r >> 3;
   return w;
 }
-// the largest unit u in [u_begin, u_end) whose work starts at or before lo
-__device__ __forceinline__ int first_unit(const TcParams &P, long long lo) {
-  int a = P.u_begin, b = P.u_end;
+// Every role walks the same sequence of unit fragments; f(w, r0, r1) handles the busy transfer vectors of
+// ranks [r0, r1) of unit w and returns false to stop.
+//   * Dense launches (every unit has all 189 transfer vectors busy, as in uniform trees): waves of whole
+//     units, unit u_begin + g + m G for CTA (pair) g, so that all CTAs stream the same transfer vector's
+//     operator at about the same time and share it through L2; the units left over after the last whole wave
+//     are split into G ranges of equal work, one per CTA.
+//   * Otherwise: the work of all units is split into G * ranges_per_cta ranges of equal work; CTA g takes
+//     ranges g, g + G, ...
+template <class F>
+__device__ __forceinline__ bool range_fragments(const TcParams &P, long long lo, long long hi, int u_from, F &f) {
+  if (lo >= hi) return true;
+  int a = u_from, b = P.u_end;  // the largest unit whose work starts at or before lo
   while (b - a > 1) {
     const int m = (a + b) >> 1;
     if (P.prefix[m] <= lo) a = m; else b = m;
   }
-  return a;
+  for (int u = a; u < P.u_end; ++u) {
+    const long long p0 = P.prefix[u], p1 = P.prefix[u + 1];
+    if (p0 >= hi) break;
+    const int r0 = (int)(max(lo, p0) - p0), r1 = (int)(min(hi, p1) - p0);
+    if (r1 <= r0) continue;
+    if (!f(decode_unit(P, u), r0, r1)) return false;
+  }
+  return true;
 }
-// Every role walks the same sequence: for each of its ranges, the units the range overlaps and, in each, the
-// busy transfer vectors of ranks [r0, r1).  f(w, bm, r0, r1) handles one unit fragment; it returns false to stop.
 template <class F>
 __device__ __forceinline__ void for_each_fragment(const TcParams &P, int g, int G, F &&f) {
+  const int U = P.u_end - P.u_begin;
   const long long base = P.prefix[P.u_begin], W = (long long)P.prefix[P.u_end] - base;
+  if (W == 189LL * U) {
+    const int nwave = U / G;
+    for (int m = 0; m < nwave; ++m)
+      if (!f(decode_unit(P, P.u_begin + g + m * G), 0, 189)) return;
+    const int ut = P.u_begin + nwave * G;
+    const long long tb = P.prefix[ut], tw = (long long)P.prefix[P.u_end] - tb;
+    range_fragments(P, tb + tw * g / G, tb + tw * (g + 1) / G, ut, f);
+    return;
+  }
   const int nr = G * P.ranges_per_cta;
   for (int m = 0; m < P.ranges_per_cta; ++m) {
     const int j = g + m * G;
-    const long long lo = base + W * j / nr, hi = base + W * (j + 1) / nr;
-    if (lo >= hi) continue;
-    for (int u = first_unit(P, lo); u < P.u_end; ++u) {
-      const long long p0 = P.prefix[u], p1 = P.prefix[u + 1];
-      if (p0 >= hi) break;
-      const int r0 = (int)(max(lo, p0) - p0), r1 = (int)(min(hi, p1) - p0);
-      if (r1 <= r0) continue;
-      if (!f(decode_unit(P, u), r0, r1)) return;
-    }
+    if (!range_fragments(P, base + W * j / nr, base + W * (j + 1) / nr, P.u_begin, f)) return;
   }
 }
 
