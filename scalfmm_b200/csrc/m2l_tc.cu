@@ -915,7 +915,7 @@ EncodeTiledFn encode_fn() {
 
 struct DenseTC {
   int KP = 0, NP = 0, NH = 0, NHALF = 0, NK = 0, stages = 0, ncols = 0, stage_bytes = 0, nbuf = 1;
-  bool pair = false;  // CTA pairs with cta_group::2 MMAs (B200FMM_TC_PAIR=0 keeps single CTAs)
+  bool pair = false;  // CTA pairs with cta_group::2 MMAs (B200FMM_TC_PAIR=1 / 0 forces them on / off)
   __half *Bhi = nullptr, *Blo = nullptr;
   // per level
   __half *Ahi[kMaxHeight] = {}, *Alo[kMaxHeight] = {};
@@ -962,7 +962,9 @@ b200fmm_status tc_init(Context &c) {
   if (t->NH % 16 != 0 || t->NH > 256) return fail(B200FMM_ERR_UNSUPPORTED, "unsupported node count for the MMA tile");
   if (t->NP > 352) return fail(B200FMM_ERR_UNSUPPORTED, "the tensor-core M2L supports orders up to 7");
   t->NK = t->KP / KCHUNK;
-  t->pair = true;
+  // CTA pairs halve each SM's operator traffic; they pay off at order 7 (two column halves, 38.9 KB instead
+  // of 61.4 KB per stage), while single CTAs are a few percent faster at orders <= 6
+  t->pair = t->NHALF == 2;
   if (const char *e = getenv("B200FMM_TC_PAIR")) t->pair = atoi(e) != 0;
   // a CTA of a pair holds NP / 2 rows of each operator chunk: NH / 2 rows of each column half
   const int b_rows = t->pair ? t->NP / 2 : t->NP;
