@@ -320,6 +320,7 @@ def run_gpu(args):
         step_e2e()
     torch.cuda.synchronize()
     m2l_pairs, p2p_pairs = f.tree_stats()
+    m2l_flops = f.m2l_flops()  # the two products of the low-rank (compressed-operator) tensor-core M2L
 
     def timed(fn, sampler_index=None):
         ms = []
@@ -357,9 +358,7 @@ def run_gpu(args):
     hbm, bf16_sus, bf16_burst, peak_src = measured_peaks()
     m2l_ms = statistics.mean(k["m2l"] for k in ktimes)
     p2p_ms = statistics.mean(k["p2p"] for k in ktimes)
-    nn = ORDER ** 3
-    m2l_flops = m2l_pairs * 2.0 * nn * nn  # logical: split products counted once
-    achieved = m2l_flops / (m2l_ms * 1e-3) / 1e12
+    achieved = m2l_flops / (m2l_ms * 1e-3) / 1e12  # split products counted once
     peak = bf16_sus / 3.0  # three FP16 products per logical product
     traffic = profile_traffic()
     p2p_tflops = p2p_pairs * FLOPS_PER_P2P_PAIR / (p2p_ms * 1e-3) / 1e12
@@ -373,10 +372,12 @@ def run_gpu(args):
         "e2e": {"value": world * n * args.steps / (t_e2e * 1e-3), "unit": "particles/s",
                 "h2d_bytes_per_step": 4 * 8 * n, "d2h_bytes_per_step": 4 * 8 * n},
         "gpu_launches": launches + launches_e2e,
-        "roofline": {"bound": "tensor", "kernel": "m2l_tc_kernel (tcgen05 split-FP16 M2L)",
+        "roofline": {"bound": "tensor", "kernel": "lr_y_kernel + m2l_tc_kernel (tcgen05 split-FP16 low-rank M2L)",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": traffic,
-                     "note": f"logical M2L flops = {m2l_pairs} pairs x 2 x {nn}^2 per launch; peak = {peak_src} "
+                     "note": f"algorithmic M2L flops per launch = {m2l_flops:.4e}: Y = V^T M per source cell "
+                             f"(2 p^3 x the ranks of the slots it feeds) + U Y per pair (2 p^3 r) over {m2l_pairs} "
+                             f"pairs, split products counted once; peak = {peak_src} "
                              f"sustained bf16 {bf16_sus} TFLOP/s / 3 (three FP16 products per logical product); "
                              f"kernel time {m2l_ms:.3f} ms (CUDA events on the launching stream)"},
         "p2p": {"pairs": p2p_pairs, "kernel_ms": p2p_ms, "gpairs_per_s": p2p_pairs / (p2p_ms * 1e-3) / 1e9,

@@ -46,8 +46,10 @@ typedef enum {
 typedef enum { B200FMM_CHEB_SYM = 0, B200FMM_CHEB_DENSE = 1, B200FMM_LAGRANGE = 2 } b200fmm_kernel;
 
 /* FP64: every operator in FP64 (parity form).  MIXED: P2P in FP32 with per-target compensated sums,
- * M2L as split-FP16 tensor-core GEMMs (tcgen05) over the dense per-transfer-vector operators with FP32
- * accumulation and FP64 cross-group sums; P2M/M2M/L2L/L2P stay FP64. */
+ * M2L as split-FP16 tensor-core GEMMs (tcgen05) with FP32 accumulation and FP64 cross-group sums --
+ * for CHEB_SYM over the compressed operators in their low-rank form (Y = V^T M per source cell, then
+ * U Y per target tile), for CHEB_DENSE / LAGRANGE over the dense per-transfer-vector operators;
+ * P2M/M2M/L2L/L2P stay FP64. */
 typedef enum { B200FMM_FP64 = 0, B200FMM_MIXED = 1 } b200fmm_precision;
 
 /* FFmmOperations (FCoreCommon.hpp:17-29) */
@@ -81,8 +83,8 @@ typedef struct b200fmm_context *b200fmm_handle;
 
 /* Lifecycle.  create() also builds the interpolation tables and, for CHEB_SYM, the 16 compressed
  * operators (own FP64 precompute: kernel evaluation at the nodes on the GPU, pACA + QR + SVD on the host,
- * following FChebSymM2LHandler.hpp:39-281); for CHEB_DENSE / LAGRANGE and MIXED it evaluates the
- * dense per-transfer-vector operators on the GPU in FP64. */
+ * following FChebSymM2LHandler.hpp:39-281); for CHEB_DENSE / LAGRANGE it evaluates the dense
+ * per-transfer-vector operators on the GPU in FP64. */
 B200FMM_API b200fmm_status b200fmm_create(const b200fmm_config *cfg, b200fmm_handle *out);
 B200FMM_API b200fmm_status b200fmm_destroy(b200fmm_handle h);
 B200FMM_API const char *b200fmm_last_error(void);
@@ -111,12 +113,19 @@ B200FMM_API b200fmm_status b200fmm_set_charges(b200fmm_handle h, const double *q
  * launches.  A stream that the caller is capturing always gets plain launches. */
 B200FMM_API b200fmm_status b200fmm_execute(b200fmm_handle h, unsigned ops);
 
-/* Tile autotuner (MIXED): times the tensor-core M2L of the current tree with the 189 transfer vectors of
- * each tile split into 1, 2, 3, 4, 6, 8 and 12 work items, keeps the fastest for this handle, and returns it
- * with its kernel time (ms); the automatic choice fills the SMs by count.  It runs the M2L several times and
- * leaves the expansions undefined: call execute() afterwards.  A no-op (splits = 0) in FP64.  The split
- * changes how the FP32 partial sums are grouped, so results move within the MIXED tolerance. */
+/* Work-range autotuner (MIXED): times the tensor-core M2L of the current tree with its work split into
+ * 1, 2, 3 and 4 ranges of equal work per CTA (pair), keeps the fastest for this handle, and returns it with
+ * its kernel time (ms).  Dense trees always run lockstep waves of whole tiles, so the choice matters for
+ * sparse trees.  It runs the M2L several times and leaves the expansions undefined: call execute()
+ * afterwards.  A no-op (splits = 0) in FP64.  The ranges change how the FP32 partial sums are grouped, so
+ * results move within the MIXED tolerance. */
 B200FMM_API b200fmm_status b200fmm_autotune(b200fmm_handle h, int *splits, double *ms);
+
+/* Algorithmic FLOPs of one M2L pass over all levels of the current tree, for the form the handle runs:
+ * dense operators 2 p^6 per interaction pair; compressed operators 2 p^3 r per pair for U Y plus, in MIXED,
+ * 2 p^3 (sum of the fed slots' ranks) per source cell for Y = V^T M (FP64 recomputes V^T M per pair:
+ * 4 p^3 r per pair).  Times the number of right-hand sides. */
+B200FMM_API b200fmm_status b200fmm_m2l_flops(b200fmm_handle h, double *flops);
 
 /* Level-batched operators (FAbstractKernels).  They accumulate (+=) like the reference kernels.
  * m2m/l2l take the parent level; m2l the level of the target cells (2..height-1). */

@@ -73,7 +73,9 @@ int run(int precision, int driver, int height, long long n, const double *x, con
 
   RefKernel kref(height, width, center, &MatrixKernel, eps);
   GpuKernel kgpu(height, width, center, KIND == 0 ? B200FMM_CHEB_SYM : B200FMM_CHEB_DENSE, precision, eps);
-  if (KIND == 0 && precision == B200FMM_FP64) {  // MIXED runs the dense operators on the tensor cores
+  // FP64 is given the reference's own compressed operators; MIXED compresses the same kernel evaluations
+  // itself (the same pACA + SVD) and runs them in their low-rank form on the tensor cores
+  if (KIND == 0 && precision == B200FMM_FP64) {
     SymmetryHandler<FReal, ORDER, HOMOGENEOUS> handler(&MatrixKernel, eps, FReal(1.), 3);
     std::vector<int> ranks(343, 0);
     std::vector<double> uv;

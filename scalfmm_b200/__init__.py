@@ -32,7 +32,7 @@ EXPORTS = (
     "b200fmm_p2p", "b200fmm_get_results", "b200fmm_synchronize", "b200fmm_tree_info", "b200fmm_get_cells",
     "b200fmm_get_permutation", "b200fmm_last_timings", "b200fmm_last_kernel_times", "b200fmm_tree_stats",
     "b200fmm_last_launch_count", "b200fmm_autotune", "b200fmm_p2p_noalloc", "b200fmm_batch_create", "b200fmm_batch_execute",
-    "b200fmm_batch_last_time", "b200fmm_batch_destroy", "b200fmm_direct",
+    "b200fmm_batch_last_time", "b200fmm_batch_destroy", "b200fmm_direct", "b200fmm_m2l_flops",
 )
 NOALLOC_MAX_PARTICLES = 262144
 
@@ -113,6 +113,7 @@ def lib():
                                           + [ctypes.c_void_p] * 3 + [ctypes.c_int, ctypes.c_double, _dp, ctypes.c_int]
                                           + [ctypes.c_void_p] * 5)
         L.b200fmm_autotune.argtypes = [ctypes.c_void_p, _ip, _dp]
+        L.b200fmm_m2l_flops.argtypes = [ctypes.c_void_p, _dp]
         L.b200fmm_batch_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                            ctypes.POINTER(ctypes.c_void_p)]
         L.b200fmm_batch_execute.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
@@ -303,6 +304,12 @@ class FMM:
         c = ctypes.c_longlong()
         _check(lib().b200fmm_last_launch_count(self._h, ctypes.byref(c)), "last_launch_count")
         return c.value
+
+    def m2l_flops(self):
+        """Algorithmic FLOPs of one M2L pass of the current tree, for the operator form this handle runs."""
+        v = ctypes.c_double()
+        _check(lib().b200fmm_m2l_flops(self._h, ctypes.byref(v)), "m2l_flops")
+        return v.value
 
 
 class Batch:

@@ -53,6 +53,21 @@ __global__ void count_m2l_pairs(long long ncells, const int *__restrict__ ilist,
     n += ilist[e] >= 0;
   atomicAdd(out, n);
 }
+// Sum over the interaction pairs of the rank of their slot (rank_of[child type][entry]) and the number of cells
+// of each child type.
+struct RankTable {
+  int r[8][189];
+};
+__global__ void count_m2l_ranks(long long ncells, const long long *__restrict__ keys, const int *__restrict__ ilist,
+                                const __grid_constant__ RankTable T, unsigned long long *__restrict__ out) {
+  const long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (cell >= ncells) return;
+  const int ct = (int)(keys[cell] & 7);
+  unsigned long long s = 0;
+  for (int e = 0; e < 189; ++e) s += ilist[cell * 189 + e] >= 0 ? (unsigned long long)T.r[ct][e] : 0ull;
+  atomicAdd(out, s);
+  atomicAdd(out + 1 + ct, 1ull);
+}
 __global__ void count_p2p_pairs(long long nleaves, const long long *__restrict__ start, const int *__restrict__ nbr,
                                 unsigned long long *__restrict__ out) {
   const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -202,9 +217,10 @@ b200fmm_status b200fmm_create(const b200fmm_config *cfg, b200fmm_handle *out) {
       st = fail(B200FMM_ERR_OOM, "status allocation failed");
   }
   if (st == B200FMM_OK) st = build_tables(*c);
-  if (st == B200FMM_OK && cfg->kernel == B200FMM_CHEB_SYM && cfg->precision == B200FMM_FP64) {
+  if (st == B200FMM_OK && cfg->kernel == B200FMM_CHEB_SYM) {
+    // the compressed operators: applied in FP64, or in their low-rank tensor-core form (MIXED)
     st = compress_sym_operators(*c);
-    if (st == B200FMM_OK) st = upload_sym_operators(*c);
+    if (st == B200FMM_OK && cfg->precision == B200FMM_FP64) st = upload_sym_operators(*c);
   }
   if (st == B200FMM_OK && cfg->kernel != B200FMM_CHEB_SYM && cfg->precision == B200FMM_FP64)
     st = build_dense_operators(*c);
@@ -631,6 +647,53 @@ b200fmm_status b200fmm_tree_stats(b200fmm_handle h, long long *m2l_pairs, long l
   B200_CUDA(cudaStreamSynchronize(c.stream));
   if (m2l_pairs) *m2l_pairs = (long long)hv[0];
   if (p2p_pairs) *p2p_pairs = (long long)hv[1];
+  return B200FMM_OK;
+}
+
+b200fmm_status b200fmm_m2l_flops(b200fmm_handle h, double *flops) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  if (!flops) return fail(B200FMM_ERR_INVALID, "null argument");
+  B200_CHECK(need_particles(c));
+  B200_CHECK(set_device(c));
+  int rank[343];
+  double fed[8];
+  const bool lr = c.cfg.precision == B200FMM_MIXED && tc_lowrank_info(c, rank, fed);
+  const bool sym64 = c.cfg.precision == B200FMM_FP64 && c.cfg.kernel == B200FMM_CHEB_SYM;
+  if (!lr && !sym64) {
+    long long pairs = 0;
+    B200_CHECK(b200fmm_tree_stats(h, &pairs, nullptr));
+    *flops = 2.0 * c.nn * (double)c.nn * (double)pairs * c.R;
+    return B200FMM_OK;
+  }
+  if (sym64) {
+    for (int t = 0; t < 343; ++t) rank[t] = 0;
+    std::vector<int> pind, pvec;
+    slot_symmetry_tables(c.p, pind, pvec);
+    for (int t = 0; t < 343; ++t) rank[t] = c.sym_ranks[pind[t]];
+  }
+  RankTable T;
+  for (int ct = 0; ct < 8; ++ct)
+    for (int e = 0; e < 189; ++e) T.r[ct][e] = rank[c.itab.slot[ct][e]];
+  B200_CHECK(ensure_scratch(c, 4096));
+  unsigned long long *d = (unsigned long long *)((char *)c.d_scratch + 2048);
+  B200_CUDA(cudaMemsetAsync(d, 0, 9 * sizeof(unsigned long long), c.stream));
+  for (int l = 2; l < c.H; ++l)
+    if (c.lv[l].n)
+      count_m2l_ranks<<<grid_for(c.lv[l].n, 256), 256, 0, c.stream>>>(c.lv[l].n, c.lv[l].keys, c.lv[l].ilist, T, d);
+  B200_CUDA(cudaGetLastError());
+  unsigned long long hv[9];
+  B200_CUDA(cudaMemcpyAsync(hv, d, sizeof(hv), cudaMemcpyDeviceToHost, c.stream));
+  B200_CUDA(cudaStreamSynchronize(c.stream));
+  if (sym64) {
+    // per pair: Y = V^T M and U Y, each 2 p^3 r
+    *flops = 4.0 * c.nn * (double)hv[0] * c.R;
+  } else {
+    // second product per pair (2 p^3 r), first product per cell over the slots its parity feeds
+    double first = 0;
+    for (int ct = 0; ct < 8; ++ct) first += (double)hv[1 + ct] * fed[ct];
+    *flops = 2.0 * c.nn * ((double)hv[0] + first) * c.R;
+  }
   return B200FMM_OK;
 }
 

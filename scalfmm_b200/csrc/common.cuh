@@ -161,6 +161,10 @@ b200fmm_status check_status(Context &c);
 b200fmm_status build_tables(Context &c);
 b200fmm_status compress_sym_operators(Context &c);
 b200fmm_status upload_sym_operators(Context &c);
+bool tc_lowrank_info(const Context &c, int *rank_of_slot, double *rank_fed);
+void slot_symmetry_tables(int p, std::vector<int> &pind, std::vector<int> &pvec);
+b200fmm_status sym_slot_factors(const Context &c, std::vector<double> &Ut, std::vector<double> &Vt,
+                                std::vector<long long> &toff, std::vector<int> &trank);
 b200fmm_status build_dense_operators(Context &c);
 // tree.cu
 b200fmm_status build_tree(Context &c, const double *x, const double *y, const double *z, const double *q,

@@ -31,6 +31,7 @@
 #include <cuda.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -102,6 +103,14 @@ struct __align__(64) TcParams {
   // per tile (level, parity, bz, by, bx): 6 words, bit e set when transfer vector e has an occupied source
   // box; bit 31 of word 5 set when the tile has an occupied target cell
   const unsigned *busy;
+  // low-rank form (symmetric Chebyshev operators K_t = U_t V_t^T): A is Y = V_t^T M, one row of 16-rank
+  // chunks per source cell, and B is U_t, both in 16-wide K chunks
+  int lr_seglen;                // K chunks per accumulator segment of a fragment's chunk stream
+  int ycht;                     // Y chunks per right-hand side (all parities)
+  int ybase[8];                 // first Y chunk of each source parity
+  unsigned char tnk[343];       // K chunks of slot t (ceil(rank / 16)), 0 for near slots
+  short uchunk0[343];           // first U chunk of slot t
+  short ychunk0[8][343];        // first Y chunk of slot t among the chunks of source parity c'
 };
 
 // ---- PTX helpers ----------------------------------------------------------------------------------
@@ -144,10 +153,22 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
       "l"(map), "r"(su32(bar)), "r"(c0), "r"(c1), "r"(c2)
       : "memory");
 }
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, unsigned long long *bar, int c0, int c1) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+          su32(dst)),
+      "l"(map), "r"(su32(bar)), "r"(c0), "r"(c1)
+      : "memory");
+}
 // UMMA shared-memory descriptor: K-major, 64-byte swizzle, rows of 64 B in 8-row groups 512 B apart.
 __device__ __forceinline__ unsigned long long sdesc(const void *p) {
   const unsigned long long a = su32(p);
   return ((a >> 4) & 0x3FFFull) | (1ull << 16) | (32ull << 32) | (1ull << 46) | (4ull << 61);
+}
+// the same for rows of 32 B (16 fp16) with the 32-byte swizzle: 8-row groups 256 B apart, layout type 6
+__device__ __forceinline__ unsigned long long sdesc32(const void *p) {
+  const unsigned long long a = su32(p);
+  return ((a >> 4) & 0x3FFFull) | (1ull << 16) | (16ull << 32) | (1ull << 46) | (6ull << 61);
 }
 __device__ __forceinline__ void mma_f16(unsigned d_tmem, unsigned long long da, unsigned long long db, unsigned idesc,
                                         unsigned accumulate) {
@@ -382,7 +403,7 @@ __device__ __forceinline__ void for_each_fragment(const TcParams &P, int g, int 
 // expects both CTAs' bytes on its full barrier, its MMA warp issues all MMAs, and the commits arrive on the
 // stage and accumulator barriers of both CTAs; the epilogue warps of both CTAs release the accumulator on
 // the even CTA's barriers (16 arrivals).
-template <int CW, int NHALF, bool PAIR>
+template <int CW, int NHALF, bool PAIR, bool LR>
 __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_constant__ TcParams P) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1024-byte aligned stage buffers (the swizzle pattern repeats every 512 B)
@@ -446,9 +467,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
     return busy_mask(P, w);
   };
 
-  const int a_bytes = TILE_X * TILE_Y * TILE_Z * KCHUNK * 2;  // 8 KB
-  const int nb_rows = PAIR ? P.NH / 2 : P.NH;                 // B rows of one column half in this CTA
-  const int b_bytes = NHALF * nb_rows * KCHUNK * 2;
+  constexpr int KCH = LR ? 16 : KCHUNK;  // fp16 per K chunk: 16 (32-byte rows) or 32 (64-byte rows)
+  constexpr int ROWB = KCH * 2;
+  const int a_bytes = TILE_X * TILE_Y * TILE_Z * ROWB;  // 4 or 8 KB
+  const int nb_rows = PAIR ? P.NH / 2 : P.NH;           // B rows of one column half in this CTA
+  const int b_bytes = NHALF * nb_rows * ROWB;
 
   if (warp == 0) {
     // ------------------------------------------------ TMA producer (both CTAs of a pair)
@@ -467,32 +490,37 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
           if (rank_e++ < r0) continue;
           const SrcBox sb = src_box(P, w, bz, e);
           const int sp = sb.sp, ox = sb.ox, oy = sb.oy, oz = sb.oz, slot = sb.slot;
-          for (int kc = 0; kc < P.NK; ++kc) {
+          // K chunks of this transfer vector and the coordinates of its A and B boxes: dense (K offset,
+          // rhs and parity, operator slot) or low rank (Y chunk and U chunk of the slot)
+          const int nk = LR ? (int)P.tnk[slot] : P.NK;
+          const int a4 = LR ? w.rhs * P.ycht + P.ybase[sp] + P.ychunk0[sp][slot] : w.rhs * 8 + sp;
+          const int b2 = LR ? P.uchunk0[slot] : slot;
+          for (int kc = 0; kc < nk; ++kc) {
             if (!wait_bar(&empty_bar[stage], phase ^ 1)) {
               give_up();
               break;
             }
             unsigned char *sbuf = smem + (size_t)stage * P.stage_bytes;
             if (leader) mbar_expect_tx(&full_bar[stage], stage_tx);
-            const int c4 = w.rhs * 8 + sp;
+            const int k0 = LR ? 0 : kc * KCHUNK;  // K coordinate of the boxes
+            const int c4 = LR ? a4 + kc : a4;
+            const int c2 = LR ? b2 + kc : b2;
             if constexpr (PAIR) {
               const unsigned fb = full0 + 8u * (unsigned)stage;
-              tma_load_5d_pair(sbuf, &P.mapA_hi[w.level], fb, kc * KCHUNK, ox, oy, oz, c4);
-              tma_load_5d_pair(sbuf + a_bytes, &P.mapA_lo[w.level], fb, kc * KCHUNK, ox, oy, oz, c4);
+              tma_load_5d_pair(sbuf, &P.mapA_hi[w.level], fb, k0, ox, oy, oz, c4);
+              tma_load_5d_pair(sbuf + a_bytes, &P.mapA_lo[w.level], fb, k0, ox, oy, oz, c4);
               for (int h = 0; h < NHALF; ++h) {
                 const int row0 = h * P.NH + (int)rank * nb_rows;
-                tma_load_3d_pair(sbuf + 2 * a_bytes + h * nb_rows * 64, &P.mapB_hi, fb, kc * KCHUNK, row0, slot);
-                tma_load_3d_pair(sbuf + 2 * a_bytes + b_bytes + h * nb_rows * 64, &P.mapB_lo, fb, kc * KCHUNK, row0,
-                                 slot);
+                tma_load_3d_pair(sbuf + 2 * a_bytes + h * nb_rows * ROWB, &P.mapB_hi, fb, k0, row0, c2);
+                tma_load_3d_pair(sbuf + 2 * a_bytes + b_bytes + h * nb_rows * ROWB, &P.mapB_lo, fb, k0, row0, c2);
               }
             } else {
-              tma_load_5d(sbuf, &P.mapA_hi[w.level], &full_bar[stage], kc * KCHUNK, ox, oy, oz, c4);
-              tma_load_5d(sbuf + a_bytes, &P.mapA_lo[w.level], &full_bar[stage], kc * KCHUNK, ox, oy, oz, c4);
+              tma_load_5d(sbuf, &P.mapA_hi[w.level], &full_bar[stage], k0, ox, oy, oz, c4);
+              tma_load_5d(sbuf + a_bytes, &P.mapA_lo[w.level], &full_bar[stage], k0, ox, oy, oz, c4);
               for (int h = 0; h < NHALF; ++h) {
-                tma_load_3d(sbuf + 2 * a_bytes + h * nb_rows * 64, &P.mapB_hi, &full_bar[stage], kc * KCHUNK,
-                            h * P.NH, slot);
-                tma_load_3d(sbuf + 2 * a_bytes + b_bytes + h * nb_rows * 64, &P.mapB_lo, &full_bar[stage],
-                            kc * KCHUNK, h * P.NH, slot);
+                tma_load_3d(sbuf + 2 * a_bytes + h * nb_rows * ROWB, &P.mapB_hi, &full_bar[stage], k0, h * P.NH, c2);
+                tma_load_3d(sbuf + 2 * a_bytes + b_bytes + h * nb_rows * ROWB, &P.mapB_lo, &full_bar[stage], k0,
+                            h * P.NH, c2);
               }
             }
             if (++stage == S) {
@@ -514,10 +542,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
           (1u << 4) | ((unsigned)(P.NH >> 3) << 17) | ((unsigned)((PAIR ? 256 : 128) >> 4) << 24);
       // descriptors of stage 0's operands: another stage, K step or column half adds (byte offset >> 4) to
       // the 14-bit start-address field, which never carries (shared addresses stay below 2^18 bytes)
-      const unsigned long long dA_hi = sdesc(smem), dA_lo = dA_hi + (unsigned)(a_bytes >> 4);
+      const unsigned long long dA_hi = LR ? sdesc32(smem) : sdesc(smem), dA_lo = dA_hi + (unsigned)(a_bytes >> 4);
       const unsigned long long dB_hi = dA_hi + (unsigned)((2 * a_bytes) >> 4), dB_lo = dB_hi + (unsigned)(b_bytes >> 4);
       const unsigned stage_step = (unsigned)P.stage_bytes >> 4;
-      const unsigned half_step = (unsigned)(nb_rows * 64) >> 4;
+      const unsigned half_step = (unsigned)(nb_rows * ROWB) >> 4;
       int stage = 0;
       unsigned phase = 0;
       auto commit = [&](unsigned long long *bar) {
@@ -532,7 +560,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
         const unsigned so = (unsigned)st * stage_step;
         const unsigned bo = so + (unsigned)h * half_step;
 #pragma unroll
-        for (int ks = 0; ks < 2; ++ks) {
+        for (int ks = 0; ks < KCH / 16; ++ks) {
           const unsigned k2 = 2u * ks;  // 16 fp16 = 32 bytes of K
           if constexpr (PAIR) {
             mma_f16_pair(d, dA_hi + so + k2, dB_lo + bo + k2, idesc, (first && ks == 0) ? 0u : 1u);
@@ -561,6 +589,49 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
       unsigned empty_par = 0xFu;  // parity to wait for, per (buffer, half): starts at 1 (passes at once)
       int seg = 0;
       for_each_fragment(P, g_id, g_count, [&](const TcItem &w, int r0, int r1) -> bool {
+        if constexpr (LR) {
+          // low rank: the fragment's K chunks (1..3 per transfer vector) form one stream, cut into
+          // segments of lr_seglen chunks; with two column halves both issuers cut it at the same places
+          const BusyMask bm = item_mask(w);
+          int cs = 0;  // chunks issued in the open segment
+          int b = 0;   // its accumulator (one column half: two alternate when they fit)
+          int rank_e = 0;
+          for (int e = 0; e < 189 && rank_e < r1 && !abort_sh; ++e) {
+            if (!bm.src(e)) continue;
+            if (rank_e++ < r0) continue;
+            const int nk = P.tnk[P.slot[w.parity][e]];
+            for (int kc = 0; kc < nk && !abort_sh; ++kc) {
+              if (cs == 0) {
+                const int hb = NHALF == 2 ? 0 : (P.nbuf == 2 ? (seg & 1) : 0);
+                const int bit = NHALF == 2 ? hh : 2 * hb;
+                if (!wait_bar(&acc_empty[hb][NHALF == 2 ? hh : 0], (empty_par >> bit) & 1u)) {
+                  give_up();
+                  break;
+                }
+                empty_par ^= 1u << bit;
+                b = hb;
+                tc_fence_after();
+              }
+              const int st = next_full();
+              if (st < 0) break;
+              if constexpr (NHALF == 2)
+                issue_half(st, hh, tmem + (unsigned)(hh * P.NH), cs == 0);
+              else
+                issue_half(st, 0, tmem + (unsigned)(b * P.NP), cs == 0);
+              commit(&empty_bar[st]);
+              if (++cs == P.lr_seglen) {
+                commit(&acc_full[b][NHALF == 2 ? hh : 0]);
+                cs = 0;
+                ++seg;
+              }
+            }
+          }
+          if (cs > 0 && !abort_sh) {
+            commit(&acc_full[b][NHALF == 2 ? hh : 0]);
+            ++seg;
+          }
+          return !abort_sh;
+        }
         // every MMA of a fragment runs the same schedule: only the count of transfer vectors matters here
         (void)w;
         for (int ev = r0; ev < r1 && !abort_sh; ++ev) {
@@ -634,7 +705,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
 #pragma unroll
     for (int i = 0; i < CW; ++i) acc[i] = 0.f;
     for_each_fragment(P, g_id, g_count, [&](const TcItem &w, int r0, int r1) -> bool {
-      const int nseg_item = (r1 - r0) * P.nseg;  // accumulator segments of this fragment
+      // accumulator segments of this fragment: nseg per transfer vector, or (low rank) one per lr_seglen
+      // K chunks of the fragment's chunk stream
+      int nseg_item = (r1 - r0) * P.nseg;
+      if constexpr (LR) {
+        const BusyMask bm = item_mask(w);
+        int nch = 0, rank_e = 0;
+        for (int e = 0; e < 189 && rank_e < r1; ++e) {
+          if (!bm.src(e)) continue;
+          if (rank_e++ >= r0) nch += P.tnk[P.slot[w.parity][e]];
+        }
+        nseg_item = (nch + P.lr_seglen - 1) / P.lr_seglen;
+      }
       for (int sgi = 0; sgi < nseg_item; ++sgi, ++seg) {
         if constexpr (NHALF == 1) {
           const int b = P.nbuf == 2 ? (seg & 1) : 0;
@@ -710,6 +792,233 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
       asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P.ncols));
     else
       asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P.ncols));
+  }
+}
+
+// ---- low-rank M2L, first product: Y = V^T M for every source cell --------------------------------------
+// For symmetric Chebyshev operators K_t = U_t V_t^T (FChebSymKernel's compression, rank 16..44 at order 7),
+// the transfer of a source cell s to a target along slot t is U_t (V_t^T M_s).  Y_t = V_t^T M_s depends on
+// the source only, so it is computed once per source cell and slot, for the slots that the cell's parity
+// grid feeds: one GEMM per level, parity and 8x4x4 tile of source cells (M = 128 cells, N = 256 rank rows =
+// 16 chunks of 16, K = p^3 in chunks of 32), A = the packed multipoles (hi, lo), B = the stacked V_t (hi,
+// lo).  The K chunks are cut into segments of segc chunks that alternate between two TMEM accumulators:
+// the tensor core's FP32 accumulation truncates, and the columns of V oscillate in sign, so long chains
+// would lose accuracy against the partial sums.  The epilogue adds the segments in registers (rounded FP32
+// adds) and writes Y as FP16 hi and lo, 16 ranks per chunk, in the parity-split grid layout that the second
+// product's TMA boxes read.
+struct __align__(64) LrYParams {
+  CUtensorMap mapA_hi[kMaxHeight], mapA_lo[kMaxHeight];  // multipoles: 5-D boxes of 32 K x 8x4x4 cells
+  CUtensorMap mapV_hi, mapV_lo;                          // V rows: 2-D boxes of 32 K x 256 rows
+  __half *Yhi[kMaxHeight], *Ylo[kMaxHeight];             // [R * ycht][HZ][HY][HX][16]
+  int HX[kMaxHeight], HY[kMaxHeight], HZ[kMaxHeight];
+  int item0[kMaxHeight], nitems[kMaxHeight];             // items of each level, finest level first
+  int l0, l1;                                            // levels of this launch
+  int R, NK, nblk;                                       // rhs, K chunks, 256-row blocks per parity
+  int segc;                                              // K chunks per accumulator segment
+  float yscale;                                          // power of two that brings |Y| below 2^15
+  int ycht, ybase[9];                                    // Y chunks per rhs; first chunk of each parity
+  int stages, stage_bytes;
+  int *status;
+};
+
+constexpr int YBLK = 256;  // rank rows per item (16 chunks of 16)
+
+__global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_constant__ LrYParams P) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *smem = (unsigned char *)(((unsigned long long)smem_raw + 1023) & ~1023ull);
+  __shared__ __align__(8) unsigned long long full_bar[MAX_STAGES], empty_bar[MAX_STAGES];
+  __shared__ __align__(8) unsigned long long acc_full[2], acc_empty[2], done_bar;
+  __shared__ unsigned tmem_base_sh;
+  __shared__ volatile int abort_sh;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int S = P.stages;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], 8);
+    }
+    mbar_init(&done_bar, 1);
+    abort_sh = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_base_sh)),
+                 "r"(2 * YBLK));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const unsigned tmem = tmem_base_sh;
+  auto give_up = [&]() {
+    atomicExch(P.status + 1, 1);
+    abort_sh = 1;
+  };
+  const int a_bytes = TILE_X * TILE_Y * TILE_Z * KCHUNK * 2;  // 8 KB
+  const int b_bytes = YBLK * KCHUNK * 2;                      // 16 KB
+  const int segc = P.segc;
+  const int nseg = (P.NK + segc - 1) / segc;                  // segments per item
+  const int nitems = P.item0[P.l0] + P.nitems[P.l0] - P.item0[P.l1];
+  // item -> level, rhs, parity, tile, block; items of a tile are consecutive (blocks innermost) so that the
+  // CTAs working at the same time share the tile's multipoles and the V blocks through L2
+  struct YItem {
+    int level, rhs, par, bx, by, bz, nb;
+  };
+  auto decode = [&](int it) {
+    YItem y;
+    int g = it + P.item0[P.l1];
+    int l = P.l1;
+    while (l > P.l0 && g >= P.item0[l] + P.nitems[l]) --l;
+    int r = g - P.item0[l];
+    y.level = l;
+    y.nb = r % P.nblk;
+    r /= P.nblk;
+    const int TX = P.HX[l] / TILE_X, TY = P.HY[l] / TILE_Y, TZ = P.HZ[l] / TILE_Z;
+    y.bx = r % TX;
+    r /= TX;
+    y.by = r % TY;
+    r /= TY;
+    y.bz = r % TZ;
+    r /= TZ;
+    y.par = r & 7;
+    y.rhs = r >> 3;
+    return y;
+  };
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int stage = 0;
+      unsigned phase = 0;
+      for (int it = blockIdx.x; it < nitems && !abort_sh; it += gridDim.x) {
+        const YItem y = decode(it);
+        const int vrow = (P.ybase[y.par] + y.nb * (YBLK / 16)) * 16;
+        for (int kc = 0; kc < P.NK; ++kc) {
+          if (!mbar_wait(&empty_bar[stage], phase ^ 1)) {
+            give_up();
+            break;
+          }
+          unsigned char *sbuf = smem + (size_t)stage * P.stage_bytes;
+          mbar_expect_tx(&full_bar[stage], 2 * a_bytes + 2 * b_bytes);
+          const int c4 = y.rhs * 8 + y.par;
+          tma_load_5d(sbuf, &P.mapA_hi[y.level], &full_bar[stage], kc * KCHUNK, y.bx * TILE_X, y.by * TILE_Y,
+                      y.bz * TILE_Z, c4);
+          tma_load_5d(sbuf + a_bytes, &P.mapA_lo[y.level], &full_bar[stage], kc * KCHUNK, y.bx * TILE_X,
+                      y.by * TILE_Y, y.bz * TILE_Z, c4);
+          tma_load_2d(sbuf + 2 * a_bytes, &P.mapV_hi, &full_bar[stage], kc * KCHUNK, vrow);
+          tma_load_2d(sbuf + 2 * a_bytes + b_bytes, &P.mapV_lo, &full_bar[stage], kc * KCHUNK, vrow);
+          if (++stage == S) {
+            stage = 0;
+            phase ^= 1;
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const unsigned idesc = (1u << 4) | ((unsigned)(YBLK >> 3) << 17) | ((unsigned)(128 >> 4) << 24);
+      const unsigned long long dA_hi = sdesc(smem), dA_lo = dA_hi + (unsigned)(a_bytes >> 4);
+      const unsigned long long dB_hi = dA_hi + (unsigned)((2 * a_bytes) >> 4), dB_lo = dB_hi + (unsigned)(b_bytes >> 4);
+      const unsigned stage_step = (unsigned)P.stage_bytes >> 4;
+      int stage = 0;
+      unsigned phase = 0, empty_par = 3u;
+      for (int it = blockIdx.x; it < nitems && !abort_sh; it += gridDim.x) {
+        for (int kc = 0; kc < P.NK && !abort_sh; ++kc) {
+          const int b = (kc / segc) & 1;
+          const bool first = kc % segc == 0;
+          if (first) {
+            if (!mbar_wait(&acc_empty[b], (empty_par >> b) & 1u)) {
+              give_up();
+              break;
+            }
+            empty_par ^= 1u << b;
+            tc_fence_after();
+          }
+          if (!mbar_wait(&full_bar[stage], phase)) {
+            give_up();
+            break;
+          }
+          const unsigned so = (unsigned)stage * stage_step;
+          const unsigned d = tmem + (unsigned)(b * YBLK);
+#pragma unroll
+          for (int ks = 0; ks < 2; ++ks) {
+            const unsigned k2 = 2u * ks;
+            mma_f16(d, dA_hi + so + k2, dB_lo + so + k2, idesc, (first && ks == 0) ? 0u : 1u);
+            mma_f16(d, dA_lo + so + k2, dB_hi + so + k2, idesc, 1u);
+            mma_f16(d, dA_hi + so + k2, dB_hi + so + k2, idesc, 1u);
+          }
+          mma_commit(&empty_bar[stage]);
+          if (++stage == S) {
+            stage = 0;
+            phase ^= 1;
+          }
+          if (kc % segc == segc - 1 || kc == P.NK - 1) mma_commit(&acc_full[b]);
+        }
+      }
+      mma_commit(&done_bar);
+      if (!mbar_wait(&done_bar, 0)) give_up();
+    }
+  } else if (warp >= 2 && warp <= 9) {
+    const int q = warp & 3;
+    const int ch = (warp - 2) >> 2;  // which 128 of the 256 columns
+    const int row = q * 32 + lane;   // source cell within the tile
+    const unsigned tlane = tmem + ((unsigned)(q * 32) << 16) + (unsigned)(ch * 128);
+    unsigned full_par = 0;
+    float acc[128];
+    for (int it = blockIdx.x; it < nitems && !abort_sh; it += gridDim.x) {
+      const YItem y = decode(it);
+#pragma unroll
+      for (int i = 0; i < 128; ++i) acc[i] = 0.f;
+      for (int sg = 0; sg < nseg; ++sg) {
+        const int b = sg & 1;
+        if (!mbar_wait(&acc_full[b], (full_par >> b) & 1u)) {
+          give_up();
+          break;
+        }
+        full_par ^= 1u << b;
+        tc_fence_after();
+        drain_cols<128>(tlane + (unsigned)(b * YBLK), acc);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acc_empty[b]);
+      }
+      if (abort_sh) break;
+      // write the 8 chunks of 16 ranks this thread holds, as FP16 hi and lo
+      const int l = y.level;
+      const int hx = y.bx * TILE_X + (row & 7), hy = y.by * TILE_Y + ((row >> 3) & 3), hz = y.bz * TILE_Z + (row >> 5);
+      const int nch = P.ybase[y.par + 1] - P.ybase[y.par];  // chunks of this parity
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int chunk = y.nb * (YBLK / 16) + ch * 8 + k;
+        if (chunk >= nch) break;
+        const long long yi = (long long)y.rhs * P.ycht + P.ybase[y.par] + chunk;
+        const long long off = (((yi * P.HZ[l] + hz) * P.HY[l] + hy) * P.HX[l] + hx) * 16;
+        unsigned hv[8], lv[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const float v0 = acc[k * 16 + 2 * i] * P.yscale, v1 = acc[k * 16 + 2 * i + 1] * P.yscale;
+          const __half h0 = __float2half_rn(v0), h1 = __float2half_rn(v1);
+          const __half l0 = __float2half_rn(v0 - __half2float(h0)), l1 = __float2half_rn(v1 - __half2float(h1));
+          hv[i] = (unsigned)__half_as_ushort(h0) | ((unsigned)__half_as_ushort(h1) << 16);
+          lv[i] = (unsigned)__half_as_ushort(l0) | ((unsigned)__half_as_ushort(l1) << 16);
+        }
+        uint4 *dh = (uint4 *)(P.Yhi[l] + off), *dl = (uint4 *)(P.Ylo[l] + off);
+        dh[0] = make_uint4(hv[0], hv[1], hv[2], hv[3]);
+        dh[1] = make_uint4(hv[4], hv[5], hv[6], hv[7]);
+        dl[0] = make_uint4(lv[0], lv[1], lv[2], lv[3]);
+        dl[1] = make_uint4(lv[4], lv[5], lv[6], lv[7]);
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * YBLK));
   }
 }
 
@@ -852,14 +1161,15 @@ __global__ void absmax_kernel(long long n, const double *__restrict__ v, unsigne
 }
 
 // 2^sA with sA chosen so that max|M| * 2^sA ~ 2^14, and the epilogue factor scale_l * 2^-(sA + SB)
-__global__ void level_scale_kernel(const unsigned long long *__restrict__ amax, double scale_l,
+// shift: the operators' own pre-scale exponent (SB for the dense K, sV + sU for the low-rank factors)
+__global__ void level_scale_kernel(const unsigned long long *__restrict__ amax, double scale_l, int shift,
                                    double *__restrict__ pre, double *__restrict__ post) {
   const double m = __longlong_as_double((long long)*amax);
   int e = 0;
   if (m > 0) frexp(m, &e);  // m = f * 2^e, f in [0.5, 1)
   const int sA = 14 - e;
   *pre = ldexp(1.0, sA);
-  *post = scale_l * ldexp(1.0, -(sA + SB));
+  *post = scale_l * ldexp(1.0, -(sA + shift));
 }
 
 __global__ void pack_multipoles(long long ncells, int R, int nn, int KP, int HX, int HY, int HZ,
@@ -936,22 +1246,196 @@ struct DenseTC {
   int built_for_gen = -1;                 // tree generation the tensor maps / pointers belong to
   TcParams *params = nullptr;             // host copy
   int grid = 0;
+  // low-rank form (symmetric Chebyshev operators): Bhi / Blo hold U in 16-wide K chunks
+  bool lr = false;
+  __half *Vhi = nullptr, *Vlo = nullptr;  // stacked V rows [16 * ycht][KP]
+  __half *Yhi[kMaxHeight] = {}, *Ylo[kMaxHeight] = {};
+  size_t Ybytes[kMaxHeight] = {};
+  int ycht = 0, nblk = 0, ystages = 0, ystage_bytes = 0;
+  int lr_shift = 0;                       // sV + sU: the power-of-two pre-scales of V and U
+  LrYParams *yparams = nullptr;           // host copy
+  double lr_rank_fed[8] = {};             // first product: sum of the ranks of the slots each parity feeds
+  int lr_rank[343] = {};                  // rank of each far slot
 };
 
 static b200fmm_status encode(CUtensorMap *map, void *base, int rank, const cuuint64_t *dims, const cuuint64_t *strides,
-                             const cuuint32_t *box) {
+                             const cuuint32_t *box, CUtensorMapSwizzle swizzle = CU_TENSOR_MAP_SWIZZLE_64B) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return fail(B200FMM_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is not available");
   cuuint32_t es[5] = {1, 1, 1, 1, 1};
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, (cuuint32_t)rank, base, dims, strides, box, es,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(B200FMM_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
   return B200FMM_OK;
 }
 
+// Low-rank operators: per far slot t, K chunks of 16 ranks; U chunks [uch][NP][16] (B of the second
+// product) and, per source parity, the stacked V rows of the slots that the parity's cells feed (B of the
+// first product), both pre-scaled by powers of two and split into FP16 hi + lo.
+static b200fmm_status tc_init_lowrank(Context &c, DenseTC &t, TcParams &P, bool &use) {
+  std::vector<double> Ut, Vt;
+  std::vector<long long> toff;
+  std::vector<int> trank;
+  B200_CHECK(sym_slot_factors(c, Ut, Vt, toff, trank));
+  const int nn = c.nn;
+  int uch = 0;
+  for (int s = 0; s < 343; ++s) t.lr_rank[s] = toff[s] < 0 ? 0 : trank[s];
+  for (int s = 0; s < 343; ++s) {
+    P.tnk[s] = 0;
+    P.uchunk0[s] = 0;
+    if (toff[s] < 0) continue;
+    P.tnk[s] = (unsigned char)((trank[s] + 15) / 16);
+    P.uchunk0[s] = (short)uch;
+    uch += P.tnk[s];
+  }
+  // the slots whose sources lie in each parity grid: target parity c + offset of its entry, per axis
+  std::vector<std::array<bool, 343>> need(8);
+  for (auto &row : need) row.fill(false);
+  for (int ct = 0; ct < 8; ++ct)
+    for (int e = 0; e < 189; ++e) {
+      const int dx = c.itab.off[ct][e][0], dy = c.itab.off[ct][e][1], dz = c.itab.off[ct][e][2];
+      const int sp = ((((ct >> 2) & 1) + dx) & 1) << 2 | ((((ct >> 1) & 1) + dy) & 1) << 1 | (((ct & 1) + dz) & 1);
+      need[sp][c.itab.slot[ct][e]] = true;
+    }
+  int ych = 0, maxch = 0;
+  for (int sp = 0; sp < 8; ++sp) {
+    P.ybase[sp] = ych;
+    int k = 0;
+    double rsum = 0;
+    for (int s = 0; s < 343; ++s) {
+      P.ychunk0[sp][s] = 0;
+      if (!need[sp][s]) continue;
+      if (P.tnk[s] == 0) return fail(B200FMM_ERR_INVALID, "low-rank M2L: an interaction slot has no operator");
+      P.ychunk0[sp][s] = (short)k;
+      k += P.tnk[s];
+      rsum += trank[s];
+    }
+    t.lr_rank_fed[sp] = rsum;
+    ych += k;
+    maxch = std::max(maxch, k);
+  }
+  t.ycht = ych;
+  P.ycht = ych;
+  t.nblk = (maxch + (YBLK / 16) - 1) / (YBLK / 16);
+  // Y of all levels must fit comfortably: else the dense form is used
+  double ybytes = 0;
+  for (int l = 2; l <= c.H - 1; ++l) {
+    const double h = (double)(1LL << (l - 1));
+    ybytes += (double)c.R * ych * std::max(h, (double)TILE_X) * std::max(h, (double)TILE_Y) *
+              std::max(h, (double)TILE_Z) * 16 * 2 * 2;
+  }
+  if (ybytes > 12e9) {
+    use = false;
+    return B200FMM_OK;
+  }
+  // pre-scales by powers of two.  The largest entries of A (level_scale_kernel), V and U lie in [2^13, 2^14),
+  // so that the lo parts of the FP16 splits stay normal numbers (smaller scales put them among the FP16
+  // subnormals and cost about 20x in accuracy); Y = V^T A, produced in FP32, is scaled by 2^-sY before its
+  // own split so that |Y| < 2^15 (column sums of V times 2^14 bound it).
+  double vmax = 0, colsum = 0, umax = 0;
+  for (int s = 0; s < 343; ++s) {
+    if (toff[s] < 0) continue;
+    const int r = trank[s];
+    for (int a = 0; a < r; ++a) {
+      double cs = 0;
+      for (int n = 0; n < nn; ++n) {
+        const double v = std::fabs(Vt[toff[s] + (size_t)n * r + a]);
+        cs += v;
+        vmax = std::max(vmax, v);
+      }
+      colsum = std::max(colsum, cs);
+    }
+    for (long long i = 0; i < (long long)nn * r; ++i) umax = std::max(umax, std::fabs(Ut[toff[s] + i]));
+  }
+  int ev = 0, eu = 0, eb = 0;
+  std::frexp(vmax, &ev);
+  std::frexp(umax, &eu);
+  const int sV = 14 - ev, sU = 14 - eu;
+  std::frexp(std::ldexp(colsum, sV + 14), &eb);
+  const int sY = eb - 15;
+  t.lr_shift = sV + sU - sY;
+  auto split = [](double v, __half &h, __half &l) {
+    h = __double2half(v);
+    l = __double2half(v - (double)__half2float(h));
+  };
+  // U chunks
+  std::vector<__half> uh((size_t)uch * t.NP * 16), ul(uh.size());
+  for (int s = 0; s < 343; ++s) {
+    if (toff[s] < 0) continue;
+    const int r = trank[s];
+    for (int kc = 0; kc < P.tnk[s]; ++kc)
+      for (int n = 0; n < t.NP; ++n)
+        for (int i = 0; i < 16; ++i) {
+          const int a = kc * 16 + i;
+          const double v = (n < nn && a < r) ? std::ldexp(Ut[toff[s] + (size_t)n * r + a], sU) : 0.0;
+          const size_t o = ((size_t)(P.uchunk0[s] + kc) * t.NP + n) * 16 + i;
+          split(v, uh[o], ul[o]);
+        }
+  }
+  // V rows: row (ybase[sp] + ychunk0[sp][s] + kc) * 16 + i holds column kc * 16 + i of V_s along K
+  std::vector<__half> vh((size_t)ych * 16 * t.KP), vl(vh.size());
+  for (int sp = 0; sp < 8; ++sp)
+    for (int s = 0; s < 343; ++s) {
+      if (!need[sp][s]) continue;
+      const int r = trank[s];
+      for (int kc = 0; kc < P.tnk[s]; ++kc)
+        for (int i = 0; i < 16; ++i) {
+          const int a = kc * 16 + i;
+          const size_t row = (size_t)(P.ybase[sp] + P.ychunk0[sp][s] + kc) * 16 + i;
+          for (int n = 0; n < t.KP; ++n) {
+            const double v = (n < nn && a < r) ? std::ldexp(Vt[toff[s] + (size_t)n * r + a], sV) : 0.0;
+            split(v, vh[row * t.KP + n], vl[row * t.KP + n]);
+          }
+        }
+    }
+  B200_CUDA(cudaMalloc(&t.Bhi, uh.size() * sizeof(__half)));
+  B200_CUDA(cudaMalloc(&t.Blo, ul.size() * sizeof(__half)));
+  B200_CUDA(cudaMalloc(&t.Vhi, vh.size() * sizeof(__half)));
+  B200_CUDA(cudaMalloc(&t.Vlo, vl.size() * sizeof(__half)));
+  B200_CUDA(cudaMemcpy(t.Bhi, uh.data(), uh.size() * sizeof(__half), cudaMemcpyHostToDevice));
+  B200_CUDA(cudaMemcpy(t.Blo, ul.data(), ul.size() * sizeof(__half), cudaMemcpyHostToDevice));
+  B200_CUDA(cudaMemcpy(t.Vhi, vh.data(), vh.size() * sizeof(__half), cudaMemcpyHostToDevice));
+  B200_CUDA(cudaMemcpy(t.Vlo, vl.data(), vl.size() * sizeof(__half), cudaMemcpyHostToDevice));
+  {
+    cuuint64_t dims[3] = {16, (cuuint64_t)t.NP, (cuuint64_t)uch};
+    cuuint64_t strides[2] = {32, (cuuint64_t)32 * t.NP};
+    cuuint32_t box[3] = {16, (cuuint32_t)(t.pair ? t.NH / 2 : t.NH), 1};
+    B200_CHECK(encode(&P.mapB_hi, t.Bhi, 3, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_32B));
+    B200_CHECK(encode(&P.mapB_lo, t.Blo, 3, dims, strides, box, CU_TENSOR_MAP_SWIZZLE_32B));
+  }
+  t.yparams = new LrYParams();
+  std::memset(t.yparams, 0, sizeof(LrYParams));
+  LrYParams &Y = *t.yparams;
+  {
+    cuuint64_t dims[2] = {(cuuint64_t)t.KP, (cuuint64_t)ych * 16};
+    cuuint64_t strides[1] = {(cuuint64_t)t.KP * 2};
+    cuuint32_t box[2] = {KCHUNK, YBLK};
+    B200_CHECK(encode(&Y.mapV_hi, t.Vhi, 2, dims, strides, box));
+    B200_CHECK(encode(&Y.mapV_lo, t.Vlo, 2, dims, strides, box));
+  }
+  for (int sp = 0; sp <= 8; ++sp) Y.ybase[sp] = sp < 8 ? P.ybase[sp] : ych;
+  Y.ycht = ych;
+  Y.nblk = t.nblk;
+  Y.NK = t.NK;
+  Y.R = c.R;
+  Y.yscale = (float)std::ldexp(1.0, -sY);
+  // first product: segments of 2 K chunks (12 MMAs); second product: segments of 4 chunks (12 MMAs)
+  Y.segc = 2;
+  if (const char *e = getenv("B200FMM_TC_LR_YSEG")) Y.segc = std::max(1, atoi(e));
+  t.ystage_bytes = 2 * (TILE_X * TILE_Y * TILE_Z * KCHUNK * 2) + 2 * YBLK * KCHUNK * 2;
+  t.ystages = std::min(MAX_STAGES, (220 * 1024) / t.ystage_bytes);
+  Y.stages = t.ystages;
+  Y.stage_bytes = t.ystage_bytes;
+  Y.status = c.d_status;
+  // segments of the second product's chunk stream: as many 16-wide K steps as a dense segment has
+  P.lr_seglen = 4;
+  if (const char *e = getenv("B200FMM_TC_LR_SEGLEN")) P.lr_seglen = std::max(1, atoi(e));
+  use = true;
+  return B200FMM_OK;
+}
+
 b200fmm_status tc_init(Context &c) {
-  B200_CHECK(build_dense_operators(c));  // FP64 K on the device
   DenseTC *t = new DenseTC();
   c.tc = t;
   const int nn = c.nn;
@@ -966,33 +1450,45 @@ b200fmm_status tc_init(Context &c) {
   // of 61.4 KB per stage), while single CTAs are a few percent faster at orders <= 6
   t->pair = t->NHALF == 2;
   if (const char *e = getenv("B200FMM_TC_PAIR")) t->pair = atoi(e) != 0;
+  t->params = new TcParams();
+  std::memset(t->params, 0, sizeof(TcParams));
+  std::memcpy(t->params->off, c.itab.off, sizeof(t->params->off));
+  std::memcpy(t->params->slot, c.itab.slot, sizeof(t->params->slot));
+  // symmetric Chebyshev operators run in their compressed (low-rank) form; B200FMM_TC_LOWRANK=0 keeps the
+  // dense operators
+  bool lr = c.cfg.kernel == B200FMM_CHEB_SYM && !c.sym_ranks.empty();
+  if (const char *e = getenv("B200FMM_TC_LOWRANK")) lr = lr && atoi(e) != 0;
+  if (lr) B200_CHECK(tc_init_lowrank(c, *t, *t->params, lr));
+  t->lr = lr;
+  const int rowb = lr ? 32 : 64;  // bytes per operand row of a stage: 16 or 32 fp16 of K
   // a CTA of a pair holds NP / 2 rows of each operator chunk: NH / 2 rows of each column half
   const int b_rows = t->pair ? t->NP / 2 : t->NP;
-  t->stage_bytes = 2 * (TILE_X * TILE_Y * TILE_Z * KCHUNK * 2) + 2 * b_rows * KCHUNK * 2;
-  t->stages = std::min(t->pair ? MAX_STAGES : MAX_STAGES_SINGLE, (220 * 1024) / t->stage_bytes);
+  t->stage_bytes = 2 * (TILE_X * TILE_Y * TILE_Z * rowb) + 2 * b_rows * rowb;
+  t->stages = std::min((t->pair || lr) ? MAX_STAGES : MAX_STAGES_SINGLE, (220 * 1024) / t->stage_bytes);
   if (t->stages < 2) return fail(B200FMM_ERR_UNSUPPORTED, "stage buffers do not fit in shared memory");
   t->nbuf = 2 * t->NP <= 512 ? 2 : 1;
   t->ncols = 32;
   while (t->ncols < t->nbuf * t->NP) t->ncols *= 2;
-  const size_t bsz = (size_t)343 * t->NP * t->KP;
-  B200_CUDA(cudaMalloc(&t->Bhi, bsz * sizeof(__half)));
-  B200_CUDA(cudaMalloc(&t->Blo, bsz * sizeof(__half)));
-  pack_operators<<<dim3(grid_for((long long)t->NP * t->KP, 256), 343), 256>>>(nn, t->KP, t->NP, c.d_dense, t->Bhi,
-                                                                            t->Blo);
-  B200_CUDA(cudaGetLastError());
-  B200_CUDA(cudaDeviceSynchronize());
-  // the FP64 dense operators are not needed by the mixed path after packing
-  cudaFree(c.d_dense);
-  c.d_dense = nullptr;
+  if (!lr) {
+    B200_CHECK(build_dense_operators(c));  // FP64 K on the device
+    const size_t bsz = (size_t)343 * t->NP * t->KP;
+    B200_CUDA(cudaMalloc(&t->Bhi, bsz * sizeof(__half)));
+    B200_CUDA(cudaMalloc(&t->Blo, bsz * sizeof(__half)));
+    pack_operators<<<dim3(grid_for((long long)t->NP * t->KP, 256), 343), 256>>>(nn, t->KP, t->NP, c.d_dense, t->Bhi,
+                                                                              t->Blo);
+    B200_CUDA(cudaGetLastError());
+    B200_CUDA(cudaDeviceSynchronize());
+    // the FP64 dense operators are not needed by the mixed path after packing
+    cudaFree(c.d_dense);
+    c.d_dense = nullptr;
+    cuuint64_t dims[3] = {(cuuint64_t)t->KP, (cuuint64_t)t->NP, 343};
+    cuuint64_t strides[2] = {(cuuint64_t)t->KP * 2, (cuuint64_t)t->KP * 2 * t->NP};
+    cuuint32_t box[3] = {KCHUNK, (cuuint32_t)(t->pair ? t->NH / 2 : t->NH), 1};
+    B200_CHECK(encode(&t->params->mapB_hi, t->Bhi, 3, dims, strides, box));
+    B200_CHECK(encode(&t->params->mapB_lo, t->Blo, 3, dims, strides, box));
+  }
   B200_CUDA(cudaMalloc(&t->scal, sizeof(double) * kMaxHeight * 2));
   B200_CUDA(cudaMalloc(&t->amax, sizeof(unsigned long long) * kMaxHeight));
-  t->params = new TcParams();
-  std::memset(t->params, 0, sizeof(TcParams));
-  cuuint64_t dims[3] = {(cuuint64_t)t->KP, (cuuint64_t)t->NP, 343};
-  cuuint64_t strides[2] = {(cuuint64_t)t->KP * 2, (cuuint64_t)t->KP * 2 * t->NP};
-  cuuint32_t box[3] = {KCHUNK, (cuuint32_t)(t->pair ? t->NH / 2 : t->NH), 1};
-  B200_CHECK(encode(&t->params->mapB_hi, t->Bhi, 3, dims, strides, box));
-  B200_CHECK(encode(&t->params->mapB_lo, t->Blo, 3, dims, strides, box));
   int dev_sms = 148;
   cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c.device);
   t->grid = dev_sms;
@@ -1012,11 +1508,17 @@ b200fmm_status tc_init(Context &c) {
     cfg.numAttrs = 1;
     int nclusters = 0;
     cudaError_t err = cudaSuccess;
+    auto occ = [&](auto kern) {
+      err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (err == cudaSuccess) err = cudaOccupancyMaxActiveClusters(&nclusters, kern, &cfg);
+    };
     switch (t->NP) {
-#define B200_TC_OCC(NPV, CWV, NHV)                                                                               \
-  case NPV:                                                                                                        \
-    err = cudaFuncSetAttribute(m2l_tc_kernel<CWV, NHV, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
-    if (err == cudaSuccess) err = cudaOccupancyMaxActiveClusters(&nclusters, m2l_tc_kernel<CWV, NHV, true>, &cfg);      \
+#define B200_TC_OCC(NPV, CWV, NHV)                 \
+  case NPV:                                        \
+    if (lr)                                        \
+      occ(m2l_tc_kernel<CWV, NHV, true, true>);    \
+    else                                           \
+      occ(m2l_tc_kernel<CWV, NHV, true, false>);   \
     break;
       B200_TC_OCC(32, 16, 1)
       B200_TC_OCC(64, 32, 1)
@@ -1034,20 +1536,28 @@ b200fmm_status tc_init(Context &c) {
     }
     t->grid = 2 * std::min(nclusters, dev_sms / 2);
   }
+  if (lr) {
+    B200_CUDA(cudaFuncSetAttribute(lr_y_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   t->ystages * t->ystage_bytes + 1024));
+  }
   return B200FMM_OK;
 }
 
 void tc_free(Context &c) {
   DenseTC *t = c.tc;
   if (!t) return;
-  for (void *p : {(void *)t->Bhi, (void *)t->Blo, (void *)t->scal, (void *)t->amax, (void *)t->prefix, (void *)t->busy})
+  for (void *p : {(void *)t->Bhi, (void *)t->Blo, (void *)t->scal, (void *)t->amax, (void *)t->prefix, (void *)t->busy,
+                  (void *)t->Vhi, (void *)t->Vlo})
     if (p) cudaFree(p);
   for (int l = 0; l < kMaxHeight; ++l) {
     if (t->Ahi[l]) cudaFree(t->Ahi[l]);
     if (t->Alo[l]) cudaFree(t->Alo[l]);
+    if (t->Yhi[l]) cudaFree(t->Yhi[l]);
+    if (t->Ylo[l]) cudaFree(t->Ylo[l]);
   }
   if (t->sat) cudaFree(t->sat);
   delete t->params;
+  delete t->yparams;
   delete t;
   c.tc = nullptr;
 }
@@ -1078,8 +1588,36 @@ static b200fmm_status tc_prepare(Context &c) {
                         (cuuint64_t)t->KP * 2 * t->HX[l] * t->HY[l],
                         (cuuint64_t)t->KP * 2 * t->HX[l] * t->HY[l] * t->HZ[l]};
     cuuint32_t box[5] = {KCHUNK, TILE_X, TILE_Y, TILE_Z, 1};
-    B200_CHECK(encode(&P.mapA_hi[l], t->Ahi[l], 5, dims, st, box));
-    B200_CHECK(encode(&P.mapA_lo[l], t->Alo[l], 5, dims, st, box));
+    if (t->lr) {
+      // the multipoles feed the first product; the second product's A is Y
+      LrYParams &Y = *t->yparams;
+      B200_CHECK(encode(&Y.mapA_hi[l], t->Ahi[l], 5, dims, st, box));
+      B200_CHECK(encode(&Y.mapA_lo[l], t->Alo[l], 5, dims, st, box));
+      const size_t yel = (size_t)c.R * t->ycht * t->HZ[l] * t->HY[l] * t->HX[l] * 16;
+      if (t->Ybytes[l] != yel * sizeof(__half)) {
+        if (t->Yhi[l]) cudaFree(t->Yhi[l]);
+        if (t->Ylo[l]) cudaFree(t->Ylo[l]);
+        t->Yhi[l] = t->Ylo[l] = nullptr;
+        B200_CUDA(cudaMalloc(&t->Yhi[l], yel * sizeof(__half)));
+        B200_CUDA(cudaMalloc(&t->Ylo[l], yel * sizeof(__half)));
+        t->Ybytes[l] = yel * sizeof(__half);
+      }
+      Y.Yhi[l] = t->Yhi[l];
+      Y.Ylo[l] = t->Ylo[l];
+      Y.HX[l] = t->HX[l];
+      Y.HY[l] = t->HY[l];
+      Y.HZ[l] = t->HZ[l];
+      cuuint64_t ydims[5] = {16, (cuuint64_t)t->HX[l], (cuuint64_t)t->HY[l], (cuuint64_t)t->HZ[l],
+                             (cuuint64_t)c.R * t->ycht};
+      cuuint64_t yst[4] = {32, (cuuint64_t)32 * t->HX[l], (cuuint64_t)32 * t->HX[l] * t->HY[l],
+                           (cuuint64_t)32 * t->HX[l] * t->HY[l] * t->HZ[l]};
+      cuuint32_t ybox[5] = {16, TILE_X, TILE_Y, TILE_Z, 1};
+      B200_CHECK(encode(&P.mapA_hi[l], t->Yhi[l], 5, ydims, yst, ybox, CU_TENSOR_MAP_SWIZZLE_32B));
+      B200_CHECK(encode(&P.mapA_lo[l], t->Ylo[l], 5, ydims, yst, ybox, CU_TENSOR_MAP_SWIZZLE_32B));
+    } else {
+      B200_CHECK(encode(&P.mapA_hi[l], t->Ahi[l], 5, dims, st, box));
+      B200_CHECK(encode(&P.mapA_lo[l], t->Alo[l], 5, dims, st, box));
+    }
     P.lv[l].HX = t->HX[l];
     P.lv[l].HY = t->HY[l];
     P.lv[l].HZ = t->HZ[l];
@@ -1103,6 +1641,16 @@ static b200fmm_status tc_prepare(Context &c) {
     nunits += P.lv[l].nunits;
   }
   t->nunits_all = nunits;
+  if (t->lr) {
+    // first-product items, finest level first: rhs, parity, tile, 256-row block
+    LrYParams &Y = *t->yparams;
+    int n = 0;
+    for (int l = LL; l >= 2; --l) {
+      Y.item0[l] = n;
+      Y.nitems[l] = c.R * 8 * (t->HZ[l] / TILE_Z) * (t->HY[l] / TILE_Y) * (t->HX[l] / TILE_X) * t->nblk;
+      n += Y.nitems[l];
+    }
+  }
   int ns = t->splits > 0 ? t->splits : 1;  // work ranges per CTA (pair), chosen by b200fmm_autotune
   if (const char *e = getenv("B200FMM_TC_SPLITS")) ns = std::max(1, std::min(64, atoi(e)));
   t->splits_used = ns;
@@ -1196,7 +1744,7 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
     const long long cnt = Lv.n * c.R * c.nn;
     absmax_kernel<<<std::min<long long>(1024, grid_for(cnt, 256)), 256, 0, c.stream>>>(cnt, Lv.M, t->amax + l);
     level_scale_kernel<<<1, 1, 0, c.stream>>>(t->amax + l, 2.0 / (c.cfg.box_width / (double)(1LL << l)),
-                                              t->scal + 2 * l, t->scal + 2 * l + 1);
+                                              t->lr ? t->lr_shift : SB, t->scal + 2 * l, t->scal + 2 * l + 1);
     pack_multipoles<<<(unsigned)Lv.n, 128, 0, c.stream>>>(Lv.n, c.R, c.nn, t->KP, t->HX[l], t->HY[l], t->HZ[l],
                                                           Lv.keys, Lv.M, t->scal + 2 * l, t->Ahi[l], t->Alo[l]);
     c.launches += 3;
@@ -1223,18 +1771,30 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
   cfg.attrs = at;
   cfg.numAttrs = t->pair ? 1 : 0;
   B200_CUDA(record_event(c, 8));
+  if (t->lr) {
+    // first product: Y = V^T M for every source cell of levels [l0, l1]
+    LrYParams &Y = *t->yparams;
+    Y.l0 = l0;
+    Y.l1 = l1;
+    const int ny = Y.item0[l0] + Y.nitems[l0] - Y.item0[l1];
+    if (ny > 0) {
+      lr_y_kernel<<<std::min(t->grid, ny), TC_THREADS, (size_t)t->ystages * t->ystage_bytes + 1024, c.stream>>>(Y);
+      ++c.launches;
+    }
+  }
+  auto launch = [&](auto kern) -> cudaError_t {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    return cudaLaunchKernelEx(&cfg, kern, P);
+  };
   switch (t->NP) {
-#define B200_TC_CASE(NPV, CWV, NHV)                                                                                 \
-  case NPV:                                                                                                           \
-    if (t->pair) {                                                                                                    \
-      B200_CUDA(cudaFuncSetAttribute(m2l_tc_kernel<CWV, NHV, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,      \
-                                     (int)smem));                                                                     \
-      B200_CUDA(cudaLaunchKernelEx(&cfg, m2l_tc_kernel<CWV, NHV, true>, P));                                          \
-    } else {                                                                                                          \
-      B200_CUDA(cudaFuncSetAttribute(m2l_tc_kernel<CWV, NHV, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
-                                     (int)smem));                                                                     \
-      B200_CUDA(cudaLaunchKernelEx(&cfg, m2l_tc_kernel<CWV, NHV, false>, P));                                         \
-    }                                                                                                                 \
+#define B200_TC_CASE(NPV, CWV, NHV)                                                                \
+  case NPV:                                                                                          \
+    if (t->pair)                                                                                     \
+      B200_CUDA(t->lr ? launch(m2l_tc_kernel<CWV, NHV, true, true>) : launch(m2l_tc_kernel<CWV, NHV, true, false>)); \
+    else                                                                                             \
+      B200_CUDA(t->lr ? launch(m2l_tc_kernel<CWV, NHV, false, true>)                                 \
+                      : launch(m2l_tc_kernel<CWV, NHV, false, false>));                              \
     break;
     B200_TC_CASE(32, 16, 1)
     B200_TC_CASE(64, 32, 1)
@@ -1262,5 +1822,14 @@ void tc_set_splits(Context &c, int splits) {
   c.tc->built_for_gen = -1;  // the item list is rebuilt by the next run
 }
 int tc_splits_used(const Context &c) { return c.tc ? c.tc->splits_used : 0; }
+
+// Low-rank form in use: the rank of every slot and, per source parity, the sum of the ranks of the slots
+// that the parity's cells feed.
+bool tc_lowrank_info(const Context &c, int *rank_of_slot, double *rank_fed) {
+  if (!c.tc || !c.tc->lr) return false;
+  std::memcpy(rank_of_slot, c.tc->lr_rank, sizeof(int) * 343);
+  std::memcpy(rank_fed, c.tc->lr_rank_fed, sizeof(double) * 8);
+  return true;
+}
 
 }  // namespace b200

@@ -403,6 +403,65 @@ b200fmm_status compress_sym_operators(Context &c) {
   return B200FMM_OK;
 }
 
+// the class slot and node permutation of every slot (sym_tables), for the other files of the library
+void slot_symmetry_tables(int p, std::vector<int> &pind, std::vector<int> &pvec) { sym_tables(p, pind, pvec); }
+
+// Per-slot permuted factors on the host: Ut[t][n][a] = U_c[pvec_t[n]][a], Vt[t][m][a] = V_c[pvec_t[m]][a]
+// (row-major p^3 x r, r = rank of the slot's class), at toff[t] for every far slot t (-1 for near slots).
+b200fmm_status sym_slot_factors(const Context &c, std::vector<double> &Ut, std::vector<double> &Vt,
+                                std::vector<long long> &toff, std::vector<int> &trank) {
+  const int nn = c.nn;
+  std::vector<int> pind, pvec;
+  sym_tables(c.p, pind, pvec);
+  std::vector<long long> off(343, -1);
+  std::vector<int> rk(343, 0);
+  long long o = 0, used = 0;
+  for (int t = 0; t < 343; ++t)
+    if (c.sym_ranks[t] > 0) {
+      off[t] = o;
+      rk[t] = c.sym_ranks[t];
+      o += (long long)rk[t] * nn;
+    }
+  // every far slot must map to a class slot that has an operator
+  for (int t = 0; t < 343; ++t) {
+    const int i = t / 49 - 3, j = (t / 7) % 7 - 3, k = t % 7 - 3;
+    if ((std::abs(i) > 1 || std::abs(j) > 1 || std::abs(k) > 1) && rk[pind[t]] == 0)
+      return fail(B200FMM_ERR_INVALID, "symmetric operators: a class slot has rank 0");
+  }
+  std::vector<double> U(o), V(o);
+  for (int t = 0; t < 343; ++t)
+    if (rk[t] > 0) {
+      const double *src = c.sym_uv.data() + used;
+      std::memcpy(U.data() + off[t], src, sizeof(double) * rk[t] * nn);
+      std::memcpy(V.data() + off[t], src + (size_t)rk[t] * nn, sizeof(double) * rk[t] * nn);
+      used += 2LL * rk[t] * nn;
+    }
+  toff.assign(343, -1);
+  trank.assign(343, 0);
+  long long tot = 0;
+  for (int t = 0; t < 343; ++t) {
+    const int i = t / 49 - 3, j = (t / 7) % 7 - 3, k = t % 7 - 3;
+    if (!(std::abs(i) > 1 || std::abs(j) > 1 || std::abs(k) > 1)) continue;
+    toff[t] = tot;
+    trank[t] = rk[pind[t]];
+    tot += (long long)trank[t] * nn;
+  }
+  Ut.assign(tot, 0.0);
+  Vt.assign(tot, 0.0);
+  for (int t = 0; t < 343; ++t) {
+    if (toff[t] < 0) continue;
+    const int cls = pind[t], r = trank[t];
+    const double *Uc = U.data() + off[cls], *Vc = V.data() + off[cls];  // [a][j] = U_c[j][a]
+    const int *pv = pvec.data() + (size_t)t * nn;
+    for (int n = 0; n < nn; ++n)
+      for (int a = 0; a < r; ++a) {
+        Ut[toff[t] + (size_t)n * r + a] = Uc[(size_t)a * nn + pv[n]];
+        Vt[toff[t] + (size_t)n * r + a] = Vc[(size_t)a * nn + pv[n]];
+      }
+  }
+  return B200FMM_OK;
+}
+
 b200fmm_status upload_sym_operators(Context &c) {
   const int nn = c.nn;
   std::vector<int> pind, pvec;
@@ -437,28 +496,11 @@ b200fmm_status upload_sym_operators(Context &c) {
     if (p) cudaFree(p);
   // per-slot permuted factors (FChebSymKernel::M2L applies the permutation around the class operator;
   // folding it into the factors once gives plain per-slot operators)
-  std::vector<long long> toff(343, -1);
-  std::vector<int> trank(343, 0);
-  long long tot = 0;
-  for (int t = 0; t < 343; ++t) {
-    const int i = t / 49 - 3, j = (t / 7) % 7 - 3, k = t % 7 - 3;
-    if (!(std::abs(i) > 1 || std::abs(j) > 1 || std::abs(k) > 1)) continue;
-    toff[t] = tot;
-    trank[t] = rk[pind[t]];
-    tot += (long long)trank[t] * nn;
-  }
-  std::vector<double> Ut(tot), Vt(tot);
-  for (int t = 0; t < 343; ++t) {
-    if (toff[t] < 0) continue;
-    const int cls = pind[t], r = trank[t];
-    const double *Uc = U.data() + off[cls], *Vc = V.data() + off[cls];  // [a][j] = U_c[j][a]
-    const int *pv = pvec.data() + (size_t)t * nn;
-    for (int n = 0; n < nn; ++n)
-      for (int a = 0; a < r; ++a) {
-        Ut[toff[t] + (size_t)n * r + a] = Uc[(size_t)a * nn + pv[n]];
-        Vt[toff[t] + (size_t)n * r + a] = Vc[(size_t)a * nn + pv[n]];
-      }
-  }
+  std::vector<long long> toff;
+  std::vector<int> trank;
+  std::vector<double> Ut, Vt;
+  B200_CHECK(sym_slot_factors(c, Ut, Vt, toff, trank));
+  const long long tot = (long long)Ut.size();
   B200_CUDA(cudaMalloc(&c.d_Ut, sizeof(double) * std::max<long long>(tot, 1)));
   B200_CUDA(cudaMalloc(&c.d_Vt, sizeof(double) * std::max<long long>(tot, 1)));
   B200_CUDA(cudaMalloc(&c.d_toff, sizeof(long long) * 343));
