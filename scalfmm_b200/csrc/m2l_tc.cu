@@ -999,11 +999,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
         unsigned hv[8], lv[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-          const float v0 = acc[k * 16 + 2 * i] * P.yscale, v1 = acc[k * 16 + 2 * i + 1] * P.yscale;
-          const __half h0 = __float2half_rn(v0), h1 = __float2half_rn(v1);
-          const __half l0 = __float2half_rn(v0 - __half2float(h0)), l1 = __float2half_rn(v1 - __half2float(h1));
-          hv[i] = (unsigned)__half_as_ushort(h0) | ((unsigned)__half_as_ushort(h1) << 16);
-          lv[i] = (unsigned)__half_as_ushort(l0) | ((unsigned)__half_as_ushort(l1) << 16);
+          // two values per packed conversion: hi = fp16(v), lo = fp16(v - hi)
+          const float2 v = make_float2(acc[k * 16 + 2 * i] * P.yscale, acc[k * 16 + 2 * i + 1] * P.yscale);
+          const __half2 h = __float22half2_rn(v);
+          const float2 hf = __half22float2(h);
+          const __half2 l = __float22half2_rn(make_float2(v.x - hf.x, v.y - hf.y));
+          hv[i] = *reinterpret_cast<const unsigned *>(&h);
+          lv[i] = *reinterpret_cast<const unsigned *>(&l);
         }
         uint4 *dh = (uint4 *)(P.Yhi[l] + off), *dl = (uint4 *)(P.Ylo[l] + off);
         dh[0] = make_uint4(hv[0], hv[1], hv[2], hv[3]);
@@ -1150,45 +1152,73 @@ __global__ void __launch_bounds__(1024) unit_scan_kernel(int n, int *__restrict_
   if (t == 1023) prefix[n] = part[1023];
 }
 
-// max |M| of a level -> bit pattern (non-negative doubles order like their bit patterns)
-__global__ void absmax_kernel(long long n, const double *__restrict__ v, unsigned long long *__restrict__ out) {
+// The multipoles of levels [l0, l1], for the three packing launches of one M2L pass.
+struct PackLevels {
+  int l0, l1;
+  const double *M[kMaxHeight];
+  long long nval[kMaxHeight];           // multipole values of the level (cells * R * p^3)
+  long long pos0[kMaxHeight + 1];       // first grid position of each level (rhs, parity, z, y, x)
+  int HX[kMaxHeight], HY[kMaxHeight], HZ[kMaxHeight], side[kMaxHeight];
+  const int *grid[kMaxHeight];          // dense cell grid of the level: cell index or -1
+  __half *hi[kMaxHeight], *lo[kMaxHeight];
+  double scale_l[kMaxHeight];           // 2 / cell width
+};
+
+// max |M| of every level (blockIdx.y = level - l0)
+__global__ void absmax_levels_kernel(const __grid_constant__ PackLevels L, unsigned long long *__restrict__ amax) {
+  const int l = L.l0 + blockIdx.y;
+  const double *v = L.M[l];
   double m = 0.0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < L.nval[l]; i += (long long)gridDim.x * blockDim.x)
     m = fmax(m, fabs(v[i]));
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+  if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(amax + l, (unsigned long long)__double_as_longlong(m));
 }
 
-// 2^sA with sA chosen so that max|M| * 2^sA ~ 2^14, and the epilogue factor scale_l * 2^-(sA + SB)
-// shift: the operators' own pre-scale exponent (SB for the dense K, sV + sU for the low-rank factors)
-__global__ void level_scale_kernel(const unsigned long long *__restrict__ amax, double scale_l, int shift,
-                                   double *__restrict__ pre, double *__restrict__ post) {
-  const double m = __longlong_as_double((long long)*amax);
+// every grid position of levels [l0, l1]: the scaled multipole of its cell, split into FP16 hi + lo, or
+// zeros where there is no cell (and in the K padding), so that the buffers need no clearing
+__global__ void pack_levels_kernel(const __grid_constant__ PackLevels L, int R, int nn, int KP,
+                                   const double *__restrict__ scal) {
+  const long long p = blockIdx.x + L.pos0[L.l0];
+  int l = L.l0;
+  while (l < L.l1 && p >= L.pos0[l + 1]) ++l;
+  long long r = p - L.pos0[l];
+  const long long base = r * KP;
+  const int hx = (int)(r % L.HX[l]);
+  r /= L.HX[l];
+  const int hy = (int)(r % L.HY[l]);
+  r /= L.HY[l];
+  const int hz = (int)(r % L.HZ[l]);
+  const int r8 = (int)(r / L.HZ[l]);
+  const int par = r8 & 7, rhs = r8 >> 3;
+  const int gx = 2 * hx + ((par >> 2) & 1), gy = 2 * hy + ((par >> 1) & 1), gz = 2 * hz + (par & 1);
+  const int side = L.side[l];
+  int cell = -1;
+  if (gx < side && gy < side && gz < side) cell = L.grid[l][((long long)gz * side + gy) * side + gx];
+  const double s = scal[2 * l];
+  const double *m = cell >= 0 ? L.M[l] + ((long long)cell * R + rhs) * nn : nullptr;
+  for (int n = threadIdx.x; n < KP; n += blockDim.x) {
+    const double a = (m && n < nn) ? m[n] * s : 0.0;
+    const __half h = __double2half(a);
+    L.hi[l][base + n] = h;
+    L.lo[l][base + n] = __double2half(a - (double)__half2float(h));
+  }
+}
+
+// 2^sA with sA chosen so that max|M| * 2^sA ~ 2^14, and the epilogue factor scale_l * 2^-(sA + shift)
+// with shift the operators' own pre-scale exponent (SB for the dense K, sV + sU - sY for the low-rank
+// factors).  One thread per level of [l0, l1].
+__global__ void level_scale_kernel(const __grid_constant__ PackLevels L, const unsigned long long *__restrict__ amax,
+                                   int shift, double *__restrict__ scal) {
+  const int l = L.l0 + (int)threadIdx.x;
+  if (l > L.l1) return;
+  const double m = __longlong_as_double((long long)amax[l]);
   int e = 0;
   if (m > 0) frexp(m, &e);  // m = f * 2^e, f in [0.5, 1)
   const int sA = 14 - e;
-  *pre = ldexp(1.0, sA);
-  *post = scale_l * ldexp(1.0, -(sA + shift));
-}
-
-__global__ void pack_multipoles(long long ncells, int R, int nn, int KP, int HX, int HY, int HZ,
-                                const long long *__restrict__ keys, const double *__restrict__ M,
-                                const double *__restrict__ pre, __half *__restrict__ hi, __half *__restrict__ lo) {
-  const long long cell = blockIdx.x;
-  int ix, iy, iz;
-  morton_decode3(keys[cell], ix, iy, iz);
-  const int c = ((ix & 1) << 2) | ((iy & 1) << 1) | (iz & 1);
-  const double s = *pre;
-  for (int r = 0; r < R; ++r) {
-    const long long base = ((((long long)(r * 8 + c) * HZ + (iz >> 1)) * HY + (iy >> 1)) * HX + (ix >> 1)) * KP;
-    for (int n = threadIdx.x; n < nn; n += blockDim.x) {
-      const double a = M[(cell * R + r) * nn + n] * s;
-      const __half h = __double2half(a);
-      hi[base + n] = h;
-      lo[base + n] = __double2half(a - (double)__half2float(h));
-    }
-  }
+  scal[2 * l] = ldexp(1.0, sA);
+  scal[2 * l + 1] = L.scale_l[l] * ldexp(1.0, -(sA + shift));
 }
 
 // operators: K[t][n][m] (FP64, source node n, target node m) -> B[t][m][n] split fp16, scaled by 2^SB
@@ -1420,8 +1450,9 @@ static b200fmm_status tc_init_lowrank(Context &c, DenseTC &t, TcParams &P, bool 
   Y.NK = t.NK;
   Y.R = c.R;
   Y.yscale = (float)std::ldexp(1.0, -sY);
-  // first product: segments of 2 K chunks (12 MMAs); second product: segments of 4 chunks (12 MMAs)
-  Y.segc = 2;
+  // first product: segments of 3 K chunks (18 MMAs); second product: segments of 6 chunks (18 MMAs).  At
+  // order 7 this keeps the M2L within 5e-7 of FP64 (longer segments: 6-9e-7 for 4-10 % less time)
+  Y.segc = 3;
   if (const char *e = getenv("B200FMM_TC_LR_YSEG")) Y.segc = std::max(1, atoi(e));
   t.ystage_bytes = 2 * (TILE_X * TILE_Y * TILE_Z * KCHUNK * 2) + 2 * YBLK * KCHUNK * 2;
   t.ystages = std::min(MAX_STAGES, (220 * 1024) / t.ystage_bytes);
@@ -1429,7 +1460,7 @@ static b200fmm_status tc_init_lowrank(Context &c, DenseTC &t, TcParams &P, bool 
   Y.stage_bytes = t.ystage_bytes;
   Y.status = c.d_status;
   // segments of the second product's chunk stream: as many 16-wide K steps as a dense segment has
-  P.lr_seglen = 4;
+  P.lr_seglen = 6;
   if (const char *e = getenv("B200FMM_TC_LR_SEGLEN")) P.lr_seglen = std::max(1, atoi(e));
   use = true;
   return B200FMM_OK;
@@ -1735,18 +1766,33 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
     t->sat_serial = c.tree_serial;
   }
   const int l0 = level == -1 ? 2 : level, l1 = level == -1 ? LL : level;
-  for (int l = l0; l <= l1; ++l) {
-    const Level &Lv = c.lv[l];
-    B200_CUDA(cudaMemsetAsync(t->amax + l, 0, sizeof(unsigned long long), c.stream));
-    B200_CUDA(cudaMemsetAsync(t->Ahi[l], 0, t->Abytes[l], c.stream));
-    B200_CUDA(cudaMemsetAsync(t->Alo[l], 0, t->Abytes[l], c.stream));
-    if (Lv.n == 0) continue;
-    const long long cnt = Lv.n * c.R * c.nn;
-    absmax_kernel<<<std::min<long long>(1024, grid_for(cnt, 256)), 256, 0, c.stream>>>(cnt, Lv.M, t->amax + l);
-    level_scale_kernel<<<1, 1, 0, c.stream>>>(t->amax + l, 2.0 / (c.cfg.box_width / (double)(1LL << l)),
-                                              t->lr ? t->lr_shift : SB, t->scal + 2 * l, t->scal + 2 * l + 1);
-    pack_multipoles<<<(unsigned)Lv.n, 128, 0, c.stream>>>(Lv.n, c.R, c.nn, t->KP, t->HX[l], t->HY[l], t->HZ[l],
-                                                          Lv.keys, Lv.M, t->scal + 2 * l, t->Ahi[l], t->Alo[l]);
+  {
+    // the multipoles of all levels of the launch: their maxima, the level scales, then the packed FP16 hi / lo
+    // grids (every position written, empty ones with zeros)
+    PackLevels L{};
+    L.l0 = l0;
+    L.l1 = l1;
+    L.pos0[l0] = 0;
+    long long maxval = 0;
+    for (int l = l0; l <= l1; ++l) {
+      L.M[l] = c.lv[l].M;
+      L.nval[l] = c.lv[l].n * c.R * c.nn;
+      maxval = std::max(maxval, L.nval[l]);
+      L.HX[l] = t->HX[l];
+      L.HY[l] = t->HY[l];
+      L.HZ[l] = t->HZ[l];
+      L.side[l] = 1 << l;
+      L.grid[l] = c.lv[l].grid;
+      L.hi[l] = t->Ahi[l];
+      L.lo[l] = t->Alo[l];
+      L.scale_l[l] = 2.0 / (c.cfg.box_width / (double)(1LL << l));
+      L.pos0[l + 1] = L.pos0[l] + 8LL * c.R * t->HZ[l] * t->HY[l] * t->HX[l];
+    }
+    B200_CUDA(cudaMemsetAsync(t->amax + l0, 0, sizeof(unsigned long long) * (l1 - l0 + 1), c.stream));
+    const unsigned gx = (unsigned)std::max<long long>(1, std::min<long long>(256, grid_for(maxval, 256)));
+    absmax_levels_kernel<<<dim3(gx, l1 - l0 + 1), 256, 0, c.stream>>>(L, t->amax);
+    level_scale_kernel<<<1, 32, 0, c.stream>>>(L, t->amax, t->lr ? t->lr_shift : SB, t->scal);
+    pack_levels_kernel<<<(unsigned)L.pos0[l1 + 1], 128, 0, c.stream>>>(L, c.R, c.nn, t->KP, t->scal);
     c.launches += 3;
   }
   // units are ordered by level, finest first: levels [l0, l1] are one contiguous range
