@@ -1450,8 +1450,8 @@ static b200fmm_status tc_init_lowrank(Context &c, DenseTC &t, TcParams &P, bool 
   Y.NK = t.NK;
   Y.R = c.R;
   Y.yscale = (float)std::ldexp(1.0, -sY);
-  // first product: segments of 3 K chunks (18 MMAs); second product: segments of 6 chunks (18 MMAs).  At
-  // order 7 this keeps the M2L within 5e-7 of FP64 (longer segments: 6-9e-7 for 4-10 % less time)
+  // first product: segments of 3 K chunks (18 MMAs); second product: segments of 12 chunks (36 MMAs).  At
+  // order 7 this keeps the M2L within 5.5e-7 of FP64 (longer segments: 6-9e-7 for a few % less time)
   Y.segc = 3;
   if (const char *e = getenv("B200FMM_TC_LR_YSEG")) Y.segc = std::max(1, atoi(e));
   t.ystage_bytes = 2 * (TILE_X * TILE_Y * TILE_Z * KCHUNK * 2) + 2 * YBLK * KCHUNK * 2;
@@ -1460,7 +1460,7 @@ static b200fmm_status tc_init_lowrank(Context &c, DenseTC &t, TcParams &P, bool 
   Y.stage_bytes = t.ystage_bytes;
   Y.status = c.d_status;
   // segments of the second product's chunk stream: as many 16-wide K steps as a dense segment has
-  P.lr_seglen = 6;
+  P.lr_seglen = 12;
   if (const char *e = getenv("B200FMM_TC_LR_SEGLEN")) P.lr_seglen = std::max(1, atoi(e));
   use = true;
   return B200FMM_OK;
