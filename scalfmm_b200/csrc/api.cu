@@ -138,6 +138,7 @@ void drop_graph(Context &c) {
 
 b200fmm_status run_m2l(Context &c, int level) {
   if (c.cfg.precision == B200FMM_MIXED) return run_m2l_tc(c, level);
+  B200_CHECK(build_ilists(c));  // built with the tree in FP64: a no-op
   return run_m2l_fp64(c, level);
 }
 
@@ -632,6 +633,7 @@ b200fmm_status b200fmm_tree_stats(b200fmm_handle h, long long *m2l_pairs, long l
   Context &c = *h;
   B200_CHECK(need_particles(c));
   B200_CHECK(set_device(c));
+  B200_CHECK(build_ilists(c));
   B200_CHECK(ensure_scratch(c, 4096));
   unsigned long long *d = (unsigned long long *)((char *)c.d_scratch + 2048);
   B200_CUDA(cudaMemsetAsync(d, 0, 2 * sizeof(unsigned long long), c.stream));
@@ -672,6 +674,7 @@ b200fmm_status b200fmm_m2l_flops(b200fmm_handle h, double *flops) {
     slot_symmetry_tables(c.p, pind, pvec);
     for (int t = 0; t < 343; ++t) rank[t] = c.sym_ranks[pind[t]];
   }
+  B200_CHECK(build_ilists(c));
   RankTable T;
   for (int ct = 0; ct < 8; ++ct)
     for (int e = 0; e < 189; ++e) T.r[ct][e] = rank[c.itab.slot[ct][e]];

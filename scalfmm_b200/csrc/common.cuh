@@ -115,6 +115,7 @@ struct Context {
   // CUDA graph of execute(): captured on the second execute() of one tree with the same operations and
   // replayed from then on (set_charges() keeps the tree; set_particles() starts a new one)
   long long tree_serial = 0;              // bumped by every set_particles()
+  long long ilist_serial = -1;            // tree whose interaction lists are built (MIXED builds them on demand)
   long long column_serial = -1;           // tree whose leaves are in the FP32 P2P column order
   long long eager_serial = -1, graph_serial = -1;
   unsigned eager_ops = 0, graph_ops = 0;
@@ -167,6 +168,7 @@ b200fmm_status sym_slot_factors(const Context &c, std::vector<double> &Ut, std::
                                 std::vector<long long> &toff, std::vector<int> &trank);
 b200fmm_status build_dense_operators(Context &c);
 // tree.cu
+b200fmm_status build_ilists(Context &c);
 b200fmm_status build_tree(Context &c, const double *x, const double *y, const double *z, const double *q,
                           bool on_device);
 b200fmm_status upload_charges(Context &c, const double *q, bool on_device);

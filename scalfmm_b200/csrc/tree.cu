@@ -732,15 +732,39 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
     }
     const long long total = C.start[LL + 1];
     if (total > 0) {
-      ilist_kernel<<<(unsigned)total, 192, 0, s>>>(C, c.d_itab);
-      ++c.tree_launches;
-      if (c.cfg.precision == B200FMM_MIXED) {
+      // the interaction lists feed the FP64 M2L; the tensor-core M2L works from the cell grids, and MIXED
+      // builds the lists only when asked for work counts (build_ilists)
+      if (c.cfg.precision == B200FMM_FP64) {
+        ilist_kernel<<<(unsigned)total, 192, 0, s>>>(C, c.d_itab);
+        ++c.tree_launches;
+        c.ilist_serial = c.tree_serial;
+      } else {
         grid_index_kernel<<<grid_for(total, 256), 256, 0, s>>>(C);
         ++c.tree_launches;
       }
     }
   }
   B200_CUDA(cudaGetLastError());
+  return B200FMM_OK;
+}
+
+// Interaction lists of levels 2..height-1 of the current tree, if not built yet.
+b200fmm_status build_ilists(Context &c) {
+  const int LL = c.H - 1;
+  if (LL < 2 || c.ilist_serial == c.tree_serial) return B200FMM_OK;
+  LevelCellsT C{};
+  C.l0 = 2;
+  C.l1 = LL;
+  C.start[2] = 0;
+  for (int l = 2; l <= LL; ++l) {
+    C.keys[l] = c.lv[l].keys;
+    C.ilist[l] = c.lv[l].ilist;
+    C.start[l + 1] = C.start[l] + c.lv[l].n;
+  }
+  const long long total = C.start[LL + 1];
+  if (total > 0) ilist_kernel<<<(unsigned)total, 192, 0, c.stream>>>(C, c.d_itab);
+  B200_CUDA(cudaGetLastError());
+  c.ilist_serial = c.tree_serial;
   return B200FMM_OK;
 }
 
