@@ -157,6 +157,9 @@ void destroy_context(b200fmm_context *c) {
   if (c->events_ready)
     for (auto &e : c->ev) cudaEventDestroy(e);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  if (c->stream2) cudaStreamDestroy(c->stream2);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
   delete c;
 }
 
@@ -205,6 +208,12 @@ b200fmm_status b200fmm_create(const b200fmm_config *cfg, b200fmm_handle *out) {
         st = fail(B200FMM_ERR_CUDA, "stream creation failed");
       c->own_stream = true;
     }
+  }
+  if (st == B200FMM_OK) {
+    if (cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess)
+      st = fail(B200FMM_ERR_CUDA, "stream creation failed");
   }
   if (st == B200FMM_OK) {
     bool ok = true;
@@ -340,10 +349,28 @@ static b200fmm_status execute_body(Context &c, unsigned ops) {
   if (!c.state_zero || c.capturing) B200_CHECK(zero_state(c));
   c.state_zero = false;
   B200_CHECK(record(c, 1));
+  // The near field needs only the tree: it runs on the second stream beside P2M and M2M and joins before the
+  // M2L (a persistent kernel that wants every SM) and before L2P adds into the same results.
+  const bool overlap = (ops & B200FMM_P2P) && (ops & (B200FMM_P2M | B200FMM_M2M));
+  c.p2p_overlapped = overlap;
+  if (overlap) {
+    B200_CUDA(cudaEventRecord(c.ev_fork, c.stream));
+    B200_CUDA(cudaStreamWaitEvent(c.stream2, c.ev_fork, 0));
+    cudaStream_t main = c.stream;
+    c.stream = c.stream2;
+    b200fmm_status st = record(c, 12);
+    if (st == B200FMM_OK) st = run_p2p(c, 0);
+    if (st == B200FMM_OK) st = record(c, 13);
+    if (st == B200FMM_OK && cudaEventRecord(c.ev_join, c.stream2) != cudaSuccess)
+      st = fail(B200FMM_ERR_CUDA, "event record failed");
+    c.stream = main;
+    B200_CHECK(st);
+  }
   if (ops & B200FMM_P2M) B200_CHECK(run_p2m(c));
   B200_CHECK(record(c, 2));
   if (ops & B200FMM_M2M)
     for (int l = LL - 1; l >= 2; --l) B200_CHECK(run_m2m(c, l));
+  if (overlap) B200_CUDA(cudaStreamWaitEvent(c.stream, c.ev_join, 0));
   B200_CHECK(record(c, 3));
   if (ops & B200FMM_M2L) {
     if (c.cfg.precision == B200FMM_MIXED)
@@ -357,7 +384,7 @@ static b200fmm_status execute_body(Context &c, unsigned ops) {
   B200_CHECK(record(c, 5));
   if (ops & B200FMM_L2P) B200_CHECK(run_l2p(c));
   B200_CHECK(record(c, 6));
-  if (ops & B200FMM_P2P) B200_CHECK(run_p2p(c, 0));
+  if ((ops & B200FMM_P2P) && !overlap) B200_CHECK(run_p2p(c, 0));
   B200_CHECK(record(c, 7));
   return B200FMM_OK;
 }
@@ -597,7 +624,8 @@ b200fmm_status b200fmm_last_timings(b200fmm_handle h, double *ms8) {
   ms8[0] = c.ms[0];
   for (int k = 1; k <= 6; ++k) {
     float t = 0;
-    if (c.last_was_graph || cudaEventElapsedTime(&t, c.ev[k], c.ev[k + 1]) != cudaSuccess) t = 0;
+    const int a = (k == 6 && c.p2p_overlapped) ? 12 : k;  // the concurrent near field has its own events
+    if (c.last_was_graph || cudaEventElapsedTime(&t, c.ev[a], c.ev[a + 1]) != cudaSuccess) t = 0;
     ms8[k] = t;
   }
   float tot = 0;

@@ -64,6 +64,9 @@ struct Context {
   int p = 0, nn = 0, H = 0, R = 1;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  cudaStream_t stream2 = nullptr;              // the near field, concurrent with the upward pass
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  bool p2p_overlapped = false;                 // the last execute() ran P2P on stream2
   int device = 0;
 
   // interpolation tables (device)
