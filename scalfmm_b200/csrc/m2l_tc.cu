@@ -220,6 +220,14 @@ __device__ __forceinline__ void tma_load_3d_pair(void *dst, const CUtensorMap *m
       "l"(map), "r"(bar_cluster), "r"(c0), "r"(c1), "r"(c2)
       : "memory");
 }
+__device__ __forceinline__ void tma_load_2d_pair(void *dst, const CUtensorMap *map, unsigned bar_cluster, int c0,
+                                                 int c1) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], "
+      "[%2];" ::"r"(su32(dst)),
+      "l"(map), "r"(bar_cluster), "r"(c0), "r"(c1)
+      : "memory");
+}
 __device__ __forceinline__ void mma_f16_pair(unsigned d_tmem, unsigned long long da, unsigned long long db,
                                              unsigned idesc, unsigned accumulate) {
   asm volatile(
@@ -823,6 +831,10 @@ struct __align__(64) LrYParams {
 
 constexpr int YBLK = 256;  // rank rows per item (16 chunks of 16)
 
+// PAIR: clusters of two CTAs on the z-adjacent tiles (bz, bz + 1) of an item, M = 256 MMAs (cta_group::2)
+// issued by the even CTA, each CTA loading its own tile of multipoles and half of the V block (the same
+// protocol as the second product's CTA pairs).
+template <bool PAIR>
 __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_constant__ LrYParams P) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *smem = (unsigned char *)(((unsigned long long)smem_raw + 1023) & ~1023ull);
@@ -832,6 +844,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
   __shared__ volatile int abort_sh;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int S = P.stages;
+  const unsigned rank = PAIR ? cluster_rank() : 0u;
+  const bool leader = rank == 0;
+  const int g_id = PAIR ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
+  const int g_count = PAIR ? (int)(gridDim.x >> 1) : (int)gridDim.x;
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(&full_bar[s], 1);
@@ -839,30 +855,43 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&acc_full[b], 1);
-      mbar_init(&acc_empty[b], 8);
+      mbar_init(&acc_empty[b], PAIR ? 16 : 8);  // the epilogue warps of both CTAs
     }
     mbar_init(&done_bar, 1);
     abort_sh = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_base_sh)),
-                 "r"(2 * YBLK));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    if constexpr (PAIR) {
+      asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_base_sh)),
+                   "r"(2 * YBLK));
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    } else {
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_base_sh)),
+                   "r"(2 * YBLK));
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
   }
   tc_fence_before();
   __syncthreads();
+  if constexpr (PAIR) cluster_sync_all();
   tc_fence_after();
   const unsigned tmem = tmem_base_sh;
   auto give_up = [&]() {
     atomicExch(P.status + 1, 1);
     abort_sh = 1;
+    if constexpr (PAIR)
+      asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(mapa_shared(su32((const void *)&abort_sh), rank ^ 1u)),
+                   "r"(1)
+                   : "memory");
   };
   const int a_bytes = TILE_X * TILE_Y * TILE_Z * KCHUNK * 2;  // 8 KB
-  const int b_bytes = YBLK * KCHUNK * 2;                      // 16 KB
+  const int vrows = PAIR ? YBLK / 2 : YBLK;                   // V rows of a block in this CTA
+  const int b_bytes = vrows * KCHUNK * 2;                     // 8 or 16 KB
   const int segc = P.segc;
   const int nseg = (P.NK + segc - 1) / segc;                  // segments per item
   const int nitems = P.item0[P.l0] + P.nitems[P.l0] - P.item0[P.l1];
+  auto tz_units = [&](int l) { return PAIR ? (P.HZ[l] / TILE_Z + 1) / 2 : P.HZ[l] / TILE_Z; };
   // item -> level, rhs, parity, tile, block; items of a tile are consecutive (blocks innermost) so that the
   // CTAs working at the same time share the tile's multipoles and the V blocks through L2
   struct YItem {
@@ -877,13 +906,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
     y.level = l;
     y.nb = r % P.nblk;
     r /= P.nblk;
-    const int TX = P.HX[l] / TILE_X, TY = P.HY[l] / TILE_Y, TZ = P.HZ[l] / TILE_Z;
+    const int TX = P.HX[l] / TILE_X, TY = P.HY[l] / TILE_Y, TZu = tz_units(l);
     y.bx = r % TX;
     r /= TX;
     y.by = r % TY;
     r /= TY;
-    y.bz = r % TZ;
-    r /= TZ;
+    y.bz = (r % TZu) * (PAIR ? 2 : 1) + (int)rank;  // this CTA's tile
+    r /= TZu;
     y.par = r & 7;
     y.rhs = r >> 3;
     return y;
@@ -893,23 +922,34 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
     if (lane == 0) {
       int stage = 0;
       unsigned phase = 0;
-      for (int it = blockIdx.x; it < nitems && !abort_sh; it += gridDim.x) {
+      const unsigned full0 = PAIR ? mapa_shared(su32(&full_bar[0]), 0u) : su32(&full_bar[0]);
+      for (int it = g_id; it < nitems && !abort_sh; it += g_count) {
         const YItem y = decode(it);
-        const int vrow = (P.ybase[y.par] + y.nb * (YBLK / 16)) * 16;
+        const int vrow = (P.ybase[y.par] + y.nb * (YBLK / 16)) * 16 + (int)rank * vrows;
         for (int kc = 0; kc < P.NK; ++kc) {
           if (!mbar_wait(&empty_bar[stage], phase ^ 1)) {
             give_up();
             break;
           }
           unsigned char *sbuf = smem + (size_t)stage * P.stage_bytes;
-          mbar_expect_tx(&full_bar[stage], 2 * a_bytes + 2 * b_bytes);
+          if (leader) mbar_expect_tx(&full_bar[stage], (PAIR ? 2 : 1) * (2 * a_bytes + 2 * b_bytes));
           const int c4 = y.rhs * 8 + y.par;
-          tma_load_5d(sbuf, &P.mapA_hi[y.level], &full_bar[stage], kc * KCHUNK, y.bx * TILE_X, y.by * TILE_Y,
-                      y.bz * TILE_Z, c4);
-          tma_load_5d(sbuf + a_bytes, &P.mapA_lo[y.level], &full_bar[stage], kc * KCHUNK, y.bx * TILE_X,
-                      y.by * TILE_Y, y.bz * TILE_Z, c4);
-          tma_load_2d(sbuf + 2 * a_bytes, &P.mapV_hi, &full_bar[stage], kc * KCHUNK, vrow);
-          tma_load_2d(sbuf + 2 * a_bytes + b_bytes, &P.mapV_lo, &full_bar[stage], kc * KCHUNK, vrow);
+          if constexpr (PAIR) {
+            const unsigned fb = full0 + 8u * (unsigned)stage;
+            tma_load_5d_pair(sbuf, &P.mapA_hi[y.level], fb, kc * KCHUNK, y.bx * TILE_X, y.by * TILE_Y, y.bz * TILE_Z,
+                             c4);
+            tma_load_5d_pair(sbuf + a_bytes, &P.mapA_lo[y.level], fb, kc * KCHUNK, y.bx * TILE_X, y.by * TILE_Y,
+                             y.bz * TILE_Z, c4);
+            tma_load_2d_pair(sbuf + 2 * a_bytes, &P.mapV_hi, fb, kc * KCHUNK, vrow);
+            tma_load_2d_pair(sbuf + 2 * a_bytes + b_bytes, &P.mapV_lo, fb, kc * KCHUNK, vrow);
+          } else {
+            tma_load_5d(sbuf, &P.mapA_hi[y.level], &full_bar[stage], kc * KCHUNK, y.bx * TILE_X, y.by * TILE_Y,
+                        y.bz * TILE_Z, c4);
+            tma_load_5d(sbuf + a_bytes, &P.mapA_lo[y.level], &full_bar[stage], kc * KCHUNK, y.bx * TILE_X,
+                        y.by * TILE_Y, y.bz * TILE_Z, c4);
+            tma_load_2d(sbuf + 2 * a_bytes, &P.mapV_hi, &full_bar[stage], kc * KCHUNK, vrow);
+            tma_load_2d(sbuf + 2 * a_bytes + b_bytes, &P.mapV_lo, &full_bar[stage], kc * KCHUNK, vrow);
+          }
           if (++stage == S) {
             stage = 0;
             phase ^= 1;
@@ -918,14 +958,26 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
       }
     }
   } else if (warp == 1) {
-    if (lane == 0) {
-      const unsigned idesc = (1u << 4) | ((unsigned)(YBLK >> 3) << 17) | ((unsigned)(128 >> 4) << 24);
+    if (lane == 0 && leader) {
+      const unsigned idesc = (1u << 4) | ((unsigned)(YBLK >> 3) << 17) | ((unsigned)((PAIR ? 256 : 128) >> 4) << 24);
+      auto mma = [&](unsigned d, unsigned long long da, unsigned long long db, unsigned acc) {
+        if constexpr (PAIR)
+          mma_f16_pair(d, da, db, idesc, acc);
+        else
+          mma_f16(d, da, db, idesc, acc);
+      };
+      auto commit = [&](unsigned long long *bar) {
+        if constexpr (PAIR)
+          mma_commit_pair_both(bar);
+        else
+          mma_commit(bar);
+      };
       const unsigned long long dA_hi = sdesc(smem), dA_lo = dA_hi + (unsigned)(a_bytes >> 4);
       const unsigned long long dB_hi = dA_hi + (unsigned)((2 * a_bytes) >> 4), dB_lo = dB_hi + (unsigned)(b_bytes >> 4);
       const unsigned stage_step = (unsigned)P.stage_bytes >> 4;
       int stage = 0;
       unsigned phase = 0, empty_par = 3u;
-      for (int it = blockIdx.x; it < nitems && !abort_sh; it += gridDim.x) {
+      for (int it = g_id; it < nitems && !abort_sh; it += g_count) {
         for (int kc = 0; kc < P.NK && !abort_sh; ++kc) {
           const int b = (kc / segc) & 1;
           const bool first = kc % segc == 0;
@@ -946,19 +998,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
 #pragma unroll
           for (int ks = 0; ks < 2; ++ks) {
             const unsigned k2 = 2u * ks;
-            mma_f16(d, dA_hi + so + k2, dB_lo + so + k2, idesc, (first && ks == 0) ? 0u : 1u);
-            mma_f16(d, dA_lo + so + k2, dB_hi + so + k2, idesc, 1u);
-            mma_f16(d, dA_hi + so + k2, dB_hi + so + k2, idesc, 1u);
+            mma(d, dA_hi + so + k2, dB_lo + so + k2, (first && ks == 0) ? 0u : 1u);
+            mma(d, dA_lo + so + k2, dB_hi + so + k2, 1u);
+            mma(d, dA_hi + so + k2, dB_hi + so + k2, 1u);
           }
-          mma_commit(&empty_bar[stage]);
+          commit(&empty_bar[stage]);
           if (++stage == S) {
             stage = 0;
             phase ^= 1;
           }
-          if (kc % segc == segc - 1 || kc == P.NK - 1) mma_commit(&acc_full[b]);
+          if (kc % segc == segc - 1 || kc == P.NK - 1) commit(&acc_full[b]);
         }
       }
-      mma_commit(&done_bar);
+      if constexpr (PAIR)
+        mma_commit_pair_local(&done_bar);
+      else
+        mma_commit(&done_bar);
       if (!mbar_wait(&done_bar, 0)) give_up();
     }
   } else if (warp >= 2 && warp <= 9) {
@@ -966,9 +1021,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
     const int ch = (warp - 2) >> 2;  // which 128 of the 256 columns
     const int row = q * 32 + lane;   // source cell within the tile
     const unsigned tlane = tmem + ((unsigned)(q * 32) << 16) + (unsigned)(ch * 128);
+    const unsigned empty0 = PAIR ? mapa_shared(su32(&acc_empty[0]), 0u) : 0u;
     unsigned full_par = 0;
     float acc[128];
-    for (int it = blockIdx.x; it < nitems && !abort_sh; it += gridDim.x) {
+    for (int it = g_id; it < nitems && !abort_sh; it += g_count) {
       const YItem y = decode(it);
 #pragma unroll
       for (int i = 0; i < 128; ++i) acc[i] = 0.f;
@@ -983,13 +1039,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
         drain_cols<128>(tlane + (unsigned)(b * YBLK), acc);
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&acc_empty[b]);
+        if (lane == 0) {
+          if constexpr (PAIR)
+            mbar_arrive_cluster(empty0 + 8u * (unsigned)b);
+          else
+            mbar_arrive(&acc_empty[b]);
+        }
       }
       if (abort_sh) break;
       // write the 8 chunks of 16 ranks this thread holds, as FP16 hi and lo
       const int l = y.level;
       const int hx = y.bx * TILE_X + (row & 7), hy = y.by * TILE_Y + ((row >> 3) & 3), hz = y.bz * TILE_Z + (row >> 5);
       const int nch = P.ybase[y.par + 1] - P.ybase[y.par];  // chunks of this parity
+      if (y.bz >= P.HZ[l] / TILE_Z) continue;                // the missing second tile of a pair at the z edge
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         const int chunk = y.nb * (YBLK / 16) + ch * 8 + k;
@@ -1017,10 +1079,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
   }
   tc_fence_before();
   __syncthreads();
+  if constexpr (PAIR) cluster_sync_all();
   if (warp == 1) {
     __syncwarp();
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * YBLK));
+    if constexpr (PAIR)
+      asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * YBLK));
+    else
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * YBLK));
   }
 }
 
@@ -1282,6 +1348,7 @@ struct DenseTC {
   __half *Yhi[kMaxHeight] = {}, *Ylo[kMaxHeight] = {};
   size_t Ybytes[kMaxHeight] = {};
   int ycht = 0, nblk = 0, ystages = 0, ystage_bytes = 0;
+  bool ypair = true;                      // first product on CTA pairs (B200FMM_TC_YPAIR=0: single CTAs)
   int lr_shift = 0;                       // sV + sU: the power-of-two pre-scales of V and U
   LrYParams *yparams = nullptr;           // host copy
   double lr_rank_fed[8] = {};             // first product: sum of the ranks of the slots each parity feeds
@@ -1437,10 +1504,11 @@ static b200fmm_status tc_init_lowrank(Context &c, DenseTC &t, TcParams &P, bool 
   t.yparams = new LrYParams();
   std::memset(t.yparams, 0, sizeof(LrYParams));
   LrYParams &Y = *t.yparams;
+  if (const char *e = getenv("B200FMM_TC_YPAIR")) t.ypair = atoi(e) != 0;
   {
     cuuint64_t dims[2] = {(cuuint64_t)t.KP, (cuuint64_t)ych * 16};
     cuuint64_t strides[1] = {(cuuint64_t)t.KP * 2};
-    cuuint32_t box[2] = {KCHUNK, YBLK};
+    cuuint32_t box[2] = {KCHUNK, (cuuint32_t)(t.ypair ? YBLK / 2 : YBLK)};
     B200_CHECK(encode(&Y.mapV_hi, t.Vhi, 2, dims, strides, box));
     B200_CHECK(encode(&Y.mapV_lo, t.Vlo, 2, dims, strides, box));
   }
@@ -1454,7 +1522,7 @@ static b200fmm_status tc_init_lowrank(Context &c, DenseTC &t, TcParams &P, bool 
   // order 7 this keeps the M2L within 5.5e-7 of FP64 (longer segments: 6-9e-7 for a few % less time)
   Y.segc = 3;
   if (const char *e = getenv("B200FMM_TC_LR_YSEG")) Y.segc = std::max(1, atoi(e));
-  t.ystage_bytes = 2 * (TILE_X * TILE_Y * TILE_Z * KCHUNK * 2) + 2 * YBLK * KCHUNK * 2;
+  t.ystage_bytes = 2 * (TILE_X * TILE_Y * TILE_Z * KCHUNK * 2) + 2 * (t.ypair ? YBLK / 2 : YBLK) * KCHUNK * 2;
   t.ystages = std::min(MAX_STAGES, (220 * 1024) / t.ystage_bytes);
   Y.stages = t.ystages;
   Y.stage_bytes = t.ystage_bytes;
@@ -1568,8 +1636,11 @@ b200fmm_status tc_init(Context &c) {
     t->grid = 2 * std::min(nclusters, dev_sms / 2);
   }
   if (lr) {
-    B200_CUDA(cudaFuncSetAttribute(lr_y_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   t->ystages * t->ystage_bytes + 1024));
+    const int ysmem = t->ystages * t->ystage_bytes + 1024;
+    if (t->ypair)
+      B200_CUDA(cudaFuncSetAttribute(lr_y_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysmem));
+    else
+      B200_CUDA(cudaFuncSetAttribute(lr_y_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysmem));
   }
   return B200FMM_OK;
 }
@@ -1678,7 +1749,8 @@ static b200fmm_status tc_prepare(Context &c) {
     int n = 0;
     for (int l = LL; l >= 2; --l) {
       Y.item0[l] = n;
-      Y.nitems[l] = c.R * 8 * (t->HZ[l] / TILE_Z) * (t->HY[l] / TILE_Y) * (t->HX[l] / TILE_X) * t->nblk;
+      const int TZ = t->HZ[l] / TILE_Z;
+      Y.nitems[l] = c.R * 8 * (t->ypair ? (TZ + 1) / 2 : TZ) * (t->HY[l] / TILE_Y) * (t->HX[l] / TILE_X) * t->nblk;
       n += Y.nitems[l];
     }
   }
@@ -1824,7 +1896,24 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
     Y.l1 = l1;
     const int ny = Y.item0[l0] + Y.nitems[l0] - Y.item0[l1];
     if (ny > 0) {
-      lr_y_kernel<<<std::min(t->grid, ny), TC_THREADS, (size_t)t->ystages * t->ystage_bytes + 1024, c.stream>>>(Y);
+      int dev_sms = 148;
+      cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c.device);
+      cudaLaunchConfig_t ycfg = {};
+      cudaLaunchAttribute yat[1];
+      yat[0].id = cudaLaunchAttributeClusterDimension;
+      yat[0].val.clusterDim.x = t->ypair ? 2 : 1;
+      yat[0].val.clusterDim.y = 1;
+      yat[0].val.clusterDim.z = 1;
+      ycfg.gridDim = dim3(t->ypair ? 2 * std::min(dev_sms / 2, ny) : std::min(dev_sms, ny));
+      ycfg.blockDim = dim3(TC_THREADS);
+      ycfg.dynamicSmemBytes = (size_t)t->ystages * t->ystage_bytes + 1024;
+      ycfg.stream = c.stream;
+      ycfg.attrs = yat;
+      ycfg.numAttrs = t->ypair ? 1 : 0;
+      if (t->ypair)
+        B200_CUDA(cudaLaunchKernelEx(&ycfg, lr_y_kernel<true>, Y));
+      else
+        B200_CUDA(cudaLaunchKernelEx(&ycfg, lr_y_kernel<false>, Y));
       ++c.launches;
     }
   }
