@@ -21,10 +21,12 @@
 //     sums held in registers with ordinary IEEE FP32 adds; at the end of a work item they add
 //     scale * 2^-(sA+sB) * sum into the FP64 locals (atomic adds: several items of the same tile contribute).
 //
-// Roles: warp 0 = TMA producer (one elected thread), warp 1 = MMA issuer (one thread) and TMEM owner,
-// warps 2..9 = epilogue (TMEM lane quarter = warp % 4, column half = (warp - 2) / 4), warp 10 = issuer of the
-// second column half at order 7, warp 11 idle (blocks are sized in whole groups of four warps).  Shared memory: STAGES x {A_hi, A_lo, B_hi, B_lo}
-// K-chunks with the 64-byte swizzle the UMMA descriptors describe.  Every mbarrier wait is bounded; a wait
+// Roles, by warpgroup: warpgroup 0 holds the TMA producer (warp 0, one elected thread), the MMA issuer and
+// TMEM owner (warp 1), the issuer of the second column half at order 7 (warp 2) and a spare warp;
+// warpgroups 1 and 2 (warps 4..11) are the epilogue (TMEM lane quarter = warp % 4, column part =
+// (warp - 4) / 4).  Kernels whose epilogue holds many running sums move registers from warpgroup 0 to the
+// epilogue with setmaxnreg.  Shared memory: STAGES x {A_hi, A_lo, B_hi, B_lo} K-chunks with the 64-byte
+// swizzle the UMMA descriptors describe, then the transfer-vector records.  Every mbarrier wait is bounded; a wait
 // that runs out sets a device status word, the CTA abandons its work, frees its TMEM and returns.
 #include "common.cuh"
 
@@ -35,12 +37,19 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <utility>
 
 namespace b200 {
 
 namespace {
 
-constexpr int TC_THREADS = 384;  // 12 warps: TMA, MMA, 8 epilogue, second MMA issuer, spare
+constexpr int TC_THREADS = 384;  // 12 warps: TMA, MMA, second MMA issuer, spare, 8 epilogue
+// Register split of the kernels with large epilogues: launched at TC_REGS per thread, warpgroup 0 gives
+// registers up (setmaxnreg.dec to REG_LOW) and the two epilogue warpgroups take them (setmaxnreg.inc to
+// REG_HIGH).  The split must add up to what the block was launched with, or the increase never completes;
+// the host checks the compiled register count before the first launch.
+constexpr int TC_REGS = 168, REG_LOW = 56, REG_HIGH = 224;
+static_assert(128 * REG_LOW + 256 * REG_HIGH == TC_THREADS * TC_REGS, "register split must match the launch");
 constexpr int TILE_X = 8, TILE_Y = 4, TILE_Z = 4;  // 128 targets
 constexpr int KCHUNK = 32;                          // fp16 elements per 64-byte swizzle row
 constexpr int SB = 15;                              // operator pre-scale 2^15
@@ -103,15 +112,25 @@ struct __align__(64) TcParams {
   // per tile (level, parity, bz, by, bx): 6 words, bit e set when transfer vector e has an occupied source
   // box; bit 31 of word 5 set when the tile has an occupied target cell
   const unsigned *busy;
+  // per target parity c and transfer vector e (8 x 189 records, copied to shared memory by every CTA)
+  const struct TvRec *tv;
   // low-rank form (symmetric Chebyshev operators K_t = U_t V_t^T): A is Y = V_t^T M, one row of 16-rank
   // chunks per source cell, and B is U_t, both in 16-wide K chunks
-  int lr_seglen;                // K chunks per accumulator segment of a fragment's chunk stream
-  int ycht;                     // Y chunks per right-hand side (all parities)
-  int ybase[8];                 // first Y chunk of each source parity
-  unsigned char tnk[343];       // K chunks of slot t (ceil(rank / 16)), 0 for near slots
-  short uchunk0[343];           // first U chunk of slot t
-  short ychunk0[8][343];        // first Y chunk of slot t among the chunks of source parity c'
+  int lr_seglen;  // K chunks per accumulator segment of a fragment's chunk stream
+  int ycht;       // Y chunks per right-hand side (all parities)
 };
+// What the producer and the MMA issuers need of transfer vector e of target parity c: the A box's
+// coordinates (offset of the source tile in half-grid cells; outer coordinate ya + rhs * (ycht or 8)), the B
+// box's outer coordinate ub, and in the low-rank form the slot's 16-wide rank chunks nk.  Dense: ya = source
+// parity, ub = operator slot.  Low rank: ya = the slot's first Y chunk in the source parity's rows, ub = its
+// first U chunk.
+struct TvRec {
+  short ya, ub;
+  unsigned char nk;
+  signed char ox, oy, oz;
+};
+static_assert(sizeof(TvRec) == 8, "8-byte records");
+constexpr int TV_BYTES = 8 * 189 * (int)sizeof(TvRec);
 
 // ---- PTX helpers ----------------------------------------------------------------------------------
 __device__ __forceinline__ unsigned su32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -260,18 +279,61 @@ __device__ __forceinline__ void tmem_ld16(unsigned taddr, unsigned *r) {
       : "r"(taddr));
 }
 
-// add N accumulator columns starting at TMEM address taddr (a multiple of 16 columns) into acc[0..N)
-template <int N>
+// add N accumulator columns starting at TMEM address taddr (a multiple of 16 columns) into acc[0..N):
+// BATCH loads of 16 columns in flight per wait
+template <int N, int BATCH = 1>
 __device__ __forceinline__ void drain_cols(unsigned taddr, float *acc) {
   static_assert(N % 16 == 0, "drained in groups of 16 columns");
 #pragma unroll
-  for (int c0 = 0; c0 < N; c0 += 16) {
-    unsigned r[16];
-    tmem_ld16(taddr + c0, r);
+  for (int c0 = 0; c0 < N; c0 += 16 * BATCH) {
+    unsigned r[16 * BATCH];
+#pragma unroll
+    for (int b = 0; b < BATCH; ++b)
+      if (c0 + 16 * b < N) tmem_ld16(taddr + c0 + 16 * b, r + 16 * b);
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int i = 0; i < 16; ++i) acc[c0 + i] += __uint_as_float(r[i]);
+    for (int b = 0; b < BATCH; ++b)
+      if (c0 + 16 * b < N) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          // the loaded registers are read only after the wait
+          asm volatile("" : "+r"(r[16 * b + i]));
+          acc[c0 + 16 * b + i] += __uint_as_float(r[16 * b + i]);
+        }
+      }
   }
+}
+
+// atomically add sc * acc[I0, I1) to dst[0, I1 - I0), the first lim of them (the nodes that exist).  Each
+// addition is one instruction group on the base address plus a constant offset, so that neither the
+// 64-bit addresses nor the FP64 products of a whole run are held in registers at once.
+template <int K>
+__device__ __forceinline__ void red_add_f64(double *dst, float v, double sc, int lim) {
+  if (K < lim)
+    asm volatile("{\n .reg .f64 t;\n cvt.f64.f32 t, %1;\n mul.rn.f64 t, t, %2;\n red.global.add.f64 [%0+%3], t;\n}\n" ::"l"(
+                     dst),
+                 "f"(v), "d"(sc), "n"(8 * K)
+                 : "memory");
+}
+template <int I0, int... K>
+__device__ __forceinline__ void flush_seq(const float *acc, double *dst, int lim, double sc,
+                                          std::integer_sequence<int, K...>) {
+  (red_add_f64<K>(dst, acc[I0 + K], sc, lim), ...);
+}
+template <int I0, int I1>
+__device__ __forceinline__ void flush_cols(const float *acc, double *dst, int lim, double sc) {
+  flush_seq<I0>(acc, dst, lim, sc, std::make_integer_sequence<int, I1 - I0>{});
+}
+
+// registers move from warpgroup 0 (producer and MMA issuers) to the epilogue warpgroups; each call sits at
+// the top of its warpgroup's branch, so that the compiler allocates each role within its own limit
+template <bool SPLIT>
+__device__ __forceinline__ void give_registers() {
+  if constexpr (SPLIT) asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(REG_LOW));
+}
+template <bool SPLIT>
+__device__ __forceinline__ void take_registers() {
+  if constexpr (SPLIT) asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(REG_HIGH));
 }
 
 // The source box of transfer vector e for an item: parity grid sp, half-grid origin (ox, oy, oz), operator
@@ -443,6 +505,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
     abort_sh = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  // the transfer-vector records, behind the stage buffers
+  TvRec *tvs = (TvRec *)(smem + (size_t)S * P.stage_bytes);
+  for (int i = threadIdx.x; i < 8 * 189; i += blockDim.x) tvs[i] = P.tv[i];
   if (warp == 1) {
     if constexpr (PAIR) {
       // both CTAs' warp 1 allocate together; the same columns are allocated in each CTA's TMEM
@@ -460,6 +525,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
   if constexpr (PAIR) cluster_sync_all();  // the peer's barriers are initialised before any remote arrival
   tc_fence_after();
   const unsigned tmem = tmem_base_sh;
+  constexpr bool SPLIT_REGS = CW >= 112;  // running sums of CW columns per epilogue thread
   // a role that gives up marks the status word and stops both CTAs of a pair
   auto give_up = [&]() {
     atomicExch(P.status + 1, 1);
@@ -481,6 +547,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
   const int nb_rows = PAIR ? P.NH / 2 : P.NH;           // B rows of one column half in this CTA
   const int b_bytes = NHALF * nb_rows * ROWB;
 
+  if (warp < 4) {
+  give_registers<SPLIT_REGS>();
   if (warp == 0) {
     // ------------------------------------------------ TMA producer (both CTAs of a pair)
     if (lane == 0) {
@@ -496,13 +564,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
         for (int e = 0; e < 189 && rank_e < r1 && !abort_sh; ++e) {
           if (!bm.src(e)) continue;
           if (rank_e++ < r0) continue;
-          const SrcBox sb = src_box(P, w, bz, e);
-          const int sp = sb.sp, ox = sb.ox, oy = sb.oy, oz = sb.oz, slot = sb.slot;
           // K chunks of this transfer vector and the coordinates of its A and B boxes: dense (K offset,
-          // rhs and parity, operator slot) or low rank (Y chunk and U chunk of the slot)
-          const int nk = LR ? (int)P.tnk[slot] : P.NK;
-          const int a4 = LR ? w.rhs * P.ycht + P.ybase[sp] + P.ychunk0[sp][slot] : w.rhs * 8 + sp;
-          const int b2 = LR ? P.uchunk0[slot] : slot;
+          // rhs and source parity, operator slot) or low rank (Y chunk and U chunk of the slot)
+          const TvRec tr = tvs[w.parity * 189 + e];
+          const int ox = w.bx * TILE_X + tr.ox, oy = w.by * TILE_Y + tr.oy, oz = bz * TILE_Z + tr.oz;
+          const int nk = LR ? (int)tr.nk : P.NK;
+          const int a4 = w.rhs * (LR ? P.ycht : 8) + tr.ya;
+          const int b2 = tr.ub;
           for (int kc = 0; kc < nk; ++kc) {
             if (!wait_bar(&empty_bar[stage], phase ^ 1)) {
               give_up();
@@ -540,9 +608,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
         return !abort_sh;
       });
     }
-  } else if (warp == 1 || (NHALF == 2 && warp == 10)) {
+  } else if (warp == 1 || (NHALF == 2 && warp == 2)) {
     // ------------------------------------------------ MMA issuers (the even CTA of a pair)
-    // With two column halves each half has its own issuing thread (warp 1: half 0, warp 10: half 1), so
+    // With two column halves each half has its own issuing thread (warp 1: half 0, warp 2: half 1), so
     // that each thread issues 6 MMAs per K chunk and each half drains while the other half's MMAs run.
     const int hh = warp == 1 ? 0 : 1;
     if (lane == 0 && leader) {
@@ -607,7 +675,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
           for (int e = 0; e < 189 && rank_e < r1 && !abort_sh; ++e) {
             if (!bm.src(e)) continue;
             if (rank_e++ < r0) continue;
-            const int nk = P.tnk[P.slot[w.parity][e]];
+            const int nk = tvs[w.parity * 189 + e].nk;
             for (int kc = 0; kc < nk && !abort_sh; ++kc) {
               if (cs == 0) {
                 const int hb = NHALF == 2 ? 0 : (P.nbuf == 2 ? (seg & 1) : 0);
@@ -688,11 +756,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
         mma_commit(&done_bar);
       if (!wait_bar(&done_bar, 0)) give_up();
     }
-  } else if (warp >= 2 && warp <= 9) {
-    // ------------------------------------------------ epilogue (warps 2..9 of both CTAs)
+  }
+  } else {
+    take_registers<SPLIT_REGS>();
+    // ------------------------------------------------ epilogue (warps 4..11 of both CTAs)
     constexpr int SPLIT = 16 * ((CW + 31) / 32);
+    constexpr int BATCH = SPLIT_REGS ? 2 : 1;  // TMEM loads in flight per wait
     const int q = warp & 3;              // TMEM lane quarter this warp may access
-    const int ch = (warp - 2) >> 2;      // which part of each half
+    const int ch = (warp - 4) >> 2;      // which part of each half
     const int row = q * 32 + lane;       // target within the tile
     const unsigned tlane = tmem + ((unsigned)(q * 32) << 16);
     // the accumulator is released on the even CTA's barriers
@@ -721,7 +792,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
         int nch = 0, rank_e = 0;
         for (int e = 0; e < 189 && rank_e < r1; ++e) {
           if (!bm.src(e)) continue;
-          if (rank_e++ >= r0) nch += P.tnk[P.slot[w.parity][e]];
+          if (rank_e++ >= r0) nch += tvs[w.parity * 189 + e].nk;
         }
         nseg_item = (nch + P.lr_seglen - 1) / P.lr_seglen;
       }
@@ -734,7 +805,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
           }
           full_par ^= 1u << b;
           tc_fence_after();
-          drain_cols<CW>(tlane + (unsigned)(b * P.NP) + ch * CW, acc);
+          drain_cols<CW, BATCH>(tlane + (unsigned)(b * P.NP) + ch * CW, acc);
           release(b, 0);
         } else {
           // each half is committed on its own barrier.  Both parts drain G = CW - SPLIT columns of each
@@ -748,8 +819,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
           }
           full_par ^= 1u;
           tc_fence_after();
-          drain_cols<G>(tlane + (ch == 0 ? 0 : SPLIT), acc);
-          if (ch == 0) drain_cols<16>(tlane + G, acc + G);
+          // part 0: half 0 columns [0, SPLIT) -> acc[0, SPLIT); part 1: columns [SPLIT, CW) -> acc[0, G)
+          if (ch == 0)
+            drain_cols<SPLIT, BATCH>(tlane, acc);
+          else
+            drain_cols<G, BATCH>(tlane + SPLIT, acc);
           release(0, 0);
           if (!wait_bar(&acc_full[0][1], (full_par >> 1) & 1u)) {
             give_up();
@@ -757,8 +831,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
           }
           full_par ^= 2u;
           tc_fence_after();
-          if (ch != 0) drain_cols<16>(tlane + CW + G, acc + G);
-          drain_cols<G>(tlane + CW + (ch == 0 ? 0 : SPLIT), acc + SPLIT);
+          // part 0: half 1 columns [0, G) -> acc[SPLIT, CW); part 1: columns [G, CW) -> acc[G, CW)
+          if (ch == 0)
+            drain_cols<G, BATCH>(tlane + CW, acc + SPLIT);
+          else
+            drain_cols<CW - G, BATCH>(tlane + CW + G, acc + G);
           release(0, 1);
         }
       }
@@ -774,14 +851,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
       if (cell >= 0) {
         const double sc = *Lv.scale_out;
         double *Lrow = Lv.L + ((long long)cell * P.R + w.rhs) * P.nn;
-        // first accumulator column of this thread's part in each half, and the part's width in half 0
-        const int n0 = NHALF == 1 ? ch * CW : (ch == 0 ? 0 : SPLIT);
-        const int w0 = NHALF == 1 ? CW : (ch == 0 ? SPLIT : CW - SPLIT);
-        const int n1 = NHALF == 1 ? 0 : (ch == 0 ? CW : 2 * CW - SPLIT);
-#pragma unroll
-        for (int i = 0; i < CW; ++i) {
-          const int n = i < w0 ? n0 + i : n1 + (i - w0);
-          if (n < P.nn) atomicAdd(Lrow + n, (double)acc[i] * sc);
+        // the runs of accumulator columns this thread holds, each with its first node index
+        const int nn = P.nn;
+        if constexpr (NHALF == 1) {
+          flush_cols<0, CW>(acc, Lrow + ch * CW, nn - ch * CW, sc);
+        } else {
+          constexpr int G = CW - SPLIT;
+          if (ch == 0) {
+            flush_cols<0, SPLIT>(acc, Lrow, nn, sc);             // half 0, nodes [0, SPLIT)
+            flush_cols<SPLIT, CW>(acc, Lrow + CW, nn - CW, sc);  // half 1, nodes CW + [0, G)
+          } else {
+            flush_cols<0, G>(acc, Lrow + SPLIT, nn - SPLIT, sc);      // half 0, nodes [SPLIT, CW)
+            flush_cols<G, CW>(acc, Lrow + CW + G, nn - CW - G, sc);   // half 1, nodes CW + [G, CW)
+          }
         }
       }
 #pragma unroll
@@ -918,6 +1000,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
     return y;
   };
 
+  if (warp < 4) {
+  give_registers<true>();  // the epilogue holds 128 running sums per thread
   if (warp == 0) {
     if (lane == 0) {
       int stage = 0;
@@ -1016,9 +1100,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
         mma_commit(&done_bar);
       if (!mbar_wait(&done_bar, 0)) give_up();
     }
-  } else if (warp >= 2 && warp <= 9) {
+  }
+  } else {
+    take_registers<true>();
     const int q = warp & 3;
-    const int ch = (warp - 2) >> 2;  // which 128 of the 256 columns
+    const int ch = (warp - 4) >> 2;  // which 128 of the 256 columns
     const int row = q * 32 + lane;   // source cell within the tile
     const unsigned tlane = tmem + ((unsigned)(q * 32) << 16) + (unsigned)(ch * 128);
     const unsigned empty0 = PAIR ? mapa_shared(su32(&acc_empty[0]), 0u) : 0u;
@@ -1036,7 +1122,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
         }
         full_par ^= 1u << b;
         tc_fence_after();
-        drain_cols<128>(tlane + (unsigned)(b * YBLK), acc);
+        drain_cols<128, 4>(tlane + (unsigned)(b * YBLK), acc);
         tc_fence_before();
         __syncwarp();
         if (lane == 0) {
@@ -1348,6 +1434,13 @@ struct DenseTC {
   __half *Yhi[kMaxHeight] = {}, *Ylo[kMaxHeight] = {};
   size_t Ybytes[kMaxHeight] = {};
   int ycht = 0, nblk = 0, ystages = 0, ystage_bytes = 0;
+  // low-rank layout (host side): 16-wide rank chunks of each slot, its first U chunk, the first Y chunk of
+  // each source parity and of each slot among that parity's chunks
+  unsigned char tnk[343] = {};
+  short uchunk0[343] = {};
+  int ybase[8] = {};
+  short ychunk0[8][343] = {};
+  TvRec *tv = nullptr;  // transfer-vector records on the device
   bool ypair = true;                      // first product on CTA pairs (B200FMM_TC_YPAIR=0: single CTAs)
   int lr_shift = 0;                       // sV + sU: the power-of-two pre-scales of V and U
   LrYParams *yparams = nullptr;           // host copy
@@ -1379,12 +1472,12 @@ static b200fmm_status tc_init_lowrank(Context &c, DenseTC &t, TcParams &P, bool 
   int uch = 0;
   for (int s = 0; s < 343; ++s) t.lr_rank[s] = toff[s] < 0 ? 0 : trank[s];
   for (int s = 0; s < 343; ++s) {
-    P.tnk[s] = 0;
-    P.uchunk0[s] = 0;
+    t.tnk[s] = 0;
+    t.uchunk0[s] = 0;
     if (toff[s] < 0) continue;
-    P.tnk[s] = (unsigned char)((trank[s] + 15) / 16);
-    P.uchunk0[s] = (short)uch;
-    uch += P.tnk[s];
+    t.tnk[s] = (unsigned char)((trank[s] + 15) / 16);
+    t.uchunk0[s] = (short)uch;
+    uch += t.tnk[s];
   }
   // the slots whose sources lie in each parity grid: target parity c + offset of its entry, per axis
   std::vector<std::array<bool, 343>> need(8);
@@ -1397,15 +1490,15 @@ static b200fmm_status tc_init_lowrank(Context &c, DenseTC &t, TcParams &P, bool 
     }
   int ych = 0, maxch = 0;
   for (int sp = 0; sp < 8; ++sp) {
-    P.ybase[sp] = ych;
+    t.ybase[sp] = ych;
     int k = 0;
     double rsum = 0;
     for (int s = 0; s < 343; ++s) {
-      P.ychunk0[sp][s] = 0;
+      t.ychunk0[sp][s] = 0;
       if (!need[sp][s]) continue;
-      if (P.tnk[s] == 0) return fail(B200FMM_ERR_INVALID, "low-rank M2L: an interaction slot has no operator");
-      P.ychunk0[sp][s] = (short)k;
-      k += P.tnk[s];
+      if (t.tnk[s] == 0) return fail(B200FMM_ERR_INVALID, "low-rank M2L: an interaction slot has no operator");
+      t.ychunk0[sp][s] = (short)k;
+      k += t.tnk[s];
       rsum += trank[s];
     }
     t.lr_rank_fed[sp] = rsum;
@@ -1461,12 +1554,12 @@ static b200fmm_status tc_init_lowrank(Context &c, DenseTC &t, TcParams &P, bool 
   for (int s = 0; s < 343; ++s) {
     if (toff[s] < 0) continue;
     const int r = trank[s];
-    for (int kc = 0; kc < P.tnk[s]; ++kc)
+    for (int kc = 0; kc < t.tnk[s]; ++kc)
       for (int n = 0; n < t.NP; ++n)
         for (int i = 0; i < 16; ++i) {
           const int a = kc * 16 + i;
           const double v = (n < nn && a < r) ? std::ldexp(Ut[toff[s] + (size_t)n * r + a], sU) : 0.0;
-          const size_t o = ((size_t)(P.uchunk0[s] + kc) * t.NP + n) * 16 + i;
+          const size_t o = ((size_t)(t.uchunk0[s] + kc) * t.NP + n) * 16 + i;
           split(v, uh[o], ul[o]);
         }
   }
@@ -1476,10 +1569,10 @@ static b200fmm_status tc_init_lowrank(Context &c, DenseTC &t, TcParams &P, bool 
     for (int s = 0; s < 343; ++s) {
       if (!need[sp][s]) continue;
       const int r = trank[s];
-      for (int kc = 0; kc < P.tnk[s]; ++kc)
+      for (int kc = 0; kc < t.tnk[s]; ++kc)
         for (int i = 0; i < 16; ++i) {
           const int a = kc * 16 + i;
-          const size_t row = (size_t)(P.ybase[sp] + P.ychunk0[sp][s] + kc) * 16 + i;
+          const size_t row = (size_t)(t.ybase[sp] + t.ychunk0[sp][s] + kc) * 16 + i;
           for (int n = 0; n < t.KP; ++n) {
             const double v = (n < nn && a < r) ? std::ldexp(Vt[toff[s] + (size_t)n * r + a], sV) : 0.0;
             split(v, vh[row * t.KP + n], vl[row * t.KP + n]);
@@ -1512,7 +1605,7 @@ static b200fmm_status tc_init_lowrank(Context &c, DenseTC &t, TcParams &P, bool 
     B200_CHECK(encode(&Y.mapV_hi, t.Vhi, 2, dims, strides, box));
     B200_CHECK(encode(&Y.mapV_lo, t.Vlo, 2, dims, strides, box));
   }
-  for (int sp = 0; sp <= 8; ++sp) Y.ybase[sp] = sp < 8 ? P.ybase[sp] : ych;
+  for (int sp = 0; sp <= 8; ++sp) Y.ybase[sp] = sp < 8 ? t.ybase[sp] : ych;
   Y.ycht = ych;
   Y.nblk = t.nblk;
   Y.NK = t.NK;
@@ -1559,11 +1652,36 @@ b200fmm_status tc_init(Context &c) {
   if (const char *e = getenv("B200FMM_TC_LOWRANK")) lr = lr && atoi(e) != 0;
   if (lr) B200_CHECK(tc_init_lowrank(c, *t, *t->params, lr));
   t->lr = lr;
+  {
+    // the transfer-vector records of both forms
+    std::vector<TvRec> tv(8 * 189);
+    for (int ct = 0; ct < 8; ++ct)
+      for (int e = 0; e < 189; ++e) {
+        const int cax[3] = {(ct >> 2) & 1, (ct >> 1) & 1, ct & 1};
+        int sp = 0, o[3];
+        for (int a = 0; a < 3; ++a) {
+          const int v = cax[a] + c.itab.off[ct][e][a];  // source position in child cells
+          o[a] = v >= 0 ? v / 2 : -((1 - v) / 2);       // floor(v / 2): the source tile's offset
+          sp = (sp << 1) | (v & 1);
+        }
+        const int slot = c.itab.slot[ct][e];
+        TvRec &r = tv[ct * 189 + e];
+        r.ox = (signed char)o[0];
+        r.oy = (signed char)o[1];
+        r.oz = (signed char)o[2];
+        r.ya = (short)(lr ? t->ybase[sp] + t->ychunk0[sp][slot] : sp);
+        r.ub = (short)(lr ? t->uchunk0[slot] : slot);
+        r.nk = lr ? t->tnk[slot] : 0;
+      }
+    B200_CUDA(cudaMalloc(&t->tv, tv.size() * sizeof(TvRec)));
+    B200_CUDA(cudaMemcpy(t->tv, tv.data(), tv.size() * sizeof(TvRec), cudaMemcpyHostToDevice));
+    t->params->tv = t->tv;
+  }
   const int rowb = lr ? 32 : 64;  // bytes per operand row of a stage: 16 or 32 fp16 of K
   // a CTA of a pair holds NP / 2 rows of each operator chunk: NH / 2 rows of each column half
   const int b_rows = t->pair ? t->NP / 2 : t->NP;
   t->stage_bytes = 2 * (TILE_X * TILE_Y * TILE_Z * rowb) + 2 * b_rows * rowb;
-  t->stages = std::min((t->pair || lr) ? MAX_STAGES : MAX_STAGES_SINGLE, (220 * 1024) / t->stage_bytes);
+  t->stages = std::min((t->pair || lr) ? MAX_STAGES : MAX_STAGES_SINGLE, (220 * 1024 - TV_BYTES) / t->stage_bytes);
   if (t->stages < 2) return fail(B200FMM_ERR_UNSUPPORTED, "stage buffers do not fit in shared memory");
   t->nbuf = 2 * t->NP <= 512 ? 2 : 1;
   t->ncols = 32;
@@ -1599,7 +1717,7 @@ b200fmm_status tc_init(Context &c) {
     at[0].val.clusterDim.x = 2;
     at[0].val.clusterDim.y = 1;
     at[0].val.clusterDim.z = 1;
-    const size_t smem = (size_t)t->stages * t->stage_bytes + 1024;
+    const size_t smem = (size_t)t->stages * t->stage_bytes + TV_BYTES + 1024;
     cfg.gridDim = dim3(dev_sms & ~1);
     cfg.blockDim = dim3(TC_THREADS);
     cfg.dynamicSmemBytes = smem;
@@ -1635,6 +1753,30 @@ b200fmm_status tc_init(Context &c) {
     }
     t->grid = 2 * std::min(nclusters, dev_sms / 2);
   }
+  {
+    // the kernels that move registers between warpgroups must run with exactly the registers the split
+    // assumes, or their setmaxnreg.inc would wait for registers that were never allocated
+    cudaFuncAttributes fa;
+    bool regs_ok = true;
+    auto check_regs = [&](auto kern) {
+      if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess || fa.numRegs != TC_REGS) regs_ok = false;
+    };
+    check_regs(lr_y_kernel<true>);
+    check_regs(lr_y_kernel<false>);
+    check_regs(m2l_tc_kernel<176, 2, true, true>);
+    check_regs(m2l_tc_kernel<176, 2, true, false>);
+    check_regs(m2l_tc_kernel<176, 2, false, true>);
+    check_regs(m2l_tc_kernel<176, 2, false, false>);
+    check_regs(m2l_tc_kernel<112, 1, true, true>);
+    check_regs(m2l_tc_kernel<112, 1, true, false>);
+    check_regs(m2l_tc_kernel<112, 1, false, true>);
+    check_regs(m2l_tc_kernel<112, 1, false, false>);
+    if (!regs_ok) {
+      cudaGetLastError();
+      return fail(B200FMM_ERR_UNSUPPORTED, "tensor-core M2L: kernels not compiled to the register count their "
+                                           "warpgroup register split needs");
+    }
+  }
   if (lr) {
     const int ysmem = t->ystages * t->ystage_bytes + 1024;
     if (t->ypair)
@@ -1649,7 +1791,7 @@ void tc_free(Context &c) {
   DenseTC *t = c.tc;
   if (!t) return;
   for (void *p : {(void *)t->Bhi, (void *)t->Blo, (void *)t->scal, (void *)t->amax, (void *)t->prefix, (void *)t->busy,
-                  (void *)t->Vhi, (void *)t->Vlo})
+                  (void *)t->Vhi, (void *)t->Vlo, (void *)t->tv})
     if (p) cudaFree(p);
   for (int l = 0; l < kMaxHeight; ++l) {
     if (t->Ahi[l]) cudaFree(t->Ahi[l]);
@@ -1874,7 +2016,7 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
   P.u_begin = P.lv[l1].unit0;
   P.u_end = P.lv[l0].unit0 + P.lv[l0].nunits;
   if (P.u_end <= P.u_begin) return B200FMM_OK;
-  const size_t smem = (size_t)t->stages * t->stage_bytes + 1024;
+  const size_t smem = (size_t)t->stages * t->stage_bytes + TV_BYTES + 1024;
   const int grid = t->grid;  // persistent: one CTA (pair) per SM (pair of SMs)
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute at[1];
