@@ -630,7 +630,12 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
     B200_CUDA(cudaMemcpyAsync(c.d_stage, x, sizeof(double) * n, cudaMemcpyHostToDevice, s));
     B200_CUDA(cudaMemcpyAsync(c.d_stage + n, y, sizeof(double) * n, cudaMemcpyHostToDevice, s));
     B200_CUDA(cudaMemcpyAsync(c.d_stage + 2 * n, z, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    B200_CUDA(cudaMemcpyAsync(c.d_stage + 3 * n, q, sizeof(double) * n * c.R, cudaMemcpyHostToDevice, s));
+    // the charges are first read by the gather after the sort: their copy, on the second stream, runs
+    // beside the keys and the sort (forked after the coordinates, joined before the gather)
+    B200_CUDA(cudaEventRecord(c.ev_fork, s));
+    B200_CUDA(cudaStreamWaitEvent(c.stream2, c.ev_fork, 0));
+    B200_CUDA(cudaMemcpyAsync(c.d_stage + 3 * n, q, sizeof(double) * n * c.R, cudaMemcpyHostToDevice, c.stream2));
+    B200_CUDA(cudaEventRecord(c.ev_join, c.stream2));
     dx = c.d_stage;
     dy = c.d_stage + n;
     dz = c.d_stage + 2 * n;
@@ -656,6 +661,7 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
     std::swap(k0, k1);
     std::swap(v0, v1);
   }
+  if (!on_device) B200_CUDA(cudaStreamWaitEvent(s, c.ev_join, 0));
   gather_particles<<<grid_for(n, 256), 256, 0, s>>>(n, c.R, v0, dx, dy, dz, dq, c.d_x, c.d_y, c.d_z, c.d_q, c.d_perm);
   head_flags<<<grid_for(n, 256), 256, 0, s>>>(n, k0, 0, flags);
   c.tree_launches += 2;
