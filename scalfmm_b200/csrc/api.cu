@@ -148,7 +148,7 @@ void destroy_context(b200fmm_context *c) {
   drop_graph(*c);
   free_tree(*c);
   tc_free(*c);
-  for (void *p : {(void *)c->d_roots, (void *)c->d_Troots, (void *)c->d_S, (void *)c->d_pindices, (void *)c->d_pvec,
+  for (void *p : {(void *)c->d_roots, (void *)c->d_S, (void *)c->d_pindices, (void *)c->d_pvec,
                   (void *)c->d_symU, (void *)c->d_symV, (void *)c->d_symoff, (void *)c->d_symrank,
                   (void *)c->d_dense, (void *)c->d_itab, (void *)c->d_class_order, (void *)c->d_cls_bounds,
                   (void *)c->d_cls_slots, (void *)c->d_status, (void *)c->d_Ut, (void *)c->d_Vt,

@@ -71,7 +71,6 @@ struct Context {
 
   // interpolation tables (device)
   double *d_roots = nullptr;     // [p]
-  double *d_Troots = nullptr;    // [p][p]  T_o(root_j) (Chebyshev only)
   double *d_S = nullptr;         // [8][3][p][p] child->parent 1-D interpolators
 
   // symmetric compressed operators (host copy + device)
@@ -177,6 +176,8 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
 b200fmm_status upload_charges(Context &c, const double *q, bool on_device);
 void free_tree(Context &c);
 // interp.cu
+// the interpolation nodes and Chebyshev values of the handle's order into the device's constant tables
+b200fmm_status upload_basis_constants(const Context &c, const double *roots, const double *Tr);
 b200fmm_status run_p2m(Context &c);
 b200fmm_status run_m2m(Context &c, int level);
 b200fmm_status run_l2l(Context &c, int level);

@@ -15,14 +15,20 @@ namespace b200 {
 
 namespace {
 
+// Interpolation nodes of every built order (3..8) and basis (Chebyshev, Lagrange), and the Chebyshev values
+// T_o(node_j): read by P2M and L2P as constant-bank operands, so that the tables hold no registers.  Set per
+// device when a handle builds its tables (upload_basis_constants); every handle of an order and basis writes
+// the same values.
+__constant__ double c_roots[2][kMaxOrder - 2][kMaxOrder];      // [basis: 1 = Lagrange][p - 3][j]
+__constant__ double c_Tr[kMaxOrder - 2][kMaxOrder * kMaxOrder];  // [p - 3][o * p + j], Chebyshev
 
 // S_j(x) and dS_j/dx for j < p.  Chebyshev: 1/p + 2/p sum_o T_o(x) T_o(xbar_j), dT_o = o U_{o-1}.
 // Lagrange (equispaced nodes): prod_{m != j} (x - x_m) / (x_j - x_m) and its derivative.  Compile-time order
 // and basis, every loop unrolled, so that S and dS stay in registers.
 template <int P, bool LAGR>
-__device__ __forceinline__ void basis_eval(double x, const double *__restrict__ roots,
-                                           const double *__restrict__ Tr, double *S, double *dS) {
+__device__ __forceinline__ void basis_eval(double x, double *S, double *dS) {
   constexpr int p = P;
+  const double *roots = c_roots[LAGR ? 1 : 0][P - 3];
   if constexpr (LAGR) {
     if (x > 1.0) x = 1.0;
     if (x < -1.0) x = -1.0;
@@ -66,7 +72,7 @@ __device__ __forceinline__ void basis_eval(double x, const double *__restrict__ 
       double s = ip, ds = 0.0;
 #pragma unroll
       for (int o = 1; o < p; ++o) {
-        const double t = 2.0 * ip * Tr[o * p + j];
+        const double t = 2.0 * ip * c_Tr[P - 3][o * p + j];
         s += T[o] * t;
         ds += (double)o * U[o - 1] * t;
       }
@@ -89,7 +95,7 @@ __global__ void __launch_bounds__(P2M_THREADS, 8) p2m_kernel(
     int R, long long N, long long nleaves, const long long *__restrict__ keys,
     const long long *__restrict__ leaf_start, const double *__restrict__ x, const double *__restrict__ y,
     const double *__restrict__ z, const double *__restrict__ q, double cx0, double cy0, double cz0, double leaf_w,
-    const double *__restrict__ roots, const double *__restrict__ Tr, double *__restrict__ M) {
+    double *__restrict__ M) {
   constexpr int p = P, nn = P * P * P, PX = (P + 1) & ~1;  // Sx rows padded to 16 bytes
   __shared__ __align__(16) double Wx[P2M_THREADS][PX];
   __shared__ double Wy[P2M_THREADS][P], Wz[P2M_THREADS][P], Q[P2M_THREADS];
@@ -115,7 +121,7 @@ __global__ void __launch_bounds__(P2M_THREADS, 8) p2m_kernel(
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
           const double a = ctr[d] - leaf_w / 2, bb = ctr[d] + leaf_w / 2;
-          basis_eval<P, LAGR>((2.0 * pos[d] - bb - a) / (bb - a), roots, Tr, wv, nullptr);
+          basis_eval<P, LAGR>((2.0 * pos[d] - bb - a) / (bb - a), wv, nullptr);
           double *dst = d == 0 ? Wx[t] : (d == 1 ? Wy[t] : Wz[t]);
 #pragma unroll
           for (int k = 0; k < p; ++k) dst[k] = wv[k];
@@ -258,7 +264,7 @@ __global__ void __launch_bounds__(L2P_WARPS * 32) l2p_kernel(
     int R, long long N, long long nleaves, const long long *__restrict__ keys,
     const long long *__restrict__ leaf_start, const double *__restrict__ x, const double *__restrict__ y,
     const double *__restrict__ z, const double *__restrict__ q, double cx0, double cy0, double cz0, double leaf_w,
-    const double *__restrict__ roots, const double *__restrict__ Tr, const double *__restrict__ L,
+    const double *__restrict__ L,
     double *__restrict__ phi, double *__restrict__ fx, double *__restrict__ fy, double *__restrict__ fz) {
   constexpr int p = P, nn = P * P * P;
   __shared__ double sL[L2P_WARPS][nn];
@@ -281,20 +287,20 @@ __global__ void __launch_bounds__(L2P_WARPS * 32) l2p_kernel(
       double wx[P], dwx[P];
       {
         double t[P], dt[P];
-        basis_eval<P, LAGR>((2.0 * y[i] - 2.0 * cy) / leaf_w, roots, Tr, t, dt);
+        basis_eval<P, LAGR>((2.0 * y[i] - 2.0 * cy) / leaf_w, t, dt);
 #pragma unroll
         for (int k = 0; k < p; ++k) {
           wy[k] = t[k];
           dwy[k] = dt[k];
         }
-        basis_eval<P, LAGR>((2.0 * z[i] - 2.0 * cz) / leaf_w, roots, Tr, t, dt);
+        basis_eval<P, LAGR>((2.0 * z[i] - 2.0 * cz) / leaf_w, t, dt);
 #pragma unroll
         for (int k = 0; k < p; ++k) {
           wz[k] = t[k];
           dwz[k] = dt[k];
         }
       }
-      basis_eval<P, LAGR>((2.0 * x[i] - 2.0 * cx) / leaf_w, roots, Tr, wx, dwx);
+      basis_eval<P, LAGR>((2.0 * x[i] - 2.0 * cx) / leaf_w, wx, dwx);
       double pv = 0, gx = 0, gy = 0, gz = 0;
 #pragma unroll 1
       for (int kz = 0; kz < p; ++kz) {
@@ -332,6 +338,17 @@ __global__ void __launch_bounds__(L2P_WARPS * 32) l2p_kernel(
 
 }  // namespace
 
+b200fmm_status upload_basis_constants(const Context &c, const double *roots, const double *Tr) {
+  const int p = c.p;
+  if (p < 3 || p > kMaxOrder) return B200FMM_OK;  // no P2M / L2P kernel is built for this order
+  const int lag = c.cfg.kernel == B200FMM_LAGRANGE ? 1 : 0;
+  B200_CUDA(cudaMemcpyToSymbol(c_roots, roots, sizeof(double) * p,
+                               sizeof(double) * ((size_t)(lag * (kMaxOrder - 2) + p - 3) * kMaxOrder)));
+  if (!lag)
+    B200_CUDA(cudaMemcpyToSymbol(c_Tr, Tr, sizeof(double) * p * p, sizeof(double) * (size_t)(p - 3) * kMaxOrder * kMaxOrder));
+  return B200FMM_OK;
+}
+
 b200fmm_status run_p2m(Context &c) {
   const int LL = c.H - 1;
   const Level &L = c.lv[LL];
@@ -344,12 +361,10 @@ b200fmm_status run_p2m(Context &c) {
   case PV:                                                                                                  \
     if (lagr)                                                                                               \
       p2m_kernel<PV, true><<<(unsigned)L.n, P2M_THREADS, 0, c.stream>>>(                                     \
-          c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, x0, y0, z0, lw, c.d_roots,        \
-          c.d_Troots, L.M);                                                                                 \
+          c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, x0, y0, z0, lw, L.M);              \
     else                                                                                                    \
       p2m_kernel<PV, false><<<(unsigned)L.n, P2M_THREADS, 0, c.stream>>>(                                    \
-          c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, x0, y0, z0, lw, c.d_roots,        \
-          c.d_Troots, L.M);                                                                                 \
+          c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, x0, y0, z0, lw, L.M);              \
     break;
   switch (c.p) {
     B200_P2M(3) B200_P2M(4) B200_P2M(5) B200_P2M(6) B200_P2M(7) B200_P2M(8)
@@ -413,12 +428,12 @@ b200fmm_status run_l2p(Context &c) {
   case PV:                                                                                                   \
     if (lagr)                                                                                                \
       l2p_kernel<PV, true><<<grid_for(L.n, L2P_WARPS), L2P_WARPS * 32, 0, c.stream>>>(                      \
-          c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, x0, y0, z0, lw, c.d_roots,         \
-          c.d_Troots, L.L, c.d_phi, c.d_fx, c.d_fy, c.d_fz);                                                 \
+          c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, x0, y0, z0, lw, L.L, c.d_phi,       \
+          c.d_fx, c.d_fy, c.d_fz);                                                 \
     else                                                                                                     \
       l2p_kernel<PV, false><<<grid_for(L.n, L2P_WARPS), L2P_WARPS * 32, 0, c.stream>>>(                     \
-          c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, x0, y0, z0, lw, c.d_roots,         \
-          c.d_Troots, L.L, c.d_phi, c.d_fx, c.d_fy, c.d_fz);                                                 \
+          c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, x0, y0, z0, lw, L.L, c.d_phi,       \
+          c.d_fx, c.d_fy, c.d_fz);                                                 \
     break;
   switch (c.p) {
     B200_L2P(3) B200_L2P(4) B200_L2P(5) B200_L2P(6) B200_L2P(7) B200_L2P(8)

@@ -258,11 +258,10 @@ b200fmm_status build_tables(Context &c) {
       }
   }
   B200_CUDA(cudaMalloc(&c.d_roots, sizeof(double) * p));
-  B200_CUDA(cudaMalloc(&c.d_Troots, sizeof(double) * p * p));
   B200_CUDA(cudaMalloc(&c.d_S, sizeof(double) * S.size()));
   B200_CUDA(cudaMemcpy(c.d_roots, roots.data(), sizeof(double) * p, cudaMemcpyHostToDevice));
-  B200_CUDA(cudaMemcpy(c.d_Troots, Tr.data(), sizeof(double) * p * p, cudaMemcpyHostToDevice));
   B200_CUDA(cudaMemcpy(c.d_S, S.data(), sizeof(double) * S.size(), cudaMemcpyHostToDevice));
+  B200_CHECK(upload_basis_constants(c, roots.data(), Tr.data()));
   build_itab(c.itab);
   B200_CUDA(cudaMalloc(&c.d_itab, sizeof(IListTable)));
   B200_CUDA(cudaMemcpy(c.d_itab, &c.itab, sizeof(IListTable), cudaMemcpyHostToDevice));
