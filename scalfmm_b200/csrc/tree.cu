@@ -625,17 +625,26 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
   if (!c.d_err) B200_CUDA(cudaMalloc(&c.d_err, 32 + sizeof(unsigned long long) * kMaxHeight));
   // inputs on the device
   const double *dx = x, *dy = y, *dz = z, *dq = q;
+  bool q_forked = false;  // the charge copy runs on the second stream
   if (!on_device) {
     B200_CHECK(grow(c, c.d_stage, c.cap_stage, (size_t)n * (3 + c.R)));
     B200_CUDA(cudaMemcpyAsync(c.d_stage, x, sizeof(double) * n, cudaMemcpyHostToDevice, s));
     B200_CUDA(cudaMemcpyAsync(c.d_stage + n, y, sizeof(double) * n, cudaMemcpyHostToDevice, s));
     B200_CUDA(cudaMemcpyAsync(c.d_stage + 2 * n, z, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    // the charges are first read by the gather after the sort: their copy, on the second stream, runs
-    // beside the keys and the sort (forked after the coordinates, joined before the gather)
-    B200_CUDA(cudaEventRecord(c.ev_fork, s));
-    B200_CUDA(cudaStreamWaitEvent(c.stream2, c.ev_fork, 0));
-    B200_CUDA(cudaMemcpyAsync(c.d_stage + 3 * n, q, sizeof(double) * n * c.R, cudaMemcpyHostToDevice, c.stream2));
-    B200_CUDA(cudaEventRecord(c.ev_join, c.stream2));
+    // the charges are first read by the gather after the sort.  From page-locked memory their copy runs on
+    // the second stream beside the keys and the sort (forked after the coordinates, joined before the
+    // gather); a pageable buffer is copied in order, since such a copy is staged by the host anyway.
+    cudaPointerAttributes qa{};
+    q_forked = cudaPointerGetAttributes(&qa, q) == cudaSuccess && qa.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    if (q_forked) {
+      B200_CUDA(cudaEventRecord(c.ev_fork, s));
+      B200_CUDA(cudaStreamWaitEvent(c.stream2, c.ev_fork, 0));
+      B200_CUDA(cudaMemcpyAsync(c.d_stage + 3 * n, q, sizeof(double) * n * c.R, cudaMemcpyHostToDevice, c.stream2));
+      B200_CUDA(cudaEventRecord(c.ev_join, c.stream2));
+    } else {
+      B200_CUDA(cudaMemcpyAsync(c.d_stage + 3 * n, q, sizeof(double) * n * c.R, cudaMemcpyHostToDevice, s));
+    }
     dx = c.d_stage;
     dy = c.d_stage + n;
     dz = c.d_stage + 2 * n;
@@ -661,7 +670,7 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
     std::swap(k0, k1);
     std::swap(v0, v1);
   }
-  if (!on_device) B200_CUDA(cudaStreamWaitEvent(s, c.ev_join, 0));
+  if (q_forked) B200_CUDA(cudaStreamWaitEvent(s, c.ev_join, 0));
   gather_particles<<<grid_for(n, 256), 256, 0, s>>>(n, c.R, v0, dx, dy, dz, dq, c.d_x, c.d_y, c.d_z, c.d_q, c.d_perm);
   head_flags<<<grid_for(n, 256), 256, 0, s>>>(n, k0, 0, flags);
   c.tree_launches += 2;
