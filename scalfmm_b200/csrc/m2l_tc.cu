@@ -1237,9 +1237,18 @@ __global__ void sat_pass_kernel(const __grid_constant__ TcParams P, const __grid
   }
 }
 
-// busy masks of every level: one thread per (tile, transfer vector); tiles are numbered across levels
+// Whether a box of a parity grid holds a cell when its level is full (every cell of the level exists):
+// the parity grids then hold exactly the positions [0, side / 2) on each axis.
+__device__ __forceinline__ bool box_nonempty_full(const TcLevel &L, int x0, int y0, int z0, int nx, int ny, int nz) {
+  const int h = L.side >> 1;
+  return x0 < h && x0 + nx > 0 && y0 < h && y0 + ny > 0 && z0 < h && z0 + nz > 0;
+}
+
+// busy masks of every level: one thread per (tile, transfer vector); tiles are numbered across levels.  Bit l
+// of full_levels marks a full level, whose boxes are tested by their bounds instead of the summed-area
+// tables (which are then not built when every level is full).
 __global__ void busy_mask_kernel(const __grid_constant__ TcParams P, int l0, int l1, long long ntiles,
-                                 unsigned *__restrict__ busy) {
+                                 unsigned full_levels, unsigned *__restrict__ busy) {
   const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (g >= ntiles * 189) return;
   const long long tg = g / 189;
@@ -1257,9 +1266,16 @@ __global__ void busy_mask_kernel(const __grid_constant__ TcParams P, int l0, int
   w.parity = (short)(tl / ((long long)TX * TY * TZ));
   unsigned *m = busy + 6 * tg;
   const SrcBox b = src_box(P, w, w.bz, e);
-  if (box_count(L, b.sp, b.ox, b.oy, b.oz, TILE_X, TILE_Y, TILE_Z) > 0) atomicOr(m + (e >> 5), 1u << (e & 31));
-  if (e == 0 && box_count(L, w.parity, w.bx * TILE_X, w.by * TILE_Y, w.bz * TILE_Z, TILE_X, TILE_Y, TILE_Z) > 0)
-    atomicOr(m + 5, 1u << 31);
+  const bool full = (full_levels >> level) & 1u;
+  const bool src = full ? box_nonempty_full(L, b.ox, b.oy, b.oz, TILE_X, TILE_Y, TILE_Z)
+                        : box_count(L, b.sp, b.ox, b.oy, b.oz, TILE_X, TILE_Y, TILE_Z) > 0;
+  if (src) atomicOr(m + (e >> 5), 1u << (e & 31));
+  if (e == 0) {
+    const int x0 = w.bx * TILE_X, y0 = w.by * TILE_Y, z0 = w.bz * TILE_Z;
+    const bool tgt = full ? box_nonempty_full(L, x0, y0, z0, TILE_X, TILE_Y, TILE_Z)
+                          : box_count(L, w.parity, x0, y0, z0, TILE_X, TILE_Y, TILE_Z) > 0;
+    if (tgt) atomicOr(m + 5, 1u << 31);
+  }
 }
 
 // Work of every unit of levels [P.l0, P.l1]: the number of transfer vectors with an occupied source box when
@@ -1958,17 +1974,25 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
       C.lines[2][l + 1] = C.lines[2][l] + 8 * (HY + 1) * (HX + 1);
     }
     const TcParams &P0 = *t->params;
-    B200_CUDA(cudaMemsetAsync(t->sat, 0, t->satn * sizeof(int), c.stream));
+    // full levels (every cell present, as in uniform trees) need no occupancy tables
+    unsigned full_levels = 0;
+    for (int l = 2; l <= LL; ++l)
+      if (c.lv[l].n == (1LL << (3 * l))) full_levels |= 1u << l;
+    const bool all_full = full_levels == (((1u << (LL + 1)) - 1u) & ~3u);
     B200_CUDA(cudaMemsetAsync(t->busy, 0, sizeof(unsigned) * 6 * t->ntiles_all, c.stream));
-    if (C.start[LL + 1] > 0) {
-      occ_mark_kernel<<<grid_for(C.start[LL + 1], 256), 256, 0, c.stream>>>(P0, C);
-      ++c.launches;
+    if (!all_full) {
+      B200_CUDA(cudaMemsetAsync(t->sat, 0, t->satn * sizeof(int), c.stream));
+      if (C.start[LL + 1] > 0) {
+        occ_mark_kernel<<<grid_for(C.start[LL + 1], 256), 256, 0, c.stream>>>(P0, C);
+        ++c.launches;
+      }
+      for (int a = 0; a < 3; ++a) {
+        sat_pass_kernel<<<grid_for(C.lines[a][LL + 1], 128), 128, 0, c.stream>>>(P0, C, a);
+        ++c.launches;
+      }
     }
-    for (int a = 0; a < 3; ++a) {
-      sat_pass_kernel<<<grid_for(C.lines[a][LL + 1], 128), 128, 0, c.stream>>>(P0, C, a);
-      ++c.launches;
-    }
-    busy_mask_kernel<<<grid_for(t->ntiles_all * 189, 256), 256, 0, c.stream>>>(P0, 2, LL, t->ntiles_all, t->busy);
+    busy_mask_kernel<<<grid_for(t->ntiles_all * 189, 256), 256, 0, c.stream>>>(P0, 2, LL, t->ntiles_all, full_levels,
+                                                                                 t->busy);
     // the work of every unit of every level and its prefix sums, from which each launch splits its units
     // into ranges of equal work
     TcParams Pw = P0;
