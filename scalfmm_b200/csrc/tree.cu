@@ -433,6 +433,16 @@ __global__ void leaf_column_keys(long long nleaves, const long long *__restrict_
   v[i] = (int)i;
 }
 
+// The same order for a full leaf level (every cell a leaf, so leaf i has Morton key i): the leaf at column
+// position r = (x * side + y) * side + z is the cell (x, y, z).
+__global__ void full_column_order(long long nleaves, int LL, int *__restrict__ order) {
+  const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (r >= nleaves) return;
+  const long long side = 1LL << LL;
+  const int ix = (int)(r / (side * side)), iy = (int)((r / side) % side), iz = (int)(r % side);
+  order[r] = (int)morton_encode3(ix, iy, iz);
+}
+
 __global__ void leaf_rank_kernel(long long nleaves, const int *__restrict__ order,
                                  const long long *__restrict__ leaf_start, int *__restrict__ rank_of,
                                  long long *__restrict__ nrec) {
@@ -796,15 +806,21 @@ b200fmm_status leaf_column_order(Context &c) {
   int *v0 = c.d_sortv, *v1 = c.d_sortv + nl;
   const long long nb = (nl + RS_TILE - 1) / RS_TILE;
   unsigned *cnt = c.d_cnt, *off = c.d_cnt + RS_BINS * nb;
-  leaf_column_keys<<<grid_for(nl, 256), 256, 0, s>>>(nl, c.lv[LL].keys, LL, k0, v0);
-  ++c.launches;
-  for (int sh = 0; sh < 2 * LL; sh += 4) {
-    rs_hist<<<(unsigned)nb, RS_THREADS, 0, s>>>(k0, nl, sh, (int)nb, cnt);
-    B200_CHECK(scan_u32(c, cnt, off, RS_BINS * nb, (unsigned *)c.d_scan));
-    rs_scatter<<<(unsigned)nb, RS_THREADS, 0, s>>>(k0, v0, k1, v1, nl, sh, (int)nb, off);
-    c.launches += 2;
-    std::swap(k0, k1);
-    std::swap(v0, v1);
+  if (nl == (1LL << (3 * LL))) {
+    // a full leaf level (uniform trees): the order follows from the cell coordinates
+    full_column_order<<<grid_for(nl, 256), 256, 0, s>>>(nl, LL, v0);
+    ++c.launches;
+  } else {
+    leaf_column_keys<<<grid_for(nl, 256), 256, 0, s>>>(nl, c.lv[LL].keys, LL, k0, v0);
+    ++c.launches;
+    for (int sh = 0; sh < 2 * LL; sh += 4) {
+      rs_hist<<<(unsigned)nb, RS_THREADS, 0, s>>>(k0, nl, sh, (int)nb, cnt);
+      B200_CHECK(scan_u32(c, cnt, off, RS_BINS * nb, (unsigned *)c.d_scan));
+      rs_scatter<<<(unsigned)nb, RS_THREADS, 0, s>>>(k0, v0, k1, v1, nl, sh, (int)nb, off);
+      c.launches += 2;
+      std::swap(k0, k1);
+      std::swap(v0, v1);
+    }
   }
   long long *nrec = c.d_flags;
   leaf_rank_kernel<<<grid_for(nl, 256), 256, 0, s>>>(nl, v0, c.d_leaf_start, c.d_leaf_rank, nrec);
