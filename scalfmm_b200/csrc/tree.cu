@@ -369,23 +369,26 @@ __device__ __forceinline__ int level_at(const LevelCellsT &C, long long g) {
   return l;
 }
 
-__global__ void leaf_neighbors_kernel(long long nleaves, const long long *__restrict__ keys, int height,
+// One thread per (leaf, neighbour position).  In a full leaf level (every cell a leaf) leaf i has Morton key
+// i, so the neighbour's index is its key; otherwise it is found by binary search.
+__global__ void leaf_neighbors_kernel(long long nleaves, const long long *__restrict__ keys, int height, int full,
                                       int *__restrict__ nbr) {
-  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (c >= nleaves) return;
+  const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (g >= nleaves * 27) return;
+  const long long c = g / 27;
+  const int p = (int)(g % 27);
   int ix, iy, iz;
   morton_decode3(keys[c], ix, iy, iz);
   const int lim = 1 << (height - 1);
-  for (int p = 0; p < 27; ++p) {
-    const int dx = p / 9 - 1, dy = (p / 3) % 3 - 1, dz = p % 3 - 1;
-    int v = -1;
-    if (p == 13) {
-      v = (int)c;
-    } else if (ix + dx >= 0 && ix + dx < lim && iy + dy >= 0 && iy + dy < lim && iz + dz >= 0 && iz + dz < lim) {
-      v = find_key(keys, nleaves, morton_encode3(ix + dx, iy + dy, iz + dz));
-    }
-    nbr[c * 27 + p] = v;
+  const int dx = p / 9 - 1, dy = (p / 3) % 3 - 1, dz = p % 3 - 1;
+  int v = -1;
+  if (p == 13) {
+    v = (int)c;
+  } else if (ix + dx >= 0 && ix + dx < lim && iy + dy >= 0 && iy + dy < lim && iz + dz >= 0 && iz + dz < lim) {
+    const long long key = morton_encode3(ix + dx, iy + dy, iz + dz);
+    v = full ? (int)key : find_key(keys, nleaves, key);
   }
+  nbr[g] = v;
 }
 
 __global__ void ilist_kernel(const __grid_constant__ LevelCellsT C, const IListTable *__restrict__ tab) {
@@ -733,7 +736,8 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
     c.tree_launches += 3;
   }
   // neighbour and interaction lists, dense grids
-  leaf_neighbors_kernel<<<grid_for(nleaves, 128), 128, 0, s>>>(nleaves, leaf.keys, H, c.d_leaf_nbr);
+  leaf_neighbors_kernel<<<grid_for(nleaves * 27, 256), 256, 0, s>>>(nleaves, leaf.keys, H,
+                                                                    nleaves == (1LL << (3 * LL)) ? 1 : 0, c.d_leaf_nbr);
   ++c.tree_launches;
   if (LL >= 2) {
     LevelCellsT C{};
