@@ -5,8 +5,9 @@
 //   leaf neighbours  FTreeCoordinate::getNeighborsIndexes (FTreeCoordinate.hpp:189-216)
 //   interaction list FTreeCoordinate::getInteractionNeighbors (FTreeCoordinate.hpp:219-264)
 //
-// The sort is a stable LSD radix sort with 4-bit digits (histogram / scan / scatter per digit); keys
-// have 3*(height-1) significant bits.
+// The particle sort is a stable LSD radix sort with 8-bit digits (histogram / scan / scatter per digit,
+// ranks within a warp by __match_any_sync); keys have 3*(height-1) significant bits, two passes at height 6.
+// The leaf sort of sparse trees uses 4-bit digits.
 #include "common.cuh"
 
 #include <algorithm>
@@ -19,6 +20,8 @@ constexpr int RS_THREADS = 256;
 constexpr int RS_ITEMS = 8;
 constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
 constexpr int RS_BINS = 16;
+constexpr int RS8_BINS = 256;  // 8-bit digits: each warp of a tile owns 256 consecutive items (8 rounds of 32)
+static_assert(RS_THREADS == RS8_BINS && RS_ITEMS == 8, "one thread per digit; 8 rounds of 32 items per warp");
 
 // --------------------------------------------------------------------------------------------------
 // keys
@@ -64,6 +67,80 @@ __global__ void rs_hist(const unsigned long long *__restrict__ keys, long long n
   }
   __syncthreads();
   if (threadIdx.x < RS_BINS) counts[(long long)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+// 8-bit digits.  Histogram of one tile: counts[d * nblocks + block].
+__global__ void rs8_hist(const unsigned long long *__restrict__ keys, long long n, int shift, int nblocks,
+                         unsigned *__restrict__ counts) {
+  __shared__ unsigned h[RS8_BINS];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const long long base = (long long)blockIdx.x * RS_TILE;
+#pragma unroll
+  for (int k = 0; k < RS_ITEMS; ++k) {
+    const long long i = base + k * RS_THREADS + threadIdx.x;
+    if (i < n) atomicAdd(&h[(keys[i] >> shift) & (RS8_BINS - 1)], 1u);
+  }
+  __syncthreads();
+  counts[(long long)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+// Stable scatter of one tile.  Warp w owns the tile's items [256 w, 256 w + 256), taken in 8 rounds of 32
+// consecutive items; within a round the lanes with the same digit find each other (__match_any_sync) and
+// rank by lane, and per-warp running counts carry the ranks across rounds.  An item's position is the
+// tile's global offset for its digit, plus the items of that digit in the tile's earlier warps, plus its
+// rank in its own warp: input order is kept within every digit.
+__global__ void __launch_bounds__(RS_THREADS) rs8_scatter(const unsigned long long *__restrict__ kin,
+                                                          const int *__restrict__ vin,
+                                                          unsigned long long *__restrict__ kout,
+                                                          int *__restrict__ vout, long long n, int shift, int nblocks,
+                                                          const unsigned *__restrict__ offsets) {
+  constexpr int W = RS_THREADS / 32;
+  __shared__ unsigned wc[W][RS8_BINS];  // per-warp counts, then the counts of the warps before
+  __shared__ unsigned boff[RS8_BINS];
+  const int t = threadIdx.x, w = t >> 5, lane = t & 31;
+#pragma unroll
+  for (int k = 0; k < W; ++k) wc[k][t] = 0;
+  boff[t] = offsets[(long long)t * nblocks + blockIdx.x];
+  __syncthreads();
+  const long long base = (long long)blockIdx.x * RS_TILE + (long long)w * (32 * RS_ITEMS);
+  const unsigned lt = (1u << lane) - 1u;
+  unsigned long long k[RS_ITEMS];
+  int v[RS_ITEMS], dg[RS_ITEMS];
+  unsigned rank[RS_ITEMS];
+#pragma unroll
+  for (int j = 0; j < RS_ITEMS; ++j) {
+    const long long i = base + j * 32 + lane;
+    const bool ok = i < n;
+    k[j] = ok ? kin[i] : 0ull;
+    v[j] = ok ? vin[i] : 0;
+    dg[j] = ok ? (int)((k[j] >> shift) & (RS8_BINS - 1)) : RS8_BINS;
+    const unsigned peers = __match_any_sync(0xffffffffu, dg[j]);
+    const unsigned before = ok ? wc[w][dg[j]] : 0u;
+    rank[j] = before + __popc(peers & lt);
+    __syncwarp();
+    if (ok && (peers & lt) == 0) wc[w][dg[j]] = before + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  {
+    // thread t: digit t, exclusive prefix over the warps
+    unsigned run = 0;
+#pragma unroll
+    for (int q = 0; q < W; ++q) {
+      const unsigned c = wc[q][t];
+      wc[q][t] = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < RS_ITEMS; ++j) {
+    if (dg[j] >= RS8_BINS) continue;
+    const unsigned pos = boff[dg[j]] + wc[w][dg[j]] + rank[j];
+    kout[pos] = k[j];
+    vout[pos] = v[j];
+  }
 }
 
 // Exclusive scan of an unsigned array in tiles of 1024 (one block per tile), block sums out.
@@ -631,9 +708,9 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
     c.cap_sort = std::max(c.cap_sort, (size_t)(2 * (n + 1)));
   }
   const long long nb = (n + RS_TILE - 1) / RS_TILE;
-  B200_CHECK(grow(c, c.d_cnt, c.cap_cnt, (size_t)2 * RS_BINS * nb));
+  B200_CHECK(grow(c, c.d_cnt, c.cap_cnt, (size_t)2 * RS8_BINS * nb));
   B200_CHECK(grow(c, c.d_scan, c.cap_scan,
-                  std::max(scan_tmp_elems<long long>(n + 1), scan_tmp_elems<unsigned>(RS_BINS * nb))));
+                  std::max(scan_tmp_elems<long long>(n + 1), scan_tmp_elems<unsigned>(RS8_BINS * nb))));
   // the domain error flag (int) followed, 16 bytes in, by the per-level cell counts
   if (!c.d_err) B200_CUDA(cudaMalloc(&c.d_err, 32 + sizeof(unsigned long long) * kMaxHeight));
   // inputs on the device
@@ -665,7 +742,7 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
   }
   unsigned long long *k0 = c.d_sortk, *k1 = c.d_sortk + n;
   int *v0 = c.d_sortv, *v1 = c.d_sortv + n;
-  unsigned *cnt = c.d_cnt, *off = c.d_cnt + RS_BINS * nb;
+  unsigned *cnt = c.d_cnt, *off = c.d_cnt + RS8_BINS * nb;
   long long *flags = c.d_flags, *idx = c.d_flags + (n + 1);
   B200_CUDA(cudaMemsetAsync(c.d_err, 0, sizeof(int), s));
   const double W = c.cfg.box_width;
@@ -675,10 +752,10 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
   ++c.tree_launches;
   // stable LSD radix sort of (key, original index)
   const int bits = 3 * LL;
-  for (int sh = 0; sh < bits; sh += 4) {
-    rs_hist<<<(unsigned)nb, RS_THREADS, 0, s>>>(k0, n, sh, (int)nb, cnt);
-    B200_CHECK(scan_u32(c, cnt, off, RS_BINS * nb, (unsigned *)c.d_scan));
-    rs_scatter<<<(unsigned)nb, RS_THREADS, 0, s>>>(k0, v0, k1, v1, n, sh, (int)nb, off);
+  for (int sh = 0; sh < bits; sh += 8) {
+    rs8_hist<<<(unsigned)nb, RS_THREADS, 0, s>>>(k0, n, sh, (int)nb, cnt);
+    B200_CHECK(scan_u32(c, cnt, off, RS8_BINS * nb, (unsigned *)c.d_scan));
+    rs8_scatter<<<(unsigned)nb, RS_THREADS, 0, s>>>(k0, v0, k1, v1, n, sh, (int)nb, off);
     c.tree_launches += 2;
     std::swap(k0, k1);
     std::swap(v0, v1);
