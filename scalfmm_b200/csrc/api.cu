@@ -151,7 +151,7 @@ void destroy_context(b200fmm_context *c) {
   for (void *p : {(void *)c->d_roots, (void *)c->d_S, (void *)c->d_pindices, (void *)c->d_pvec,
                   (void *)c->d_symU, (void *)c->d_symV, (void *)c->d_symoff, (void *)c->d_symrank,
                   (void *)c->d_dense, (void *)c->d_itab, (void *)c->d_class_order, (void *)c->d_cls_bounds,
-                  (void *)c->d_cls_slots, (void *)c->d_status, (void *)c->d_Ut, (void *)c->d_Vt,
+                  (void *)c->d_cls_slots, (void *)c->d_status, (void *)c->d_mmax, (void *)c->d_Ut, (void *)c->d_Vt,
                   (void *)c->d_toff, (void *)c->d_trank, c->d_scratch})
     if (p) cudaFree(p);
   if (c->events_ready)
@@ -223,7 +223,8 @@ b200fmm_status b200fmm_create(const b200fmm_config *cfg, b200fmm_handle *out) {
   }
   if (st == B200FMM_OK) {
     if (cudaMalloc(&c->d_status, 16 * sizeof(int)) != cudaSuccess ||
-        cudaMemset(c->d_status, 0, 16 * sizeof(int)) != cudaSuccess)
+        cudaMemset(c->d_status, 0, 16 * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&c->d_mmax, sizeof(unsigned long long) * kMaxHeight * kMmaxSlots) != cudaSuccess)
       st = fail(B200FMM_ERR_OOM, "status allocation failed");
   }
   if (st == B200FMM_OK) st = build_tables(*c);
@@ -348,6 +349,15 @@ static b200fmm_status execute_body(Context &c, unsigned ops) {
   // skipped right after set_particles, which zeroed them; always part of a captured graph
   if (!c.state_zero || c.capturing) B200_CHECK(zero_state(c));
   c.state_zero = false;
+  // MIXED records the multipole maxima during a full upward pass for the tensor-core M2L
+  c.mmax_out = nullptr;
+  c.mmax_ready = false;
+  const bool fuse_max = c.cfg.precision == B200FMM_MIXED && (ops & B200FMM_P2M) && (ops & B200FMM_M2M) &&
+                        (ops & B200FMM_M2L);
+  if (fuse_max) {
+    B200_CUDA(cudaMemsetAsync(c.d_mmax, 0, sizeof(unsigned long long) * kMaxHeight * kMmaxSlots, c.stream));
+    c.mmax_out = c.d_mmax;
+  }
   B200_CHECK(record(c, 1));
   // The near field needs only the tree: it runs on the second stream beside P2M and M2M and joins before the
   // M2L (a persistent kernel that wants every SM) and before L2P adds into the same results.
@@ -370,14 +380,20 @@ static b200fmm_status execute_body(Context &c, unsigned ops) {
   B200_CHECK(record(c, 2));
   if (ops & B200FMM_M2M)
     for (int l = LL - 1; l >= 2; --l) B200_CHECK(run_m2m(c, l));
+  c.mmax_out = nullptr;
+  c.mmax_ready = fuse_max;
   if (overlap) B200_CUDA(cudaStreamWaitEvent(c.stream, c.ev_join, 0));
   B200_CHECK(record(c, 3));
   if (ops & B200FMM_M2L) {
+    b200fmm_status st = B200FMM_OK;
     if (c.cfg.precision == B200FMM_MIXED)
-      B200_CHECK(run_m2l_tc(c, -1));  // one launch for every level
+      st = run_m2l_tc(c, -1);  // one launch for every level
     else
-      for (int l = 2; l <= LL; ++l) B200_CHECK(run_m2l_fp64(c, l));
+      for (int l = 2; l <= LL && st == B200FMM_OK; ++l) st = run_m2l_fp64(c, l);
+    c.mmax_ready = false;
+    B200_CHECK(st);
   }
+  c.mmax_ready = false;
   B200_CHECK(record(c, 4));
   if (ops & B200FMM_L2L)
     for (int l = 2; l <= LL - 1; ++l) B200_CHECK(run_l2l(c, l));

@@ -15,6 +15,8 @@ namespace b200 {
 
 constexpr int kMaxOrder = 8;
 constexpr int kMaxHeight = 12;
+// slots per level of the multipole maxima that P2M and M2M record (spread to keep atomics uncontended)
+constexpr int kMmaxSlots = 64;
 constexpr int kMaxNrhs = 32;
 
 // Error reporting: the last message per host thread.
@@ -141,6 +143,13 @@ struct Context {
   // device status words set by kernels whose bounded waits ran out (0 = fine); checked by the host at
   // every synchronising call
   int *d_status = nullptr;
+  // max |M| of every level as P2M and M2M write it, [kMaxHeight][kMmaxSlots] bit patterns of non-negative
+  // doubles (which order like the doubles).  execute() points mmax_out at it for its upward pass; after a
+  // complete upward pass from zeroed expansions mmax_ready tells the tensor-core M2L that the maxima of the
+  // current multipoles are there, so that it needs no pass of its own over them.
+  unsigned long long *d_mmax = nullptr;
+  unsigned long long *mmax_out = nullptr;
+  bool mmax_ready = false;
 
   // scratch
   void *d_scratch = nullptr;

@@ -82,6 +82,15 @@ __device__ __forceinline__ void basis_eval(double x, double *S, double *dS) {
   }
 }
 
+// Record the largest |value| a warp wrote (mx per lane; every lane of the warp calls it) into one of the
+// level's kMmaxSlots slots, chosen by block: non-negative doubles order like their bit patterns.
+__device__ __forceinline__ void record_max(unsigned long long *slots, double mx) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0 && mx > 0.0)
+    atomicMax(slots + blockIdx.x % kMmaxSlots, (unsigned long long)__double_as_longlong(mx));
+}
+
 // ---- P2M: one 64-thread block per leaf -------------------------------------------------------------
 // M[nx,ny,nz] = sum_j q_j Sx_j[nx] Sy_j[ny] Sz_j[nz].  The threads first evaluate the 1-D weights of up to 64
 // particles (one each) into shared memory; then thread t < p^2 owns the node line (ny, nz) = (t % p, t / p)
@@ -95,7 +104,7 @@ __global__ void __launch_bounds__(P2M_THREADS, 8) p2m_kernel(
     int R, long long N, long long nleaves, const long long *__restrict__ keys,
     const long long *__restrict__ leaf_start, const double *__restrict__ x, const double *__restrict__ y,
     const double *__restrict__ z, const double *__restrict__ q, double cx0, double cy0, double cz0, double leaf_w,
-    double *__restrict__ M) {
+    double *__restrict__ M, unsigned long long *__restrict__ mmax) {
   constexpr int p = P, nn = P * P * P, PX = (P + 1) & ~1;  // Sx rows padded to 16 bytes
   __shared__ __align__(16) double Wx[P2M_THREADS][PX];
   __shared__ double Wy[P2M_THREADS][P], Wz[P2M_THREADS][P], Q[P2M_THREADS];
@@ -137,11 +146,17 @@ __global__ void __launch_bounds__(P2M_THREADS, 8) p2m_kernel(
         }
       }
     }
+    double mx = 0.0;
     if (owner) {
       double *out = M + (leaf * R + r) * nn + (nz * p + ny) * p;
 #pragma unroll
-      for (int k = 0; k < p; ++k) out[k] += acc[k];
+      for (int k = 0; k < p; ++k) {
+        const double v = out[k] + acc[k];
+        out[k] = v;
+        mx = fmax(mx, fabs(v));
+      }
     }
+    if (mmax) record_max(mmax, mx);
   }
 }
 
@@ -198,7 +213,7 @@ __device__ __forceinline__ void warp_lines(const double *__restrict__ A, int d, 
 template <int P>
 __global__ void __launch_bounds__(256) m2m_kernel(int R, long long nparents, const int *__restrict__ child,
                                                   const double *__restrict__ S, const double *__restrict__ Mc,
-                                                  double *__restrict__ Mp) {
+                                                  double *__restrict__ Mp, unsigned long long *__restrict__ mmax) {
   constexpr int p = P, nn = P * P * P;
   extern __shared__ double sh[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -218,12 +233,16 @@ __global__ void __launch_bounds__(256) m2m_kernel(int R, long long nparents, con
       for (int e = lane; e < nn; e += 32) b1[e] = 0.0;
     }
     __syncthreads();
+    double mx = 0.0;
     for (int e = threadIdx.x; e < nn; e += blockDim.x) {
       double s = 0.0;
 #pragma unroll
       for (int k = 0; k < 8; ++k) s += sh[(size_t)k * 2 * nn + nn + e];
-      Mp[(pc * R + r) * nn + e] += s;
+      const double v = Mp[(pc * R + r) * nn + e] + s;
+      Mp[(pc * R + r) * nn + e] = v;
+      mx = fmax(mx, fabs(v));
     }
+    if (mmax) record_max(mmax, mx);
     __syncthreads();
   }
 }
@@ -357,14 +376,15 @@ b200fmm_status run_p2m(Context &c) {
   const double x0 = c.cfg.center[0] - W / 2, y0 = c.cfg.center[1] - W / 2, z0 = c.cfg.center[2] - W / 2;
   const double lw = W / (double)(1 << LL);
   const bool lagr = c.cfg.kernel == B200FMM_LAGRANGE;
+  unsigned long long *mmax = c.mmax_out ? c.mmax_out + (size_t)LL * kMmaxSlots : nullptr;
 #define B200_P2M(PV)                                                                                        \
   case PV:                                                                                                  \
     if (lagr)                                                                                               \
       p2m_kernel<PV, true><<<(unsigned)L.n, P2M_THREADS, 0, c.stream>>>(                                     \
-          c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, x0, y0, z0, lw, L.M);              \
+          c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, x0, y0, z0, lw, L.M, mmax);              \
     else                                                                                                    \
       p2m_kernel<PV, false><<<(unsigned)L.n, P2M_THREADS, 0, c.stream>>>(                                    \
-          c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, x0, y0, z0, lw, L.M);              \
+          c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, x0, y0, z0, lw, L.M, mmax);              \
     break;
   switch (c.p) {
     B200_P2M(3) B200_P2M(4) B200_P2M(5) B200_P2M(6) B200_P2M(7) B200_P2M(8)
@@ -381,10 +401,11 @@ b200fmm_status run_m2m(Context &c, int level) {
   const Level &P = c.lv[level], &C = c.lv[level + 1];
   if (P.n == 0) return B200FMM_OK;
   const size_t sh = sizeof(double) * 16 * c.nn;
+  unsigned long long *mmax = c.mmax_out ? c.mmax_out + (size_t)level * kMmaxSlots : nullptr;
 #define B200_M2M(PV)                                                                                        \
   case PV:                                                                                                  \
     B200_CUDA(cudaFuncSetAttribute(m2m_kernel<PV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));   \
-    m2m_kernel<PV><<<(unsigned)P.n, 256, sh, c.stream>>>(c.R, P.n, P.child, c.d_S, C.M, P.M);               \
+    m2m_kernel<PV><<<(unsigned)P.n, 256, sh, c.stream>>>(c.R, P.n, P.child, c.d_S, C.M, P.M, mmax);         \
     break;
   switch (c.p) {
     B200_M2M(3) B200_M2M(4) B200_M2M(5) B200_M2M(6) B200_M2M(7) B200_M2M(8)

@@ -1376,12 +1376,14 @@ __global__ void pack_levels_kernel(const __grid_constant__ PackLevels L, int R, 
 
 // 2^sA with sA chosen so that max|M| * 2^sA ~ 2^14, and the epilogue factor scale_l * 2^-(sA + shift)
 // with shift the operators' own pre-scale exponent (SB for the dense K, sV + sU - sY for the low-rank
-// factors).  One thread per level of [l0, l1].
+// factors).  One thread per level of [l0, l1]; max|M| of level l is the largest of amax[l * nslots + s].
 __global__ void level_scale_kernel(const __grid_constant__ PackLevels L, const unsigned long long *__restrict__ amax,
-                                   int shift, double *__restrict__ scal) {
+                                   int nslots, int shift, double *__restrict__ scal) {
   const int l = L.l0 + (int)threadIdx.x;
   if (l > L.l1) return;
-  const double m = __longlong_as_double((long long)amax[l]);
+  unsigned long long bits = 0;
+  for (int q = 0; q < nslots; ++q) bits = max(bits, amax[(size_t)l * nslots + q]);
+  const double m = __longlong_as_double((long long)bits);
   int e = 0;
   if (m > 0) frexp(m, &e);  // m = f * 2^e, f in [0.5, 1)
   const int sA = 14 - e;
@@ -2026,12 +2028,19 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
       L.scale_l[l] = 2.0 / (c.cfg.box_width / (double)(1LL << l));
       L.pos0[l + 1] = L.pos0[l] + 8LL * c.R * t->HZ[l] * t->HY[l] * t->HX[l];
     }
-    B200_CUDA(cudaMemsetAsync(t->amax + l0, 0, sizeof(unsigned long long) * (l1 - l0 + 1), c.stream));
-    const unsigned gx = (unsigned)std::max<long long>(1, std::min<long long>(256, grid_for(maxval, 256)));
-    absmax_levels_kernel<<<dim3(gx, l1 - l0 + 1), 256, 0, c.stream>>>(L, t->amax);
-    level_scale_kernel<<<1, 32, 0, c.stream>>>(L, t->amax, t->lr ? t->lr_shift : SB, t->scal);
+    const int shift = t->lr ? t->lr_shift : SB;
+    if (c.mmax_ready) {
+      // the upward pass of this evaluation recorded the maxima as it wrote the multipoles
+      level_scale_kernel<<<1, 32, 0, c.stream>>>(L, c.d_mmax, kMmaxSlots, shift, t->scal);
+    } else {
+      B200_CUDA(cudaMemsetAsync(t->amax + l0, 0, sizeof(unsigned long long) * (l1 - l0 + 1), c.stream));
+      const unsigned gx = (unsigned)std::max<long long>(1, std::min<long long>(256, grid_for(maxval, 256)));
+      absmax_levels_kernel<<<dim3(gx, l1 - l0 + 1), 256, 0, c.stream>>>(L, t->amax);
+      level_scale_kernel<<<1, 32, 0, c.stream>>>(L, t->amax, 1, shift, t->scal);
+      ++c.launches;
+    }
     pack_levels_kernel<<<(unsigned)L.pos0[l1 + 1], 128, 0, c.stream>>>(L, c.R, c.nn, t->KP, t->scal);
-    c.launches += 3;
+    c.launches += 2;
   }
   // units are ordered by level, finest first: levels [l0, l1] are one contiguous range
   TcParams &P = *t->params;
