@@ -307,25 +307,26 @@ __global__ void gather_charges(long long n, int R, const long long *__restrict__
   for (int r = 0; r < R; ++r) qs[(long long)r * n + i] = q[(long long)r * n + j];
 }
 
-// head[i] = 1 when keys[i] (shifted) differs from its predecessor
-__global__ void head_flags(long long n, const unsigned long long *__restrict__ keys, int shift,
-                           long long *__restrict__ flags) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  flags[i] = (i == 0 || (keys[i] >> shift) != (keys[i - 1] >> shift)) ? 1 : 0;
-}
-
-// cells of every level 0..LL: one per change of the sorted particle key above that level's bits
+// cells of every level 0..LL: one per change of the sorted particle key above that level's bits, counted
+// per warp (ballot), then per block in shared memory, then one atomic per block and level; the leaf level's
+// changes are also written as flags[i] for the leaf compaction
 __global__ void level_counts_kernel(long long n, const unsigned long long *__restrict__ keys, int LL,
-                                    unsigned long long *__restrict__ counts) {
+                                    long long *__restrict__ flags, unsigned long long *__restrict__ counts) {
+  __shared__ unsigned bc[kMaxHeight];
+  if (threadIdx.x < kMaxHeight) bc[threadIdx.x] = 0;
+  __syncthreads();
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
+  const unsigned long long k = i < n ? keys[i] : 0ull, kp = (i > 0 && i < n) ? keys[i - 1] : 0ull;
   for (int l = 0; l <= LL; ++l) {
     const int shift = 3 * (LL - l);
-    const bool head = i < n && (i == 0 || (keys[i] >> shift) != (keys[i - 1] >> shift));
+    const bool head = i < n && (i == 0 || (k >> shift) != (kp >> shift));
+    if (l == LL && i < n) flags[i] = head ? 1 : 0;
     const unsigned m = __ballot_sync(0xffffffffu, head);
-    if (lane == 0 && m) atomicAdd(counts + l, (unsigned long long)__popc(m));
+    if (lane == 0 && m) atomicAdd(&bc[l], (unsigned)__popc(m));
   }
+  __syncthreads();
+  if (threadIdx.x <= LL && bc[threadIdx.x]) atomicAdd(counts + threadIdx.x, (unsigned long long)bc[threadIdx.x]);
 }
 
 __global__ void compact_leaves(long long n, const unsigned long long *__restrict__ keys,
@@ -762,14 +763,12 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
   }
   if (q_forked) B200_CUDA(cudaStreamWaitEvent(s, c.ev_join, 0));
   gather_particles<<<grid_for(n, 256), 256, 0, s>>>(n, c.R, v0, dx, dy, dz, dq, c.d_x, c.d_y, c.d_z, c.d_q, c.d_perm);
-  head_flags<<<grid_for(n, 256), 256, 0, s>>>(n, k0, 0, flags);
-  c.tree_launches += 2;
-  B200_CHECK(scan_i64(c, flags, idx, n, (long long *)c.d_scan));
-  // the cell count of every level at once, then the build's one synchronisation
+  // the cell count of every level at once (and the leaf heads), then the build's one synchronisation
   unsigned long long *counts = (unsigned long long *)(c.d_err + 4);
   B200_CUDA(cudaMemsetAsync(counts, 0, sizeof(unsigned long long) * kMaxHeight, s));
-  level_counts_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, k0, LL, counts);
-  ++c.tree_launches;
+  level_counts_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, k0, LL, flags, counts);
+  c.tree_launches += 2;
+  B200_CHECK(scan_i64(c, flags, idx, n, (long long *)c.d_scan));
   B200_CUDA(cudaMemcpyAsync(c.h_pinned + 2, c.d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
   B200_CUDA(cudaMemcpyAsync(c.h_pinned + 8, counts, sizeof(long long) * (LL + 1), cudaMemcpyDeviceToHost, s));
   B200_CUDA(cudaStreamSynchronize(s));
