@@ -166,7 +166,7 @@ __device__ __forceinline__ void two_sum(float &hi, float &lo, float v) {
 }
 
 constexpr int P2P32_WARPS = 4;   // target leaves per CTA (one warp each)
-constexpr int P2P32_STAGE = 48;  // source records (96 particles) per bulk-copy stage
+constexpr int P2P32_STAGE = 32;  // source records (64 particles) per bulk-copy stage: 24 KB per CTA, 7 CTAs per SM
 constexpr int P2P32_NBUF = 3;    // stages in flight per warp
 
 __device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -230,7 +230,7 @@ __device__ __forceinline__ void p2p_record(const float4 *__restrict__ s, int k, 
 // each split into stages of <= P2P32_STAGE records copied by one bulk copy into a ring of P2P32_NBUF buffers,
 // issued P2P32_NBUF - 1 stages ahead of the math.  Per stage the partial sums enter the target's (hi, lo)
 // accumulators by a two-sum.
-__global__ void __launch_bounds__(P2P32_WARPS * 32, 6) p2p_fp32_kernel(
+__global__ void __launch_bounds__(P2P32_WARPS * 32, 7) p2p_fp32_kernel(
     int R, long long N, long long nleaves, const long long *__restrict__ leaf_start, const int *__restrict__ nbr,
     int variant, const int *__restrict__ rank_of, const long long *__restrict__ rec_base,
     const float4 *__restrict__ pq, const float4 *__restrict__ plo, const float4 *__restrict__ src,
