@@ -35,6 +35,7 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "tests"))  # the seeded distributions of the workloads
 os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
 
 METRIC = "particles/s per FMM eval (1M uniform, Chebyshev p=7, height 6, mixed precision)"
@@ -53,6 +54,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batch-of-problems measurement")
+    ap.add_argument("--no-pins", action="store_true",
+                    help="skip the CPU reference runs that pin the FP64 GPU FMM at the full workload sizes")
     return ap.parse_args()
 
 
@@ -322,6 +325,19 @@ def run_gpu(args):
     m2l_pairs, p2p_pairs = f.tree_stats()
     m2l_flops = f.m2l_flops()  # the two products of the low-rank (compressed-operator) tensor-core M2L
 
+    phases = []  # e2e steps: (set_particles from host, execute, get_results to host) in ms
+
+    def step_e2e_phased():
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record(stream)
+        f.set_particles(hx, hy, hz, hq)
+        ev[1].record(stream)
+        f.execute()
+        ev[2].record(stream)
+        f.results_into(*out_h)
+        ev[3].record(stream)
+        phases.append(ev)
+
     def timed(fn, sampler_index=None):
         ms = []
         kernel = []
@@ -346,7 +362,7 @@ def run_gpu(args):
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
-        ms_e2e, _, launches_e2e = timed(step_e2e)
+        ms_e2e, _, launches_e2e = timed(step_e2e_phased)
     torch.cuda.synchronize()
     t_dev = sum(ms_dev)
     t_e2e = sum(ms_e2e)
@@ -359,7 +375,9 @@ def run_gpu(args):
     m2l_ms = statistics.mean(k["m2l"] for k in ktimes)
     p2p_ms = statistics.mean(k["p2p"] for k in ktimes)
     achieved = m2l_flops / (m2l_ms * 1e-3) / 1e12  # split products counted once
-    peak = bf16_sus / 3.0  # three FP16 products per logical product
+    # the kernel runs about 1.4 ms inside a 3 ms step and the timed region lasts well under a second: the burst
+    # figure applies; three FP16 products per logical product
+    peak = bf16_burst / 3.0
     traffic = profile_traffic()
     p2p_tflops = p2p_pairs * FLOPS_PER_P2P_PAIR / (p2p_ms * 1e-3) / 1e12
     fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12
@@ -378,29 +396,42 @@ def run_gpu(args):
                      "note": f"algorithmic M2L flops per launch = {m2l_flops:.4e}: Y = V^T M per source cell "
                              f"(2 p^3 x the ranks of the slots it feeds) + U Y per pair (2 p^3 r) over {m2l_pairs} "
                              f"pairs, split products counted once; peak = {peak_src} "
-                             f"sustained bf16 {bf16_sus} TFLOP/s / 3 (three FP16 products per logical product); "
+                             f"burst bf16 {bf16_burst} TFLOP/s / 3 (three FP16 products per logical product); "
                              f"kernel time {m2l_ms:.3f} ms (CUDA events on the launching stream)"},
         "p2p": {"pairs": p2p_pairs, "kernel_ms": p2p_ms, "gpairs_per_s": p2p_pairs / (p2p_ms * 1e-3) / 1e9,
                 "tflops_at_20_per_pair": p2p_tflops, "frac_fp32_peak": p2p_tflops / fp32_peak,
                 "fp32_peak_note": "148 SMs x 128 FP32 lanes x 2 x 1965 MHz (nominal)"},
         "pass_ms": f.timings(),
+        "e2e_phases_ms": {
+            "set_particles_host": statistics.mean(a[0].elapsed_time(a[1]) for a in phases),
+            "execute": statistics.mean(a[1].elapsed_time(a[2]) for a in phases),
+            "get_results_host": statistics.mean(a[2].elapsed_time(a[3]) for a in phases),
+            "note": "set_particles_host = H2D of x, y, z, q (32 MB, pinned) + GPU tree build; get_results_host = "
+                    "un-permutation + D2H of phi, fx, fy, fz (32 MB, pinned); tree build alone (device arrays): "
+                    "pass_ms.tree"},
         "autotuned_m2l_splits": tuned_splits,
         "clocks": clk.summary(),
     }
     f.close()
 
+    ref_times = None
     if rank == 0 and not args.no_accuracy:
-        line["accuracy"] = accuracy(S, torch, dev, stream, x, y, z, q, line)
+        line["accuracy"], ref_times = accuracy(S, torch, dev, stream, x, y, z, q, pins=not args.no_pins)
+        line["multi_rhs"] = multi_rhs_measure(S, torch, dev, stream, x, y, z, pins=not args.no_pins)
+        line["ellipsoid"] = ellipsoid_measure(S, torch, dev, stream, pins=not args.no_pins)
     if rank == 0 and not args.no_batch:
         line["batch"] = batch_measure(S, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            times, kind, cores, sample = cpu_eval(x, y, z, q, steps=1)
-            line["cpu_baseline"] = {"value": n / times[0], "unit": "particles/s", "cores": cores, "kind": kind,
-                                    "sample": sample}
+            if ref_times is None:
+                ref_times, kind, cores, sample = cpu_eval(x, y, z, q, steps=1)
+            else:
+                kind, cores, sample = "reference", os.cpu_count() or 1, REF_SAMPLE
+            line["cpu_baseline"] = {"value": n / ref_times[0], "unit": "particles/s", "cores": cores, "kind": kind,
+                                    "cpu_model": cpu_model(), "sample": sample}
         except Exception as exc:  # the baseline is reported, never the target
             line["cpu_baseline"] = {"value": None, "unit": "particles/s", "cores": os.cpu_count(), "kind": "reference",
-                                    "sample": f"failed: {exc}"}
+                                    "cpu_model": cpu_model(), "sample": f"failed: {exc}"}
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
@@ -409,41 +440,203 @@ def run_gpu(args):
     return 0
 
 
-def accuracy(S, torch, dev, stream, x, y, z, q, line):
-    """Mixed vs the plain FP64 GPU FMM (same tree) over all particles, and both against the FP64 direct sum on
-    a seeded 10,000-target subsample; also times the plain FP64 GPU FMM (same step definition)."""
+REF_SAMPLE = ("ScalFMM FFmmAlgorithmThread + FChebSymKernel (order 7, height 6) built from its sources, algo.execute() "
+              "of the full workload (the run whose outputs pin the FP64 GPU FMM in accuracy)")
+FIELDS = ("phi", "fx", "fy", "fz")
+
+
+def cpu_model():
+    try:
+        for ln in Path("/proc/cpuinfo").read_text().splitlines():
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def device_eval(S, torch, f, stream, arrays, reps=3):
+    """Best device time (ms) of set_particles (device arrays) + execute over `reps` runs after one untimed run,
+    and the results of the last run."""
+    f.set_particles(*arrays)
+    f.execute()
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(reps):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        f.set_particles(*arrays)
+        f.execute()
+        e.record(stream)
+        e.synchronize()
+        ms.append(s.elapsed_time(e))
+    return min(ms), f.results()
+
+
+def timed_create(S, *a, **k):
+    t0 = time.perf_counter()
+    f = S.FMM(*a, **k)
+    return f, 1e3 * (time.perf_counter() - t0)
+
+
+def accuracy(S, torch, dev, stream, x, y, z, q, pins=True):
+    """The headline workload (1M uniform, Chebyshev order 7, height 6):
+    * MIXED vs the plain FP64 GPU FMM (same tree, same operators) over all particles, and the time of both;
+    * the FP64 GPU FMM loaded with the reference's own compressed operators against the reference's
+      FFmmAlgorithmThread + FChebSymKernel on the same particles, all outputs (parity bar 1e-12), and MIXED
+      against the same reference outputs;
+    * both forms, at order 7 and order 8, against the FP64 direct sum on a seeded 10,000-target subsample;
+    * the operator precompute (create()) time of each form.
+    Returns the fields and the reference's algo.execute() time (None without the reference)."""
+    from oracle import oracle as O
+
     n = x.size
     out = {}
     res = {}
+    arrays = [torch.from_numpy(a).to(dev) for a in (x, y, z, q)]
     for prec in ("fp64", "mixed"):
-        f = S.FMM("cheb_sym", ORDER, HEIGHT, precision=prec, device=dev.index, stream=stream.cuda_stream)
-        dx, dy, dz, dq = (torch.from_numpy(a).to(dev) for a in (x, y, z, q))
-        f.set_particles(dx, dy, dz, dq)
-        f.execute()
-        torch.cuda.synchronize()
-        ms = []
-        for _ in range(3):
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s.record(stream)
-            f.set_particles(dx, dy, dz, dq)
-            f.execute()
-            e.record(stream)
-            e.synchronize()
-            ms.append(s.elapsed_time(e))
-        res[prec] = f.results()
-        out[f"{prec}_ms_per_eval"] = min(ms)
+        f, out[f"{prec}_create_ms"] = timed_create(S, "cheb_sym", ORDER, HEIGHT, precision=prec, device=dev.index,
+                                                   stream=stream.cuda_stream)
+        out[f"{prec}_ms_per_eval"], res[prec] = device_eval(S, torch, f, stream, arrays)
         out[f"{prec}_pass_ms"] = f.timings()
+        if prec == "fp64":
+            out["fp64_m2l_flops"] = f.m2l_flops()
+            out["fp64_m2l_tflops"] = out["fp64_m2l_flops"] / (out["fp64_pass_ms"]["m2l"] * 1e-3) / 1e12
         f.close()
     out["fp64_particles_per_s"] = n / (out["fp64_ms_per_eval"] * 1e-3)
     out["mixed_over_fp64_speedup"] = out["fp64_ms_per_eval"] / out["mixed_ms_per_eval"]
-    for k in ("phi", "fx", "fy", "fz"):
+    for k in FIELDS:
+        out[f"mixed_vs_fp64_rel_l2_{k}"] = S.rel_l2(res["mixed"][k], res["fp64"][k])
+    t = np.random.default_rng(7).choice(n, 10000, replace=False)
+    d = S.direct(x, y, z, q, targets=t)
+    for prec in ("fp64", "mixed"):
+        for k in FIELDS:
+            out[f"{prec}_vs_direct_rel_l2_{k}"] = S.rel_l2(res[prec][k][t], d[k])
+    out["gate_mixed_vs_fp64_le_1e-6"] = bool(out["mixed_vs_fp64_rel_l2_phi"] <= 1e-6)
+    # order 8: the order at which the FMM's own truncation error drops below 1e-6 against the direct sum
+    for prec in ("fp64", "mixed"):
+        try:
+            f = S.FMM("cheb_sym", 8, HEIGHT, precision=prec, device=dev.index, stream=stream.cuda_stream)
+        except S.B200FmmError as exc:  # a form not built for order 8 says so
+            out[f"order8_{prec}"] = f"not built: {exc}"
+            continue
+        ms, r8 = device_eval(S, torch, f, stream, arrays, reps=2)
+        f.close()
+        out[f"order8_{prec}_ms_per_eval"] = ms
+        for k in FIELDS:
+            out[f"order8_{prec}_vs_direct_rel_l2_{k}"] = S.rel_l2(r8[k][t], d[k])
+        out[f"gate_order8_{prec}_vs_direct_phi_le_1e-6"] = bool(out[f"order8_{prec}_vs_direct_rel_l2_phi"] <= 1e-6)
+    ref_times = None
+    if pins and O.ref_available():
+        with _StdoutToStderr():
+            ranks, uv, _, _ = O.ref_sym_operators(ORDER)
+            ref = O.ref_fmm(O.CHEB_SYM, ORDER, HEIGHT, 1.0, (0.5, 0.5, 0.5), x, y, z, q, nthreads=os.cpu_count() or 1)
+        ref_times = [ref["times"]["execute"]]
+        f = S.FMM("cheb_sym", ORDER, HEIGHT, precision="fp64", device=dev.index, stream=stream.cuda_stream)
+        f.set_sym_operators(ranks, uv)
+        _, r64 = device_eval(S, torch, f, stream, arrays, reps=1)
+        f.close()
+        for k in FIELDS:
+            out[f"pin_fp64_refops_vs_reference_rel_l2_{k}"] = S.rel_l2(r64[k], ref[k])
+            out[f"pin_fp64_vs_reference_rel_l2_{k}"] = S.rel_l2(res["fp64"][k], ref[k])
+            out[f"pin_mixed_vs_reference_rel_l2_{k}"] = S.rel_l2(res["mixed"][k], ref[k])
+        out["pin_gate_fp64_refops_le_1e-12"] = bool(max(out[f"pin_fp64_refops_vs_reference_rel_l2_{k}"]
+                                                        for k in FIELDS) <= 1e-12)
+        out["pin_reference"] = ("ScalFMM FFmmAlgorithmThread + FChebSymKernel<order 7> (oracle/_ref, built from the "
+                                "reference sources), same particles, all outputs; FP64 GPU loaded with the "
+                                "reference's compressed operators (FChebSymM2LHandler export)")
+        out["pin_reference_times_s"] = ref["times"]
+    return out, ref_times
+
+
+def multi_rhs_measure(S, torch, dev, stream, x, y, z, pins=True, nrhs=16):
+    """Multi-RHS workload: the headline positions with 16 independent charge vectors U[-1,1] on one tree,
+    Chebyshev order 7, height 6.  MIXED throughput (particles x RHS per second, device time of set_particles +
+    execute), the M2L's algorithmic rate, MIXED vs the FP64 GPU FMM, and the FP64 GPU FMM (reference operators)
+    against the reference's FFmmAlgorithmThread with NVALS = 16 on the same inputs."""
+    from oracle import oracle as O
+
+    n = x.size
+    qm = np.random.default_rng(SEED + 1).uniform(-1.0, 1.0, (nrhs, n))
+    arrays = [torch.from_numpy(a).to(dev) for a in (x, y, z, qm.ravel())]
+    out = {"workload": f"{n} uniform particles (the headline positions) x {nrhs} charge vectors U[-1,1] (seed "
+                       f"{SEED + 1}), Chebyshev order 7, height 6", "nrhs": nrhs}
+    f = S.FMM("cheb_sym", ORDER, HEIGHT, nrhs=nrhs, precision="mixed", device=dev.index, stream=stream.cuda_stream)
+    ms, rm = device_eval(S, torch, f, stream, arrays)
+    f.set_particles(*arrays)
+    f.execute()
+    kt = f.kernel_times()
+    flops = f.m2l_flops()
+    _, bf16_sus, bf16_burst, src = measured_peaks()
+    f.close()
+    out["mixed_ms_per_eval"] = ms
+    out["particle_rhs_per_s"] = n * nrhs / (ms * 1e-3)
+    out["m2l"] = {"kernel_ms": kt["m2l"], "flops": flops, "achieved_tflops": flops / (kt["m2l"] * 1e-3) / 1e12,
+                  "frac": flops / (kt["m2l"] * 1e-3) / 1e12 / (bf16_burst / 3.0),
+                  "peak_note": f"{src} burst bf16 {bf16_burst} TFLOP/s / 3"}
+    f = S.FMM("cheb_sym", ORDER, HEIGHT, nrhs=nrhs, precision="fp64", device=dev.index, stream=stream.cuda_stream)
+    ranks = uv = None
+    if pins and O.ref_available():
+        with _StdoutToStderr():
+            ranks, uv, _, _ = O.ref_sym_operators(ORDER)
+        f.set_sym_operators(ranks, uv)
+    ms64, r64 = device_eval(S, torch, f, stream, arrays, reps=1)
+    f.close()
+    out["fp64_ms_per_eval"] = ms64
+    for k in FIELDS:
+        out[f"mixed_vs_fp64_rel_l2_{k}"] = S.rel_l2(rm[k], r64[k])
+    if ranks is not None:
+        with _StdoutToStderr():
+            ref = O.ref_fmm(O.CHEB_SYM, ORDER, HEIGHT, 1.0, (0.5, 0.5, 0.5), x, y, z, qm,
+                            nthreads=os.cpu_count() or 1)
+        for k in FIELDS:
+            out[f"pin_fp64_refops_vs_reference_rel_l2_{k}"] = S.rel_l2(r64[k], ref[k])
+        out["pin_gate_fp64_refops_le_1e-12"] = bool(max(out[f"pin_fp64_refops_vs_reference_rel_l2_{k}"]
+                                                        for k in FIELDS) <= 1e-12)
+        out["pin_reference"] = "ScalFMM FFmmAlgorithmThread + FChebSymKernel<order 7, NVALS 16> (oracle/_ref)"
+        out["pin_reference_times_s"] = ref["times"]
+    return out
+
+
+def ellipsoid_measure(S, torch, dev, stream, pins=True, n=2_000_000):
+    """Ellipsoid-surface workload: 2M area-uniform points on the surface of the ellipsoid with semi-axes
+    (0.5, 0.3, 0.2) centred in the unit cube, charges U[0,1], Lagrange (uniform) interpolation order 6, height 7.
+    MIXED throughput, MIXED vs the FP64 GPU FMM, the FP64 GPU FMM against the C restatement of the reference's
+    FUnifKernel FMM (oracle/fmm_oracle.c) on all particles, and both against the direct sum on 10,000 targets."""
+    from distributions import ellipsoid_surface
+    from oracle import oracle as O
+
+    x, y, z = ellipsoid_surface(n, 3)
+    q = np.random.default_rng(4).random(n)
+    arrays = [torch.from_numpy(a).to(dev) for a in (x, y, z, q)]
+    out = {"workload": f"{n} area-uniform points on the ellipsoid (0.5, 0.3, 0.2) surface centred in the unit cube "
+                       "(seed 3), q~U[0,1] (seed 4), Lagrange order 6, height 7"}
+    res = {}
+    for prec in ("mixed", "fp64"):
+        f = S.FMM("lagrange", 6, 7, precision=prec, device=dev.index, stream=stream.cuda_stream)
+        out[f"{prec}_ms_per_eval"], res[prec] = device_eval(S, torch, f, stream, arrays, reps=3 if prec == "mixed" else 1)
+        out[f"{prec}_pass_ms"] = f.timings()
+        if prec == "mixed":
+            nc, _ = f.tree_info()
+            out["cells_per_level"] = [int(v) for v in nc]
+            out["m2l_pairs"], out["p2p_pairs"] = f.tree_stats()
+        f.close()
+    out["mixed_particles_per_s"] = n / (out["mixed_ms_per_eval"] * 1e-3)
+    for k in FIELDS:
         out[f"mixed_vs_fp64_rel_l2_{k}"] = S.rel_l2(res["mixed"][k], res["fp64"][k])
     t = np.random.default_rng(7).choice(n, 10000, replace=False)
     d = S.direct(x, y, z, q, targets=t)
     for prec in ("fp64", "mixed"):
         for k in ("phi", "fx"):
             out[f"{prec}_vs_direct_rel_l2_{k}"] = S.rel_l2(res[prec][k][t], d[k])
-    out["gate_mixed_vs_fp64_le_1e-6"] = bool(out["mixed_vs_fp64_rel_l2_phi"] <= 1e-6)
+    if pins:
+        t0 = time.perf_counter()
+        o = O.fmm(O.LAGRANGE, 6, 7, 1.0, (0.5, 0.5, 0.5), x, y, z, q)
+        out["pin_oracle_s"] = time.perf_counter() - t0
+        for k in FIELDS:
+            out[f"pin_fp64_vs_oracle_rel_l2_{k}"] = S.rel_l2(res["fp64"][k], o[k])
+        out["pin_gate_fp64_le_1e-12"] = bool(max(out[f"pin_fp64_vs_oracle_rel_l2_{k}"] for k in FIELDS) <= 1e-12)
+        out["pin_reference"] = "C restatement of FUnifKernel's FMM (oracle/fmm_oracle.c, pinned against the reference)"
     return out
 
 

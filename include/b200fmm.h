@@ -152,6 +152,16 @@ B200FMM_API b200fmm_status b200fmm_synchronize(b200fmm_handle h);
 B200FMM_API b200fmm_status b200fmm_tree_info(b200fmm_handle h, long long *ncells, long long *nparticles);
 B200FMM_API b200fmm_status b200fmm_get_cells(b200fmm_handle h, int level, long long *keys, double *multipoles,
                                  double *locals);
+/* The tree's lists (host memory), in the cell numbering of get_cells.
+ * get_leaf_neighbors: nbr[nleaves*27], for each leaf the leaf at neighbour position ((dx+1)*3+(dy+1))*3+(dz+1)
+ *   (FAbstractKernels.hpp:134-136; 13 = the leaf itself), -1 when that leaf is empty or outside the box -- the
+ *   neighbours FOctree::getLeafsNeighbors returns (Src/Containers/FOctree.hpp:1364-1400).
+ * get_interaction_lists: for one level (2..height-1), src[ncells*189] the source cell of each of a cell's 189
+ *   interaction-list candidates and pos[ncells*189] its position ((dx+3)*7+(dy+3))*7+(dz+3), both -1 where that
+ *   cell is empty or outside the box -- the far neighbours FOctree::getInteractionNeighbors returns
+ *   (FOctree.hpp:914-975, FTreeCoordinate.hpp:219-264).  Either pointer may be NULL. */
+B200FMM_API b200fmm_status b200fmm_get_leaf_neighbors(b200fmm_handle h, int *nbr);
+B200FMM_API b200fmm_status b200fmm_get_interaction_lists(b200fmm_handle h, int level, int *src, int *pos);
 /* Sorted position -> original particle index. */
 B200FMM_API b200fmm_status b200fmm_get_permutation(b200fmm_handle h, long long *perm);
 
@@ -170,20 +180,26 @@ B200FMM_API b200fmm_status b200fmm_tree_stats(b200fmm_handle h, long long *m2l_p
 B200FMM_API b200fmm_status b200fmm_last_launch_count(b200fmm_handle h, long long *count);
 
 /* Allocation-free near field.  This entry point has no counterpart in the reference.  It is for callers
- * that must not allocate device memory while they run this step: code being captured into a CUDA graph by
- * a framework that forbids allocations during capture, applications that hand all device memory to their
- * own pool up front, or real-time loops where cudaMalloc's implicit synchronisation is not acceptable.
- * It runs the MIXED-precision P2P of b200fmm_p2p (variant 0 or 1) on caller-owned device arrays and calls
- * no cudaMalloc, cudaFree or other allocating routine: its scratch (the FP32 leaf-local copies of the
- * particles) lives in a fixed 24 MiB device array inside this library, so it accepts at most
- * B200FMM_NOALLOC_MAX_PARTICLES particles and returns B200FMM_ERR_INVALID above that.
+ * that cannot allocate device memory while this step runs: applications that hand all device memory to their
+ * own pool up front (so a cudaMalloc inside a library fails or steals from the pool), and loops where
+ * cudaMalloc's implicit device synchronisation is not acceptable.  It runs the MIXED-precision P2P of
+ * b200fmm_p2p (variant 0 or 1) on caller-owned device arrays and calls no cudaMalloc, cudaFree or other
+ * allocating routine: its scratch (the FP32 leaf-local copies of the particles) lives in a fixed 24 MiB device
+ * array inside this library, which every GPU that loads the library holds until the process exits, so it
+ * accepts at most B200FMM_NOALLOC_MAX_PARTICLES particles and returns B200FMM_ERR_INVALID above that.
  *   x, y, z, q: n particles sorted by leaf (FP64, device); leaf_keys[nleaves] Morton keys of the non-empty
- *   leaves in increasing order; leaf_start[nleaves+1] their particle ranges; leaf_nbr[nleaves*27] the leaf
- *   index of each neighbour position ((dx+1)*3+(dy+1))*3+(dz+1) (13 = the leaf itself), -1 when empty;
- *   phi, fx, fy, fz: n outputs (FP64, device) to which the near field is ADDED.  stream: cudaStream_t.
+ *   leaves in increasing order; leaf_start[nleaves+1] their particle ranges (leaf_start[0] = 0,
+ *   leaf_start[nleaves] = n); leaf_nbr[nleaves*27] the leaf index of each neighbour position
+ *   ((dx+1)*3+(dy+1))*3+(dz+1) (13 = the leaf itself), -1 when empty; phi, fx, fy, fz: n outputs (FP64,
+ *   device) to which the near field is ADDED.  stream: cudaStream_t.
+ * The leaf tables are checked on the device before anything is read through them; inconsistent tables
+ * return B200FMM_ERR_INVALID and leave the outputs untouched.  The call blocks the calling thread: it reads
+ * the result of that check back before the near field runs, and the status of the near field's bounded waits
+ * before it returns.
  * The first call on a device looks up that array's device address (cudaGetSymbolAddress) with the device
  * current; make that first call before any stream capture.  All calls share the one array and its status
- * word, so calls whose executions overlap on the GPU race: serialise them (one stream, or events). */
+ * words, and it keeps the last call's contents; calls whose executions overlap on the GPU race on it:
+ * serialise them (one stream, or events). */
 #define B200FMM_NOALLOC_MAX_PARTICLES 262144LL
 B200FMM_API b200fmm_status b200fmm_p2p_noalloc(long long n, const double *x, const double *y, const double *z,
                                                const double *q, long long nleaves, const long long *leaf_keys,

@@ -33,6 +33,7 @@ EXPORTS = (
     "b200fmm_get_permutation", "b200fmm_last_timings", "b200fmm_last_kernel_times", "b200fmm_tree_stats",
     "b200fmm_last_launch_count", "b200fmm_autotune", "b200fmm_p2p_noalloc", "b200fmm_batch_create", "b200fmm_batch_execute",
     "b200fmm_batch_last_time", "b200fmm_batch_destroy", "b200fmm_direct", "b200fmm_m2l_flops",
+    "b200fmm_get_leaf_neighbors", "b200fmm_get_interaction_lists",
 )
 NOALLOC_MAX_PARTICLES = 262144
 
@@ -105,6 +106,8 @@ def lib():
         L.b200fmm_tree_info.argtypes = [ctypes.c_void_p, _lp, _lp]
         L.b200fmm_get_cells.argtypes = [ctypes.c_void_p, ctypes.c_int, _lp, _dp, _dp]
         L.b200fmm_get_permutation.argtypes = [ctypes.c_void_p, _lp]
+        L.b200fmm_get_leaf_neighbors.argtypes = [ctypes.c_void_p, _ip]
+        L.b200fmm_get_interaction_lists.argtypes = [ctypes.c_void_p, ctypes.c_int, _ip, _ip]
         L.b200fmm_last_timings.argtypes = [ctypes.c_void_p, _dp]
         L.b200fmm_last_launch_count.argtypes = [ctypes.c_void_p, _lp]
         L.b200fmm_last_kernel_times.argtypes = [ctypes.c_void_p, _dp]
@@ -284,6 +287,23 @@ class FMM:
         perm = np.zeros(self.n, np.int64)
         _check(lib().b200fmm_get_permutation(self._h, _ptr(perm, _lp)), "get_permutation")
         return perm
+
+    def leaf_neighbors(self):
+        """[nleaves, 27] leaf index at each neighbour position ((dx+1)*3+(dy+1))*3+(dz+1), -1 if empty."""
+        nc, _ = self.tree_info()
+        nbr = np.zeros(int(nc[self.height - 1]) * 27, np.int32)
+        _check(lib().b200fmm_get_leaf_neighbors(self._h, _ptr(nbr, _ip)), "get_leaf_neighbors")
+        return nbr.reshape(-1, 27)
+
+    def interaction_lists(self, level):
+        """([ncells, 189] source cell, [ncells, 189] position ((dx+3)*7+(dy+3))*7+(dz+3)), -1 if absent."""
+        nc, _ = self.tree_info()
+        n = int(nc[level])
+        src = np.zeros(n * 189, np.int32)
+        pos = np.zeros(n * 189, np.int32)
+        _check(lib().b200fmm_get_interaction_lists(self._h, level, _ptr(src, _ip), _ptr(pos, _ip)),
+               "get_interaction_lists")
+        return src.reshape(n, 189), pos.reshape(n, 189)
 
     def timings(self):
         ms = np.zeros(8)

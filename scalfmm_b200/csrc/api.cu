@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <vector>
 
 namespace b200 {
 
@@ -148,6 +149,7 @@ void destroy_context(b200fmm_context *c) {
   drop_graph(*c);
   free_tree(*c);
   tc_free(*c);
+  sym64_free(*c);
   for (void *p : {(void *)c->d_roots, (void *)c->d_S, (void *)c->d_pindices, (void *)c->d_pvec,
                   (void *)c->d_symU, (void *)c->d_symV, (void *)c->d_symoff, (void *)c->d_symrank,
                   (void *)c->d_dense, (void *)c->d_itab, (void *)c->d_class_order, (void *)c->d_cls_bounds,
@@ -631,6 +633,45 @@ b200fmm_status b200fmm_get_permutation(b200fmm_handle h, long long *perm) {
   return B200FMM_OK;
 }
 
+b200fmm_status b200fmm_get_leaf_neighbors(b200fmm_handle h, int *nbr) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  B200_CHECK(need_particles(c));
+  if (!nbr) return fail(B200FMM_ERR_INVALID, "null argument");
+  B200_CHECK(set_device(c));
+  const Level &L = c.lv[c.H - 1];
+  B200_CUDA(cudaMemcpyAsync(nbr, c.d_leaf_nbr, sizeof(int) * 27 * (size_t)L.n, cudaMemcpyDeviceToHost, c.stream));
+  B200_CUDA(cudaStreamSynchronize(c.stream));
+  return B200FMM_OK;
+}
+
+b200fmm_status b200fmm_get_interaction_lists(b200fmm_handle h, int level, int *src, int *pos) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  B200_CHECK(need_particles(c));
+  if (level < 2 || level > c.H - 1) return fail(B200FMM_ERR_INVALID, "level must be in [2, height-1]");
+  if (!src && !pos) return fail(B200FMM_ERR_INVALID, "null argument");
+  B200_CHECK(set_device(c));
+  B200_CHECK(build_ilists(c));  // MIXED builds them on demand only
+  const Level &L = c.lv[level];
+  std::vector<int> s((size_t)L.n * 189);
+  std::vector<long long> keys((size_t)L.n);
+  if (L.n) {
+    B200_CUDA(cudaMemcpyAsync(s.data(), L.ilist, sizeof(int) * s.size(), cudaMemcpyDeviceToHost, c.stream));
+    B200_CUDA(cudaMemcpyAsync(keys.data(), L.keys, sizeof(long long) * keys.size(), cudaMemcpyDeviceToHost,
+                              c.stream));
+  }
+  B200_CUDA(cudaStreamSynchronize(c.stream));
+  // entry e of a cell with Morton child index ct sits at position itab.slot[ct][e]
+  for (long long i = 0; i < L.n; ++i)
+    for (int e = 0; e < 189; ++e) {
+      const size_t k = (size_t)i * 189 + e;
+      if (src) src[k] = s[k];
+      if (pos) pos[k] = s[k] >= 0 ? c.itab.slot[keys[i] & 7][e] : -1;
+    }
+  return B200FMM_OK;
+}
+
 b200fmm_status b200fmm_last_timings(b200fmm_handle h, double *ms8) {
   B200_CHECK(check_handle(h));
   Context &c = *h;
@@ -706,6 +747,9 @@ b200fmm_status b200fmm_m2l_flops(b200fmm_handle h, double *flops) {
   double fed[8];
   const bool lr = c.cfg.precision == B200FMM_MIXED && tc_lowrank_info(c, rank, fed);
   const bool sym64 = c.cfg.precision == B200FMM_FP64 && c.cfg.kernel == B200FMM_CHEB_SYM;
+  // the FP64 symmetric M2L runs as two GEMMs: V^T M per source cell over the slots its parity feeds, then U Y
+  // per pair -- the same work as the low-rank tensor-core form
+  const bool two_gemm = sym64 && sym64_fed_ranks(c, fed);
   if (!lr && !sym64) {
     long long pairs = 0;
     B200_CHECK(b200fmm_tree_stats(h, &pairs, nullptr));
@@ -732,7 +776,7 @@ b200fmm_status b200fmm_m2l_flops(b200fmm_handle h, double *flops) {
   unsigned long long hv[9];
   B200_CUDA(cudaMemcpyAsync(hv, d, sizeof(hv), cudaMemcpyDeviceToHost, c.stream));
   B200_CUDA(cudaStreamSynchronize(c.stream));
-  if (sym64) {
+  if (sym64 && !two_gemm) {
     // per pair: Y = V^T M and U Y, each 2 p^3 r
     *flops = 4.0 * c.nn * (double)hv[0] * c.R;
   } else {

@@ -60,6 +60,7 @@ struct IListTable {
 };
 
 struct DenseTC;  // tensor-core M2L state (m2l_tc.cu)
+struct Sym64;    // two-GEMM FP64 symmetric M2L state (m2l_sym64.cu)
 
 struct Context {
   b200fmm_config cfg{};
@@ -156,6 +157,7 @@ struct Context {
   size_t scratch_bytes = 0;
 
   DenseTC *tc = nullptr;
+  Sym64 *s64 = nullptr;
 
   // timings / counters
   cudaEvent_t ev[16];
@@ -198,6 +200,13 @@ b200fmm_status run_p2p(Context &c, int variant);
 b200fmm_status leaf_column_order(Context &c);
 // m2l_fp64.cu
 b200fmm_status run_m2l_fp64(Context &c, int level);
+// m2l_sym64.cu: the FP64 symmetric M2L as two GEMMs per level (stacked V_t^T, then concatenated U_t)
+b200fmm_status sym64_prepare(Context &c, const std::vector<double> &Ut, const std::vector<double> &Vt,
+                             const std::vector<long long> &toff, const std::vector<int> &trank);
+void sym64_free(Context &c);
+b200fmm_status run_m2l_sym64(Context &c, int level);
+// rows of the stacked V of each source parity (the ranks of the slots that parity feeds)
+bool sym64_fed_ranks(const Context &c, double *fed);
 // m2l_tc.cu
 b200fmm_status tc_init(Context &c);
 void tc_free(Context &c);

@@ -11,6 +11,8 @@
 //  scale = 2 / cell width (FInterpMatrixKernelR::getScaleFactor, FInterpMatrixKernel.hpp:124-133).
 #include "common.cuh"
 
+#include <cstdlib>
+
 namespace b200 {
 
 namespace {
@@ -206,6 +208,13 @@ b200fmm_status run_m2l_fp64(Context &c, int level) {
   if (T.n == 0) return B200FMM_OK;
   const double scale = 2.0 / (c.cfg.box_width / (double)(1LL << level));
   if (c.cfg.kernel == B200FMM_CHEB_SYM && c.cfg.precision == B200FMM_FP64) {
+    // the two-GEMM form (m2l_sym64.cu); the per-target kernel below remains for trees whose largest level
+    // would need more than the two-GEMM form's cap on Y, and on request (B200FMM_SYM64=0)
+    const char *env = std::getenv("B200FMM_SYM64");
+    if (c.s64 && !(env && env[0] == '0')) {
+      const b200fmm_status st = run_m2l_sym64(c, level);
+      if (st != B200FMM_ERR_UNSUPPORTED) return st;
+    }
     SymArgs a;
     a.R = c.R;
     a.scale = scale;

@@ -156,6 +156,11 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity
   }
   return false;
 }
+// The same wait taken by all 32 lanes of an epilogue warp: the warp agrees on the outcome, so that no lane
+// reaches the warp-collective TMEM loads (.sync.aligned) after another lane has given up.
+__device__ __forceinline__ bool mbar_wait_warp(unsigned long long *b, unsigned parity) {
+  return __all_sync(0xffffffffu, mbar_wait(b, parity));
+}
 __device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, unsigned long long *bar, int c0, int c1,
                                             int c2, int c3, int c4) {
   asm volatile(
@@ -799,7 +804,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
       for (int sgi = 0; sgi < nseg_item; ++sgi, ++seg) {
         if constexpr (NHALF == 1) {
           const int b = P.nbuf == 2 ? (seg & 1) : 0;
-          if (!wait_bar(&acc_full[b][0], (full_par >> b) & 1u)) {
+          if (!mbar_wait_warp(&acc_full[b][0], (full_par >> b) & 1u)) {
             give_up();
             break;
           }
@@ -813,7 +818,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
           // half 0 for part 0 and half 1 for part 1
           constexpr int G = CW - SPLIT;
           static_assert(SPLIT - G == 16, "one extra group of 16 columns");
-          if (!wait_bar(&acc_full[0][0], full_par & 1u)) {
+          if (!mbar_wait_warp(&acc_full[0][0], full_par & 1u)) {
             give_up();
             break;
           }
@@ -825,7 +830,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
           else
             drain_cols<G, BATCH>(tlane + SPLIT, acc);
           release(0, 0);
-          if (!wait_bar(&acc_full[0][1], (full_par >> 1) & 1u)) {
+          if (!mbar_wait_warp(&acc_full[0][1], (full_par >> 1) & 1u)) {
             give_up();
             break;
           }
@@ -1116,7 +1121,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
       for (int i = 0; i < 128; ++i) acc[i] = 0.f;
       for (int sg = 0; sg < nseg; ++sg) {
         const int b = sg & 1;
-        if (!mbar_wait(&acc_full[b], (full_par >> b) & 1u)) {
+        if (!mbar_wait_warp(&acc_full[b], (full_par >> b) & 1u)) {
           give_up();
           break;
         }

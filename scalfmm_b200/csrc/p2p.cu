@@ -190,6 +190,11 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned phas
   }
   return false;
 }
+// The same wait taken by a whole warp: every lane polls, and the warp agrees on the outcome, so that either all
+// lanes go on or all give up (a lane that left alone would break the full-mask shuffles that follow).
+__device__ __forceinline__ bool mbar_wait_warp(unsigned long long *bar, unsigned phase) {
+  return __all_sync(0xffffffffu, mbar_wait(bar, phase));
+}
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                    smem_addr(dst)),
@@ -329,8 +334,16 @@ __global__ void __launch_bounds__(P2P32_WARPS * 32, 7) p2p_fp32_kernel(
         int cn;
         next_stage(ce, cp, cn);
         const int b = done % P2P32_NBUF;
-        if (!mbar_wait(&bar[w][b], (phase_bits >> b) & 1u)) {
-          if (lane == 0) atomicExch(status, 1);
+        if (!mbar_wait_warp(&bar[w][b], (phase_bits >> b) & 1u)) {
+          // give up: flag it, and let the copies still in flight land (bounded) before the CTA leaves
+          if (lane == 0) {
+            atomicExch(status, 1);
+            for (int k = done; k < issued; ++k) {
+              const int bk = k % P2P32_NBUF;
+              mbar_wait(&bar[w][bk], (phase_bits >> bk) & 1u);
+            }
+          }
+          __syncwarp();
           return;
         }
         phase_bits ^= 1u << b;
@@ -439,9 +452,10 @@ b200fmm_status run_p2p(Context &c, int variant) {
 
 // ---- allocation-free entry point -------------------------------------------------------------------
 // Scratch of b200fmm_p2p_noalloc: the FP32 copies of the particles -- targets (hi, lo) and
-// pair-packed sources, 6 float4 per particle plus 8 (24 MiB at 2^18 particles) -- and the status word of the
-// kernel's bounded waits.  In host code these names are host-side stand-ins, not device addresses: the host
-// passes the addresses looked up with cudaGetSymbolAddress.
+// pair-packed sources, 6 float4 per particle plus 8 (24 MiB at 2^18 particles) -- and the status words:
+// [0] a bounded wait of the near-field kernel ran out, [1] the caller's leaf tables failed the checks.  In host
+// code these names are host-side stand-ins, not device addresses: the host passes the addresses looked up with
+// cudaGetSymbolAddress.
 static __device__ __align__(256) float4 g_noalloc_stage[6 * B200FMM_NOALLOC_MAX_PARTICLES + 8];
 static __device__ __align__(256) int g_noalloc_status[4];
 
@@ -469,6 +483,30 @@ b200fmm_status noalloc_addresses(float4 **stage, int **status) {
   *status = g_noalloc_status_ptr[dev];
   return B200FMM_OK;
 }
+
+// The caller's leaf tables are checked before any kernel indexes memory through them: leaf_start rises from 0
+// to n, the leaf keys rise strictly inside the leaf level, every neighbour entry is -1 or a leaf index, and
+// position 13 names the leaf itself.  With these, every particle index the packing and near-field kernels form
+// lies in [0, n) and every source record in [0, n + 2), inside the scratch array.  A failure sets status[1].
+__global__ void noalloc_check_tables(long long n, long long nleaves, const long long *__restrict__ leaf_keys,
+                                     const long long *__restrict__ leaf_start, const int *__restrict__ nbr,
+                                     long long key_end, int *__restrict__ status) {
+  bool bad = false;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nleaves * 27; i += stride) {
+    const int v = nbr[i];
+    const long long leaf = i / 27;
+    bad |= v < -1 || v >= nleaves || (i % 27 == 13 && v != leaf);
+    if (i % 27 == 0) {
+      const long long s0 = leaf_start[leaf], s1 = leaf_start[leaf + 1], k = leaf_keys[leaf];
+      bad |= s0 < 0 || s1 < s0 || s1 > n || k < 0 || k >= key_end;
+      bad |= leaf == 0 && s0 != 0;
+      bad |= leaf == nleaves - 1 && s1 != n;
+      bad |= leaf > 0 && leaf_keys[leaf - 1] >= k;
+    }
+  }
+  if (bad) atomicExch(status + 1, 1);
+}
 }  // namespace
 }  // namespace b200
 
@@ -490,7 +528,20 @@ extern "C" b200fmm_status b200fmm_p2p_noalloc(long long n, const double *x, cons
   int *status = nullptr;
   B200_CHECK(noalloc_addresses(&stage, &status));
   cudaStream_t s = (cudaStream_t)stream;
+  int st[2] = {0, 0};
+  // 1) the tables, read back before anything indexes through them
   B200_CUDA(cudaMemsetAsync(status, 0, sizeof(int) * 4, s));
+  const long long key_end = 1LL << (3 * (height - 1));
+  noalloc_check_tables<<<grid_for(nleaves * 27, 256) < 1184 ? grid_for(nleaves * 27, 256) : 1184, 256, 0, s>>>(
+      n, nleaves, leaf_keys, leaf_start, leaf_nbr, key_end, status);
+  B200_CUDA(cudaGetLastError());
+  B200_CUDA(cudaMemcpyAsync(st, status, sizeof(st), cudaMemcpyDeviceToHost, s));
+  B200_CUDA(cudaStreamSynchronize(s));
+  if (st[1])
+    return fail(B200FMM_ERR_INVALID,
+                "p2p_noalloc: inconsistent leaf tables (leaf_start must rise from 0 to n, leaf keys rise strictly "
+                "inside the leaf level, neighbour entries be -1 or a leaf index with position 13 the leaf itself)");
+  // 2) the FP32 copies and the near field
   pack_records32<<<(unsigned)nleaves, 64, 0, s>>>(n, 1, leaf_start, nullptr, nullptr, x, y, z, q,
                                                  center[0] - box_width / 2, center[1] - box_width / 2,
                                                  center[2] - box_width / 2, stage, stage + n, stage + 2 * n);
@@ -498,10 +549,8 @@ extern "C" b200fmm_status b200fmm_p2p_noalloc(long long n, const double *x, cons
       1, n, nleaves, leaf_start, leaf_nbr, variant, nullptr, nullptr, stage, stage + n, stage + 2 * n, phi, fx, fy, fz,
       status);
   B200_CUDA(cudaGetLastError());
-  int st = 0;
-  B200_CUDA(cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  B200_CUDA(cudaMemcpyAsync(st, status, sizeof(st), cudaMemcpyDeviceToHost, s));
   B200_CUDA(cudaStreamSynchronize(s));
-  if (st) return fail(B200FMM_ERR_CUDA, "p2p_noalloc: a device wait ran out of its iteration budget");
+  if (st[0]) return fail(B200FMM_ERR_CUDA, "p2p_noalloc: a device wait ran out of its iteration budget");
   return B200FMM_OK;
 }
-

@@ -499,6 +499,7 @@ b200fmm_status upload_sym_operators(Context &c) {
   std::vector<int> trank;
   std::vector<double> Ut, Vt;
   B200_CHECK(sym_slot_factors(c, Ut, Vt, toff, trank));
+  B200_CHECK(sym64_prepare(c, Ut, Vt, toff, trank));
   const long long tot = (long long)Ut.size();
   B200_CUDA(cudaMalloc(&c.d_Ut, sizeof(double) * std::max<long long>(tot, 1)));
   B200_CUDA(cudaMalloc(&c.d_Vt, sizeof(double) * std::max<long long>(tot, 1)));

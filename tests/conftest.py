@@ -10,7 +10,9 @@ sys.path.insert(0, str(ROOT))
 os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
 
 GOLDEN = ROOT / "tests" / "golden"
-REFERENCE_DATA = Path("/root/reference/Data")
+# the reference source tree (read as data where it exists): SCALFMM_REFERENCE, by default /root/reference
+REFERENCE = Path(os.environ.get("SCALFMM_REFERENCE", "/root/reference"))
+REFERENCE_DATA = REFERENCE / "Data"
 
 
 def pytest_configure(config):

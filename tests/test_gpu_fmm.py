@@ -121,6 +121,54 @@ def test_tree_is_bit_exact_with_oracle():
     f.close()
 
 
+def _tree_case(kind, n, seed):
+    from distributions import ellipsoid_surface, plummer
+
+    rng = np.random.default_rng(seed)
+    if kind == "uniform":
+        x, y, z = rng.random((3, n))
+    elif kind == "plummer":
+        x, y, z = plummer(n, seed)
+    else:
+        x, y, z = ellipsoid_surface(n, seed)
+    return x, y, z, rng.uniform(-1, 1, n)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("kind", ["uniform", "plummer", "ellipsoid"])
+def test_tree_lists_are_bit_exact_with_oracle(kind, precision):
+    """The 26-neighbour leaf lists and the 189-candidate interaction lists of every level, element by element,
+    against the oracle's restatement of FTreeCoordinate::getNeighborsIndexes / getInteractionNeighbors
+    (Src/Containers/FTreeCoordinate.hpp:189-264) filtered to the cells that exist, as FOctree does
+    (Src/Containers/FOctree.hpp:914-975, 1364-1400)."""
+    H = 5
+    x, y, z, q = _tree_case(kind, 20000, 11)
+    f = S.FMM("cheb_sym", 3, H, precision=precision)
+    f.set_particles(x, y, z, q)
+    leaf_keys, _, _ = f.cells(H - 1, expansions=False)
+    index = {int(k): i for i, k in enumerate(leaf_keys)}
+    nbr = f.leaf_neighbors()
+    assert nbr.shape == (leaf_keys.size, 27)
+    for i, k in enumerate(leaf_keys):
+        ok, opos = O.leaf_neighbors(*O.morton_decode(int(k)), H)
+        want = np.full(27, -1, np.int32)
+        want[13] = i
+        for kk, pp in zip(ok.tolist(), opos.tolist()):
+            want[pp] = index.get(kk, -1)
+        assert (nbr[i] == want).all(), (i, nbr[i], want)
+    for lvl in range(2, H):
+        keys, _, _ = f.cells(lvl, expansions=False)
+        idx = {int(k): i for i, k in enumerate(keys)}
+        src, pos = f.interaction_lists(lvl)
+        for i, k in enumerate(keys):
+            ok, opos = O.interaction_list(*O.morton_decode(int(k)), lvl)
+            want = sorted((pp, idx[kk]) for kk, pp in zip(ok.tolist(), opos.tolist()) if kk in idx)
+            got = sorted((int(p_), int(s_)) for p_, s_ in zip(pos[i], src[i]) if s_ >= 0)
+            assert got == want, (lvl, i)
+            assert ((src[i] >= 0) == (pos[i] >= 0)).all()
+    f.close()
+
+
 def test_direct_gpu_matches_reference(golden):
     g = golden("direct_n1500.npz")
     d = S.direct(g["x"], g["y"], g["z"], g["q"])
