@@ -161,6 +161,9 @@ B200FMM_API b200fmm_status b200fmm_get_cells(b200fmm_handle h, int level, long l
  *   cell is empty or outside the box -- the far neighbours FOctree::getInteractionNeighbors returns
  *   (FOctree.hpp:914-975, FTreeCoordinate.hpp:219-264).  Either pointer may be NULL. */
 B200FMM_API b200fmm_status b200fmm_get_leaf_neighbors(b200fmm_handle h, int *nbr);
+/* start[nleaves+1]: the particles of leaf i are sorted positions start[i] .. start[i+1]-1 (get_permutation maps
+ * them to the caller's order) -- the leaf containers of FOctree (FOctree.hpp:174-181). */
+B200FMM_API b200fmm_status b200fmm_get_leaf_ranges(b200fmm_handle h, long long *start);
 B200FMM_API b200fmm_status b200fmm_get_interaction_lists(b200fmm_handle h, int level, int *src, int *pos);
 /* Sorted position -> original particle index. */
 B200FMM_API b200fmm_status b200fmm_get_permutation(b200fmm_handle h, long long *perm);
@@ -227,6 +230,18 @@ B200FMM_API b200fmm_status b200fmm_batch_execute(b200fmm_batch b, int nproblems,
 /* Host wall time of the last batch_execute(), milliseconds. */
 B200FMM_API b200fmm_status b200fmm_batch_last_time(b200fmm_batch b, double *ms);
 B200FMM_API b200fmm_status b200fmm_batch_destroy(b200fmm_batch b);
+
+/* Particle files of ScalFMM's FFmaGenericLoader / FFmaGenericWriter (Src/Files/FFmaGenericLoader.hpp:189-477):
+ * binary when the name contains ".bfma" (unsigned int {8, nvalues}, long long n, double half width, double
+ * centre[3], then n records of nvalues doubles), text when it contains ".fma" (the same fields, whitespace
+ * separated, one particle per line).  Records are x, y, z, q and, with 8 values, phi, fx, fy, fz.
+ * fma_read fills n, nvalues, box_width (twice the stored half width) and centre, and, when data is not NULL, the
+ * n * nvalues values (B200FMM_ERR_INVALID if cap is smaller); call it once with data = NULL to size the buffer.
+ * Host memory only; no GPU is involved. */
+B200FMM_API b200fmm_status b200fmm_fma_read(const char *path, long long *n, int *nvalues, double *box_width,
+                                            double *center, double *data, long long cap);
+B200FMM_API b200fmm_status b200fmm_fma_write(const char *path, long long n, int nvalues, double box_width,
+                                             const double *center, const double *data);
 
 /* FP64 direct sum on the GPU (Examples/DirectComputation.cpp:104-142) for the listed targets (all if
  * ntargets < 0).  Host pointers; outputs have ntargets (or n) entries. */

@@ -33,7 +33,8 @@ EXPORTS = (
     "b200fmm_get_permutation", "b200fmm_last_timings", "b200fmm_last_kernel_times", "b200fmm_tree_stats",
     "b200fmm_last_launch_count", "b200fmm_autotune", "b200fmm_p2p_noalloc", "b200fmm_batch_create", "b200fmm_batch_execute",
     "b200fmm_batch_last_time", "b200fmm_batch_destroy", "b200fmm_direct", "b200fmm_m2l_flops",
-    "b200fmm_get_leaf_neighbors", "b200fmm_get_interaction_lists",
+    "b200fmm_get_leaf_neighbors", "b200fmm_get_interaction_lists", "b200fmm_fma_read", "b200fmm_fma_write",
+    "b200fmm_get_leaf_ranges",
 )
 NOALLOC_MAX_PARTICLES = 262144
 
@@ -107,6 +108,9 @@ def lib():
         L.b200fmm_get_cells.argtypes = [ctypes.c_void_p, ctypes.c_int, _lp, _dp, _dp]
         L.b200fmm_get_permutation.argtypes = [ctypes.c_void_p, _lp]
         L.b200fmm_get_leaf_neighbors.argtypes = [ctypes.c_void_p, _ip]
+        L.b200fmm_get_leaf_ranges.argtypes = [ctypes.c_void_p, _lp]
+        L.b200fmm_fma_read.argtypes = [ctypes.c_char_p, _lp, _ip, _dp, _dp, _dp, ctypes.c_longlong]
+        L.b200fmm_fma_write.argtypes = [ctypes.c_char_p, ctypes.c_longlong, ctypes.c_int, ctypes.c_double, _dp, _dp]
         L.b200fmm_get_interaction_lists.argtypes = [ctypes.c_void_p, ctypes.c_int, _ip, _ip]
         L.b200fmm_last_timings.argtypes = [ctypes.c_void_p, _dp]
         L.b200fmm_last_launch_count.argtypes = [ctypes.c_void_p, _lp]
@@ -386,6 +390,28 @@ def direct(x, y, z, q, targets=None):
     _check(lib().b200fmm_direct(x.size, _ptr(x), _ptr(y), _ptr(z), _ptr(q), -1 if t is None else nt,
                                 None if t is None else _ptr(t, _lp), *[_ptr(o) for o in out]), "direct")
     return dict(zip(("phi", "fx", "fy", "fz"), out))
+
+
+def read_fma(path):
+    """A .fma (text) or .bfma (binary) particle file (FFmaGenericLoader): dict(box_width, center, data[n, nvalues])."""
+    n, nv = ctypes.c_longlong(), ctypes.c_int()
+    w = ctypes.c_double()
+    c = np.zeros(3)
+    p = str(path).encode()
+    _check(lib().b200fmm_fma_read(p, ctypes.byref(n), ctypes.byref(nv), ctypes.byref(w), _ptr(c), None, 0),
+           "fma_read")
+    data = np.zeros(n.value * nv.value)
+    _check(lib().b200fmm_fma_read(p, ctypes.byref(n), ctypes.byref(nv), ctypes.byref(w), _ptr(c), _ptr(data),
+                                  data.size), "fma_read")
+    return dict(box_width=w.value, center=tuple(c), data=data.reshape(n.value, nv.value))
+
+
+def write_fma(path, data, box_width=1.0, center=(0.5, 0.5, 0.5)):
+    """Write particles (an [n, nvalues] array: x, y, z, q[, phi, fx, fy, fz]) as .fma or .bfma."""
+    data = np.ascontiguousarray(data, dtype=np.float64)
+    c = _f64(center)
+    _check(lib().b200fmm_fma_write(str(path).encode(), data.shape[0], data.shape[1], box_width, _ptr(c), _ptr(data)),
+           "fma_write")
 
 
 def rel_l2(a, b):

@@ -645,6 +645,19 @@ b200fmm_status b200fmm_get_leaf_neighbors(b200fmm_handle h, int *nbr) {
   return B200FMM_OK;
 }
 
+b200fmm_status b200fmm_get_leaf_ranges(b200fmm_handle h, long long *start) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  B200_CHECK(need_particles(c));
+  if (!start) return fail(B200FMM_ERR_INVALID, "null argument");
+  B200_CHECK(set_device(c));
+  const Level &L = c.lv[c.H - 1];
+  B200_CUDA(cudaMemcpyAsync(start, c.d_leaf_start, sizeof(long long) * ((size_t)L.n + 1), cudaMemcpyDeviceToHost,
+                            c.stream));
+  B200_CUDA(cudaStreamSynchronize(c.stream));
+  return B200FMM_OK;
+}
+
 b200fmm_status b200fmm_get_interaction_lists(b200fmm_handle h, int level, int *src, int *pos) {
   B200_CHECK(check_handle(h));
   Context &c = *h;

@@ -1538,7 +1538,12 @@ static b200fmm_status tc_init_lowrank(Context &c, DenseTC &t, TcParams &P, bool 
     ybytes += (double)c.R * ych * std::max(h, (double)TILE_X) * std::max(h, (double)TILE_Y) *
               std::max(h, (double)TILE_Z) * 16 * 2 * 2;
   }
-  if (ybytes > 12e9) {
+  // the cap: 30 % of the device's memory (54 GB on a B200; 16 right-hand sides at height 6 take 14 GB), at
+  // least 12 GB
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) total_b = 0;
+  cudaGetLastError();
+  if (ybytes > std::max(12e9, 0.3 * (double)total_b)) {
     use = false;
     return B200FMM_OK;
   }
