@@ -33,6 +33,19 @@
  * Src/Kernels/Chebyshev/FChebCell.hpp:39-55); ContainerClass needs getNbParticles(), getPositions(),
  * getPhysicalValues(rhs), getPotentials(rhs), getForcesX/Y/Z(rhs) (FP2PParticleContainer,
  * Src/Kernels/P2P/FP2PParticleContainer.hpp).
+ *
+ * FB200GroupKernel is the same adapter for the blocked tree FGroupTree (Src/GroupTree/Core/FGroupTree.hpp),
+ * driven by FGroupSeqAlgorithm (Src/GroupTree/Core/FGroupSeqAlgorithm.hpp:58-404).  There the cells and leaves
+ * the driver passes are views built on the fly over the blocks' arrays -- FChebCellPOD
+ * (Src/GroupTree/Chebyshev/FChebCellPOD.hpp) points at a cell's symbolic data, multipole and local inside
+ * FGroupOfCells (Src/GroupTree/Core/FGroupOfCells.hpp:18-120); FP2PGroupParticleContainer points at a leaf's
+ * slice of FGroupOfParticles (Src/GroupTree/Core/FGroupOfParticles.hpp:21-200) -- and live only for the call.
+ * The group adapter therefore keeps copies of the views (their pointers stay valid, the blocks are the tree's),
+ * and reads particles from and writes expansions and results into the block arrays through them.  The
+ * driver splits the transfer and direct passes into in-block calls and out-of-block pairs (M2L / P2POuter
+ * with one source); the level-batched GPU operators cover both, so the first P2P call of a direct pass runs
+ * the whole near field and the P2POuter calls that complete it across blocks add nothing more.  The driver
+ * calls no finishedLevelM2L: a level's M2L runs when the driver moves to the next level or operator.
  */
 #ifndef B200FMM_SCALFMM_HPP
 #define B200FMM_SCALFMM_HPP
@@ -43,6 +56,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "b200fmm.h"
@@ -53,9 +67,37 @@ inline void check(b200fmm_status st, const char *what) {
   if (st != B200FMM_OK) throw std::runtime_error(std::string("FB200Kernel: ") + what + ": " + b200fmm_last_error());
 }
 
-template <class CellClass, class ContainerClass, int ORDER, int NVALS = 1>
-class FB200Kernel {
+// VIEWS = false: the driver's cells and containers are long-lived objects (FOctree), kept by pointer;
+// VIEWS = true: they are views valid only during the call (FGroupTree), kept by value.
+template <class CellClass, class ContainerClass, int ORDER, int NVALS = 1, bool VIEWS = false>
+class FB200KernelT {
   enum class Op { None, P2M, M2M, M2L, L2L, Direct };
+  using CellRef = typename std::conditional<VIEWS, CellClass, CellClass *>::type;
+  using ContRef = typename std::conditional<VIEWS, ContainerClass, ContainerClass *>::type;
+  static CellRef keep(CellClass *c) {
+    if constexpr (VIEWS)
+      return *c;
+    else
+      return c;
+  }
+  static ContRef keep(ContainerClass *c) {
+    if constexpr (VIEWS)
+      return *c;
+    else
+      return c;
+  }
+  static CellClass &use(CellRef &c) {
+    if constexpr (VIEWS)
+      return c;
+    else
+      return *c;
+  }
+  static ContainerClass &use(ContRef &c) {
+    if constexpr (VIEWS)
+      return c;
+    else
+      return *c;
+  }
 
   struct State {
     b200fmm_handle h = nullptr;
@@ -64,10 +106,9 @@ class FB200Kernel {
     Op pending = Op::None;
     int pending_level = -1;
     bool tree_ready = false, l2p_done = false, p2p_done = false, p2p_outer_done = false;
-    std::vector<CellClass *> leaf_cells;
-    std::vector<const ContainerClass *> leaf_src;
-    std::vector<ContainerClass *> leaf_tgt;
-    std::vector<CellClass *> cells;  // cells waiting for the write-back of the pending operator
+    std::vector<CellRef> leaf_cells;
+    std::vector<ContRef> leaf_tgt;  // the leaves' containers, sources and targets alike
+    std::vector<CellRef> cells;     // cells waiting for the write-back of the pending operator
     std::vector<long long> m2l_flushed;
     ~State() {
       if (h) b200fmm_destroy(h);
@@ -82,8 +123,8 @@ class FB200Kernel {
    * (Src/Kernels/Chebyshev/FChebSymKernel.hpp:136-140); the matrix kernel is 1/r.  PointClass has
    * getX/getY/getZ (FPoint).  kernel: b200fmm_kernel, precision: b200fmm_precision. */
   template <class PointClass>
-  FB200Kernel(int treeHeight, double boxWidth, const PointClass &boxCenter, int kernel = B200FMM_CHEB_SYM,
-              int precision = B200FMM_FP64, double epsilon = -1.0, void *stream = nullptr, int device = -1)
+  FB200KernelT(int treeHeight, double boxWidth, const PointClass &boxCenter, int kernel = B200FMM_CHEB_SYM,
+               int precision = B200FMM_FP64, double epsilon = -1.0, void *stream = nullptr, int device = -1)
       : s_(std::make_shared<State>()) {
     b200fmm_config cfg{};
     cfg.kernel = kernel;
@@ -101,7 +142,7 @@ class FB200Kernel {
     check(b200fmm_create(&cfg, &s_->h), "create");
     s_->height = treeHeight;
   }
-  FB200Kernel(const FB200Kernel &) = default;  // copies share the state (FFmmAlgorithmThread copies kernels)
+  FB200KernelT(const FB200KernelT &) = default;  // copies share the state (FFmmAlgorithmThread copies kernels)
 
   b200fmm_handle handle() const { return s_->h; }
 
@@ -118,29 +159,27 @@ class FB200Kernel {
     State &s = *s_;
     if (s.pending != Op::P2M) {  // a new bottom pass: a new evaluation
       s.leaf_cells.clear();
-      s.leaf_src.clear();
       s.leaf_tgt.clear();
       s.tree_ready = false;
       s.l2p_done = s.p2p_done = s.p2p_outer_done = false;
       s.m2l_flushed.clear();
       s.pending = Op::P2M;
     }
-    s.leaf_cells.push_back(pole);
-    s.leaf_src.push_back(particles);
-    s.leaf_tgt.push_back(const_cast<ContainerClass *>(particles));
+    s.leaf_cells.push_back(keep(pole));
+    s.leaf_tgt.push_back(keep(const_cast<ContainerClass *>(particles)));
   }
 
   void M2M(CellClass *const pole, const CellClass *const *const /*child*/, const int level) {
     std::lock_guard<std::mutex> g(s_->mu);
     begin(Op::M2M, level);
-    s_->cells.push_back(pole);
+    s_->cells.push_back(keep(pole));
   }
 
   void M2L(CellClass *const local, const CellClass * /*distantNeighbors*/[], const int /*neighborPositions*/[],
            const int /*size*/, const int level) {
     std::lock_guard<std::mutex> g(s_->mu);
     begin(Op::M2L, level);
-    s_->cells.push_back(local);
+    s_->cells.push_back(keep(local));
   }
 
   void finishedLevelM2L(const int level) {
@@ -155,7 +194,7 @@ class FB200Kernel {
     std::lock_guard<std::mutex> g(s_->mu);
     begin(Op::L2L, level);
     for (int k = 0; k < 8; ++k)
-      if (child[k]) s_->cells.push_back(child[k]);
+      if (child[k]) s_->cells.push_back(keep(child[k]));
   }
 
   void L2P(const CellClass *const /*local*/, ContainerClass *const /*particles*/) {
@@ -183,6 +222,9 @@ class FB200Kernel {
                 ContainerClass *const /*directNeighbors*/[], const int /*neighborPositions*/[], const int /*size*/) {
     std::lock_guard<std::mutex> g(s_->mu);
     begin(Op::Direct, -1);
+    // the blocked driver completes its in-block P2P calls with cross-block P2POuter pairs: the whole near field
+    // ran at the first P2P call already
+    if (VIEWS && s_->p2p_done) return;
     if (s_->p2p_outer_done) return;
     run_direct([&] { check(b200fmm_p2p(s_->h, 1), "p2p (neighbours only)"); });
     s_->p2p_outer_done = true;
@@ -228,7 +270,8 @@ class FB200Kernel {
     std::vector<double> v((size_t)n * NVALS * nnodes);
     check(b200fmm_get_cells(s.h, level, keys.data(), multipoles ? v.data() : nullptr, multipoles ? nullptr : v.data()),
           "get_cells");
-    for (CellClass *c : s.cells) {
+    for (CellRef &cr : s.cells) {
+      CellClass *c = &use(cr);
       const long long key = (long long)c->getMortonIndex();
       const auto it = std::lower_bound(keys.begin(), keys.end(), key);
       if (it == keys.end() || *it != key) throw std::runtime_error("FB200Kernel: a cell of the driver's tree is not in the GPU tree");
@@ -268,10 +311,11 @@ class FB200Kernel {
   void flush_p2m() {
     State &s = *s_;
     long long n = 0;
-    for (const ContainerClass *c : s.leaf_src) n += (long long)c->getNbParticles();
+    for (ContRef &cr : s.leaf_tgt) n += (long long)use(cr).getNbParticles();
     std::vector<double> x((size_t)n), y((size_t)n), z((size_t)n), q((size_t)n * NVALS);
     long long off = 0;
-    for (const ContainerClass *c : s.leaf_src) {
+    for (ContRef &cr : s.leaf_tgt) {
+      const ContainerClass *c = &use(cr);
       const long long m = (long long)c->getNbParticles();
       const auto *const *pos = c->getPositions();
       for (long long k = 0; k < m; ++k) {
@@ -305,7 +349,8 @@ class FB200Kernel {
     std::vector<double> phi((size_t)n * NVALS), fx(phi.size()), fy(phi.size()), fz(phi.size());
     check(b200fmm_get_results(s.h, phi.data(), fx.data(), fy.data(), fz.data(), 0), "get_results");
     long long off = 0;
-    for (ContainerClass *c : s.leaf_tgt) {
+    for (ContRef &cr : s.leaf_tgt) {
+      ContainerClass *c = &use(cr);
       const long long m = (long long)c->getNbParticles();
       for (int r = 0; r < NVALS; ++r) {
         auto *p = c->getPotentials(r);
@@ -324,6 +369,13 @@ class FB200Kernel {
     }
   }
 };
+
+// The adapter for the pointer octree FOctree (FFmmAlgorithm, FFmmAlgorithmThread).
+template <class CellClass, class ContainerClass, int ORDER, int NVALS = 1>
+using FB200Kernel = FB200KernelT<CellClass, ContainerClass, ORDER, NVALS, false>;
+// The adapter for the blocked tree FGroupTree (FGroupSeqAlgorithm), whose cells and leaves are views.
+template <class CellClass, class ContainerClass, int ORDER, int NVALS = 1>
+using FB200GroupKernel = FB200KernelT<CellClass, ContainerClass, ORDER, NVALS, true>;
 
 }  // namespace b200fmm_scalfmm
 

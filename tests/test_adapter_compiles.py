@@ -31,7 +31,8 @@ struct Container {
   double *getForcesZ(int = 0) { return v; }
 };
 struct Coord {};
-template class b200fmm_scalfmm::FB200Kernel<Cell, Container, 4, 2>;
+template class b200fmm_scalfmm::FB200KernelT<Cell, Container, 4, 2, false>;
+template class b200fmm_scalfmm::FB200KernelT<Cell, Container, 4, 2, true>;
 void use(b200fmm_scalfmm::FB200Kernel<Cell, Container, 4, 2> &k, Cell *c, Container *t, Cell **ch,
          const Cell **nb, const int *pos, Container **nbp) {
   static_assert(b200fmm_scalfmm::FB200Kernel<Cell, Container, 4, 2>::NeedFinishedM2LEvent(), "flush event");

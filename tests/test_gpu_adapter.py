@@ -1,6 +1,7 @@
 """Drop-in check of the FB200Kernel adapter (include/b200fmm_scalfmm.hpp).
 
-The reference's own algorithm drivers (FFmmAlgorithm, and FFmmAlgorithmThread with one thread) run on two
+The reference's own algorithm drivers (FFmmAlgorithm, FFmmAlgorithmThread with one thread, and FGroupSeqAlgorithm
+over the blocked tree FGroupTree with FB200GroupKernel) run on two
 copies of one octree: once with the reference's FChebSymKernel / FChebDenseKernel, once with the adapter
 over the GPU library.  Potentials and forces of every particle and the multipoles and locals of every
 cell are compared (relative L2, FMath::FAccurater).  The check program is built from the reference sources
@@ -54,3 +55,21 @@ def test_adapter_mixed_close_to_reference():
     for k in ("phi", "fx", "fy", "fz"):
         assert e[k] <= 2e-6, e
     assert e["multipole"] <= 1e-12, e  # P2M/M2M stay FP64 in MIXED
+
+
+@pytest.mark.parametrize("order,height,n", [(5, 4, 3000), (4, 5, 4000)])
+def test_group_tree_adapter_fp64_is_a_drop_in(order, height, n):
+    """The blocked tree (FGroupTree of FChebCellPOD cells and FP2PGroupParticleContainer leaves, blocks of 30
+    cells) driven by the reference's FGroupSeqAlgorithm: its in-block calls, its cross-block M2L and P2POuter
+    pairs and its cell and leaf views all go through FB200GroupKernel, which reads and writes the block arrays.
+    Every particle output and every cell expansion of levels 2..height-1 matches FChebSymKernel on the same
+    blocked tree to 1e-12 (FP64, the reference's compressed operators)."""
+    e = check(kind=0, order=order, precision=FP64, driver=2, height=height, n=n)
+    assert max(e.values()) <= 1e-12, e
+
+
+def test_group_tree_adapter_mixed_close_to_reference():
+    e = check(kind=0, order=7, precision=MIXED, driver=2, height=4, n=3000)
+    for k in ("phi", "fx", "fy", "fz"):
+        assert e[k] <= 2e-6, e
+    assert e["multipole"] <= 1e-12, e
