@@ -18,6 +18,13 @@ constexpr int kMaxHeight = 12;
 // slots per level of the multipole maxima that P2M and M2M record (spread to keep atomics uncontended)
 constexpr int kMmaxSlots = 64;
 constexpr int kMaxNrhs = 32;
+// work items of the FP32 near field (one warp each): a leaf of at most kP2PWholeLeaf targets is one item, a
+// larger leaf is cut into items of kP2PItemTargets targets, so that dense leaves spread over many warps
+constexpr int kP2PWholeLeaf = 64;
+constexpr int kP2PItemTargets = 32;
+__host__ __device__ inline long long p2p_leaf_items(long long n) {
+  return n <= kP2PWholeLeaf ? 1 : (n + kP2PItemTargets - 1) / kP2PItemTargets;
+}
 
 // Error reporting: the last message per host thread.
 void set_error(const std::string &msg);
@@ -112,6 +119,9 @@ struct Context {
   float4 *d_pq32 = nullptr;                               // FP32 near-field copies (MIXED), see p2p.cu
   int *d_leaf_rank = nullptr;      // [nleaves] position of each leaf in the column-major record order (MIXED P2P)
   long long *d_rec_base = nullptr; // [nleaves+1] first source record of each leaf, in that order
+  // [nleaves+1] first work item of each leaf in the FP32 near field (p2p_leaf_items per leaf,
+  // each a work item of its own (the last entry is the item count), so that dense leaves spread over many warps
+  long long *d_chunk_base = nullptr;
   double *d_phi = nullptr, *d_fx = nullptr, *d_fy = nullptr, *d_fz = nullptr;  // [R][N] sorted results
   Level lv[kMaxHeight];
   bool has_particles = false;

@@ -914,6 +914,12 @@ struct __align__(64) LrYParams {
   int ycht, ybase[9];                                    // Y chunks per rhs; first chunk of each parity
   int stages, stage_bytes;
   int *status;
+  // sparse trees: an item whose tile (either tile of a pair) holds no cell is not computed.  Its Y rows must
+  // still read as zero for the second product, so ydirty[2 * item + rank] records whether this CTA's tile rows
+  // of the item hold values of an earlier computation; those are zeroed once, when the tile has become empty.
+  const unsigned *busy;                                  // the second product's tile masks (bit 191: occupied)
+  int tile0[kMaxHeight];                                 // first tile of each level in busy
+  unsigned char *ydirty;                                 // [2 * items of all levels]
 };
 
 constexpr int YBLK = 256;  // rank rows per item (16 chunks of 16)
@@ -1004,6 +1010,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
     y.rhs = r >> 3;
     return y;
   };
+  // whether the item's tile (a pair: either tile) holds a cell; all roles skip the others alike
+  auto occupied = [&](const YItem &y) -> bool {
+    const int l = y.level, TX = P.HX[l] / TILE_X, TY = P.HY[l] / TILE_Y, TZ = P.HZ[l] / TILE_Z;
+    const int bz0 = PAIR ? y.bz - (int)rank : y.bz;
+    auto tile = [&](int bz) {
+      const long long id = P.tile0[l] + (((long long)y.par * TZ + bz) * TY + y.by) * TX + y.bx;
+      return (P.busy[6 * id + 5] >> 31) & 1u;
+    };
+    bool o = bz0 < TZ && tile(bz0);
+    if (PAIR && bz0 + 1 < TZ) o = o || tile(bz0 + 1);
+    return o;
+  };
 
   if (warp < 4) {
   give_registers<true>();  // the epilogue holds 128 running sums per thread
@@ -1014,6 +1032,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
       const unsigned full0 = PAIR ? mapa_shared(su32(&full_bar[0]), 0u) : su32(&full_bar[0]);
       for (int it = g_id; it < nitems && !abort_sh; it += g_count) {
         const YItem y = decode(it);
+        if (!occupied(y)) continue;
         const int vrow = (P.ybase[y.par] + y.nb * (YBLK / 16)) * 16 + (int)rank * vrows;
         for (int kc = 0; kc < P.NK; ++kc) {
           if (!mbar_wait(&empty_bar[stage], phase ^ 1)) {
@@ -1067,6 +1086,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
       int stage = 0;
       unsigned phase = 0, empty_par = 3u;
       for (int it = g_id; it < nitems && !abort_sh; it += g_count) {
+        if (!occupied(decode(it))) continue;
         for (int kc = 0; kc < P.NK && !abort_sh; ++kc) {
           const int b = (kc / segc) & 1;
           const bool first = kc % segc == 0;
@@ -1117,6 +1137,31 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
     float acc[128];
     for (int it = g_id; it < nitems && !abort_sh; it += g_count) {
       const YItem y = decode(it);
+      // one flag per (item, CTA of the pair, epilogue warp): whether this warp's rows of the item hold values
+      unsigned char *dirty = P.ydirty + ((2 * (size_t)(it + P.item0[P.l1]) + rank) * 8 + (warp - 4));
+      if (!occupied(y)) {
+        // an empty tile: its rows of Y must read as zero; clear them if an earlier tree left values there
+        const bool was = *dirty != 0;
+        __syncwarp();
+        if (was) {
+          const int l = y.level;
+          const int hx = y.bx * TILE_X + (row & 7), hy = y.by * TILE_Y + ((row >> 3) & 3),
+                    hz = y.bz * TILE_Z + (row >> 5);
+          const int nch = P.ybase[y.par + 1] - P.ybase[y.par];
+          if (y.bz < P.HZ[l] / TILE_Z)
+            for (int k = 0; k < 8; ++k) {
+              const int chunk = y.nb * (YBLK / 16) + ch * 8 + k;
+              if (chunk >= nch) break;
+              const long long yi = (long long)y.rhs * P.ycht + P.ybase[y.par] + chunk;
+              const long long off = (((yi * P.HZ[l] + hz) * P.HY[l] + hy) * P.HX[l] + hx) * 16;
+              uint4 *dh = (uint4 *)(P.Yhi[l] + off), *dl = (uint4 *)(P.Ylo[l] + off);
+              dh[0] = dh[1] = dl[0] = dl[1] = make_uint4(0u, 0u, 0u, 0u);
+            }
+          __syncwarp();
+          if (lane == 0) *dirty = 0;
+        }
+        continue;
+      }
 #pragma unroll
       for (int i = 0; i < 128; ++i) acc[i] = 0.f;
       for (int sg = 0; sg < nseg; ++sg) {
@@ -1166,6 +1211,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
         dl[0] = make_uint4(lv[0], lv[1], lv[2], lv[3]);
         dl[1] = make_uint4(lv[4], lv[5], lv[6], lv[7]);
       }
+      if (lane == 0) *dirty = 1;
     }
   }
   tc_fence_before();
@@ -1455,6 +1501,8 @@ struct DenseTC {
   bool lr = false;
   __half *Vhi = nullptr, *Vlo = nullptr;  // stacked V rows [16 * ycht][KP]
   __half *Yhi[kMaxHeight] = {}, *Ylo[kMaxHeight] = {};
+  unsigned char *ydirty = nullptr;  // first product: per item, CTA of the pair and epilogue warp, rows hold values
+  size_t ydirty_n = 0;
   size_t Ybytes[kMaxHeight] = {};
   int ycht = 0, nblk = 0, ystages = 0, ystage_bytes = 0;
   // low-rank layout (host side): 16-wide rank chunks of each slot, its first U chunk, the first Y chunk of
@@ -1828,6 +1876,7 @@ void tc_free(Context &c) {
     if (t->Ylo[l]) cudaFree(t->Ylo[l]);
   }
   if (t->sat) cudaFree(t->sat);
+  if (t->ydirty) cudaFree(t->ydirty);
   delete t->params;
   delete t->yparams;
   delete t;
@@ -1841,6 +1890,7 @@ static b200fmm_status tc_prepare(Context &c) {
   const int LL = c.H - 1;
   t->ntiles_all = 0;
   size_t sat_total = 0;
+  bool y_moved = false;  // a level's Y was (re)allocated: every Y row and dirty flag starts from zero
   for (int l = 2; l <= LL; ++l) {
     const int h = 1 << (l - 1);
     t->HX[l] = std::max(h, TILE_X);
@@ -1873,6 +1923,7 @@ static b200fmm_status tc_prepare(Context &c) {
         B200_CUDA(cudaMalloc(&t->Yhi[l], yel * sizeof(__half)));
         B200_CUDA(cudaMalloc(&t->Ylo[l], yel * sizeof(__half)));
         t->Ybytes[l] = yel * sizeof(__half);
+        y_moved = true;
       }
       Y.Yhi[l] = t->Yhi[l];
       Y.Ylo[l] = t->Ylo[l];
@@ -1923,6 +1974,25 @@ static b200fmm_status tc_prepare(Context &c) {
       Y.nitems[l] = c.R * 8 * (t->ypair ? (TZ + 1) / 2 : TZ) * (t->HY[l] / TILE_Y) * (t->HX[l] / TILE_X) * t->nblk;
       n += Y.nitems[l];
     }
+    // the first product skips items of empty tiles; their Y rows must read as zero (dirty flags: 2 CTAs x 8
+    // epilogue warps per item)
+    const size_t nd = (size_t)16 * std::max(n, 1);
+    if (t->ydirty_n != nd) {
+      if (t->ydirty) cudaFree(t->ydirty);
+      t->ydirty = nullptr;
+      B200_CUDA(cudaMalloc(&t->ydirty, nd));
+      t->ydirty_n = nd;
+      y_moved = true;
+    }
+    if (y_moved) {
+      B200_CUDA(cudaMemsetAsync(t->ydirty, 0, nd, c.stream));
+      for (int l = 2; l <= LL; ++l) {
+        B200_CUDA(cudaMemsetAsync(t->Yhi[l], 0, t->Ybytes[l], c.stream));
+        B200_CUDA(cudaMemsetAsync(t->Ylo[l], 0, t->Ybytes[l], c.stream));
+      }
+    }
+    Y.ydirty = t->ydirty;
+    for (int l = 2; l <= LL; ++l) Y.tile0[l] = P.lv[l].tile0;
   }
   int ns = t->splits > 0 ? t->splits : 1;  // work ranges per CTA (pair), chosen by b200fmm_autotune
   if (const char *e = getenv("B200FMM_TC_SPLITS")) ns = std::max(1, std::min(64, atoi(e)));
@@ -1936,6 +2006,7 @@ static b200fmm_status tc_prepare(Context &c) {
   if (t->busy) cudaFree(t->busy);
   B200_CUDA(cudaMalloc(&t->busy, sizeof(unsigned) * 6 * std::max<long long>(t->ntiles_all, 1)));
   P.busy = t->busy;
+  if (t->lr) t->yparams->busy = t->busy;
   if (t->prefix) cudaFree(t->prefix);
   B200_CUDA(cudaMalloc(&t->prefix, sizeof(int) * (nunits + 1)));
   P.prefix = t->prefix;

@@ -235,27 +235,61 @@ __device__ __forceinline__ void p2p_record(const float4 *__restrict__ s, int k, 
 // each split into stages of <= P2P32_STAGE records copied by one bulk copy into a ring of P2P32_NBUF buffers,
 // issued P2P32_NBUF - 1 stages ahead of the math.  Per stage the partial sums enter the target's (hi, lo)
 // accumulators by a two-sum.
+// With chunk_base, warp (CTA x, warp w) takes the work item blockIdx.x * P2P32_WARPS + w: a leaf of at most
+// kP2PWholeLeaf targets, or kP2PItemTargets targets of a larger one (a dense leaf spreads over many warps; items
+// past the count leave at once).  Without it (the allocation-free entry point) a warp takes a whole leaf.
+__device__ __forceinline__ bool p2p_item(long long item, long long nleaves, const long long *__restrict__ leaf_start,
+                                         const long long *__restrict__ chunk_base, long long &leaf, long long &c0,
+                                         long long &c1) {
+  if (!chunk_base) {
+    if (item >= nleaves) return false;
+    leaf = item;
+    c0 = leaf_start[leaf];
+    c1 = leaf_start[leaf + 1];
+    return true;
+  }
+  if (item >= chunk_base[nleaves]) return false;
+  long long lo = 0, hi = nleaves - 1;  // the last leaf whose first item is <= item
+  while (lo < hi) {
+    const long long mid = (lo + hi + 1) >> 1;
+    if (chunk_base[mid] <= item)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  leaf = lo;
+  const long long s0 = leaf_start[leaf], s1 = leaf_start[leaf + 1];
+  if (s1 - s0 <= kP2PWholeLeaf) {
+    c0 = s0;
+    c1 = s1;
+  } else {
+    c0 = s0 + (long long)kP2PItemTargets * (item - chunk_base[leaf]);
+    c1 = min(c0 + kP2PItemTargets, s1);
+  }
+  return true;
+}
+
 __global__ void __launch_bounds__(P2P32_WARPS * 32, 7) p2p_fp32_kernel(
     int R, long long N, long long nleaves, const long long *__restrict__ leaf_start, const int *__restrict__ nbr,
     int variant, const int *__restrict__ rank_of, const long long *__restrict__ rec_base,
-    const float4 *__restrict__ pq, const float4 *__restrict__ plo, const float4 *__restrict__ src,
-    double *__restrict__ phi, double *__restrict__ fx, double *__restrict__ fy, double *__restrict__ fz,
-    int *__restrict__ status) {
+    const long long *__restrict__ chunk_base, const float4 *__restrict__ pq, const float4 *__restrict__ plo,
+    const float4 *__restrict__ src, double *__restrict__ phi, double *__restrict__ fx, double *__restrict__ fy,
+    double *__restrict__ fz, int *__restrict__ status) {
   __shared__ __align__(128) float4 buf[P2P32_WARPS][P2P32_NBUF][4 * P2P32_STAGE];
   __shared__ __align__(8) unsigned long long bar[P2P32_WARPS][P2P32_NBUF];
   __shared__ long long rbase[P2P32_WARPS][27];
   __shared__ int rcount[P2P32_WARPS][27];
   __shared__ unsigned char rself[P2P32_WARPS][27];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long long leaf = (long long)blockIdx.x * P2P32_WARPS + w;
   if (lane == 0) {
     for (int b = 0; b < P2P32_NBUF; ++b) mbar_init(&bar[w][b], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncwarp();
-  if (leaf >= nleaves) return;
+  long long leaf, c0, c1;
+  if (!p2p_item((long long)blockIdx.x * P2P32_WARPS + w, nleaves, leaf_start, chunk_base, leaf, c0, c1)) return;
   const long long P = p2p_pairs_capacity(N);
-  const long long t0 = leaf_start[leaf], t1 = leaf_start[leaf + 1];
+  const long long t0 = leaf_start[leaf];
   const int my_rank = rank_of ? rank_of[leaf] : (int)leaf;
   const long long self_rec = rec_begin(rec_base, leaf_start, my_rank);
   // the runs of this leaf: lane e < 27 looks at neighbour position e = ((dx+1)*3 + dy+1)*3 + dz+1
@@ -290,8 +324,8 @@ __global__ void __launch_bounds__(P2P32_WARPS * 32, 7) p2p_fp32_kernel(
   for (int r = 0; r < R; ++r) {
     const float4 *pr = pq + (long long)r * N;
     const float4 *sr = src + (long long)r * P * 4;
-    for (long long tb = t0; tb < t1; tb += 32) {
-      const int m = (int)min(32LL, t1 - tb);
+    for (long long tb = c0; tb < c1; tb += 32) {
+      const int m = (int)min(32LL, c1 - tb);
       const int T = m <= 8 ? 8 : (m <= 16 ? 16 : 32);  // targets per lane group
       const int G = 32 / T;                             // lane groups, each on every G-th record
       const int tl = lane & (T - 1), g = lane / T;
@@ -408,13 +442,305 @@ __global__ void __launch_bounds__(P2P32_WARPS * 32, 7) p2p_fp32_kernel(
   }
 }
 
+// ---- several right-hand sides ------------------------------------------------------------------------
+//
+// With nrhs > 1 the charge vectors share the positions, so the geometry of a pair (differences, r^2, rsqrt,
+// 1/r^3) is formed once for MR_G right-hand sides at a time, as the reference's multi-RHS near field forms it
+// once for all NVALS vectors (FP2P::FullMutualMultiRhs, Src/Kernels/P2P/FP2PMultiRhs.hpp:10-189).  Layout:
+//   tgt_hi[N] float4 (x_hi, y_hi, z_hi, 0), tgt_lo[N] float4 (x_lo, y_lo, z_lo, 0), tgt_q[R][N] float;
+//   src[G][N+2][5] float4 for each group of MR_G right-hand sides, two sources per 80-byte record:
+//     (-x0,-x1,-y0,-y1) (-z0,-z1,-lz0,-lz1) (-lx0,-lx1,-ly0,-ly1) (q0,q1 of rhs 0; q0,q1 of rhs 1) (rhs 2; rhs 3),
+//   charges of right-hand sides past R are zero.  Record order and runs are those of the single-RHS kernel.
+constexpr int MR_G = 4;
+constexpr int MR_REC = 5;  // float4 per record
+
+__global__ void pack_records32_mrhs(long long N, int R, const long long *__restrict__ leaf_start,
+                                    const int *__restrict__ rank_of, const long long *__restrict__ rec_base,
+                                    const double *__restrict__ x, const double *__restrict__ y,
+                                    const double *__restrict__ z, const double *__restrict__ q, double x0, double y0,
+                                    double z0, float4 *__restrict__ hi, float4 *__restrict__ lo, float *__restrict__ qt,
+                                    float4 *__restrict__ src) {
+  const long long leaf = blockIdx.x;
+  const long long s0 = leaf_start[leaf], s1 = leaf_start[leaf + 1];
+  const long long rank = rank_of ? rank_of[leaf] : leaf;
+  const long long b0 = rec_begin(rec_base, leaf_start, rank), b1 = rec_begin(rec_base, leaf_start, rank + 1);
+  for (long long i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
+    const double lx = x[i] - x0, ly = y[i] - y0, lz = z[i] - z0;
+    const float hx = (float)lx, hy = (float)ly, hz = (float)lz;
+    hi[i] = make_float4(hx, hy, hz, 0.f);
+    lo[i] = make_float4((float)(lx - (double)hx), (float)(ly - (double)hy), (float)(lz - (double)hz), 0.f);
+    for (int r = 0; r < R; ++r) qt[(long long)r * N + i] = (float)q[(long long)r * N + i];
+  }
+  const long long P = p2p_pairs_capacity(N);
+  const int G = (R + MR_G - 1) / MR_G;
+  for (long long pp = threadIdx.x; pp < b1 - b0; pp += blockDim.x) {
+    float h[2][3], l[2][3];
+    bool real[2];
+    for (int u = 0; u < 2; ++u) {
+      const long long j = s0 + 2 * pp + u;
+      real[u] = j < s1;
+      const double d[3] = {real[u] ? x[j] - x0 : P2P32_PAD, real[u] ? y[j] - y0 : P2P32_PAD,
+                           real[u] ? z[j] - z0 : P2P32_PAD};
+      for (int a = 0; a < 3; ++a) {
+        h[u][a] = (float)d[a];
+        l[u][a] = (float)(d[a] - (double)h[u][a]);
+      }
+    }
+    const long long j0 = s0 + 2 * pp;
+    auto charge = [&](int r, int u) -> float {
+      return (r < R && real[u]) ? (float)q[(long long)r * N + j0 + u] : 0.f;
+    };
+    for (int g = 0; g < G; ++g) {
+      float4 *rec = src + ((long long)g * P + b0 + pp) * MR_REC;
+      rec[0] = make_float4(-h[0][0], -h[1][0], -h[0][1], -h[1][1]);
+      rec[1] = make_float4(-h[0][2], -h[1][2], -l[0][2], -l[1][2]);
+      rec[2] = make_float4(-l[0][0], -l[1][0], -l[0][1], -l[1][1]);
+      const int r0 = MR_G * g;
+      rec[3] = make_float4(charge(r0, 0), charge(r0, 1), charge(r0 + 1, 0), charge(r0 + 1, 1));
+      rec[4] = make_float4(charge(r0 + 2, 0), charge(r0 + 2, 1), charge(r0 + 3, 0), charge(r0 + 3, 1));
+    }
+  }
+}
+
+// One record (two sources) against the lane's target for MR_G right-hand sides: the geometry once, then per
+// right-hand side phi += q / r and the force sums q d / r^3.
+template <bool SELF>
+__device__ __forceinline__ void p2p_record_mrhs(const float4 *__restrict__ s, int k, int self_rel, float2 th_x,
+                                                float2 th_y, float2 th_z, float2 tl_x, float2 tl_y, float2 tl_z,
+                                                float2 (&pv)[MR_G], float2 (&ax)[MR_G], float2 (&ay)[MR_G],
+                                                float2 (&az)[MR_G]) {
+  const float4 A = s[MR_REC * k], B = s[MR_REC * k + 1], C = s[MR_REC * k + 2], Q0 = s[MR_REC * k + 3],
+               Q1 = s[MR_REC * k + 4];
+  const float2 dx = __fadd2_rn(__fadd2_rn(th_x, make_float2(A.x, A.y)), __fadd2_rn(tl_x, make_float2(C.x, C.y)));
+  const float2 dy = __fadd2_rn(__fadd2_rn(th_y, make_float2(A.z, A.w)), __fadd2_rn(tl_y, make_float2(C.z, C.w)));
+  const float2 dz = __fadd2_rn(__fadd2_rn(th_z, make_float2(B.x, B.y)), __fadd2_rn(tl_z, make_float2(B.z, B.w)));
+  float2 r2 = __fmul2_rn(dx, dx);
+  r2 = __ffma2_rn(dy, dy, r2);
+  r2 = __ffma2_rn(dz, dz, r2);
+  float2 inv;
+  if (SELF) {
+    inv = make_float2(2 * k == self_rel ? 0.f : rsqrtf(r2.x), 2 * k + 1 == self_rel ? 0.f : rsqrtf(r2.y));
+  } else {
+    inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+  }
+  const float2 inv2 = __fmul2_rn(inv, inv);
+  const float2 q[MR_G] = {make_float2(Q0.x, Q0.y), make_float2(Q0.z, Q0.w), make_float2(Q1.x, Q1.y),
+                          make_float2(Q1.z, Q1.w)};
+#pragma unroll
+  for (int g = 0; g < MR_G; ++g) {
+    const float2 qi = __fmul2_rn(q[g], inv);
+    const float2 qi3 = __fmul2_rn(qi, inv2);
+    pv[g] = __fadd2_rn(pv[g], qi);
+    ax[g] = __ffma2_rn(dx, qi3, ax[g]);
+    ay[g] = __ffma2_rn(dy, qi3, ay[g]);
+    az[g] = __ffma2_rn(dz, qi3, az[g]);
+  }
+}
+
+// The single-RHS kernel's walk (one warp per target leaf, runs of records in bulk-copy stages, lane groups for
+// small leaves, per-stage two-sums), with MR_G right-hand sides per pass over the sources.
+__global__ void __launch_bounds__(P2P32_WARPS * 32, 4) p2p_fp32_mrhs_kernel(
+    int R, long long N, long long nleaves, const long long *__restrict__ leaf_start, const int *__restrict__ nbr,
+    int variant, const int *__restrict__ rank_of, const long long *__restrict__ rec_base,
+    const long long *__restrict__ chunk_base, const float4 *__restrict__ pq, const float4 *__restrict__ plo,
+    const float *__restrict__ qt, const float4 *__restrict__ src,
+    double *__restrict__ phi, double *__restrict__ fx, double *__restrict__ fy, double *__restrict__ fz,
+    int *__restrict__ status) {
+  __shared__ __align__(128) float4 buf[P2P32_WARPS][P2P32_NBUF][MR_REC * P2P32_STAGE];
+  __shared__ __align__(8) unsigned long long bar[P2P32_WARPS][P2P32_NBUF];
+  __shared__ long long rbase[P2P32_WARPS][27];
+  __shared__ int rcount[P2P32_WARPS][27];
+  __shared__ unsigned char rself[P2P32_WARPS][27];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    for (int b = 0; b < P2P32_NBUF; ++b) mbar_init(&bar[w][b], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  long long leaf, c0, c1;
+  if (!p2p_item((long long)blockIdx.x * P2P32_WARPS + w, nleaves, leaf_start, chunk_base, leaf, c0, c1)) return;
+  const long long P = p2p_pairs_capacity(N);
+  const long long t0 = leaf_start[leaf];
+  const int my_rank = rank_of ? rank_of[leaf] : (int)leaf;
+  const long long self_rec = rec_begin(rec_base, leaf_start, my_rank);
+  int nr = 0;
+  {
+    const int e = lane < 27 ? lane : 26;
+    int nb = lane < 27 ? nbr[leaf * 27 + e] : -1;
+    if (variant == 1 && e == 13) nb = -1;
+    const int rk = nb >= 0 ? (rank_of ? rank_of[nb] : nb) : -1;
+    const int dz = e % 3;
+    const int rk_prev = __shfl_up_sync(0xffffffffu, rk, 1);
+    const int rk_next = __shfl_down_sync(0xffffffffu, rk, 1);
+    const int rk_next2 = __shfl_down_sync(0xffffffffu, rk, 2);
+    const bool start = lane < 27 && rk >= 0 && !(dz > 0 && rk_prev >= 0 && rk_prev + 1 == rk);
+    int last = rk;
+    if (dz < 2 && rk_next >= 0 && rk_next == last + 1) {
+      last = rk_next;
+      if (dz == 0 && rk_next2 >= 0 && rk_next2 == last + 1) last = rk_next2;
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, start);
+    if (start) {
+      const int k = __popc(mask & ((1u << lane) - 1u));
+      const long long b0 = rec_begin(rec_base, leaf_start, rk), b1 = rec_begin(rec_base, leaf_start, last + 1);
+      rbase[w][k] = b0;
+      rcount[w][k] = (int)(b1 - b0);
+      rself[w][k] = (variant == 0 && e / 3 == 4 && rk <= my_rank && my_rank <= last) ? 1 : 0;
+    }
+    nr = __popc(mask);
+    __syncwarp();
+  }
+  unsigned phase_bits = 0;
+  const int G = (R + MR_G - 1) / MR_G;
+  for (int grp = 0; grp < G; ++grp) {
+    const float4 *sr = src + (long long)grp * P * MR_REC;
+    for (long long tb = c0; tb < c1; tb += 32) {
+      const int m = (int)min(32LL, c1 - tb);
+      const int T = m <= 8 ? 8 : (m <= 16 ? 16 : 32);
+      const int Gl = 32 / T;  // lane groups, each on every Gl-th record
+      const int tl = lane & (T - 1), g = lane / T;
+      const long long i = tb + tl;
+      const bool active = tl < m;
+      const float4 me = active ? pq[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 mel = active ? plo[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+      const long long self_slot = 2 * self_rec + (i - t0);
+      const float2 th_x = make_float2(me.x, me.x), th_y = make_float2(me.y, me.y), th_z = make_float2(me.z, me.z);
+      const float2 tl_x = make_float2(mel.x, mel.x), tl_y = make_float2(mel.y, mel.y), tl_z = make_float2(mel.z, mel.z);
+      float ph_hi[MR_G], ph_lo[MR_G], gx_hi[MR_G], gx_lo[MR_G], gy_hi[MR_G], gy_lo[MR_G], gz_hi[MR_G], gz_lo[MR_G];
+#pragma unroll
+      for (int k = 0; k < MR_G; ++k)
+        ph_hi[k] = ph_lo[k] = gx_hi[k] = gx_lo[k] = gy_hi[k] = gy_lo[k] = gz_hi[k] = gz_lo[k] = 0.f;
+      int ie = 0, ip = 0, ce = 0, cp = 0, issued = 0, done = 0;
+      auto next_stage = [&](int &e, int &p0, int &n) -> bool {
+        while (e < nr && p0 >= rcount[w][e]) {
+          ++e;
+          p0 = 0;
+        }
+        if (e >= nr) return false;
+        n = min(P2P32_STAGE, rcount[w][e] - p0);
+        return true;
+      };
+      auto issue = [&]() {
+        int n;
+        if (!next_stage(ie, ip, n)) return false;
+        const int b = issued % P2P32_NBUF;
+        if (lane == 0) {
+          mbar_expect_tx(&bar[w][b], n * MR_REC * 16);
+          bulk_g2s(&buf[w][b][0], sr + (rbase[w][ie] + ip) * MR_REC, n * MR_REC * 16, &bar[w][b]);
+        }
+        ip += n;
+        ++issued;
+        return true;
+      };
+      for (int k = 0; k < P2P32_NBUF - 1; ++k)
+        if (!issue()) break;
+      while (done < issued) {
+        int cn;
+        next_stage(ce, cp, cn);
+        const int b = done % P2P32_NBUF;
+        if (!mbar_wait_warp(&bar[w][b], (phase_bits >> b) & 1u)) {
+          if (lane == 0) {
+            atomicExch(status, 1);
+            for (int k = done; k < issued; ++k) {
+              const int bk = k % P2P32_NBUF;
+              mbar_wait(&bar[w][bk], (phase_bits >> bk) & 1u);
+            }
+          }
+          __syncwarp();
+          return;
+        }
+        phase_bits ^= 1u << b;
+        float2 pv[MR_G], ax[MR_G], ay[MR_G], az[MR_G];
+#pragma unroll
+        for (int k = 0; k < MR_G; ++k) pv[k] = ax[k] = ay[k] = az[k] = make_float2(0.f, 0.f);
+        const float4 *s = buf[w][b];
+        if (rself[w][ce]) {
+          const int self_rel = (int)(self_slot - 2 * (rbase[w][ce] + cp));
+          for (int k = g; k < cn; k += Gl)
+            p2p_record_mrhs<true>(s, k, self_rel, th_x, th_y, th_z, tl_x, tl_y, tl_z, pv, ax, ay, az);
+        } else {
+#pragma unroll 2
+          for (int k = g; k < cn; k += Gl)
+            p2p_record_mrhs<false>(s, k, 0, th_x, th_y, th_z, tl_x, tl_y, tl_z, pv, ax, ay, az);
+        }
+#pragma unroll
+        for (int k = 0; k < MR_G; ++k) {
+          two_sum(ph_hi[k], ph_lo[k], pv[k].x + pv[k].y);
+          two_sum(gx_hi[k], gx_lo[k], ax[k].x + ax[k].y);
+          two_sum(gy_hi[k], gy_lo[k], ay[k].x + ay[k].y);
+          two_sum(gz_hi[k], gz_lo[k], az[k].x + az[k].y);
+        }
+        cp += cn;
+        ++done;
+        __syncwarp();
+        issue();
+      }
+#pragma unroll
+      for (int k = 0; k < MR_G; ++k) {
+        for (int off = T; off < 32; off <<= 1) {
+          float oh = __shfl_xor_sync(0xffffffffu, ph_hi[k], off), ol = __shfl_xor_sync(0xffffffffu, ph_lo[k], off);
+          two_sum(ph_hi[k], ph_lo[k], oh);
+          ph_lo[k] += ol;
+          oh = __shfl_xor_sync(0xffffffffu, gx_hi[k], off);
+          ol = __shfl_xor_sync(0xffffffffu, gx_lo[k], off);
+          two_sum(gx_hi[k], gx_lo[k], oh);
+          gx_lo[k] += ol;
+          oh = __shfl_xor_sync(0xffffffffu, gy_hi[k], off);
+          ol = __shfl_xor_sync(0xffffffffu, gy_lo[k], off);
+          two_sum(gy_hi[k], gy_lo[k], oh);
+          gy_lo[k] += ol;
+          oh = __shfl_xor_sync(0xffffffffu, gz_hi[k], off);
+          ol = __shfl_xor_sync(0xffffffffu, gz_lo[k], off);
+          two_sum(gz_hi[k], gz_lo[k], oh);
+          gz_lo[k] += ol;
+        }
+        const int r = MR_G * grp + k;
+        if (active && g == 0 && r < R) {
+          const long long j = (long long)r * N + i;
+          const double tq = -(double)qt[j];
+          phi[j] += (double)ph_hi[k] + (double)ph_lo[k];
+          fx[j] += tq * ((double)gx_hi[k] + (double)gx_lo[k]);
+          fy[j] += tq * ((double)gy_hi[k] + (double)gy_lo[k]);
+          fz[j] += tq * ((double)gz_hi[k] + (double)gz_lo[k]);
+        }
+      }
+    }
+  }
+}
+
 }  // namespace
 
 b200fmm_status run_p2p(Context &c, int variant) {
   const int LL = c.H - 1;
   const Level &L = c.lv[LL];
   if (L.n == 0) return B200FMM_OK;
-  if (c.cfg.precision == B200FMM_MIXED) {
+  if (c.cfg.precision == B200FMM_MIXED && c.R > 1) {
+    // several right-hand sides: targets hi [N], lo [N], charges [R][N] (floats), then the record groups; the
+    // buffer sized for the single-RHS layout of R vectors holds this one
+    float4 *hi = c.d_pq32, *lo = c.d_pq32 + c.N;
+    float *qt = (float *)(c.d_pq32 + 2 * c.N);
+    float4 *src = c.d_pq32 + 2 * c.N + (c.N * c.R + 3) / 4;
+    if (!c.packed32) {
+      c.packed32 = true;
+      if (c.column_serial != c.tree_serial) {
+        B200_CHECK(leaf_column_order(c));
+        c.column_serial = c.tree_serial;
+      }
+      const double W = c.cfg.box_width;
+      pack_records32_mrhs<<<(unsigned)L.n, 64, 0, c.stream>>>(
+          c.N, c.R, c.d_leaf_start, c.d_leaf_rank, c.d_rec_base, c.d_x, c.d_y, c.d_z, c.d_q, c.cfg.center[0] - W / 2,
+          c.cfg.center[1] - W / 2, c.cfg.center[2] - W / 2, hi, lo, qt, src);
+      ++c.launches;
+    }
+    // work items (p2p_leaf_items per leaf): nleaves + N / kP2PItemTargets bounds their count
+    const unsigned blocks = grid_for(L.n + c.N / kP2PItemTargets, P2P32_WARPS);
+    B200_CUDA(record_event(c, 10));
+    p2p_fp32_mrhs_kernel<<<blocks, P2P32_WARPS * 32, 0, c.stream>>>(
+        c.R, c.N, L.n, c.d_leaf_start, c.d_leaf_nbr, variant, c.d_leaf_rank, c.d_rec_base, c.d_chunk_base, hi, lo, qt,
+        src, c.d_phi, c.d_fx, c.d_fy, c.d_fz, c.d_status);
+    B200_CUDA(record_event(c, 11));
+    ++c.launches;
+  } else if (c.cfg.precision == B200FMM_MIXED) {
     float4 *hi = c.d_pq32, *lo = c.d_pq32 + c.N * c.R, *src = c.d_pq32 + c.N * (c.R + 1);
     if (!c.packed32) {
       c.packed32 = true;
@@ -429,11 +755,12 @@ b200fmm_status run_p2p(Context &c, int variant) {
       ++c.launches;
     }
     int *status = c.d_status;
-    const unsigned blocks = grid_for(L.n, P2P32_WARPS);
+    // work items (p2p_leaf_items per leaf): nleaves + N / kP2PItemTargets bounds their count
+    const unsigned blocks = grid_for(L.n + c.N / kP2PItemTargets, P2P32_WARPS);
     B200_CUDA(record_event(c, 10));
     p2p_fp32_kernel<<<blocks, P2P32_WARPS * 32, 0, c.stream>>>(c.R, c.N, L.n, c.d_leaf_start, c.d_leaf_nbr, variant,
-                                                               c.d_leaf_rank, c.d_rec_base, hi, lo, src, c.d_phi,
-                                                               c.d_fx, c.d_fy, c.d_fz, status);
+                                                               c.d_leaf_rank, c.d_rec_base, c.d_chunk_base, hi, lo,
+                                                               src, c.d_phi, c.d_fx, c.d_fy, c.d_fz, status);
     B200_CUDA(record_event(c, 11));
     ++c.launches;
   } else {
@@ -546,8 +873,8 @@ extern "C" b200fmm_status b200fmm_p2p_noalloc(long long n, const double *x, cons
                                                  center[0] - box_width / 2, center[1] - box_width / 2,
                                                  center[2] - box_width / 2, stage, stage + n, stage + 2 * n);
   p2p_fp32_kernel<<<grid_for(nleaves, P2P32_WARPS), P2P32_WARPS * 32, 0, s>>>(
-      1, n, nleaves, leaf_start, leaf_nbr, variant, nullptr, nullptr, stage, stage + n, stage + 2 * n, phi, fx, fy, fz,
-      status);
+      1, n, nleaves, leaf_start, leaf_nbr, variant, nullptr, nullptr, nullptr, stage, stage + n, stage + 2 * n, phi, fx,
+      fy, fz, status);
   B200_CUDA(cudaGetLastError());
   B200_CUDA(cudaMemcpyAsync(st, status, sizeof(st), cudaMemcpyDeviceToHost, s));
   B200_CUDA(cudaStreamSynchronize(s));

@@ -538,6 +538,14 @@ __global__ void rec_total_kernel(long long nleaves, const long long *__restrict_
   base[nleaves] = base[nleaves - 1] + nrec[nleaves - 1];
 }
 
+// work items of the near field per leaf (p2p_leaf_items)
+__global__ void leaf_chunks_kernel(long long nleaves, const long long *__restrict__ leaf_start,
+                                   long long *__restrict__ nch) {
+  const long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (l >= nleaves) return;
+  nch[l] = p2p_leaf_items(leaf_start[l + 1] - leaf_start[l]);
+}
+
 // grow-only device buffer: reallocates (and bumps the tree generation) only when n exceeds the capacity
 template <class T>
 b200fmm_status grow(Context &c, T *&p, size_t &cap, size_t n) {
@@ -603,6 +611,7 @@ void free_tree(Context &c) {
   dfree(c.d_leaf_nbr);
   dfree(c.d_leaf_rank);
   dfree(c.d_rec_base);
+  dfree(c.d_chunk_base);
   dfree(c.d_pq32);
   dfree(c.d_phi);
   dfree(c.d_fx);
@@ -785,6 +794,8 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
     B200_CHECK(grow(c, c.d_leaf_rank, cl, (size_t)nleaves + 1));
     cl = c.cap_leaf;
     B200_CHECK(grow(c, c.d_rec_base, cl, (size_t)nleaves + 1));
+    cl = c.cap_leaf;
+    B200_CHECK(grow(c, c.d_chunk_base, cl, (size_t)nleaves + 1));
     c.cap_leaf = std::max(c.cap_leaf, (size_t)nleaves + 1);
   }
   compact_leaves<<<grid_for(n, 256), 256, 0, s>>>(n, k0, flags, idx, leaf.keys, c.d_leaf_start);
@@ -906,7 +917,11 @@ b200fmm_status leaf_column_order(Context &c) {
   leaf_rank_kernel<<<grid_for(nl, 256), 256, 0, s>>>(nl, v0, c.d_leaf_start, c.d_leaf_rank, nrec);
   B200_CHECK(scan_i64(c, nrec, c.d_rec_base, nl, (long long *)c.d_scan));
   rec_total_kernel<<<1, 1, 0, s>>>(nl, nrec, c.d_rec_base);
-  c.launches += 2;
+  // the near field's work items, leaf by leaf (nrec is free again)
+  leaf_chunks_kernel<<<grid_for(nl, 256), 256, 0, s>>>(nl, c.d_leaf_start, nrec);
+  B200_CHECK(scan_i64(c, nrec, c.d_chunk_base, nl, (long long *)c.d_scan));
+  rec_total_kernel<<<1, 1, 0, s>>>(nl, nrec, c.d_chunk_base);
+  c.launches += 4;
   B200_CUDA(cudaGetLastError());
   return B200FMM_OK;
 }

@@ -562,3 +562,31 @@ def test_autotune_keeps_mixed_accuracy():
     g.close()
     for key in FIELDS:
         assert S.rel_l2(got[key], want[key]) < 2e-6, key
+
+
+def test_mixed_handle_reused_from_dense_to_sparse_tree():
+    """The low-rank M2L's first product skips the tiles of a sparse tree that hold no cell; the Y rows of such a
+    tile must still read as zero when an earlier, denser tree on the same handle wrote values there.  A handle
+    that evaluated a uniform tree and then a clustered one gives the clustered tree's results of a fresh
+    handle (to rounding: both run the same operators and work split)."""
+    from distributions import plummer
+
+    rng = np.random.default_rng(31)
+    n, H = 30000, 5
+    xu, yu, zu = rng.random((3, n))
+    xp, yp, zp = plummer(n, seed=32)
+    q = rng.uniform(-1.0, 1.0, n)
+    reused = S.FMM("cheb_sym", 6, H, precision="mixed")
+    reused.set_particles(xu, yu, zu, q)
+    reused.execute()
+    reused.set_particles(xp, yp, zp, q)
+    reused.execute()
+    got = reused.results()
+    reused.close()
+    fresh = S.FMM("cheb_sym", 6, H, precision="mixed")
+    fresh.set_particles(xp, yp, zp, q)
+    fresh.execute()
+    want = fresh.results()
+    fresh.close()
+    for k in FIELDS:
+        assert S.rel_l2(got[k], want[k]) < 1e-12, (k, S.rel_l2(got[k], want[k]))
