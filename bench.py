@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=N_PART)
     ap.add_argument("--height", type=int, default=HEIGHT, help="octree height (profiling of small cases only)")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                    help="form of the timed steps (the headline is mixed; fp64 times the plain form, for profiles)")
+    ap.add_argument("--nrhs", type=int, default=1, help="charge vectors per step (profiles of the multi-RHS path)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batch-of-problems measurement")
@@ -127,11 +130,16 @@ def batch_measure(S, device):
                       "best of 3 after one untimed run"}
 
 
-def workload_config(n, height=HEIGHT):
-    return {"workload": f"{n} particles uniform in [0,1)^3, q~U[-1,1] (seed {SEED}), Laplace 1/r, Chebyshev order "
-                        f"{ORDER}, height {height}", "particles": n, "order": ORDER, "height": height,
-            "precision": "mixed: FP32 compensated P2P, split-FP16 x3 tcgen05 M2L, FP64 P2M/M2M/L2L/L2P",
-            "l2": "flushed between timed steps (512 MiB write)", "parallelism": "replicas"}
+def workload_config(n, height=HEIGHT, precision="mixed", nrhs=1):
+    cfg = {"workload": f"{n} particles uniform in [0,1)^3, q~U[-1,1] (seed {SEED}), Laplace 1/r, Chebyshev order "
+                       f"{ORDER}, height {height}", "particles": n, "order": ORDER, "height": height,
+           "precision": "mixed: FP32 compensated P2P, split-FP16 x3 tcgen05 M2L, FP64 P2M/M2M/L2L/L2P",
+           "l2": "flushed between timed steps (512 MiB write)", "parallelism": "replicas"}
+    if precision != "mixed":
+        cfg["precision"] = "fp64: every operator in FP64 (the plain form)"
+    if nrhs > 1:
+        cfg["nrhs"] = nrhs
+    return cfg
 
 
 # ------------------------------------------------------------------------------------------------------
@@ -300,12 +308,16 @@ def run_gpu(args):
     torch.cuda.set_stream(stream)
     n = args.n
     x, y, z, q = particles(n)
-    dx, dy, dz, dq = (torch.from_numpy(a).to(dev) for a in (x, y, z, q))
-    hx, hy, hz, hq = (torch.from_numpy(a).pin_memory() for a in (x, y, z, q))
-    out_h = [torch.empty(n, dtype=torch.float64).pin_memory() for _ in range(4)]
+    qt = q  # charges of the timed steps: the headline's vector, or nrhs vectors (profiles of the multi-RHS path)
+    if args.nrhs > 1:
+        qt = np.random.default_rng(SEED + 1).uniform(-1.0, 1.0, (args.nrhs, n)).ravel()
+    dx, dy, dz, dq = (torch.from_numpy(a).to(dev) for a in (x, y, z, qt))
+    hx, hy, hz, hq = (torch.from_numpy(a).pin_memory() for a in (x, y, z, qt))
+    out_h = [torch.empty(n * args.nrhs, dtype=torch.float64).pin_memory() for _ in range(4)]
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
-    f = S.FMM("cheb_sym", ORDER, args.height, precision="mixed", device=local, stream=stream.cuda_stream)
+    f = S.FMM("cheb_sym", ORDER, args.height, nrhs=args.nrhs, precision=args.precision, device=local,
+              stream=stream.cuda_stream)
 
     def step_device():
         f.set_particles(dx, dy, dz, dq)
@@ -386,7 +398,7 @@ def run_gpu(args):
         "metric": METRIC, "value": world * n * args.steps / (t_dev * 1e-3), "unit": "particles/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_dev / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32/f16x3 (mixed), f64 far-field bookkeeping",
-        "data": "synthetic", "config": workload_config(n, args.height),
+        "data": "synthetic", "config": workload_config(n, args.height, args.precision, args.nrhs),
         "e2e": {"value": world * n * args.steps / (t_e2e * 1e-3), "unit": "particles/s",
                 "h2d_bytes_per_step": 4 * 8 * n, "d2h_bytes_per_step": 4 * 8 * n},
         "gpu_launches": launches + launches_e2e,
