@@ -329,7 +329,8 @@ def run_gpu(args):
         f.results_into(*out_h)
 
     step_device()
-    tuned_splits, _ = f.autotune()  # tensor-core M2L work split for this tree shape, kept by the handle
+    f.autotune()  # M2L work split and near-field work items for this tree shape, kept by the handle
+    tuned = f.tuning()
     for _ in range(args.warmup):
         step_device()
         step_e2e()
@@ -421,7 +422,7 @@ def run_gpu(args):
             "note": "set_particles_host = H2D of x, y, z, q (32 MB, pinned) + GPU tree build; get_results_host = "
                     "un-permutation + D2H of phi, fx, fy, fz (32 MB, pinned); tree build alone (device arrays): "
                     "pass_ms.tree"},
-        "autotuned_m2l_splits": tuned_splits,
+        "autotuned": {"m2l_splits": tuned[0], "p2p_whole_leaf": tuned[1], "p2p_item_targets": tuned[2]},
         "clocks": clk.summary(),
     }
     f.close()

@@ -113,13 +113,19 @@ B200FMM_API b200fmm_status b200fmm_set_charges(b200fmm_handle h, const double *q
  * launches.  A stream that the caller is capturing always gets plain launches. */
 B200FMM_API b200fmm_status b200fmm_execute(b200fmm_handle h, unsigned ops);
 
-/* Work-range autotuner (MIXED): times the tensor-core M2L of the current tree with its work split into
- * 1, 2, 3 and 4 ranges of equal work per CTA (pair), keeps the fastest for this handle, and returns it with
- * its kernel time (ms).  Dense trees always run lockstep waves of whole tiles, so the choice matters for
- * sparse trees.  It runs the M2L several times and leaves the expansions undefined: call execute()
- * afterwards.  A no-op (splits = 0) in FP64.  The ranges change how the FP32 partial sums are grouped, so
- * results move within the MIXED tolerance. */
+/* Autotuner (MIXED), on the current tree; the choices are kept by the handle:
+ *  - the tensor-core M2L's work split: 1, 2, 3 or 4 ranges of equal work per CTA (pair); returned in splits
+ *    with its kernel time (ms).  Dense trees always run lockstep waves of whole tiles, so the choice matters
+ *    for sparse trees;
+ *  - the near field's work items: the largest leaf one warp takes whole (32, 64 or 128 targets) and the size
+ *    of the pieces a larger leaf is cut into (16, 32 or 64 targets).
+ * It runs the M2L and the near field several times and leaves the expansions and results undefined: call
+ * execute() afterwards.  A no-op (splits = 0) in FP64.  The choices change how FP32 partial sums are grouped,
+ * so results move within the MIXED tolerance. */
 B200FMM_API b200fmm_status b200fmm_autotune(b200fmm_handle h, int *splits, double *ms);
+/* The handle's current choices: values[0] M2L work ranges per CTA (pair), values[1] the largest leaf taken
+ * whole by one warp of the near field, values[2] the targets per piece of a larger leaf. */
+B200FMM_API b200fmm_status b200fmm_get_tuning(b200fmm_handle h, int *values);
 
 /* Algorithmic FLOPs of one M2L pass over all levels of the current tree, for the form the handle runs:
  * dense operators 2 p^6 per interaction pair; compressed operators 2 p^3 r per pair for U Y plus, in MIXED,

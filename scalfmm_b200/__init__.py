@@ -34,7 +34,7 @@ EXPORTS = (
     "b200fmm_last_launch_count", "b200fmm_autotune", "b200fmm_p2p_noalloc", "b200fmm_batch_create", "b200fmm_batch_execute",
     "b200fmm_batch_last_time", "b200fmm_batch_destroy", "b200fmm_direct", "b200fmm_m2l_flops",
     "b200fmm_get_leaf_neighbors", "b200fmm_get_interaction_lists", "b200fmm_fma_read", "b200fmm_fma_write",
-    "b200fmm_get_leaf_ranges",
+    "b200fmm_get_leaf_ranges", "b200fmm_get_tuning",
 )
 NOALLOC_MAX_PARTICLES = 262144
 
@@ -109,6 +109,7 @@ def lib():
         L.b200fmm_get_permutation.argtypes = [ctypes.c_void_p, _lp]
         L.b200fmm_get_leaf_neighbors.argtypes = [ctypes.c_void_p, _ip]
         L.b200fmm_get_leaf_ranges.argtypes = [ctypes.c_void_p, _lp]
+        L.b200fmm_get_tuning.argtypes = [ctypes.c_void_p, _ip]
         L.b200fmm_fma_read.argtypes = [ctypes.c_char_p, _lp, _ip, _dp, _dp, _dp, ctypes.c_longlong]
         L.b200fmm_fma_write.argtypes = [ctypes.c_char_p, ctypes.c_longlong, ctypes.c_int, ctypes.c_double, _dp, _dp]
         L.b200fmm_get_interaction_lists.argtypes = [ctypes.c_void_p, ctypes.c_int, _ip, _ip]
@@ -308,6 +309,12 @@ class FMM:
         _check(lib().b200fmm_get_interaction_lists(self._h, level, _ptr(src, _ip), _ptr(pos, _ip)),
                "get_interaction_lists")
         return src.reshape(n, 189), pos.reshape(n, 189)
+
+    def tuning(self):
+        """(M2L work ranges per CTA, largest leaf the near field takes whole, targets per piece of a larger leaf)."""
+        v = np.zeros(3, np.int32)
+        _check(lib().b200fmm_get_tuning(self._h, _ptr(v, _ip)), "get_tuning")
+        return tuple(int(a) for a in v)
 
     def timings(self):
         ms = np.zeros(8)

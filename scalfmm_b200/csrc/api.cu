@@ -502,9 +502,51 @@ b200fmm_status b200fmm_autotune(b200fmm_handle h, int *splits, double *ms) {
     }
   }
   tc_set_splits(c, best);
+  // the near field's work items: the largest leaf taken whole and the size of the pieces of larger leaves,
+  // timed on the current tree (the item table is rebuilt with each rule)
+  const int rules[][2] = {{64, 32}, {32, 32}, {128, 32}, {64, 16}, {128, 64}, {32, 16}};
+  int bw = c.p2p_whole, bi = c.p2p_item;
+  float bt = 0.f;
+  bool have = false;
+  for (const auto &rule : rules) {
+    c.p2p_whole = rule[0];
+    c.p2p_item = rule[1];
+    c.column_serial = -1;
+    c.packed32 = false;
+    float t = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {  // the first run rebuilds the item table
+      B200_CHECK(run_p2p(c, 0));
+      B200_CUDA(cudaEventSynchronize(c.ev[11]));
+      B200_CHECK(check_status(c));
+      if (cudaEventElapsedTime(&t, c.ev[10], c.ev[11]) != cudaSuccess) {
+        cudaGetLastError();
+        t = 1e30f;
+      }
+    }
+    if (!have || t < bt) {
+      have = true;
+      bt = t;
+      bw = rule[0];
+      bi = rule[1];
+    }
+  }
+  c.p2p_whole = bw;
+  c.p2p_item = bi;
+  c.column_serial = -1;
+  c.packed32 = false;
   c.state_zero = false;
   if (splits) *splits = best;
   if (ms) *ms = best_ms;
+  return B200FMM_OK;
+}
+
+b200fmm_status b200fmm_get_tuning(b200fmm_handle h, int *values) {
+  B200_CHECK(check_handle(h));
+  if (!values) return fail(B200FMM_ERR_INVALID, "null argument");
+  Context &c = *h;
+  values[0] = c.tc ? tc_splits_used(c) : 0;
+  values[1] = c.p2p_whole;
+  values[2] = c.p2p_item;
   return B200FMM_OK;
 }
 

@@ -18,12 +18,13 @@ constexpr int kMaxHeight = 12;
 // slots per level of the multipole maxima that P2M and M2M record (spread to keep atomics uncontended)
 constexpr int kMmaxSlots = 64;
 constexpr int kMaxNrhs = 32;
-// work items of the FP32 near field (one warp each): a leaf of at most kP2PWholeLeaf targets is one item, a
-// larger leaf is cut into items of kP2PItemTargets targets, so that dense leaves spread over many warps
+// work items of the FP32 near field (one warp each): a leaf of at most `whole` targets is one item, a larger leaf
+// is cut into items of `item` targets, so that dense leaves spread over many warps.  Defaults 64 / 32;
+// b200fmm_autotune picks them per handle.
 constexpr int kP2PWholeLeaf = 64;
 constexpr int kP2PItemTargets = 32;
-__host__ __device__ inline long long p2p_leaf_items(long long n) {
-  return n <= kP2PWholeLeaf ? 1 : (n + kP2PItemTargets - 1) / kP2PItemTargets;
+__host__ __device__ inline long long p2p_leaf_items(long long n, int whole, int item) {
+  return n <= whole ? 1 : (n + item - 1) / item;
 }
 
 // Error reporting: the last message per host thread.
@@ -122,6 +123,7 @@ struct Context {
   // [nleaves+1] first work item of each leaf in the FP32 near field (p2p_leaf_items per leaf,
   // each a work item of its own (the last entry is the item count), so that dense leaves spread over many warps
   long long *d_chunk_base = nullptr;
+  int p2p_whole = kP2PWholeLeaf, p2p_item = kP2PItemTargets;  // the work-item rule d_chunk_base was built with
   double *d_phi = nullptr, *d_fx = nullptr, *d_fy = nullptr, *d_fz = nullptr;  // [R][N] sorted results
   Level lv[kMaxHeight];
   bool has_particles = false;
@@ -211,8 +213,8 @@ b200fmm_status leaf_column_order(Context &c);
 // m2l_fp64.cu
 b200fmm_status run_m2l_fp64(Context &c, int level);
 // m2l_sym64.cu: the FP64 symmetric M2L as two GEMMs per level (stacked V_t^T, then concatenated U_t)
-b200fmm_status sym64_prepare(Context &c, const std::vector<double> &Ut, const std::vector<double> &Vt,
-                             const std::vector<long long> &toff, const std::vector<int> &trank);
+b200fmm_status sym64_prepare(Context &c, const double *d_Ut, const double *d_Vt, const std::vector<long long> &toff,
+                             const std::vector<int> &trank);
 void sym64_free(Context &c);
 b200fmm_status run_m2l_sym64(Context &c, int level);
 // rows of the stacked V of each source parity (the ranks of the slots that parity feeds)

@@ -258,6 +258,24 @@ __global__ void __launch_bounds__(G_THREADS, 1) sym64_l_kernel(const __grid_cons
   }
 }
 
+// out[row][m] = Vt[foff + m * rank + q] for the row's (foff, rank, q)
+__global__ void gather_vs_kernel(long long nrows, int nn, const int3 *__restrict__ rows, const double *__restrict__ Vt,
+                                 double *__restrict__ out) {
+  const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (g >= nrows * nn) return;
+  const int3 r = rows[g / nn];
+  out[g] = Vt[r.x + (long long)(g % nn) * r.y + r.z];
+}
+// out[m][k] = Ut[foff + m * rank + q] for column k's (foff, rank, q)
+__global__ void gather_uc_kernel(int K, int nn, const int3 *__restrict__ cols, const double *__restrict__ Ut,
+                                 double *__restrict__ out) {
+  const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (g >= (long long)nn * K) return;
+  const int k = (int)(g % K), m = (int)(g / K);
+  const int3 col = cols[k];
+  out[g] = Ut[col.x + (long long)m * col.y + col.z];
+}
+
 int sm_count(const Context &c) {
   int v = 148;
   cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, c.device);
@@ -277,9 +295,10 @@ void sym64_free(Context &c) {
   c.s64 = nullptr;
 }
 
-// The stacked operators of both phases from the per-slot factors (row-major p^3 x r each).
-b200fmm_status sym64_prepare(Context &c, const std::vector<double> &Ut, const std::vector<double> &Vt,
-                             const std::vector<long long> &toff, const std::vector<int> &trank) {
+// The stacked operators of both phases, gathered on the device from the per-slot factors (d_Ut, d_Vt: row-major
+// p^3 x r each, at the slot's offset toff).
+b200fmm_status sym64_prepare(Context &c, const double *d_Ut, const double *d_Vt, const std::vector<long long> &toff,
+                             const std::vector<int> &trank) {
   sym64_free(c);
   Sym64 *s = new Sym64();
   s->h_loff = new long long[kMaxHeight]();
@@ -309,15 +328,14 @@ b200fmm_status sym64_prepare(Context &c, const std::vector<double> &Ut, const st
     vs_total += (long long)rows * nn;
     s->ystride = std::max(s->ystride, rows);
   }
-  std::vector<double> vs((size_t)vs_total);
+  // rows of the stacked V (gathered on the device): row (sp, ybase + q) is column q of V_t
+  std::vector<int3> vrows((size_t)(vs_total / nn));
   for (int sp = 0; sp < 8; ++sp)
     for (int t = 0; t < 343; ++t) {
       const int b = ybase[sp * 343 + t];
       if (b < 0) continue;
-      const int r = trank[t];
-      for (int q = 0; q < r; ++q)
-        for (int m = 0; m < nn; ++m)
-          vs[(size_t)s->vs_off[sp] + (size_t)(b + q) * nn + m] = Vt[(size_t)toff[t] + (size_t)m * r + q];
+      for (int q = 0; q < trank[t]; ++q)
+        vrows[(size_t)(s->vs_off[sp] / nn) + b + q] = make_int3((int)toff[t], trank[t], q);
     }
   long long uc_total = 0, km_total = 0;
   for (int ct = 0; ct < 8; ++ct) {
@@ -329,7 +347,8 @@ b200fmm_status sym64_prepare(Context &c, const std::vector<double> &Ut, const st
     uc_total += (long long)K * nn;
     km_total += K;
   }
-  std::vector<double> uc((size_t)uc_total);
+  // columns of the concatenated U (gathered on the device): column k of Uc_ct is column q of U_t of entry e
+  std::vector<int3> ucols((size_t)km_total);
   std::vector<int2> km((size_t)km_total);
   for (int ct = 0; ct < 8; ++ct) {
     int k = 0;
@@ -340,18 +359,29 @@ b200fmm_status sym64_prepare(Context &c, const std::vector<double> &Ut, const st
       const int yb = ybase[((px << 2) | (py << 1) | pz) * 343 + t];
       for (int q = 0; q < r; ++q, ++k) {
         km[(size_t)s->km_off[ct] + k] = make_int2(e, yb + q);
-        for (int m = 0; m < nn; ++m)
-          uc[(size_t)s->uc_off[ct] + (size_t)m * s->kct[ct] + k] = Ut[(size_t)toff[t] + (size_t)m * r + q];
+        ucols[(size_t)s->km_off[ct] + k] = make_int3((int)toff[t], r, q);
       }
     }
   }
+  int3 *d_vrows = nullptr, *d_ucols = nullptr;
   B200_CUDA(cudaMalloc(&s->d_vs, sizeof(double) * std::max<long long>(vs_total, 1)));
   B200_CUDA(cudaMalloc(&s->d_uc, sizeof(double) * std::max<long long>(uc_total, 1)));
   B200_CUDA(cudaMalloc(&s->d_kmap, sizeof(int2) * std::max<long long>(km_total, 1)));
   B200_CUDA(cudaMalloc(&s->d_pcnt, sizeof(int) * 2 * kMaxHeight * 8));
-  B200_CUDA(cudaMemcpy(s->d_vs, vs.data(), sizeof(double) * vs_total, cudaMemcpyHostToDevice));
-  B200_CUDA(cudaMemcpy(s->d_uc, uc.data(), sizeof(double) * uc_total, cudaMemcpyHostToDevice));
+  B200_CUDA(cudaMalloc(&d_vrows, sizeof(int3) * std::max<size_t>(vrows.size(), 1)));
+  B200_CUDA(cudaMalloc(&d_ucols, sizeof(int3) * std::max<size_t>(ucols.size(), 1)));
   B200_CUDA(cudaMemcpy(s->d_kmap, km.data(), sizeof(int2) * km_total, cudaMemcpyHostToDevice));
+  B200_CUDA(cudaMemcpy(d_vrows, vrows.data(), sizeof(int3) * vrows.size(), cudaMemcpyHostToDevice));
+  B200_CUDA(cudaMemcpy(d_ucols, ucols.data(), sizeof(int3) * ucols.size(), cudaMemcpyHostToDevice));
+  gather_vs_kernel<<<grid_for(vs_total, 256), 256>>>((long long)vrows.size(), nn, d_vrows, d_Vt, s->d_vs);
+  for (int ct = 0; ct < 8; ++ct)
+    if (s->kct[ct] > 0)
+      gather_uc_kernel<<<grid_for((long long)nn * s->kct[ct], 256), 256>>>(s->kct[ct], nn, d_ucols + s->km_off[ct],
+                                                                         d_Ut, s->d_uc + s->uc_off[ct]);
+  B200_CUDA(cudaGetLastError());
+  B200_CUDA(cudaDeviceSynchronize());
+  cudaFree(d_vrows);
+  cudaFree(d_ucols);
   return B200FMM_OK;
 }
 

@@ -1534,6 +1534,34 @@ static b200fmm_status encode(CUtensorMap *map, void *base, int rank, const cuuin
 // Low-rank operators: per far slot t, K chunks of 16 ranks; U chunks [uch][NP][16] (B of the second
 // product) and, per source parity, the stacked V rows of the slots that the parity's cells feed (B of the
 // first product), both pre-scaled by powers of two and split into FP16 hi + lo.
+// Packing of the low-rank operators on the device, from the per-slot FP64 factors F (row-major p^3 x rank per
+// slot, at the slot's offset): each value is scaled by 2^sc and split into FP16 hi = fp16(v), lo = fp16(v - hi).
+//   U chunks [uch][NP][16]: chunk (foff, rank, kc), node n, lane i -> U[n][kc * 16 + i];
+//   V rows [nrows][KP]: row (foff, rank, a), node n -> V[n][a].
+// Entries past the node count or the rank are zero.
+__global__ void pack_lr_u(long long nel, int NP, int nn, const int3 *__restrict__ chunks, const double *__restrict__ F,
+                          int sc, __half *__restrict__ hi, __half *__restrict__ lo) {
+  const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (g >= nel) return;
+  const int3 ch = chunks[g / ((long long)NP * 16)];
+  const int rem = (int)(g % ((long long)NP * 16)), n = rem / 16, a = ch.z * 16 + rem % 16;
+  const double v = (n < nn && a < ch.y) ? ldexp(F[ch.x + (long long)n * ch.y + a], sc) : 0.0;
+  const __half h = __double2half(v);
+  hi[g] = h;
+  lo[g] = __double2half(v - (double)__half2float(h));
+}
+__global__ void pack_lr_v(long long nrows, int KP, int nn, const int3 *__restrict__ rows, const double *__restrict__ F,
+                          int sc, __half *__restrict__ hi, __half *__restrict__ lo) {
+  const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (g >= nrows * KP) return;
+  const int3 r = rows[g / KP];
+  const int n = (int)(g % KP);
+  const double v = (n < nn && r.z < r.y) ? ldexp(F[r.x + (long long)n * r.y + r.z], sc) : 0.0;
+  const __half h = __double2half(v);
+  hi[g] = h;
+  lo[g] = __double2half(v - (double)__half2float(h));
+}
+
 static b200fmm_status tc_init_lowrank(Context &c, DenseTC &t, TcParams &P, bool &use) {
   std::vector<double> Ut, Vt;
   std::vector<long long> toff;
@@ -1621,48 +1649,44 @@ static b200fmm_status tc_init_lowrank(Context &c, DenseTC &t, TcParams &P, bool 
   std::frexp(std::ldexp(colsum, sV + 14), &eb);
   const int sY = eb - 15;
   t.lr_shift = sV + sU - sY;
-  auto split = [](double v, __half &h, __half &l) {
-    h = __double2half(v);
-    l = __double2half(v - (double)__half2float(h));
-  };
-  // U chunks
-  std::vector<__half> uh((size_t)uch * t.NP * 16), ul(uh.size());
+  // the packed operators are written on the device from the per-slot factors: U chunks [uch][NP][16] and,
+  // per source parity, the stacked V rows [ych * 16][KP], each value scaled and split into FP16 hi + lo
+  std::vector<int3> uchunks((size_t)uch), vrows((size_t)ych * 16);
   for (int s = 0; s < 343; ++s) {
     if (toff[s] < 0) continue;
-    const int r = trank[s];
-    for (int kc = 0; kc < t.tnk[s]; ++kc)
-      for (int n = 0; n < t.NP; ++n)
-        for (int i = 0; i < 16; ++i) {
-          const int a = kc * 16 + i;
-          const double v = (n < nn && a < r) ? std::ldexp(Ut[toff[s] + (size_t)n * r + a], sU) : 0.0;
-          const size_t o = ((size_t)(t.uchunk0[s] + kc) * t.NP + n) * 16 + i;
-          split(v, uh[o], ul[o]);
-        }
+    for (int kc = 0; kc < t.tnk[s]; ++kc) uchunks[t.uchunk0[s] + kc] = make_int3((int)toff[s], trank[s], kc);
   }
   // V rows: row (ybase[sp] + ychunk0[sp][s] + kc) * 16 + i holds column kc * 16 + i of V_s along K
-  std::vector<__half> vh((size_t)ych * 16 * t.KP), vl(vh.size());
   for (int sp = 0; sp < 8; ++sp)
     for (int s = 0; s < 343; ++s) {
       if (!need[sp][s]) continue;
-      const int r = trank[s];
       for (int kc = 0; kc < t.tnk[s]; ++kc)
-        for (int i = 0; i < 16; ++i) {
-          const int a = kc * 16 + i;
-          const size_t row = (size_t)(t.ybase[sp] + t.ychunk0[sp][s] + kc) * 16 + i;
-          for (int n = 0; n < t.KP; ++n) {
-            const double v = (n < nn && a < r) ? std::ldexp(Vt[toff[s] + (size_t)n * r + a], sV) : 0.0;
-            split(v, vh[row * t.KP + n], vl[row * t.KP + n]);
-          }
-        }
+        for (int i = 0; i < 16; ++i)
+          vrows[(size_t)(t.ybase[sp] + t.ychunk0[sp][s] + kc) * 16 + i] = make_int3((int)toff[s], trank[s], kc * 16 + i);
     }
-  B200_CUDA(cudaMalloc(&t.Bhi, uh.size() * sizeof(__half)));
-  B200_CUDA(cudaMalloc(&t.Blo, ul.size() * sizeof(__half)));
-  B200_CUDA(cudaMalloc(&t.Vhi, vh.size() * sizeof(__half)));
-  B200_CUDA(cudaMalloc(&t.Vlo, vl.size() * sizeof(__half)));
-  B200_CUDA(cudaMemcpy(t.Bhi, uh.data(), uh.size() * sizeof(__half), cudaMemcpyHostToDevice));
-  B200_CUDA(cudaMemcpy(t.Blo, ul.data(), ul.size() * sizeof(__half), cudaMemcpyHostToDevice));
-  B200_CUDA(cudaMemcpy(t.Vhi, vh.data(), vh.size() * sizeof(__half), cudaMemcpyHostToDevice));
-  B200_CUDA(cudaMemcpy(t.Vlo, vl.data(), vl.size() * sizeof(__half), cudaMemcpyHostToDevice));
+  double *dU = nullptr, *dV = nullptr;
+  int3 *dUc = nullptr, *dVr = nullptr;
+  const size_t uel = (size_t)uch * t.NP * 16, vel = (size_t)ych * 16 * t.KP;
+  B200_CUDA(cudaMalloc(&dU, sizeof(double) * Ut.size()));
+  B200_CUDA(cudaMalloc(&dV, sizeof(double) * Vt.size()));
+  B200_CUDA(cudaMalloc(&dUc, sizeof(int3) * std::max<size_t>(uchunks.size(), 1)));
+  B200_CUDA(cudaMalloc(&dVr, sizeof(int3) * std::max<size_t>(vrows.size(), 1)));
+  B200_CUDA(cudaMemcpy(dU, Ut.data(), sizeof(double) * Ut.size(), cudaMemcpyHostToDevice));
+  B200_CUDA(cudaMemcpy(dV, Vt.data(), sizeof(double) * Vt.size(), cudaMemcpyHostToDevice));
+  B200_CUDA(cudaMemcpy(dUc, uchunks.data(), sizeof(int3) * uchunks.size(), cudaMemcpyHostToDevice));
+  B200_CUDA(cudaMemcpy(dVr, vrows.data(), sizeof(int3) * vrows.size(), cudaMemcpyHostToDevice));
+  B200_CUDA(cudaMalloc(&t.Bhi, uel * sizeof(__half)));
+  B200_CUDA(cudaMalloc(&t.Blo, uel * sizeof(__half)));
+  B200_CUDA(cudaMalloc(&t.Vhi, vel * sizeof(__half)));
+  B200_CUDA(cudaMalloc(&t.Vlo, vel * sizeof(__half)));
+  pack_lr_u<<<grid_for((long long)uel, 256), 256>>>((long long)uel, t.NP, nn, dUc, dU, sU, t.Bhi, t.Blo);
+  pack_lr_v<<<grid_for((long long)vel, 256), 256>>>((long long)ych * 16, t.KP, nn, dVr, dV, sV, t.Vhi, t.Vlo);
+  B200_CUDA(cudaGetLastError());
+  B200_CUDA(cudaDeviceSynchronize());
+  cudaFree(dU);
+  cudaFree(dV);
+  cudaFree(dUc);
+  cudaFree(dVr);
   {
     cuuint64_t dims[3] = {16, (cuuint64_t)t.NP, (cuuint64_t)uch};
     cuuint64_t strides[2] = {32, (cuuint64_t)32 * t.NP};

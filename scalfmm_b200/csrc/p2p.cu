@@ -236,11 +236,11 @@ __device__ __forceinline__ void p2p_record(const float4 *__restrict__ s, int k, 
 // issued P2P32_NBUF - 1 stages ahead of the math.  Per stage the partial sums enter the target's (hi, lo)
 // accumulators by a two-sum.
 // With chunk_base, warp (CTA x, warp w) takes the work item blockIdx.x * P2P32_WARPS + w: a leaf of at most
-// kP2PWholeLeaf targets, or kP2PItemTargets targets of a larger one (a dense leaf spreads over many warps; items
-// past the count leave at once).  Without it (the allocation-free entry point) a warp takes a whole leaf.
+// `whole` targets, or `isize` targets of a larger one (a dense leaf spreads over many warps; items past the count
+// leave at once).  Without it (the allocation-free entry point) a warp takes a whole leaf.
 __device__ __forceinline__ bool p2p_item(long long item, long long nleaves, const long long *__restrict__ leaf_start,
-                                         const long long *__restrict__ chunk_base, long long &leaf, long long &c0,
-                                         long long &c1) {
+                                         const long long *__restrict__ chunk_base, int whole, int isize,
+                                         long long &leaf, long long &c0, long long &c1) {
   if (!chunk_base) {
     if (item >= nleaves) return false;
     leaf = item;
@@ -259,12 +259,12 @@ __device__ __forceinline__ bool p2p_item(long long item, long long nleaves, cons
   }
   leaf = lo;
   const long long s0 = leaf_start[leaf], s1 = leaf_start[leaf + 1];
-  if (s1 - s0 <= kP2PWholeLeaf) {
+  if (s1 - s0 <= whole) {
     c0 = s0;
     c1 = s1;
   } else {
-    c0 = s0 + (long long)kP2PItemTargets * (item - chunk_base[leaf]);
-    c1 = min(c0 + kP2PItemTargets, s1);
+    c0 = s0 + (long long)isize * (item - chunk_base[leaf]);
+    c1 = min(c0 + isize, s1);
   }
   return true;
 }
@@ -272,8 +272,8 @@ __device__ __forceinline__ bool p2p_item(long long item, long long nleaves, cons
 __global__ void __launch_bounds__(P2P32_WARPS * 32, 7) p2p_fp32_kernel(
     int R, long long N, long long nleaves, const long long *__restrict__ leaf_start, const int *__restrict__ nbr,
     int variant, const int *__restrict__ rank_of, const long long *__restrict__ rec_base,
-    const long long *__restrict__ chunk_base, const float4 *__restrict__ pq, const float4 *__restrict__ plo,
-    const float4 *__restrict__ src, double *__restrict__ phi, double *__restrict__ fx, double *__restrict__ fy,
+    const long long *__restrict__ chunk_base, int whole, int isize, const float4 *__restrict__ pq,
+    const float4 *__restrict__ plo, const float4 *__restrict__ src, double *__restrict__ phi, double *__restrict__ fx, double *__restrict__ fy,
     double *__restrict__ fz, int *__restrict__ status) {
   __shared__ __align__(128) float4 buf[P2P32_WARPS][P2P32_NBUF][4 * P2P32_STAGE];
   __shared__ __align__(8) unsigned long long bar[P2P32_WARPS][P2P32_NBUF];
@@ -287,7 +287,8 @@ __global__ void __launch_bounds__(P2P32_WARPS * 32, 7) p2p_fp32_kernel(
   }
   __syncwarp();
   long long leaf, c0, c1;
-  if (!p2p_item((long long)blockIdx.x * P2P32_WARPS + w, nleaves, leaf_start, chunk_base, leaf, c0, c1)) return;
+  if (!p2p_item((long long)blockIdx.x * P2P32_WARPS + w, nleaves, leaf_start, chunk_base, whole, isize, leaf, c0, c1))
+    return;
   const long long P = p2p_pairs_capacity(N);
   const long long t0 = leaf_start[leaf];
   const int my_rank = rank_of ? rank_of[leaf] : (int)leaf;
@@ -542,8 +543,8 @@ __device__ __forceinline__ void p2p_record_mrhs(const float4 *__restrict__ s, in
 __global__ void __launch_bounds__(P2P32_WARPS * 32, 4) p2p_fp32_mrhs_kernel(
     int R, long long N, long long nleaves, const long long *__restrict__ leaf_start, const int *__restrict__ nbr,
     int variant, const int *__restrict__ rank_of, const long long *__restrict__ rec_base,
-    const long long *__restrict__ chunk_base, const float4 *__restrict__ pq, const float4 *__restrict__ plo,
-    const float *__restrict__ qt, const float4 *__restrict__ src,
+    const long long *__restrict__ chunk_base, int whole, int isize, const float4 *__restrict__ pq,
+    const float4 *__restrict__ plo, const float *__restrict__ qt, const float4 *__restrict__ src,
     double *__restrict__ phi, double *__restrict__ fx, double *__restrict__ fy, double *__restrict__ fz,
     int *__restrict__ status) {
   __shared__ __align__(128) float4 buf[P2P32_WARPS][P2P32_NBUF][MR_REC * P2P32_STAGE];
@@ -558,7 +559,8 @@ __global__ void __launch_bounds__(P2P32_WARPS * 32, 4) p2p_fp32_mrhs_kernel(
   }
   __syncwarp();
   long long leaf, c0, c1;
-  if (!p2p_item((long long)blockIdx.x * P2P32_WARPS + w, nleaves, leaf_start, chunk_base, leaf, c0, c1)) return;
+  if (!p2p_item((long long)blockIdx.x * P2P32_WARPS + w, nleaves, leaf_start, chunk_base, whole, isize, leaf, c0, c1))
+    return;
   const long long P = p2p_pairs_capacity(N);
   const long long t0 = leaf_start[leaf];
   const int my_rank = rank_of ? rank_of[leaf] : (int)leaf;
@@ -732,12 +734,12 @@ b200fmm_status run_p2p(Context &c, int variant) {
           c.cfg.center[1] - W / 2, c.cfg.center[2] - W / 2, hi, lo, qt, src);
       ++c.launches;
     }
-    // work items (p2p_leaf_items per leaf): nleaves + N / kP2PItemTargets bounds their count
-    const unsigned blocks = grid_for(L.n + c.N / kP2PItemTargets, P2P32_WARPS);
+    // work items (p2p_leaf_items per leaf): nleaves + N / item bounds their count
+    const unsigned blocks = grid_for(L.n + c.N / c.p2p_item, P2P32_WARPS);
     B200_CUDA(record_event(c, 10));
     p2p_fp32_mrhs_kernel<<<blocks, P2P32_WARPS * 32, 0, c.stream>>>(
-        c.R, c.N, L.n, c.d_leaf_start, c.d_leaf_nbr, variant, c.d_leaf_rank, c.d_rec_base, c.d_chunk_base, hi, lo, qt,
-        src, c.d_phi, c.d_fx, c.d_fy, c.d_fz, c.d_status);
+        c.R, c.N, L.n, c.d_leaf_start, c.d_leaf_nbr, variant, c.d_leaf_rank, c.d_rec_base, c.d_chunk_base, c.p2p_whole,
+        c.p2p_item, hi, lo, qt, src, c.d_phi, c.d_fx, c.d_fy, c.d_fz, c.d_status);
     B200_CUDA(record_event(c, 11));
     ++c.launches;
   } else if (c.cfg.precision == B200FMM_MIXED) {
@@ -755,12 +757,12 @@ b200fmm_status run_p2p(Context &c, int variant) {
       ++c.launches;
     }
     int *status = c.d_status;
-    // work items (p2p_leaf_items per leaf): nleaves + N / kP2PItemTargets bounds their count
-    const unsigned blocks = grid_for(L.n + c.N / kP2PItemTargets, P2P32_WARPS);
+    // work items (p2p_leaf_items per leaf): nleaves + N / item bounds their count
+    const unsigned blocks = grid_for(L.n + c.N / c.p2p_item, P2P32_WARPS);
     B200_CUDA(record_event(c, 10));
-    p2p_fp32_kernel<<<blocks, P2P32_WARPS * 32, 0, c.stream>>>(c.R, c.N, L.n, c.d_leaf_start, c.d_leaf_nbr, variant,
-                                                               c.d_leaf_rank, c.d_rec_base, c.d_chunk_base, hi, lo,
-                                                               src, c.d_phi, c.d_fx, c.d_fy, c.d_fz, status);
+    p2p_fp32_kernel<<<blocks, P2P32_WARPS * 32, 0, c.stream>>>(
+        c.R, c.N, L.n, c.d_leaf_start, c.d_leaf_nbr, variant, c.d_leaf_rank, c.d_rec_base, c.d_chunk_base, c.p2p_whole,
+        c.p2p_item, hi, lo, src, c.d_phi, c.d_fx, c.d_fy, c.d_fz, status);
     B200_CUDA(record_event(c, 11));
     ++c.launches;
   } else {
@@ -873,8 +875,8 @@ extern "C" b200fmm_status b200fmm_p2p_noalloc(long long n, const double *x, cons
                                                  center[0] - box_width / 2, center[1] - box_width / 2,
                                                  center[2] - box_width / 2, stage, stage + n, stage + 2 * n);
   p2p_fp32_kernel<<<grid_for(nleaves, P2P32_WARPS), P2P32_WARPS * 32, 0, s>>>(
-      1, n, nleaves, leaf_start, leaf_nbr, variant, nullptr, nullptr, nullptr, stage, stage + n, stage + 2 * n, phi, fx,
-      fy, fz, status);
+      1, n, nleaves, leaf_start, leaf_nbr, variant, nullptr, nullptr, nullptr, 0, 0, stage, stage + n, stage + 2 * n,
+      phi, fx, fy, fz, status);
   B200_CUDA(cudaGetLastError());
   B200_CUDA(cudaMemcpyAsync(st, status, sizeof(st), cudaMemcpyDeviceToHost, s));
   B200_CUDA(cudaStreamSynchronize(s));

@@ -499,7 +499,6 @@ b200fmm_status upload_sym_operators(Context &c) {
   std::vector<int> trank;
   std::vector<double> Ut, Vt;
   B200_CHECK(sym_slot_factors(c, Ut, Vt, toff, trank));
-  B200_CHECK(sym64_prepare(c, Ut, Vt, toff, trank));
   const long long tot = (long long)Ut.size();
   B200_CUDA(cudaMalloc(&c.d_Ut, sizeof(double) * std::max<long long>(tot, 1)));
   B200_CUDA(cudaMalloc(&c.d_Vt, sizeof(double) * std::max<long long>(tot, 1)));
@@ -509,6 +508,7 @@ b200fmm_status upload_sym_operators(Context &c) {
   B200_CUDA(cudaMemcpy(c.d_Vt, Vt.data(), sizeof(double) * tot, cudaMemcpyHostToDevice));
   B200_CUDA(cudaMemcpy(c.d_toff, toff.data(), sizeof(long long) * 343, cudaMemcpyHostToDevice));
   B200_CUDA(cudaMemcpy(c.d_trank, trank.data(), sizeof(int) * 343, cudaMemcpyHostToDevice));
+  B200_CHECK(sym64_prepare(c, c.d_Ut, c.d_Vt, toff, trank));
   B200_CUDA(cudaMalloc(&c.d_pindices, sizeof(int) * 343));
   B200_CUDA(cudaMalloc(&c.d_pvec, sizeof(int) * 343 * nn));
   B200_CUDA(cudaMalloc(&c.d_symU, sizeof(double) * std::max<long long>(o, 1)));

@@ -539,11 +539,11 @@ __global__ void rec_total_kernel(long long nleaves, const long long *__restrict_
 }
 
 // work items of the near field per leaf (p2p_leaf_items)
-__global__ void leaf_chunks_kernel(long long nleaves, const long long *__restrict__ leaf_start,
+__global__ void leaf_chunks_kernel(long long nleaves, const long long *__restrict__ leaf_start, int whole, int item,
                                    long long *__restrict__ nch) {
   const long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (l >= nleaves) return;
-  nch[l] = p2p_leaf_items(leaf_start[l + 1] - leaf_start[l]);
+  nch[l] = p2p_leaf_items(leaf_start[l + 1] - leaf_start[l], whole, item);
 }
 
 // grow-only device buffer: reallocates (and bumps the tree generation) only when n exceeds the capacity
@@ -918,7 +918,7 @@ b200fmm_status leaf_column_order(Context &c) {
   B200_CHECK(scan_i64(c, nrec, c.d_rec_base, nl, (long long *)c.d_scan));
   rec_total_kernel<<<1, 1, 0, s>>>(nl, nrec, c.d_rec_base);
   // the near field's work items, leaf by leaf (nrec is free again)
-  leaf_chunks_kernel<<<grid_for(nl, 256), 256, 0, s>>>(nl, c.d_leaf_start, nrec);
+  leaf_chunks_kernel<<<grid_for(nl, 256), 256, 0, s>>>(nl, c.d_leaf_start, c.p2p_whole, c.p2p_item, nrec);
   B200_CHECK(scan_i64(c, nrec, c.d_chunk_base, nl, (long long *)c.d_scan));
   rec_total_kernel<<<1, 1, 0, s>>>(nl, nrec, c.d_chunk_base);
   c.launches += 4;
