@@ -82,7 +82,7 @@ typedef struct {
 typedef struct b200fmm_context *b200fmm_handle;
 
 /* Lifecycle.  create() also builds the interpolation tables and, for CHEB_SYM, the 16 compressed
- * operators (own FP64 precompute: kernel evaluation at the nodes on the GPU, pACA + QR + SVD on the host,
+ * operators (own FP64 precompute on the GPU: kernel evaluation at the nodes, then pACA + QR + SVD,
  * following FChebSymM2LHandler.hpp:39-281); for CHEB_DENSE / LAGRANGE it evaluates the dense
  * per-transfer-vector operators on the GPU in FP64. */
 B200FMM_API b200fmm_status b200fmm_create(const b200fmm_config *cfg, b200fmm_handle *out);

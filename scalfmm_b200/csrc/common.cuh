@@ -186,6 +186,10 @@ b200fmm_status check_status(Context &c);
 // precompute.cu
 b200fmm_status build_tables(Context &c);
 b200fmm_status compress_sym_operators(Context &c);
+// ACA + QR + SVD compression of ncls weighted class matrices (device, row-major nn x nn each) with node
+// weights dw: ranks per class and the factors in the reference layout (per class: U rows, then V rows)
+b200fmm_status compress_classes(Context &c, int ncls, const double *dA, const double *dw, double eps,
+                                std::vector<int> &ranks, std::vector<double> &uv);
 b200fmm_status upload_sym_operators(Context &c);
 bool tc_lowrank_info(const Context &c, int *rank_of_slot, double *rank_fed);
 void slot_symmetry_tables(int p, std::vector<int> &pind, std::vector<int> &pvec);

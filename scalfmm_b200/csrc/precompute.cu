@@ -4,9 +4,8 @@
 //    Lagrange roots (Src/Kernels/Uniform/FUnifRoots.hpp:35-39); child->parent interpolators
 //    (FChebInterpolator::initTensorM2MandL2L, Src/Kernels/Chebyshev/FChebInterpolator.hpp:300-338).
 //  * symmetric compression (Src/Kernels/Chebyshev/FChebSymM2LHandler.hpp:39-281): the weighted kernel
-//    matrices of the 16 canonical transfer vectors are evaluated on the GPU; partially pivoted ACA
-//    (Src/Utils/FAca.hpp:141-225), Householder QR of both factors, a one-sided Jacobi SVD of Ru Rv^T and the
-//    rank rule of FSvd::getRank (Src/Utils/FSvd.hpp:53-64) run on the host (matrices of at most p^3 x ~60).
+//    matrices of the 16 canonical transfer vectors are evaluated on the GPU and compressed there
+//    (compress.cu: partially pivoted ACA, Householder QR of both factors, Jacobi SVD, rank rule), all in FP64.
 //  * symmetry tables (Src/Kernels/Interpolation/FInterpSymmetries.hpp:18-125).
 //  * dense per-transfer-vector operators K(X_m, Y_n) at reference width 2
 //    (FChebDenseM2LHandler::Compute, Src/Kernels/Chebyshev/FChebDenseM2LHandler.hpp:178-215), evaluated on
@@ -145,101 +144,6 @@ __global__ void eval_dense(int p, const double *__restrict__ roots, double *__re
   K[(long long)t * nn * nn + e] = v;
 }
 
-// ---- host dense linear algebra (column-major) -------------------------------------------------------
-
-// Householder QR of A (m x k, col-major, m >= k): on return Q (m x k) and R (k x k upper, col-major).
-void householder_qr(int m, int k, std::vector<double> &A, std::vector<double> &Q, std::vector<double> &R) {
-  std::vector<double> V((size_t)m * k, 0.0), beta(k, 0.0);
-  for (int j = 0; j < k; ++j) {
-    double norm = 0.0;
-    for (int i = j; i < m; ++i) norm += A[(size_t)j * m + i] * A[(size_t)j * m + i];
-    norm = std::sqrt(norm);
-    const double a0 = A[(size_t)j * m + j];
-    const double alpha = a0 >= 0 ? -norm : norm;
-    double vnorm2 = 0.0;
-    for (int i = j; i < m; ++i) {
-      const double v = A[(size_t)j * m + i] - (i == j ? alpha : 0.0);
-      V[(size_t)j * m + i] = v;
-      vnorm2 += v * v;
-    }
-    beta[j] = vnorm2 > 0 ? 2.0 / vnorm2 : 0.0;
-    for (int c = j; c < k; ++c) {
-      double d = 0.0;
-      for (int i = j; i < m; ++i) d += V[(size_t)j * m + i] * A[(size_t)c * m + i];
-      d *= beta[j];
-      for (int i = j; i < m; ++i) A[(size_t)c * m + i] -= d * V[(size_t)j * m + i];
-    }
-  }
-  R.assign((size_t)k * k, 0.0);
-  for (int c = 0; c < k; ++c)
-    for (int i = 0; i <= c; ++i) R[(size_t)c * k + i] = A[(size_t)c * m + i];
-  Q.assign((size_t)m * k, 0.0);
-  for (int c = 0; c < k; ++c) Q[(size_t)c * m + c] = 1.0;
-  for (int j = k - 1; j >= 0; --j)
-    for (int c = 0; c < k; ++c) {
-      double d = 0.0;
-      for (int i = j; i < m; ++i) d += V[(size_t)j * m + i] * Q[(size_t)c * m + i];
-      d *= beta[j];
-      for (int i = j; i < m; ++i) Q[(size_t)c * m + i] -= d * V[(size_t)j * m + i];
-    }
-}
-
-// One-sided Jacobi SVD of a square k x k matrix A (col-major): A = U diag(s) V^T, s descending.
-bool jacobi_svd(int k, std::vector<double> A, std::vector<double> &U, std::vector<double> &s,
-                std::vector<double> &V) {
-  V.assign((size_t)k * k, 0.0);
-  for (int i = 0; i < k; ++i) V[(size_t)i * k + i] = 1.0;
-  bool converged = false;
-  for (int sweep = 0; sweep < 80 && !converged; ++sweep) {
-    converged = true;
-    for (int a = 0; a < k - 1; ++a)
-      for (int b = a + 1; b < k; ++b) {
-        double alpha = 0, bet = 0, gam = 0;
-        for (int i = 0; i < k; ++i) {
-          const double x = A[(size_t)a * k + i], y = A[(size_t)b * k + i];
-          alpha += x * x;
-          bet += y * y;
-          gam += x * y;
-        }
-        if (std::fabs(gam) <= 1e-15 * std::sqrt(alpha * bet) || gam == 0.0) continue;
-        converged = false;
-        const double zeta = (bet - alpha) / (2.0 * gam);
-        const double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1.0 + zeta * zeta));
-        const double cs = 1.0 / std::sqrt(1.0 + t * t), sn = cs * t;
-        for (int i = 0; i < k; ++i) {
-          const double x = A[(size_t)a * k + i], y = A[(size_t)b * k + i];
-          A[(size_t)a * k + i] = cs * x - sn * y;
-          A[(size_t)b * k + i] = sn * x + cs * y;
-          const double vx = V[(size_t)a * k + i], vy = V[(size_t)b * k + i];
-          V[(size_t)a * k + i] = cs * vx - sn * vy;
-          V[(size_t)b * k + i] = sn * vx + cs * vy;
-        }
-      }
-  }
-  std::vector<double> sv(k);
-  for (int j = 0; j < k; ++j) {
-    double nrm = 0;
-    for (int i = 0; i < k; ++i) nrm += A[(size_t)j * k + i] * A[(size_t)j * k + i];
-    sv[j] = std::sqrt(nrm);
-  }
-  std::vector<int> order(k);
-  for (int j = 0; j < k; ++j) order[j] = j;
-  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return sv[x] > sv[y]; });
-  U.assign((size_t)k * k, 0.0);
-  s.assign(k, 0.0);
-  std::vector<double> V2((size_t)k * k);
-  for (int jj = 0; jj < k; ++jj) {
-    const int j = order[jj];
-    s[jj] = sv[j];
-    for (int i = 0; i < k; ++i) {
-      U[(size_t)jj * k + i] = sv[j] > 0 ? A[(size_t)j * k + i] / sv[j] : 0.0;
-      V2[(size_t)jj * k + i] = V[(size_t)j * k + i];
-    }
-  }
-  V.swap(V2);
-  return converged;
-}
-
 }  // namespace
 
 b200fmm_status build_tables(Context &c) {
@@ -292,113 +196,16 @@ b200fmm_status compress_sym_operators(Context &c) {
   B200_CUDA(cudaMemcpy(dw, w.data(), sizeof(double) * nn, cudaMemcpyHostToDevice));
   B200_CUDA(cudaMemcpy(dc, cls.data(), sizeof(int) * ncls, cudaMemcpyHostToDevice));
   eval_weighted_classes<<<dim3(grid_for((long long)nn * nn, 256), ncls), 256>>>(p, dr, dc, dw, dA);
-  B200_CUDA(cudaGetLastError());
-  std::vector<double> A((size_t)ncls * nn * nn);
-  B200_CUDA(cudaMemcpy(A.data(), dA, sizeof(double) * A.size(), cudaMemcpyDeviceToHost));
+  b200fmm_status st = cudaGetLastError() == cudaSuccess ? B200FMM_OK : fail(B200FMM_ERR_CUDA, "class matrices");
+  std::vector<int> ranks;
+  if (st == B200FMM_OK) st = compress_classes(c, ncls, dA, dw, eps, ranks, c.sym_uv);
   cudaFree(dA);
   cudaFree(dr);
   cudaFree(dw);
   cudaFree(dc);
-
+  if (st != B200FMM_OK) return st;
   c.sym_ranks.assign(343, 0);
-  c.sym_uv.clear();
-  for (int ci = 0; ci < ncls; ++ci) {
-    const double *Am = A.data() + (size_t)ci * nn * nn;  // Am[t*nn + s]
-    // partially pivoted ACA (FAca.hpp:141-225)
-    std::vector<char> rfree(nn, 1), cfree(nn, 1);
-    std::vector<std::vector<double>> Uc, Vc;
-    double norm2S = 0.0;
-    int I = 0, J = 0;
-    const double eps2 = eps * eps;
-    while (true) {
-      std::vector<double> v(Am + (size_t)I * nn, Am + (size_t)I * nn + nn);
-      rfree[I] = 0;
-      for (size_t l = 0; l < Uc.size(); ++l)
-        for (int j = 0; j < nn; ++j) v[j] -= Uc[l][I] * Vc[l][j];
-      double mx = 0.0;
-      for (int j = 0; j < nn; ++j)
-        if (cfree[j] && mx < std::fabs(v[j])) {
-          mx = std::fabs(v[j]);
-          J = j;
-        }
-      if (v[J] == 0.0) return fail(B200FMM_ERR_NUMERIC, "ACA breakdown (zero pivot)");
-      const double piv = 1.0 / v[J];
-      for (int j = 0; j < nn; ++j) v[j] *= piv;
-      std::vector<double> u(nn);
-      for (int i = 0; i < nn; ++i) u[i] = Am[(size_t)i * nn + J];
-      cfree[J] = 0;
-      for (size_t l = 0; l < Uc.size(); ++l)
-        for (int i = 0; i < nn; ++i) u[i] -= Vc[l][J] * Uc[l][i];
-      mx = 0.0;
-      for (int i = 0; i < nn; ++i)
-        if (rfree[i] && mx < std::fabs(u[i])) {
-          mx = std::fabs(u[i]);
-          I = i;
-        }
-      double cross = 0.0;
-      for (size_t l = 0; l < Uc.size(); ++l) {
-        double a = 0, b = 0;
-        for (int i = 0; i < nn; ++i) a += u[i] * Uc[l][i];
-        for (int j = 0; j < nn; ++j) b += Vc[l][j] * v[j];
-        cross += a * b;
-      }
-      double uu = 0, vv = 0;
-      for (int i = 0; i < nn; ++i) uu += u[i] * u[i];
-      for (int j = 0; j < nn; ++j) vv += v[j] * v[j];
-      const double norm2uv = uu * vv;
-      norm2S += norm2uv + 2.0 * cross;
-      Uc.push_back(u);
-      Vc.push_back(v);
-      if (!(norm2uv > eps2 * norm2S) || (int)Uc.size() >= nn) break;
-    }
-    const int k = (int)Uc.size();
-    std::vector<double> UU((size_t)nn * k), VV((size_t)nn * k);
-    for (int l = 0; l < k; ++l)
-      for (int i = 0; i < nn; ++i) {
-        UU[(size_t)l * nn + i] = Uc[l][i];
-        VV[(size_t)l * nn + i] = Vc[l][i];
-      }
-    std::vector<double> Qu, Ru, Qv, Rv;
-    householder_qr(nn, k, UU, Qu, Ru);
-    householder_qr(nn, k, VV, Qv, Rv);
-    std::vector<double> phi((size_t)k * k, 0.0);  // Ru Rv^T
-    for (int b = 0; b < k; ++b)
-      for (int a = 0; a < k; ++a) {
-        double s = 0;
-        for (int l = 0; l < k; ++l) s += Ru[(size_t)l * k + a] * Rv[(size_t)l * k + b];
-        phi[(size_t)b * k + a] = s;
-      }
-    std::vector<double> Ur, sr, Vr;
-    if (!jacobi_svd(k, phi, Ur, sr, Vr)) return fail(B200FMM_ERR_NUMERIC, "SVD did not converge");
-    // FSvd::getRank
-    double nrm2 = 0;
-    for (int i = 0; i < k; ++i) nrm2 += sr[i] * sr[i];
-    int rank = 0;
-    double acc = 0;
-    for (int i = k; i > 0; --i) {
-      acc += sr[i - 1] * sr[i - 1];
-      if (acc > eps * eps * nrm2) {
-        rank = i;
-        break;
-      }
-    }
-    if (rank == 0) return fail(B200FMM_ERR_NUMERIC, "rank rule failed");
-    const int slot = cls[ci];
-    c.sym_ranks[slot] = rank;
-    const size_t off = c.sym_uv.size();
-    c.sym_uv.resize(off + 2 * (size_t)rank * nn);
-    double *Uo = c.sym_uv.data() + off, *Vo = Uo + (size_t)rank * nn;
-    for (int r = 0; r < rank; ++r)
-      for (int i = 0; i < nn; ++i) {
-        double su = 0, sv = 0;
-        for (int l = 0; l < k; ++l) {
-          su += Qu[(size_t)l * nn + i] * Ur[(size_t)r * k + l];
-          sv += Qv[(size_t)l * nn + i] * Vr[(size_t)r * k + l];
-        }
-        Uo[(size_t)r * nn + i] = su * sr[r] / w[i];  // un-weighting (FChebSymM2LHandler.hpp:257-261)
-        Vo[(size_t)r * nn + i] = sv / w[i];
-      }
-  }
+  for (int ci = 0; ci < ncls; ++ci) c.sym_ranks[cls[ci]] = ranks[ci];
   return B200FMM_OK;
 }
 
