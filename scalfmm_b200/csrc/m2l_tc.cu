@@ -919,6 +919,8 @@ struct __align__(64) LrYParams {
   // of the item hold values of an earlier computation; those are zeroed once, when the tile has become empty.
   const unsigned *busy;                                  // the second product's tile masks (bit 191: occupied)
   int tile0[kMaxHeight];                                 // first tile of each level in busy
+  unsigned full_levels;                                  // bit l: every cell of level l is present
+  int issuers;                                           // MMA-issuing threads: 1, or 2 (one per accumulator)
   unsigned char *ydirty;                                 // [2 * items of all levels]
 };
 
@@ -950,7 +952,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
       mbar_init(&acc_full[b], 1);
       mbar_init(&acc_empty[b], PAIR ? 16 : 8);  // the epilogue warps of both CTAs
     }
-    mbar_init(&done_bar, 1);
+    mbar_init(&done_bar, P.issuers);
     abort_sh = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -1014,6 +1016,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
   auto occupied = [&](const YItem &y) -> bool {
     const int l = y.level, TX = P.HX[l] / TILE_X, TY = P.HY[l] / TILE_Y, TZ = P.HZ[l] / TILE_Z;
     const int bz0 = PAIR ? y.bz - (int)rank : y.bz;
+    if ((P.full_levels >> l) & 1u) {
+      // a full level: a tile holds cells when it overlaps the parity grid [0, 2^(l-1))^3 (no memory read)
+      const int sh = 1 << (l - 1);
+      return y.bx * TILE_X < sh && y.by * TILE_Y < sh && (bz0 * TILE_Z < sh || (PAIR && (bz0 + 1) * TILE_Z < sh));
+    }
     auto tile = [&](int bz) {
       const long long id = P.tile0[l] + (((long long)y.par * TZ + bz) * TY + y.by) * TX + y.bx;
       return (P.busy[6 * id + 5] >> 31) & 1u;
@@ -1065,8 +1072,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
         }
       }
     }
-  } else if (warp == 1) {
+  } else if (warp == 1 || (warp == 2 && P.issuers == 2)) {
+    // MMA issue: one thread for both accumulators, or one per accumulator (warp 1: segments into accumulator
+    // 0, warp 2: into accumulator 1), so that one thread's waits and bookkeeping leave the other's MMAs queued
     if (lane == 0 && leader) {
+      const unsigned mine = P.issuers == 2 ? (unsigned)(warp - 1) : 2u;
       const unsigned idesc = (1u << 4) | ((unsigned)(YBLK >> 3) << 17) | ((unsigned)((PAIR ? 256 : 128) >> 4) << 24);
       auto mma = [&](unsigned d, unsigned long long da, unsigned long long db, unsigned acc) {
         if constexpr (PAIR)
@@ -1085,38 +1095,53 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
       const unsigned stage_step = (unsigned)P.stage_bytes >> 4;
       int stage = 0;
       unsigned phase = 0, empty_par = 3u;
-      for (int it = g_id; it < nitems && !abort_sh; it += g_count) {
+      // The tensor pipe keeps only a few MMAs queued, so every cycle this thread spends between MMA groups
+      // (barrier tests, bookkeeping) idles it: the loop keeps per-chunk work to the two waits and counters.
+      for (int it = g_id; it < nitems; it += g_count) {
+        if (abort_sh) break;
         if (!occupied(decode(it))) continue;
-        for (int kc = 0; kc < P.NK && !abort_sh; ++kc) {
-          const int b = (kc / segc) & 1;
-          const bool first = kc % segc == 0;
-          if (first) {
-            if (!mbar_wait(&acc_empty[b], (empty_par >> b) & 1u)) {
-              give_up();
+        unsigned b = 0;  // accumulator of the current segment
+        int sc = 0;      // chunks issued into it
+        bool failed = false;
+        for (int kc = 0; kc < P.NK; ++kc) {
+          const bool own = mine == 2u || b == mine;
+          if (own) {
+            if (sc == 0) {
+              if (!mbar_wait(&acc_empty[b], (empty_par >> b) & 1u)) {
+                failed = true;
+                break;
+              }
+              empty_par ^= 1u << b;
+              tc_fence_after();
+            }
+            if (!mbar_wait(&full_bar[stage], phase)) {
+              failed = true;
               break;
             }
-            empty_par ^= 1u << b;
-            tc_fence_after();
-          }
-          if (!mbar_wait(&full_bar[stage], phase)) {
-            give_up();
-            break;
-          }
-          const unsigned so = (unsigned)stage * stage_step;
-          const unsigned d = tmem + (unsigned)(b * YBLK);
+            const unsigned so = (unsigned)stage * stage_step;
+            const unsigned d = tmem + b * (unsigned)YBLK;
 #pragma unroll
-          for (int ks = 0; ks < 2; ++ks) {
-            const unsigned k2 = 2u * ks;
-            mma(d, dA_hi + so + k2, dB_lo + so + k2, (first && ks == 0) ? 0u : 1u);
-            mma(d, dA_lo + so + k2, dB_hi + so + k2, 1u);
-            mma(d, dA_hi + so + k2, dB_hi + so + k2, 1u);
+            for (int ks = 0; ks < 2; ++ks) {
+              const unsigned k2 = 2u * ks;
+              mma(d, dA_hi + so + k2, dB_lo + so + k2, (sc == 0 && ks == 0) ? 0u : 1u);
+              mma(d, dA_lo + so + k2, dB_hi + so + k2, 1u);
+              mma(d, dA_hi + so + k2, dB_hi + so + k2, 1u);
+            }
+            commit(&empty_bar[stage]);
           }
-          commit(&empty_bar[stage]);
           if (++stage == S) {
             stage = 0;
             phase ^= 1;
           }
-          if (kc % segc == segc - 1 || kc == P.NK - 1) commit(&acc_full[b]);
+          if (++sc == segc || kc == P.NK - 1) {
+            if (own) commit(&acc_full[b]);
+            sc = 0;
+            b ^= 1u;
+          }
+        }
+        if (failed) {
+          give_up();
+          break;
         }
       }
       if constexpr (PAIR)
@@ -1512,7 +1537,7 @@ struct DenseTC {
   int ybase[8] = {};
   short ychunk0[8][343] = {};
   TvRec *tv = nullptr;  // transfer-vector records on the device
-  bool ypair = true;                      // first product on CTA pairs (B200FMM_TC_YPAIR=0: single CTAs)
+  bool ypair = false;                     // first product on CTA pairs (B200FMM_TC_YPAIR=1) or single CTAs
   int lr_shift = 0;                       // sV + sU: the power-of-two pre-scales of V and U
   LrYParams *yparams = nullptr;           // host copy
   double lr_rank_fed[8] = {};             // first product: sum of the ranks of the slots each parity feeds
@@ -1715,6 +1740,8 @@ static b200fmm_status tc_init_lowrank(Context &c, DenseTC &t, TcParams &P, bool 
   // order 7 this keeps the M2L within 5.5e-7 of FP64 (longer segments: 6-9e-7 for a few % less time)
   Y.segc = 3;
   if (const char *e = getenv("B200FMM_TC_LR_YSEG")) Y.segc = std::max(1, atoi(e));
+  Y.issuers = 2;
+  if (const char *e = getenv("B200FMM_TC_YISSUERS")) Y.issuers = atoi(e) == 1 ? 1 : 2;
   t.ystage_bytes = 2 * (TILE_X * TILE_Y * TILE_Z * KCHUNK * 2) + 2 * (t.ypair ? YBLK / 2 : YBLK) * KCHUNK * 2;
   t.ystages = std::min(MAX_STAGES, (220 * 1024) / t.ystage_bytes);
   Y.stages = t.ystages;
@@ -2086,6 +2113,7 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
     for (int l = 2; l <= LL; ++l)
       if (c.lv[l].n == (1LL << (3 * l))) full_levels |= 1u << l;
     const bool all_full = full_levels == (((1u << (LL + 1)) - 1u) & ~3u);
+    if (t->lr) t->yparams->full_levels = full_levels;
     B200_CUDA(cudaMemsetAsync(t->busy, 0, sizeof(unsigned) * 6 * t->ntiles_all, c.stream));
     if (!all_full) {
       B200_CUDA(cudaMemsetAsync(t->sat, 0, t->satn * sizeof(int), c.stream));
