@@ -946,7 +946,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(&full_bar[s], 1);
-      mbar_init(&empty_bar[s], 1);
+      // a stage is released by every issuing thread: the owner of its chunk commits, the other arrives
+      mbar_init(&empty_bar[s], PAIR ? 1 : P.issuers);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&acc_full[b], 1);
@@ -1105,19 +1106,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
         bool failed = false;
         for (int kc = 0; kc < P.NK; ++kc) {
           const bool own = mine == 2u || b == mine;
-          if (own) {
-            if (sc == 0) {
-              if (!mbar_wait(&acc_empty[b], (empty_par >> b) & 1u)) {
-                failed = true;
-                break;
-              }
-              empty_par ^= 1u << b;
-              tc_fence_after();
-            }
-            if (!mbar_wait(&full_bar[stage], phase)) {
+          if (own && sc == 0) {
+            if (!mbar_wait(&acc_empty[b], (empty_par >> b) & 1u)) {
               failed = true;
               break;
             }
+            empty_par ^= 1u << b;
+            tc_fence_after();
+          }
+          // Every issuing thread waits for every stage, its own chunks or not, and a stage is refilled only
+          // after both threads have passed it: a thread that skipped the other's chunks could otherwise wait
+          // on a stage's full barrier two phases ahead, where the parity test passes before the data is in.
+          if (!mbar_wait(&full_bar[stage], phase)) {
+            failed = true;
+            break;
+          }
+          if (own) {
             const unsigned so = (unsigned)stage * stage_step;
             const unsigned d = tmem + b * (unsigned)YBLK;
 #pragma unroll
@@ -1128,6 +1132,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
               mma(d, dA_hi + so + k2, dB_hi + so + k2, 1u);
             }
             commit(&empty_bar[stage]);
+          } else {
+            mbar_arrive(&empty_bar[stage]);  // this thread's share of the stage's release
           }
           if (++stage == S) {
             stage = 0;
@@ -1742,6 +1748,7 @@ static b200fmm_status tc_init_lowrank(Context &c, DenseTC &t, TcParams &P, bool 
   if (const char *e = getenv("B200FMM_TC_LR_YSEG")) Y.segc = std::max(1, atoi(e));
   Y.issuers = 2;
   if (const char *e = getenv("B200FMM_TC_YISSUERS")) Y.issuers = atoi(e) == 1 ? 1 : 2;
+  if (t.ypair) Y.issuers = 1;  // on CTA pairs the stage release is the leader's multicast commit alone
   t.ystage_bytes = 2 * (TILE_X * TILE_Y * TILE_Z * KCHUNK * 2) + 2 * (t.ypair ? YBLK / 2 : YBLK) * KCHUNK * 2;
   t.ystages = std::min(MAX_STAGES, (220 * 1024) / t.ystage_bytes);
   Y.stages = t.ystages;

@@ -8,6 +8,8 @@ Tolerances (relative L2 over the whole vector, FMath::FAccurater):
   * MIXED path: 2e-6 against the FP64 path (FP32 P2P + split-FP16 tensor-core M2L); the bench gates the
     1M-particle headline case at 1e-6 on the potential.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -280,6 +282,36 @@ def test_mixed_close_to_fp64(kernel):
         f.close()
     for k in FIELDS:
         assert S.rel_l2(out["mixed"][k], out["fp64"][k]) < 2e-6, (k, S.rel_l2(out["mixed"][k], out["fp64"][k]))
+
+
+@pytest.mark.parametrize("order", [5, 6, 7])
+def test_first_product_issuers_agree(order):
+    """The low-rank M2L's first product issues its MMAs from one thread or from two (one per TMEM
+    accumulator, each skipping the other's chunks but passing every stage).  Each accumulator receives the
+    same MMAs in the same order either way, so the results are bit-identical; order 6 (three segments of
+    3, 3 and 1 K chunks) is where the second thread skips a chunk that the stage ring reuses."""
+    from distributions import plummer
+
+    x, y, z = plummer(40000, seed=71)
+    q = np.random.default_rng(72).uniform(-1.0, 1.0, x.size)
+    out = {}
+    for issuers in ("1", "2"):
+        old = os.environ.get("B200FMM_TC_YISSUERS")
+        os.environ["B200FMM_TC_YISSUERS"] = issuers
+        try:
+            f = S.FMM("cheb_sym", order, 6, precision="mixed")
+            f.set_particles(x, y, z, q)
+            f.execute()
+            f.execute()
+            out[issuers] = f.results()
+            f.close()
+        finally:
+            if old is None:
+                os.environ.pop("B200FMM_TC_YISSUERS", None)
+            else:
+                os.environ["B200FMM_TC_YISSUERS"] = old
+    for k in FIELDS:
+        assert np.array_equal(out["1"][k], out["2"][k]), (k, S.rel_l2(out["1"][k], out["2"][k]))
 
 
 @pytest.mark.parametrize("name", ["lagrange_p4_h4_n2000", "lagrange_p6_h3_n1000"])
