@@ -562,6 +562,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
       // the barrier that counts this stage's bytes: this CTA's, or the even CTA's in a pair
       const unsigned full0 = PAIR ? mapa_shared(su32(&full_bar[0]), 0u) : su32(&full_bar[0]);
       const int stage_tx = (PAIR ? 2 : 1) * (2 * a_bytes + 2 * b_bytes);
+      unsigned loaded = 0, lpar = 0;  // stages that received a load, and the phase parity of the last one
       for_each_fragment(P, g_id, g_count, [&](const TcItem &w, int r0, int r1) -> bool {
         const BusyMask bm = item_mask(w);
         const int bz = w.bz + (int)rank;
@@ -604,6 +605,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
                             h * P.NH, c2);
               }
             }
+            loaded |= 1u << stage;
+            lpar = (lpar & ~(1u << stage)) | (phase << stage);
             if (++stage == S) {
               stage = 0;
               phase ^= 1;
@@ -612,6 +615,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
         }
         return !abort_sh;
       });
+      // No bulk copy may still be landing in shared memory when the CTA exits, which a run that gave up can
+      // leave behind: wait (bounded) for the last load of every stage.  The even CTA's barriers count the bytes
+      // of both CTAs of a pair, and the cluster barrier at the end holds the odd CTA until then.
+      if (leader)
+        for (int st = 0; st < S; ++st)
+          if ((loaded >> st) & 1u) mbar_wait(&full_bar[st], (lpar >> st) & 1u);
     }
   } else if (warp == 1 || (NHALF == 2 && warp == 2)) {
     // ------------------------------------------------ MMA issuers (the even CTA of a pair)
@@ -1037,6 +1046,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
     if (lane == 0) {
       int stage = 0;
       unsigned phase = 0;
+      unsigned loaded = 0, lpar = 0;  // stages that received a load, and the phase parity of the last one
       const unsigned full0 = PAIR ? mapa_shared(su32(&full_bar[0]), 0u) : su32(&full_bar[0]);
       for (int it = g_id; it < nitems && !abort_sh; it += g_count) {
         const YItem y = decode(it);
@@ -1066,12 +1076,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
             tma_load_2d(sbuf + 2 * a_bytes, &P.mapV_hi, &full_bar[stage], kc * KCHUNK, vrow);
             tma_load_2d(sbuf + 2 * a_bytes + b_bytes, &P.mapV_lo, &full_bar[stage], kc * KCHUNK, vrow);
           }
+          loaded |= 1u << stage;
+          lpar = (lpar & ~(1u << stage)) | (phase << stage);
           if (++stage == S) {
             stage = 0;
             phase ^= 1;
           }
         }
       }
+      // as in the second product: no bulk copy may be landing when the CTA exits
+      if (leader)
+        for (int st = 0; st < S; ++st)
+          if ((loaded >> st) & 1u) mbar_wait(&full_bar[st], (lpar >> st) & 1u);
     }
   } else if (warp == 1 || (warp == 2 && P.issuers == 2)) {
     // MMA issue: one thread for both accumulators, or one per accumulator (warp 1: segments into accumulator
