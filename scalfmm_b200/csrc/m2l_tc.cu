@@ -931,6 +931,14 @@ struct __align__(64) LrYParams {
   unsigned full_levels;                                  // bit l: every cell of level l is present
   int issuers;                                           // MMA-issuing threads: 1, or 2 (one per accumulator)
   unsigned char *ydirty;                                 // [2 * items of all levels]
+  int dirty0[kMaxHeight];                                // each level's first item in the tile-mode numbering of ydirty
+  // Compacted levels (sparse levels, one right-hand side, single CTAs): the items run over blocks of 128
+  // occupied cells of one parity instead of the parity grid's tiles, so that a level whose few cells touch
+  // most tiles costs its cells, not its grid.
+  unsigned compact_levels;                               // bit l: level l is compacted
+  CUtensorMap mapC_hi[kMaxHeight], mapC_lo[kMaxHeight];  // compacted multipoles [rows][KP]: 2-D boxes of 32 K x 128 rows
+  const int *crow[kMaxHeight];                           // [rows]: (parity << 28) | (hz * HY + hy) * HX + hx, or -1
+  int cblk0[kMaxHeight][9];                              // first 128-row block of each parity; [8] = blocks
 };
 
 constexpr int YBLK = 256;  // rank rows per item (16 chunks of 16)
@@ -1000,7 +1008,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
   // item -> level, rhs, parity, tile, block; items of a tile are consecutive (blocks innermost) so that the
   // CTAs working at the same time share the tile's multipoles and the V blocks through L2
   struct YItem {
-    int level, rhs, par, bx, by, bz, nb;
+    int level, rhs, par, bx, by, bz, nb, blk;  // blk: the 128-row block of a compacted level, else -1
+    int g;                                     // the item's index over all levels
   };
   auto decode = [&](int it) {
     YItem y;
@@ -1009,8 +1018,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
     while (l > P.l0 && g >= P.item0[l] + P.nitems[l]) --l;
     int r = g - P.item0[l];
     y.level = l;
+    y.g = g;
     y.nb = r % P.nblk;
     r /= P.nblk;
+    y.blk = -1;
+    if ((P.compact_levels >> l) & 1u) {
+      int p = 0;
+      while (p < 7 && r >= P.cblk0[l][p + 1]) ++p;
+      y.blk = r;
+      y.par = p;
+      y.rhs = 0;
+      y.bx = y.by = y.bz = 0;
+      return y;
+    }
     const int TX = P.HX[l] / TILE_X, TY = P.HY[l] / TILE_Y, TZu = tz_units(l);
     y.bx = r % TX;
     r /= TX;
@@ -1024,6 +1044,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
   };
   // whether the item's tile (a pair: either tile) holds a cell; all roles skip the others alike
   auto occupied = [&](const YItem &y) -> bool {
+    if (y.blk >= 0) return true;  // a block of a compacted level holds at least one cell
     const int l = y.level, TX = P.HX[l] / TILE_X, TY = P.HY[l] / TILE_Y, TZ = P.HZ[l] / TILE_Z;
     const int bz0 = PAIR ? y.bz - (int)rank : y.bz;
     if ((P.full_levels >> l) & 1u) {
@@ -1068,6 +1089,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
                              y.bz * TILE_Z, c4);
             tma_load_2d_pair(sbuf + 2 * a_bytes, &P.mapV_hi, fb, kc * KCHUNK, vrow);
             tma_load_2d_pair(sbuf + 2 * a_bytes + b_bytes, &P.mapV_lo, fb, kc * KCHUNK, vrow);
+          } else if (y.blk >= 0) {
+            tma_load_2d(sbuf, &P.mapC_hi[y.level], &full_bar[stage], kc * KCHUNK, y.blk * 128);
+            tma_load_2d(sbuf + a_bytes, &P.mapC_lo[y.level], &full_bar[stage], kc * KCHUNK, y.blk * 128);
+            tma_load_2d(sbuf + 2 * a_bytes, &P.mapV_hi, &full_bar[stage], kc * KCHUNK, vrow);
+            tma_load_2d(sbuf + 2 * a_bytes + b_bytes, &P.mapV_lo, &full_bar[stage], kc * KCHUNK, vrow);
           } else {
             tma_load_5d(sbuf, &P.mapA_hi[y.level], &full_bar[stage], kc * KCHUNK, y.bx * TILE_X, y.by * TILE_Y,
                         y.bz * TILE_Z, c4);
@@ -1185,7 +1211,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
     for (int it = g_id; it < nitems && !abort_sh; it += g_count) {
       const YItem y = decode(it);
       // one flag per (item, CTA of the pair, epilogue warp): whether this warp's rows of the item hold values
-      unsigned char *dirty = P.ydirty + ((2 * (size_t)(it + P.item0[P.l1]) + rank) * 8 + (warp - 4));
+      // (tile-mode levels only; the item's index in the tile-mode numbering)
+      unsigned char *dirty =
+          P.ydirty + ((2 * (size_t)(P.dirty0[y.level] + y.g - P.item0[y.level]) + rank) * 8 + (warp - 4));
       if (!occupied(y)) {
         // an empty tile: its rows of Y must read as zero; clear them if an earlier tree left values there
         const bool was = *dirty != 0;
@@ -1232,15 +1260,25 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
       if (abort_sh) break;
       // write the 8 chunks of 16 ranks this thread holds, as FP16 hi and lo
       const int l = y.level;
-      const int hx = y.bx * TILE_X + (row & 7), hy = y.by * TILE_Y + ((row >> 3) & 3), hz = y.bz * TILE_Z + (row >> 5);
+      const long long plane = (long long)P.HZ[l] * P.HY[l] * P.HX[l];
+      long long pos = 0;  // the row's cell in the parity grid: (hz * HY + hy) * HX + hx
+      bool real = true;   // false for a padding row of a compacted parity's last block (lanes stay together)
+      if (y.blk >= 0) {
+        const int code = P.crow[l][y.blk * 128 + row];
+        real = code >= 0;
+        pos = real ? (code & 0x0FFFFFFF) : 0;
+      } else {
+        if (y.bz >= P.HZ[l] / TILE_Z) continue;  // the missing second tile of a pair at the z edge
+        const int hx = y.bx * TILE_X + (row & 7), hy = y.by * TILE_Y + ((row >> 3) & 3), hz = y.bz * TILE_Z + (row >> 5);
+        pos = ((long long)hz * P.HY[l] + hy) * P.HX[l] + hx;
+      }
       const int nch = P.ybase[y.par + 1] - P.ybase[y.par];  // chunks of this parity
-      if (y.bz >= P.HZ[l] / TILE_Z) continue;                // the missing second tile of a pair at the z edge
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         const int chunk = y.nb * (YBLK / 16) + ch * 8 + k;
         if (chunk >= nch) break;
         const long long yi = (long long)y.rhs * P.ycht + P.ybase[y.par] + chunk;
-        const long long off = (((yi * P.HZ[l] + hz) * P.HY[l] + hy) * P.HX[l] + hx) * 16;
+        const long long off = (yi * plane + pos) * 16;
         unsigned hv[8], lv[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
@@ -1252,13 +1290,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
           hv[i] = *reinterpret_cast<const unsigned *>(&h);
           lv[i] = *reinterpret_cast<const unsigned *>(&l);
         }
-        uint4 *dh = (uint4 *)(P.Yhi[l] + off), *dl = (uint4 *)(P.Ylo[l] + off);
-        dh[0] = make_uint4(hv[0], hv[1], hv[2], hv[3]);
-        dh[1] = make_uint4(hv[4], hv[5], hv[6], hv[7]);
-        dl[0] = make_uint4(lv[0], lv[1], lv[2], lv[3]);
-        dl[1] = make_uint4(lv[4], lv[5], lv[6], lv[7]);
+        if (real) {
+          uint4 *dh = (uint4 *)(P.Yhi[l] + off), *dl = (uint4 *)(P.Ylo[l] + off);
+          dh[0] = make_uint4(hv[0], hv[1], hv[2], hv[3]);
+          dh[1] = make_uint4(hv[4], hv[5], hv[6], hv[7]);
+          dl[0] = make_uint4(lv[0], lv[1], lv[2], lv[3]);
+          dl[1] = make_uint4(lv[4], lv[5], lv[6], lv[7]);
+        }
       }
-      if (lane == 0) *dirty = 1;
+      if (y.blk < 0 && lane == 0) *dirty = 1;
     }
   }
   tc_fence_before();
@@ -1472,6 +1512,59 @@ __global__ void pack_levels_kernel(const __grid_constant__ PackLevels L, int R, 
   }
 }
 
+// ---- compacted first-product levels ----------------------------------------------------------------
+// Cells of a sparse level grouped by parity into blocks of 128 rows: counts, then placement with per-parity
+// cursors (the order inside a parity does not matter: each Y row depends on its own cell only).
+__global__ void ccount_kernel(const long long *__restrict__ keys, long long n, int *__restrict__ cnt) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int ix, iy, iz;
+  morton_decode3(keys[i], ix, iy, iz);
+  atomicAdd(cnt + (((ix & 1) << 2) | ((iy & 1) << 1) | (iz & 1)), 1);
+}
+struct CPlace {
+  int blk0[9];  // first 128-row block of each parity (cplace), or first Y chunk of each parity (cclear)
+  int HX, HY;
+};
+__global__ void cplace_kernel(const long long *__restrict__ keys, long long n, const __grid_constant__ CPlace C,
+                              int *__restrict__ cursor, int *__restrict__ crow, int *__restrict__ ccell) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int ix, iy, iz;
+  morton_decode3(keys[i], ix, iy, iz);
+  const int par = ((ix & 1) << 2) | ((iy & 1) << 1) | (iz & 1);
+  const int row = C.blk0[par] * 128 + atomicAdd(cursor + par, 1);
+  crow[row] = (par << 28) | (((iz >> 1) * C.HY + (iy >> 1)) * C.HX + (ix >> 1));
+  ccell[row] = (int)i;
+}
+// zero the Y rows (every chunk of the row's parity) of the cells a compacted level wrote for an earlier tree
+__global__ void cclear_kernel(const int *__restrict__ crow, long long plane, const __grid_constant__ CPlace B,
+                              __half *__restrict__ yhi, __half *__restrict__ ylo) {
+  const int code = crow[blockIdx.x];
+  if (code < 0) return;
+  const int par = code >> 28;
+  const long long pos = code & 0x0FFFFFFF;
+  for (int ch = B.blk0[par] + (int)threadIdx.x; ch < B.blk0[par + 1]; ch += blockDim.x) {
+    uint4 *dh = (uint4 *)(yhi + ((long long)ch * plane + pos) * 16), *dl = (uint4 *)(ylo + ((long long)ch * plane + pos) * 16);
+    dh[0] = dh[1] = dl[0] = dl[1] = make_uint4(0u, 0u, 0u, 0u);
+  }
+}
+// the compacted multipoles of one evaluation: row -> its cell's multipole scaled and split as pack_levels does
+__global__ void pack_compact_kernel(const int *__restrict__ ccell, const double *__restrict__ M, int nn, int KP,
+                                    const double *__restrict__ scal_l, __half *__restrict__ hi,
+                                    __half *__restrict__ lo) {
+  const long long row = blockIdx.x;
+  const int cell = ccell[row];
+  const double s = *scal_l;
+  const double *m = cell >= 0 ? M + (long long)cell * nn : nullptr;
+  for (int n = threadIdx.x; n < KP; n += blockDim.x) {
+    const double a = (m && n < nn) ? m[n] * s : 0.0;
+    const __half h = __double2half(a);
+    hi[row * KP + n] = h;
+    lo[row * KP + n] = __double2half(a - (double)__half2float(h));
+  }
+}
+
 // 2^sA with sA chosen so that max|M| * 2^sA ~ 2^14, and the epilogue factor scale_l * 2^-(sA + shift)
 // with shift the operators' own pre-scale exponent (SB for the dense K, sV + sU - sY for the low-rank
 // factors).  One thread per level of [l0, l1]; max|M| of level l is the largest of amax[l * nslots + s].
@@ -1564,6 +1657,15 @@ struct DenseTC {
   LrYParams *yparams = nullptr;           // host copy
   double lr_rank_fed[8] = {};             // first product: sum of the ranks of the slots each parity feeds
   int lr_rank[343] = {};                  // rank of each far slot
+  // first product on compacted levels (sparse levels of a tree): per level
+  int titem0[kMaxHeight] = {}, tnitems[kMaxHeight] = {};  // tile-mode item numbering (the ydirty flags)
+  int ymode[kMaxHeight] = {};             // what Y holds besides zeros: 0 nothing, 1 tile-mode rows, 2 compacted rows
+  int *crow[kMaxHeight] = {};             // [rows]: (parity << 28) | position in the parity grid, or -1
+  int *ccell[kMaxHeight] = {};            // [rows]: cell index, or -1
+  __half *Chi[kMaxHeight] = {}, *Clo[kMaxHeight] = {};  // compacted multipoles [rows][KP]
+  long long ccap[kMaxHeight] = {};        // rows allocated
+  int crows[kMaxHeight] = {};             // rows of the current tree (128-row blocks of each parity)
+  int *ccnt = nullptr;                    // [kMaxHeight][16]: cells of each parity, then placement cursors
 };
 
 static b200fmm_status encode(CUtensorMap *map, void *base, int rank, const cuuint64_t *dims, const cuuint64_t *strides,
@@ -1948,7 +2050,10 @@ void tc_free(Context &c) {
     if (t->Alo[l]) cudaFree(t->Alo[l]);
     if (t->Yhi[l]) cudaFree(t->Yhi[l]);
     if (t->Ylo[l]) cudaFree(t->Ylo[l]);
+    for (void *q : {(void *)t->crow[l], (void *)t->ccell[l], (void *)t->Chi[l], (void *)t->Clo[l]})
+      if (q) cudaFree(q);
   }
+  if (t->ccnt) cudaFree(t->ccnt);
   if (t->sat) cudaFree(t->sat);
   if (t->ydirty) cudaFree(t->ydirty);
   delete t->params;
@@ -2046,8 +2151,11 @@ static b200fmm_status tc_prepare(Context &c) {
       Y.item0[l] = n;
       const int TZ = t->HZ[l] / TILE_Z;
       Y.nitems[l] = c.R * 8 * (t->ypair ? (TZ + 1) / 2 : TZ) * (t->HY[l] / TILE_Y) * (t->HX[l] / TILE_X) * t->nblk;
+      t->titem0[l] = Y.dirty0[l] = Y.item0[l];
+      t->tnitems[l] = Y.nitems[l];
       n += Y.nitems[l];
     }
+    Y.compact_levels = 0;
     // the first product skips items of empty tiles; their Y rows must read as zero (dirty flags: 2 CTAs x 8
     // epilogue warps per item)
     const size_t nd = (size_t)16 * std::max(n, 1);
@@ -2059,6 +2167,7 @@ static b200fmm_status tc_prepare(Context &c) {
       y_moved = true;
     }
     if (y_moved) {
+      for (int l = 0; l < kMaxHeight; ++l) t->ymode[l] = 0;
       B200_CUDA(cudaMemsetAsync(t->ydirty, 0, nd, c.stream));
       for (int l = 2; l <= LL; ++l) {
         B200_CUDA(cudaMemsetAsync(t->Yhi[l], 0, t->Ybytes[l], c.stream));
@@ -2106,6 +2215,98 @@ static b200fmm_status tc_prepare(Context &c) {
   P.status = c.d_status;
   t->built_for_N = c.N;
   t->built_for_gen = c.tree_gen;
+  return B200FMM_OK;
+}
+
+// Per tree, low-rank form: which levels the first product runs compacted (a level less than half full, one
+// right-hand side, single CTAs), their cells grouped by parity into 128-row blocks, the tensor maps of their
+// compacted multipoles and the item numbering.  Y must read as zero wherever no cell is: rows that an earlier
+// tree's compacted level wrote are cleared here, and a level that turns compacted after tile-mode runs has its
+// Y and tile flags cleared (tile mode keeps clearing its own rows through the flags).  One host synchronisation
+// (the per-parity counts) when some level is compacted.
+static b200fmm_status y_compact_setup(Context &c, DenseTC &t) {
+  LrYParams &Y = *t.yparams;
+  const int LL = c.H - 1;
+  const char *env = getenv("B200FMM_TC_YCOMPACT");
+  const bool allow = !t.ypair && c.R == 1 && !(env && atoi(env) == 0);
+  unsigned mask = 0;
+  for (int l = 2; l <= LL; ++l) {
+    const long long plane = (long long)t.HX[l] * t.HY[l] * t.HZ[l];
+    const bool sparse = c.lv[l].n > 0 && 2 * c.lv[l].n < (1LL << (3 * l));
+    if (allow && sparse && plane < (1LL << 28)) mask |= 1u << l;
+  }
+  CPlace chunks{};
+  for (int p = 0; p <= 8; ++p) chunks.blk0[p] = p < 8 ? t.ybase[p] : t.ycht;
+  for (int l = 2; l <= LL; ++l) {
+    const long long plane = (long long)t.HX[l] * t.HY[l] * t.HZ[l];
+    if (t.ymode[l] == 2 && t.crows[l] > 0) {
+      cclear_kernel<<<(unsigned)t.crows[l], 64, 0, c.stream>>>(t.crow[l], plane, chunks, t.Yhi[l], t.Ylo[l]);
+      ++c.launches;
+    }
+    if (((mask >> l) & 1u) && t.ymode[l] == 1) {
+      B200_CUDA(cudaMemsetAsync(t.Yhi[l], 0, t.Ybytes[l], c.stream));
+      B200_CUDA(cudaMemsetAsync(t.Ylo[l], 0, t.Ybytes[l], c.stream));
+      B200_CUDA(cudaMemsetAsync(t.ydirty + 16 * (size_t)t.titem0[l], 0, 16 * (size_t)t.tnitems[l], c.stream));
+    }
+    t.crows[l] = 0;
+  }
+  int cnt[kMaxHeight][16] = {};
+  if (mask) {
+    if (!t.ccnt) B200_CUDA(cudaMalloc(&t.ccnt, sizeof(int) * kMaxHeight * 16));
+    B200_CUDA(cudaMemsetAsync(t.ccnt, 0, sizeof(int) * kMaxHeight * 16, c.stream));
+    for (int l = 2; l <= LL; ++l)
+      if ((mask >> l) & 1u) {
+        ccount_kernel<<<grid_for(c.lv[l].n, 256), 256, 0, c.stream>>>(c.lv[l].keys, c.lv[l].n, t.ccnt + 16 * l);
+        ++c.launches;
+      }
+    B200_CUDA(cudaMemcpyAsync(cnt, t.ccnt, sizeof(cnt), cudaMemcpyDeviceToHost, c.stream));
+    B200_CUDA(cudaStreamSynchronize(c.stream));
+  }
+  int n = 0;
+  for (int l = LL; l >= 2; --l) {
+    Y.item0[l] = n;
+    if (!((mask >> l) & 1u)) {
+      Y.nitems[l] = t.tnitems[l];
+      n += Y.nitems[l];
+      t.ymode[l] = 1;
+      continue;
+    }
+    CPlace C{};
+    C.blk0[0] = 0;
+    for (int p = 0; p < 8; ++p) C.blk0[p + 1] = C.blk0[p] + (cnt[l][p] + 127) / 128;
+    C.HX = t.HX[l];
+    C.HY = t.HY[l];
+    const long long rows = 128LL * C.blk0[8];
+    if (t.ccap[l] < rows) {
+      for (void *q : {(void *)t.crow[l], (void *)t.ccell[l], (void *)t.Chi[l], (void *)t.Clo[l]})
+        if (q) cudaFree(q);
+      t.crow[l] = t.ccell[l] = nullptr;
+      t.Chi[l] = t.Clo[l] = nullptr;
+      t.ccap[l] = 0;
+      B200_CUDA(cudaMalloc(&t.crow[l], sizeof(int) * rows));
+      B200_CUDA(cudaMalloc(&t.ccell[l], sizeof(int) * rows));
+      B200_CUDA(cudaMalloc(&t.Chi[l], sizeof(__half) * rows * t.KP));
+      B200_CUDA(cudaMalloc(&t.Clo[l], sizeof(__half) * rows * t.KP));
+      t.ccap[l] = rows;
+    }
+    B200_CUDA(cudaMemsetAsync(t.crow[l], 0xFF, sizeof(int) * rows, c.stream));
+    B200_CUDA(cudaMemsetAsync(t.ccell[l], 0xFF, sizeof(int) * rows, c.stream));
+    cplace_kernel<<<grid_for(c.lv[l].n, 256), 256, 0, c.stream>>>(c.lv[l].keys, c.lv[l].n, C, t.ccnt + 16 * l + 8,
+                                                                   t.crow[l], t.ccell[l]);
+    ++c.launches;
+    cuuint64_t dims[2] = {(cuuint64_t)t.KP, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)t.KP * 2};
+    cuuint32_t box[2] = {KCHUNK, 128};
+    B200_CHECK(encode(&Y.mapC_hi[l], t.Chi[l], 2, dims, strides, box));
+    B200_CHECK(encode(&Y.mapC_lo[l], t.Clo[l], 2, dims, strides, box));
+    Y.crow[l] = t.crow[l];
+    for (int p = 0; p <= 8; ++p) Y.cblk0[l][p] = C.blk0[p];
+    t.crows[l] = (int)rows;
+    Y.nitems[l] = C.blk0[8] * t.nblk;
+    n += Y.nitems[l];
+    t.ymode[l] = 2;
+  }
+  Y.compact_levels = mask;
   return B200FMM_OK;
 }
 
@@ -2159,6 +2360,7 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
     unit_work_kernel<<<grid_for(t->nunits_all, 256), 256, 0, c.stream>>>(Pw, t->nunits_all, t->prefix);
     unit_scan_kernel<<<1, 1024, 0, c.stream>>>(t->nunits_all, t->prefix);
     c.launches += 3;
+    if (t->lr) B200_CHECK(y_compact_setup(c, *t));
     t->sat_serial = c.tree_serial;
   }
   const int l0 = level == -1 ? 2 : level, l1 = level == -1 ? LL : level;
@@ -2182,7 +2384,8 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
       L.hi[l] = t->Ahi[l];
       L.lo[l] = t->Alo[l];
       L.scale_l[l] = 2.0 / (c.cfg.box_width / (double)(1LL << l));
-      L.pos0[l + 1] = L.pos0[l] + 8LL * c.R * t->HZ[l] * t->HY[l] * t->HX[l];
+      const bool compact = t->lr && ((t->yparams->compact_levels >> l) & 1u);
+      L.pos0[l + 1] = L.pos0[l] + (compact ? 0LL : 8LL * c.R * t->HZ[l] * t->HY[l] * t->HX[l]);
     }
     const int shift = t->lr ? t->lr_shift : SB;
     if (c.mmax_ready) {
@@ -2195,8 +2398,18 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
       level_scale_kernel<<<1, 32, 0, c.stream>>>(L, t->amax, 1, shift, t->scal);
       ++c.launches;
     }
-    pack_levels_kernel<<<(unsigned)L.pos0[l1 + 1], 128, 0, c.stream>>>(L, c.R, c.nn, t->KP, t->scal);
-    c.launches += 2;
+    if (L.pos0[l1 + 1] > 0) {
+      pack_levels_kernel<<<(unsigned)L.pos0[l1 + 1], 128, 0, c.stream>>>(L, c.R, c.nn, t->KP, t->scal);
+      ++c.launches;
+    }
+    ++c.launches;
+    if (t->lr)
+      for (int l = l0; l <= l1; ++l)
+        if (((t->yparams->compact_levels >> l) & 1u) && t->crows[l] > 0) {
+          pack_compact_kernel<<<(unsigned)t->crows[l], 128, 0, c.stream>>>(t->ccell[l], c.lv[l].M, c.nn, t->KP,
+                                                                           t->scal + 2 * l, t->Chi[l], t->Clo[l]);
+          ++c.launches;
+        }
   }
   // units are ordered by level, finest first: levels [l0, l1] are one contiguous range
   TcParams &P = *t->params;

@@ -314,6 +314,24 @@ def test_first_product_issuers_agree(order):
         assert np.array_equal(out["1"][k], out["2"][k]), (k, S.rel_l2(out["1"][k], out["2"][k]))
 
 
+def test_mixed_close_to_fp64_clustered_order7():
+    """MIXED against FP64 on a clustered (Plummer) tree at order 7, height 6: the sparse levels run the
+    low-rank first product compacted."""
+    from distributions import plummer
+
+    x, y, z = plummer(60000, seed=61)
+    q = np.random.default_rng(62).uniform(-1.0, 1.0, x.size)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        f = S.FMM("cheb_sym", 7, 6, precision=prec)
+        f.set_particles(x, y, z, q)
+        f.execute()
+        out[prec] = f.results()
+        f.close()
+    for k in FIELDS:
+        assert S.rel_l2(out["mixed"][k], out["fp64"][k]) < 2e-6, (k, S.rel_l2(out["mixed"][k], out["fp64"][k]))
+
+
 @pytest.mark.parametrize("name", ["lagrange_p4_h4_n2000", "lagrange_p6_h3_n1000"])
 def test_lagrange_matches_reference(golden, name):
     """The reference's FUnifKernel (Fourier-space M2L) against the dense Lagrange M2L here: FP64 to 1e-12,
@@ -622,3 +640,57 @@ def test_mixed_handle_reused_from_dense_to_sparse_tree():
     fresh.close()
     for k in FIELDS:
         assert S.rel_l2(got[k], want[k]) < 1e-12, (k, S.rel_l2(got[k], want[k]))
+
+
+def _mixed_eval(x, y, z, q, H, env=None, order=6):
+    old = {k: os.environ.get(k) for k in (env or {})}
+    os.environ.update(env or {})
+    try:
+        f = S.FMM("cheb_sym", order, H, precision="mixed")
+        f.set_particles(x, y, z, q)
+        f.execute()
+        r = f.results()
+        f.close()
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    return r
+
+
+@pytest.mark.parametrize("order", [5, 6, 7])
+def test_compacted_first_product_matches_tile_mode(order):
+    """A level less than half full runs the first product over blocks of 128 occupied cells instead of the
+    parity grid's tiles; every Y row depends on its own cell only, so the results equal those of the tile mode
+    (B200FMM_TC_YCOMPACT=0) on the same clustered tree."""
+    from distributions import plummer
+
+    x, y, z = plummer(30000, seed=41)
+    q = np.random.default_rng(42).uniform(-1.0, 1.0, x.size)
+    got = _mixed_eval(x, y, z, q, 6, order=order)
+    want = _mixed_eval(x, y, z, q, 6, {"B200FMM_TC_YCOMPACT": "0"}, order=order)
+    for k in FIELDS:
+        assert np.array_equal(got[k], want[k]), (k, S.rel_l2(got[k], want[k]))
+
+
+def test_mixed_handle_reused_across_sparse_and_dense_trees():
+    """One handle evaluates clustered, clustered, uniform and clustered trees in turn: the Y rows a compacted
+    level wrote for one tree are cleared before the next, and levels switch between compacted and tile mode;
+    each evaluation gives the results of a fresh handle."""
+    from distributions import plummer
+
+    rng = np.random.default_rng(51)
+    n, H = 30000, 6
+    trees = [plummer(n, seed=52), plummer(n, seed=53), tuple(rng.random((3, n))), plummer(n, seed=52)]
+    q = rng.uniform(-1.0, 1.0, n)
+    reused = S.FMM("cheb_sym", 6, H, precision="mixed")
+    for x, y, z in trees:
+        reused.set_particles(x, y, z, q)
+        reused.execute()
+        got = reused.results()
+        want = _mixed_eval(x, y, z, q, H)
+        for k in FIELDS:
+            assert S.rel_l2(got[k], want[k]) < 1e-12, (k, S.rel_l2(got[k], want[k]))
+    reused.close()
