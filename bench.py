@@ -116,18 +116,20 @@ def batch_measure(S, device):
     total = sum(p["x"].size for p in problems)
     b = S.Batch("cheb_sym", "mixed", nstreams=4, device=device)
     b.run(problems)  # handles, operators and buffers of every (order, height)
-    ms = []
-    for _ in range(3):
+    dev, wall = [], []
+    for _ in range(5):
         b.run(problems)
-        ms.append(b.last_time_ms())
+        dev.append(b.last_device_ms())
+        wall.append(b.last_time_ms())
     b.close()
-    best = min(ms)
-    return {"problems": len(problems), "particles": total, "ms": best, "particles_per_s": total / (best * 1e-3),
+    med = statistics.median(dev)
+    return {"problems": len(problems), "particles": total, "ms": med, "particles_per_s": total / (med * 1e-3),
+            "device_ms_runs": dev, "wall_ms_runs": wall,
             "workload": "64 problems, n log-uniform in [1e4, 5e5], Plummer (a = 0.1) truncated to the unit cube, "
                         "Chebyshev order 5..7, height 4..7 for ~30 particles per leaf as a particle sees it, MIXED, "
                         "4 worker streams",
-            "timing": "host wall time of b200fmm_batch_execute (host arrays in and out, tree builds included), "
-                      "best of 3 after one untimed run"}
+            "timing": "device time of b200fmm_batch_execute (CUDA events: start to the last worker stream's end; "
+                      "host arrays in and out, tree builds included), median of 5 after one untimed run"}
 
 
 def workload_config(n, height=HEIGHT, precision="mixed", nrhs=1):

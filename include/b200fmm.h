@@ -176,7 +176,9 @@ B200FMM_API b200fmm_status b200fmm_get_permutation(b200fmm_handle h, long long *
 
 /* Device time of the passes of the last execute(), milliseconds:
  * [0] tree build (last set_particles), [1] P2M, [2] M2M, [3] M2L, [4] L2L, [5] L2P, [6] P2P, [7] total.
- * After an execute() that replayed a CUDA graph only [0] and [7] are measured; [1]..[6] are 0. */
+ * When P2P runs together with P2M or M2M it runs on a second stream beside them, so [6] overlaps [1] and [2]
+ * and [7] is less than their sum.  After an execute() that replayed a CUDA graph only [0] and [7] are
+ * measured; [1]..[6] are 0. */
 B200FMM_API b200fmm_status b200fmm_last_timings(b200fmm_handle h, double *ms8);
 /* Device time of single kernels of the last execute(), milliseconds: [0] the M2L kernel (the tensor-core
  * kernel alone in MIXED, the whole M2L pass in FP64), [1] the P2P kernel, [2] P2M, [3] L2P (all 0 after a
@@ -217,11 +219,13 @@ B200FMM_API b200fmm_status b200fmm_p2p_noalloc(long long n, const double *x, con
                                                double *fx, double *fy, double *fz, void *stream);
 
 /* Batches of independent problems of uneven size, each with its own order, height and box (the reference
- * runs one FFmmAlgorithm per problem).  The problems are spread over nstreams worker streams, each driven by
- * its own host thread, largest first, so that one problem's tree build overlaps other problems' passes;
- * every worker keeps one handle per (order, height, box) it has met, so operators are computed once and
- * device buffers are reused by later calls.  Host memory in and out; nrhs = 1.  execute() returns when
- * every problem's results are written, or the first failure (its message names the problem). */
+ * runs one FFmmAlgorithm per problem).  The problems are dealt to nstreams worker streams, each driven by
+ * its own host thread, by estimated cost (largest first, each to the least loaded worker), so that one
+ * problem's tree build overlaps other problems' passes; every worker keeps one handle per (order, height, box)
+ * it has met, so operators are computed once and device buffers are reused by later calls.  The schedule
+ * depends only on the problem list, so a repeated call with the same list allocates nothing.  Host memory in
+ * and out; nrhs = 1.  execute() returns when every problem's results are written, or the first failure (its
+ * message names the problem). */
 typedef struct {
   long long n;                  /* particles */
   const double *x, *y, *z, *q;  /* n each */
@@ -235,6 +239,9 @@ B200FMM_API b200fmm_status b200fmm_batch_create(int kernel, int precision, int n
 B200FMM_API b200fmm_status b200fmm_batch_execute(b200fmm_batch b, int nproblems, const b200fmm_problem *problems);
 /* Host wall time of the last batch_execute(), milliseconds. */
 B200FMM_API b200fmm_status b200fmm_batch_last_time(b200fmm_batch b, double *ms);
+/* Device time of the last batch_execute(), milliseconds: from an event recorded before the first problem to
+ * the last worker stream's end (CUDA events), host gaps between a worker's problems included. */
+B200FMM_API b200fmm_status b200fmm_batch_last_device_time(b200fmm_batch b, double *ms);
 B200FMM_API b200fmm_status b200fmm_batch_destroy(b200fmm_batch b);
 
 /* Particle files of ScalFMM's FFmaGenericLoader / FFmaGenericWriter (Src/Files/FFmaGenericLoader.hpp:189-477):

@@ -32,7 +32,7 @@ EXPORTS = (
     "b200fmm_p2p", "b200fmm_get_results", "b200fmm_synchronize", "b200fmm_tree_info", "b200fmm_get_cells",
     "b200fmm_get_permutation", "b200fmm_last_timings", "b200fmm_last_kernel_times", "b200fmm_tree_stats",
     "b200fmm_last_launch_count", "b200fmm_autotune", "b200fmm_p2p_noalloc", "b200fmm_batch_create", "b200fmm_batch_execute",
-    "b200fmm_batch_last_time", "b200fmm_batch_destroy", "b200fmm_direct", "b200fmm_m2l_flops",
+    "b200fmm_batch_last_time", "b200fmm_batch_last_device_time", "b200fmm_batch_destroy", "b200fmm_direct", "b200fmm_m2l_flops",
     "b200fmm_get_leaf_neighbors", "b200fmm_get_interaction_lists", "b200fmm_fma_read", "b200fmm_fma_write",
     "b200fmm_get_leaf_ranges", "b200fmm_get_tuning",
 )
@@ -126,6 +126,7 @@ def lib():
                                            ctypes.POINTER(ctypes.c_void_p)]
         L.b200fmm_batch_execute.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
         L.b200fmm_batch_last_time.argtypes = [ctypes.c_void_p, _dp]
+        L.b200fmm_batch_last_device_time.argtypes = [ctypes.c_void_p, _dp]
         L.b200fmm_batch_destroy.argtypes = [ctypes.c_void_p]
         L.b200fmm_direct.argtypes = [ctypes.c_longlong, _dp, _dp, _dp, _dp, ctypes.c_longlong, _lp, _dp, _dp, _dp, _dp]
         _lib = L
@@ -374,6 +375,12 @@ class Batch:
     def last_time_ms(self):
         ms = ctypes.c_double()
         _check(lib().b200fmm_batch_last_time(self._h, ctypes.byref(ms)), "batch_last_time")
+        return ms.value
+
+    def last_device_ms(self):
+        """Device time of the last run: start event to the last worker stream's end event."""
+        ms = ctypes.c_double()
+        _check(lib().b200fmm_batch_last_device_time(self._h, ctypes.byref(ms)), "batch_last_device_time")
         return ms.value
 
     def close(self):

@@ -172,7 +172,7 @@ struct Context {
   Sym64 *s64 = nullptr;
 
   // timings / counters
-  cudaEvent_t ev[16];
+  cudaEvent_t ev[17];  // [16]: the end of M2M, before the wait for a concurrent near field
   bool events_ready = false;
   double ms[8] = {0};
   long long launches = 0;       // kernel launches of the last execute()

@@ -59,9 +59,11 @@ constexpr long long WAIT_LIMIT = 1LL << 22;
 
 // A work unit: one target tile (CTA pairs: the z-adjacent tiles bz, bz + 1) of one level and right-hand side,
 // with the 189 transfer vectors of its parity.  Its work is the number of those whose source box is occupied.
+// On a compacted level a unit is instead one block of 128 cells of one parity (CTA pairs: blocks blk, blk + 1).
 struct TcItem {
   int level, rhs, parity;
   int bx, by, bz;
+  int blk;  // compacted block, or -1 for a grid tile
 };
 
 struct TcLevel {
@@ -74,6 +76,15 @@ struct TcLevel {
   int tile0;           // first tile of this level in the busy masks
   int unit0, nunits;   // work units of this level: [unit0, unit0 + nunits), ordered rhs, parity, z, y, x
   int TZu;             // units along z: tiles, or pairs of tiles
+  // compacted targets (sparse levels): the units are blocks of 128 cells of one parity, whose A rows are
+  // gathered row by row from the source grid (ghi / glo: Y in the low-rank form, else the packed multipoles)
+  int cmode;           // 1: this level's units are compacted blocks
+  int cblk0[9];        // first block of each parity (an even count per parity for CTA pairs)
+  int cb0;             // first block of the level in the compacted busy masks
+  const int *crow;     // [blocks * 128]: (parity << 28) | position in the parity grid, or -1
+  const int *ccell;    // [blocks * 128]: cell index, or -1
+  const __half *ghi, *glo;
+  long long plane;     // positions of one parity grid: HX * HY * HZ
 };
 
 // Occupied cells of parity grid `par` in the box [x0, x0+nx) x [y0, y0+ny) x [z0, z0+nz) (clipped).
@@ -118,6 +129,10 @@ struct __align__(64) TcParams {
   // chunks per source cell, and B is U_t, both in 16-wide K chunks
   int lr_seglen;  // K chunks per accumulator segment of a fragment's chunk stream
   int ycht;       // Y chunks per right-hand side (all parities)
+  // compacted target blocks: 6 mask words per block as for tiles; gather = some level of the launch is
+  // compacted; growlen = fp16 per gathered grid row (16 for Y chunks, KP for multipoles)
+  const unsigned *cbusy;
+  int gather, growlen;
 };
 // What the producer and the MMA issuers need of transfer vector e of target parity c: the A box's
 // coordinates (offset of the source tile in half-grid cells; outer coordinate ya + rhs * (ycht or 8)), the B
@@ -161,6 +176,37 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity
 __device__ __forceinline__ bool mbar_wait_warp(unsigned long long *b, unsigned parity) {
   return __all_sync(0xffffffffu, mbar_wait(b, parity));
 }
+// the same with cluster-scope acquire: for phases completed by a release arrival from the other CTA of a pair
+__device__ __forceinline__ bool mbar_wait_cluster(unsigned long long *b, unsigned parity) {
+  for (long long it = 0; it < WAIT_LIMIT; ++it) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(su32(b)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+// n arrivals at once (a gathering warp that has nothing to copy for a stage)
+__device__ __forceinline__ void mbar_arrive_n(unsigned bar, unsigned n) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(n) : "memory");
+}
+// arrival on the other CTA's barrier that publishes this CTA's shared-memory writes to it
+__device__ __forceinline__ void mbar_arrive_cluster_release(unsigned cluster_addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+// 16-byte copy global -> shared through L2; src_bytes = 0 writes 16 zero bytes and reads nothing
+__device__ __forceinline__ void cp_async16(unsigned dst, const void *src, unsigned src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+// one arrival on the barrier once every cp.async that this thread has issued so far has landed
+__device__ __forceinline__ void cp_async_arrive_noinc(unsigned bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 __device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, unsigned long long *bar, int c0, int c1,
                                             int c2, int c3, int c4) {
   asm volatile(
@@ -375,8 +421,11 @@ struct BusyMask {
   }
   __device__ __forceinline__ bool src(int e) const { return (word(e >> 5) >> (e & 31)) & 1u; }
 };
+// G: the launch may hold compacted blocks (kernels without them compile the tile form alone)
+template <bool G = true>
 __device__ __forceinline__ BusyMask busy_mask(const TcParams &P, const TcItem &w) {
-  const unsigned *m = P.busy + 6 * tile_id(P, w.level, w.parity, w.bx, w.by, w.bz);
+  const unsigned *m = (G && w.blk >= 0) ? P.cbusy + 6LL * (P.lv[w.level].cb0 + w.blk)
+                                 : P.busy + 6 * tile_id(P, w.level, w.parity, w.bx, w.by, w.bz);
   BusyMask b;
 #pragma unroll
   for (int k = 0; k < 6; ++k) b.w[k] = m[k];
@@ -386,9 +435,15 @@ __device__ __forceinline__ BusyMask busy_mask(const TcParams &P, const TcItem &w
 // a transfer vector (or the item) only when it is idle for both tiles.  A level with an odd number of z tiles
 // has no tile bz + 1 in its last pair; that tile's A boxes lie outside the grid (zero-filled loads) and its
 // rows map to no cell.
+template <bool G = true>
 __device__ __forceinline__ BusyMask busy_mask_pair(const TcParams &P, const TcItem &w) {
-  BusyMask b = busy_mask(P, w);
-  if (w.bz + 1 < P.lv[w.level].HZ / TILE_Z) {
+  BusyMask b = busy_mask<G>(P, w);
+  if (G && w.blk >= 0) {
+    // compacted blocks come in pairs of one parity: block blk + 1 always exists (possibly without cells)
+    const unsigned *m = P.cbusy + 6LL * (P.lv[w.level].cb0 + w.blk + 1);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) b.w[k] |= m[k];
+  } else if (w.bz + 1 < P.lv[w.level].HZ / TILE_Z) {
     const unsigned *m = P.busy + 6 * tile_id(P, w.level, w.parity, w.bx, w.by, w.bz + 1);
 #pragma unroll
     for (int k = 0; k < 6; ++k) b.w[k] |= m[k];
@@ -396,6 +451,7 @@ __device__ __forceinline__ BusyMask busy_mask_pair(const TcParams &P, const TcIt
   return b;
 }
 
+template <bool G = true>
 __device__ __forceinline__ TcItem decode_unit(const TcParams &P, int u) {
   int level = P.l1;
   while (level > P.l0 && u >= P.lv[level].unit0 + P.lv[level].nunits) --level;
@@ -404,6 +460,18 @@ __device__ __forceinline__ TcItem decode_unit(const TcParams &P, int u) {
   int r = u - L.unit0;
   TcItem w;
   w.level = level;
+  if (G && L.cmode) {
+    // one right-hand side; blocks of parity p are [cblk0[p], cblk0[p + 1])
+    w.rhs = 0;
+    w.bx = w.by = w.bz = 0;
+    w.blk = r * (P.pair ? 2 : 1);
+    int p = 0;
+#pragma unroll
+    for (int q = 1; q < 8; ++q) p += w.blk >= L.cblk0[q] ? 1 : 0;
+    w.parity = p;
+    return w;
+  }
+  w.blk = -1;
   w.bx = r % TX;
   r /= TX;
   w.by = r % TY;
@@ -422,7 +490,7 @@ __device__ __forceinline__ TcItem decode_unit(const TcParams &P, int u) {
 //     are split into G ranges of equal work, one per CTA.
 //   * Otherwise: the work of all units is split into G * ranges_per_cta ranges of equal work; CTA g takes
 //     ranges g, g + G, ...
-template <class F>
+template <bool G, class F>
 __device__ __forceinline__ bool range_fragments(const TcParams &P, long long lo, long long hi, int u_from, F &f) {
   if (lo >= hi) return true;
   int a = u_from, b = P.u_end;  // the largest unit whose work starts at or before lo
@@ -435,27 +503,27 @@ __device__ __forceinline__ bool range_fragments(const TcParams &P, long long lo,
     if (p0 >= hi) break;
     const int r0 = (int)(max(lo, p0) - p0), r1 = (int)(min(hi, p1) - p0);
     if (r1 <= r0) continue;
-    if (!f(decode_unit(P, u), r0, r1)) return false;
+    if (!f(decode_unit<G>(P, u), r0, r1)) return false;
   }
   return true;
 }
-template <class F>
+template <bool GA, class F>
 __device__ __forceinline__ void for_each_fragment(const TcParams &P, int g, int G, F &&f) {
   const int U = P.u_end - P.u_begin;
   const long long base = P.prefix[P.u_begin], W = (long long)P.prefix[P.u_end] - base;
   if (W == 189LL * U) {
     const int nwave = U / G;
     for (int m = 0; m < nwave; ++m)
-      if (!f(decode_unit(P, P.u_begin + g + m * G), 0, 189)) return;
+      if (!f(decode_unit<GA>(P, P.u_begin + g + m * G), 0, 189)) return;
     const int ut = P.u_begin + nwave * G;
     const long long tb = P.prefix[ut], tw = (long long)P.prefix[P.u_end] - tb;
-    range_fragments(P, tb + tw * g / G, tb + tw * (g + 1) / G, ut, f);
+    range_fragments<GA>(P, tb + tw * g / G, tb + tw * (g + 1) / G, ut, f);
     return;
   }
   const int nr = G * P.ranges_per_cta;
   for (int m = 0; m < P.ranges_per_cta; ++m) {
     const int j = g + m * G;
-    if (!range_fragments(P, base + W * j / nr, base + W * (j + 1) / nr, P.u_begin, f)) return;
+    if (!range_fragments<GA>(P, base + W * j / nr, base + W * (j + 1) / nr, P.u_begin, f)) return;
   }
 }
 
@@ -478,12 +546,13 @@ __device__ __forceinline__ void for_each_fragment(const TcParams &P, int g, int 
 // expects both CTAs' bytes on its full barrier, its MMA warp issues all MMAs, and the commits arrive on the
 // stage and accumulator barriers of both CTAs; the epilogue warps of both CTAs release the accumulator on
 // the even CTA's barriers (16 arrivals).
-template <int CW, int NHALF, bool PAIR, bool LR>
+template <int CW, int NHALF, bool PAIR, bool LR, bool GATHER>
 __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_constant__ TcParams P) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1024-byte aligned stage buffers (the swizzle pattern repeats every 512 B)
   unsigned char *smem = (unsigned char *)(((unsigned long long)smem_raw + 1023) & ~1023ull);
   __shared__ __align__(8) unsigned long long full_bar[MAX_STAGES], empty_bar[MAX_STAGES];
+  __shared__ __align__(8) unsigned long long gfull_bar[MAX_STAGES];  // odd CTA of a pair: its gathers landed
   __shared__ __align__(8) unsigned long long acc_full[2][2], acc_empty[2][2], done_bar;
   __shared__ unsigned tmem_base_sh;
   __shared__ volatile int abort_sh;
@@ -496,8 +565,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
   const int g_id = PAIR ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
   const int g_count = PAIR ? (int)(gridDim.x >> 1) : (int)gridDim.x;
   if (threadIdx.x == 0) {
+    // A stage is full once the producer's expected bytes have landed and, in a launch with compacted blocks,
+    // once the 32 gathering lanes of this CTA have arrived (each after its own copies landed) and, in a pair,
+    // the odd CTA's relay has arrived for that CTA's gathers.
+    const unsigned full_count = GATHER ? (PAIR ? 34u : 33u) : 1u;
     for (int s = 0; s < S; ++s) {
-      mbar_init(&full_bar[s], 1);
+      mbar_init(&full_bar[s], full_count);
+      mbar_init(&gfull_bar[s], 32);
       mbar_init(&empty_bar[s], NHALF);  // one commit per MMA issuer
     }
     for (int b = 0; b < 2; ++b) {
@@ -542,8 +616,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
   };
   auto wait_bar = [&](unsigned long long *b, unsigned parity) -> bool { return mbar_wait(b, parity); };
   auto item_mask = [&](const TcItem &w) -> BusyMask {
-    if constexpr (PAIR) return busy_mask_pair(P, w);
-    return busy_mask(P, w);
+    if constexpr (PAIR) return busy_mask_pair<GATHER>(P, w);
+    return busy_mask<GATHER>(P, w);
   };
 
   constexpr int KCH = LR ? 16 : KCHUNK;  // fp16 per K chunk: 16 (32-byte rows) or 32 (64-byte rows)
@@ -562,8 +636,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
       // the barrier that counts this stage's bytes: this CTA's, or the even CTA's in a pair
       const unsigned full0 = PAIR ? mapa_shared(su32(&full_bar[0]), 0u) : su32(&full_bar[0]);
       const int stage_tx = (PAIR ? 2 : 1) * (2 * a_bytes + 2 * b_bytes);
+      const int stage_tx_b = (PAIR ? 2 : 1) * 2 * b_bytes;  // compacted blocks: the A rows are gathered
       unsigned loaded = 0, lpar = 0;  // stages that received a load, and the phase parity of the last one
-      for_each_fragment(P, g_id, g_count, [&](const TcItem &w, int r0, int r1) -> bool {
+      for_each_fragment<GATHER>(P, g_id, g_count, [&](const TcItem &w, int r0, int r1) -> bool {
         const BusyMask bm = item_mask(w);
         const int bz = w.bz + (int)rank;
         int rank_e = 0;
@@ -583,22 +658,26 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
               break;
             }
             unsigned char *sbuf = smem + (size_t)stage * P.stage_bytes;
-            if (leader) mbar_expect_tx(&full_bar[stage], stage_tx);
+            if (leader) mbar_expect_tx(&full_bar[stage], (GATHER && w.blk >= 0) ? stage_tx_b : stage_tx);
             const int k0 = LR ? 0 : kc * KCHUNK;  // K coordinate of the boxes
             const int c4 = LR ? a4 + kc : a4;
             const int c2 = LR ? b2 + kc : b2;
             if constexpr (PAIR) {
               const unsigned fb = full0 + 8u * (unsigned)stage;
-              tma_load_5d_pair(sbuf, &P.mapA_hi[w.level], fb, k0, ox, oy, oz, c4);
-              tma_load_5d_pair(sbuf + a_bytes, &P.mapA_lo[w.level], fb, k0, ox, oy, oz, c4);
+              if (!GATHER || w.blk < 0) {
+                tma_load_5d_pair(sbuf, &P.mapA_hi[w.level], fb, k0, ox, oy, oz, c4);
+                tma_load_5d_pair(sbuf + a_bytes, &P.mapA_lo[w.level], fb, k0, ox, oy, oz, c4);
+              }
               for (int h = 0; h < NHALF; ++h) {
                 const int row0 = h * P.NH + (int)rank * nb_rows;
                 tma_load_3d_pair(sbuf + 2 * a_bytes + h * nb_rows * ROWB, &P.mapB_hi, fb, k0, row0, c2);
                 tma_load_3d_pair(sbuf + 2 * a_bytes + b_bytes + h * nb_rows * ROWB, &P.mapB_lo, fb, k0, row0, c2);
               }
             } else {
-              tma_load_5d(sbuf, &P.mapA_hi[w.level], &full_bar[stage], k0, ox, oy, oz, c4);
-              tma_load_5d(sbuf + a_bytes, &P.mapA_lo[w.level], &full_bar[stage], k0, ox, oy, oz, c4);
+              if (!GATHER || w.blk < 0) {
+                tma_load_5d(sbuf, &P.mapA_hi[w.level], &full_bar[stage], k0, ox, oy, oz, c4);
+                tma_load_5d(sbuf + a_bytes, &P.mapA_lo[w.level], &full_bar[stage], k0, ox, oy, oz, c4);
+              }
               for (int h = 0; h < NHALF; ++h) {
                 tma_load_3d(sbuf + 2 * a_bytes + h * nb_rows * ROWB, &P.mapB_hi, &full_bar[stage], k0, h * P.NH, c2);
                 tma_load_3d(sbuf + 2 * a_bytes + b_bytes + h * nb_rows * ROWB, &P.mapB_lo, &full_bar[stage], k0,
@@ -665,7 +744,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
       };
       // the next stage in order once its operands have landed, or -1
       auto next_full = [&]() -> int {
-        if (!wait_bar(&full_bar[stage], phase)) {
+        // a pair's stages with gathered rows are completed by the odd CTA's release arrival
+        if (!((PAIR && GATHER) ? mbar_wait_cluster(&full_bar[stage], phase) : wait_bar(&full_bar[stage], phase))) {
           give_up();
           return -1;
         }
@@ -678,7 +758,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
       };
       unsigned empty_par = 0xFu;  // parity to wait for, per (buffer, half): starts at 1 (passes at once)
       int seg = 0;
-      for_each_fragment(P, g_id, g_count, [&](const TcItem &w, int r0, int r1) -> bool {
+      for_each_fragment<GATHER>(P, g_id, g_count, [&](const TcItem &w, int r0, int r1) -> bool {
         if constexpr (LR) {
           // low rank: the fragment's K chunks (1..3 per transfer vector) form one stream, cut into
           // segments of lr_seglen chunks; with two column halves both issuers cut it at the same places
@@ -770,6 +850,119 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
         mma_commit(&done_bar);
       if (!wait_bar(&done_bar, 0)) give_up();
     }
+    if (GATHER && PAIR && !leader && warp == 1 && lane == 0) {
+      // ------------------------------------------------ relay (odd CTA of a pair)
+      // The gathering lanes can only arrive on this CTA's own barriers: once a stage's rows of this CTA have
+      // landed (gfull), one release arrival on the even CTA's full barrier hands them over, stage by stage.
+      const unsigned full0r = mapa_shared(su32(&full_bar[0]), 0u);
+      int stage = 0;
+      unsigned phase = 0;
+      for_each_fragment<GATHER>(P, g_id, g_count, [&](const TcItem &w, int r0, int r1) -> bool {
+        const BusyMask bm = item_mask(w);
+        int rank_e = 0;
+        for (int e = 0; e < 189 && rank_e < r1 && !abort_sh; ++e) {
+          if (!bm.src(e)) continue;
+          if (rank_e++ < r0) continue;
+          const int nk = LR ? (int)tvs[w.parity * 189 + e].nk : P.NK;
+          for (int kc = 0; kc < nk; ++kc) {
+            if (!wait_bar(&gfull_bar[stage], phase)) {
+              give_up();
+              break;
+            }
+            mbar_arrive_cluster_release(full0r + 8u * (unsigned)stage);
+            if (++stage == S) {
+              stage = 0;
+              phase ^= 1;
+            }
+          }
+        }
+        return !abort_sh;
+      });
+    }
+  } else if (GATHER && warp == 3) {
+    // ------------------------------------------------ row gathers of compacted blocks (all 32 lanes)
+    // A compacted block's A tile holds, for transfer vector e, the source row of each of its 128 cells: the
+    // cell's half-grid position shifted by the box offset of e, in the source parity's grid (rows outside the
+    // grid read as zero, as the TMA boxes of the tile form do).  Lane l copies rows l, l + 32, l + 64, l + 96
+    // in 16-byte pieces, placed where the TMA unit's 32- or 64-byte swizzle would put them, and arrives once
+    // its copies have landed.  Stages of grid tiles (TMA-loaded A) get the 32 arrivals at once.
+    constexpr int PPR = ROWB / 16;                     // 16-byte pieces per row: 2 or 4
+    constexpr int SWZ_SHIFT = ROWB == 32 ? 2 : 1;      // row bits that select the XOR of the piece index
+    unsigned long long *gbar = (PAIR && !leader) ? gfull_bar : full_bar;
+    int stage = 0;
+    unsigned phase = 0;
+    for_each_fragment<GATHER>(P, g_id, g_count, [&](const TcItem &w, int r0, int r1) -> bool {
+      const BusyMask bm = item_mask(w);
+      const bool cmp = w.blk >= 0;
+      const TcLevel &Lv = P.lv[w.level];
+      unsigned hc[4];  // this lane's rows: half-grid x | y << 10 | z << 20, or ~0u for no cell
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        hc[i] = ~0u;
+        if (cmp) {
+          const int code = Lv.crow[(long long)(w.blk + (int)rank) * 128 + lane + 32 * i];
+          if (code >= 0) {
+            const int pos = code & 0x0FFFFFFF;
+            const int yz = pos / Lv.HX;
+            hc[i] = (unsigned)(pos - yz * Lv.HX) | ((unsigned)(yz % Lv.HY) << 10) | ((unsigned)(yz / Lv.HY) << 20);
+          }
+        }
+      }
+      bool stop = false;
+      int rank_e = 0;
+      for (int e = 0; e < 189 && rank_e < r1 && !stop; ++e) {
+        if (!bm.src(e)) continue;
+        if (rank_e++ < r0) continue;
+        const TvRec tr = tvs[w.parity * 189 + e];
+        const int nk = LR ? (int)tr.nk : P.NK;
+        for (int kc = 0; kc < nk; ++kc) {
+          // lane 0 waits for the stage to be free; the warp follows its outcome
+          int ok = 1;
+          if (lane == 0) ok = wait_bar(&empty_bar[stage], phase ^ 1) ? 1 : 0;
+          ok = __shfl_sync(0xffffffffu, ok, 0);
+          if (!ok) {
+            if (lane == 0) give_up();
+            stop = true;
+            break;
+          }
+          const unsigned bar = su32(&gbar[stage]);
+          if (cmp) {
+            const unsigned sa = su32(smem + (size_t)stage * P.stage_bytes);
+            // the grid rows of this K chunk: Y chunk tr.ya + kc of the source parity (low rank), or the source
+            // parity's multipoles at K offset kc * 32 (dense); row numbers fit 32 bits (checked on the host)
+            const int grow0 = (w.rhs * (LR ? P.ycht : 8) + tr.ya + (LR ? kc : 0)) * (int)Lv.plane;
+            const int kel = LR ? 0 : kc * KCHUNK;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              const int r = lane + 32 * i;
+              const int x = (int)(hc[i] & 1023u) + tr.ox, y = (int)((hc[i] >> 10) & 1023u) + tr.oy,
+                        z = (int)(hc[i] >> 20) + tr.oz;
+              const bool v = hc[i] != ~0u && x >= 0 && x < Lv.HX && y >= 0 && y < Lv.HY && z >= 0 && z < Lv.HZ;
+              const long long o = v ? (long long)(grow0 + (z * Lv.HY + y) * Lv.HX + x) * P.growlen + kel : 0;
+              const unsigned nb = v ? 16u : 0u;
+#pragma unroll
+              for (int j = 0; j < PPR; ++j) {
+                const unsigned d = sa + (unsigned)(r * ROWB) + ((unsigned)(j ^ ((r >> SWZ_SHIFT) & (PPR - 1))) << 4);
+                cp_async16(d, Lv.ghi + o + 8 * j, nb);
+                cp_async16(d + (unsigned)a_bytes, Lv.glo + o + 8 * j, nb);
+              }
+            }
+            cp_async_arrive_noinc(bar);
+          } else {
+            __syncwarp();
+            if (lane == 0) mbar_arrive_n(bar, 32);
+          }
+          if (++stage == S) {
+            stage = 0;
+            phase ^= 1;
+          }
+        }
+      }
+      stop = __any_sync(0xffffffffu, stop || abort_sh != 0);
+      return !stop;
+    });
+    // no copy of this warp may still be landing when the CTA exits
+    cp_async_wait_all();
   }
   } else {
     take_registers<SPLIT_REGS>();
@@ -797,7 +990,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
     float acc[CW];
 #pragma unroll
     for (int i = 0; i < CW; ++i) acc[i] = 0.f;
-    for_each_fragment(P, g_id, g_count, [&](const TcItem &w, int r0, int r1) -> bool {
+    for_each_fragment<GATHER>(P, g_id, g_count, [&](const TcItem &w, int r0, int r1) -> bool {
       // accumulator segments of this fragment: nseg per transfer vector, or (low rank) one per lr_seglen
       // K chunks of the fragment's chunk stream
       int nseg_item = (r1 - r0) * P.nseg;
@@ -856,12 +1049,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
       if (abort_sh) return false;
       // flush the fragment's sums into the FP64 locals
       const TcLevel &Lv = P.lv[w.level];
-      const int c = w.parity;
-      const int bz = w.bz + (int)rank;
-      const int hx = w.bx * TILE_X + (row & 7), hy = w.by * TILE_Y + ((row >> 3) & 3), hz = bz * TILE_Z + (row >> 5);
-      const int gx = 2 * hx + ((c >> 2) & 1), gy = 2 * hy + ((c >> 1) & 1), gz = 2 * hz + (c & 1);
       int cell = -1;
-      if (gx < Lv.side && gy < Lv.side && gz < Lv.side) cell = Lv.grid[((long long)gz * Lv.side + gy) * Lv.side + gx];
+      if (GATHER && w.blk >= 0) {
+        cell = Lv.ccell[(long long)(w.blk + (int)rank) * 128 + row];
+      } else {
+        const int c = w.parity;
+        const int bz = w.bz + (int)rank;
+        const int hx = w.bx * TILE_X + (row & 7), hy = w.by * TILE_Y + ((row >> 3) & 3), hz = bz * TILE_Z + (row >> 5);
+        const int gx = 2 * hx + ((c >> 2) & 1), gy = 2 * hy + ((c >> 1) & 1), gz = 2 * hz + (c & 1);
+        if (gx < Lv.side && gy < Lv.side && gz < Lv.side) cell = Lv.grid[((long long)gz * Lv.side + gy) * Lv.side + gx];
+      }
       if (cell >= 0) {
         const double sc = *Lv.scale_out;
         double *Lrow = Lv.L + ((long long)cell * P.R + w.rhs) * P.nn;
@@ -1398,6 +1595,7 @@ __global__ void busy_mask_kernel(const __grid_constant__ TcParams P, int l0, int
   const int TX = L.HX / TILE_X, TY = L.HY / TILE_Y, TZ = L.HZ / TILE_Z;
   TcItem w;
   w.level = (short)level;
+  w.blk = -1;
   w.bx = (short)(tl % TX);
   w.by = (short)((tl / TX) % TY);
   w.bz = (short)((tl / ((long long)TX * TY)) % TZ);
@@ -1512,30 +1710,114 @@ __global__ void pack_levels_kernel(const __grid_constant__ PackLevels L, int R, 
   }
 }
 
-// ---- compacted first-product levels ----------------------------------------------------------------
-// Cells of a sparse level grouped by parity into blocks of 128 rows: counts, then placement with per-parity
-// cursors (the order inside a parity does not matter: each Y row depends on its own cell only).
-__global__ void ccount_kernel(const long long *__restrict__ keys, long long n, int *__restrict__ cnt) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  int ix, iy, iz;
-  morton_decode3(keys[i], ix, iy, iz);
-  atomicAdd(cnt + (((ix & 1) << 2) | ((iy & 1) << 1) | (iz & 1)), 1);
+// ---- compacted levels ------------------------------------------------------------------------------
+// Cells of a sparse level grouped by parity into blocks of 128 rows, in Morton order inside each parity (so
+// that a block's cells, and the sources of each transfer vector, lie close together, and the placement is the
+// same on every run): per group of 1024 cells the count of each parity, then per parity the exclusive
+// offsets of the groups and the total, then each cell's row.
+__device__ __forceinline__ int key_parity(long long key, int &ix, int &iy, int &iz) {
+  morton_decode3(key, ix, iy, iz);
+  return ((ix & 1) << 2) | ((iy & 1) << 1) | (iz & 1);
+}
+__global__ void __launch_bounds__(1024) cgroup_count_kernel(const long long *__restrict__ keys, long long n,
+                                                            int *__restrict__ gcnt) {
+  __shared__ int cnt[8];
+  if (threadIdx.x < 8) cnt[threadIdx.x] = 0;
+  __syncthreads();
+  const long long i = blockIdx.x * 1024LL + threadIdx.x;
+  if (i < n) {
+    int ix, iy, iz;
+    atomicAdd(&cnt[key_parity(keys[i], ix, iy, iz)], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x < 8) gcnt[blockIdx.x * 8 + threadIdx.x] = cnt[threadIdx.x];
+}
+// one warp per parity: the group counts become exclusive offsets in place, the total goes to tot[p]
+__global__ void __launch_bounds__(256) cgroup_scan_kernel(int ngroups, int *__restrict__ gcnt, int *__restrict__ tot) {
+  const int p = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int run = 0;
+  for (int g0 = 0; g0 < ngroups; g0 += 32) {
+    const int g = g0 + lane;
+    const int v = g < ngroups ? gcnt[g * 8 + p] : 0;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (g < ngroups) gcnt[g * 8 + p] = run + x - v;
+    run += __shfl_sync(0xffffffffu, x, 31);
+  }
+  if (lane == 0) tot[p] = run;
 }
 struct CPlace {
-  int blk0[9];  // first 128-row block of each parity (cplace), or first Y chunk of each parity (cclear)
+  int blk0[9];  // first 128-row block of each parity (placement), or first Y chunk of each parity (cclear)
   int HX, HY;
 };
-__global__ void cplace_kernel(const long long *__restrict__ keys, long long n, const __grid_constant__ CPlace C,
-                              int *__restrict__ cursor, int *__restrict__ crow, int *__restrict__ ccell) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  int ix, iy, iz;
-  morton_decode3(keys[i], ix, iy, iz);
-  const int par = ((ix & 1) << 2) | ((iy & 1) << 1) | (iz & 1);
-  const int row = C.blk0[par] * 128 + atomicAdd(cursor + par, 1);
+__global__ void __launch_bounds__(1024) cgroup_place_kernel(const long long *__restrict__ keys, long long n,
+                                                            const __grid_constant__ CPlace C,
+                                                            const int *__restrict__ goff, int *__restrict__ crow,
+                                                            int *__restrict__ ccell) {
+  __shared__ int wcnt[32][8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long i = blockIdx.x * 1024LL + threadIdx.x;
+  int ix = 0, iy = 0, iz = 0, par = -1;
+  if (i < n) par = key_parity(keys[i], ix, iy, iz);
+  const unsigned same = __match_any_sync(0xffffffffu, par);
+  const int rk = __popc(same & ((1u << lane) - 1u));  // earlier lanes of this warp with the same parity
+  (&wcnt[0][0])[threadIdx.x & 255] = 0;
+  __syncthreads();
+  if (par >= 0 && rk == 0) wcnt[warp][par] = __popc(same);
+  __syncthreads();
+  if (par < 0) return;
+  int before = 0;
+  for (int w = 0; w < warp; ++w) before += wcnt[w][par];
+  const int row = C.blk0[par] * 128 + goff[blockIdx.x * 8 + par] + before + rk;
   crow[row] = (par << 28) | (((iz >> 1) * C.HY + (iy >> 1)) * C.HX + (ix >> 1));
   ccell[row] = (int)i;
+}
+// Busy masks of the compacted blocks of every compacted level (one CTA of 128 threads per block, blocks
+// numbered across levels from b0): bit e set when the source of some row under transfer vector e is a cell,
+// bit 31 of word 5 when the block holds a cell.
+struct CBlocks {
+  int l0, l1;
+  int b0[kMaxHeight + 1];  // first block of each level; levels that are not compacted have none
+};
+__global__ void __launch_bounds__(128) cbusy_kernel(const __grid_constant__ TcParams P, const __grid_constant__ CBlocks B,
+                                                    unsigned *__restrict__ cbusy) {
+  __shared__ unsigned m[6];
+  const int gb = blockIdx.x;
+  int l = B.l0;
+  while (l < B.l1 && gb >= B.b0[l + 1]) ++l;
+  const TcLevel &L = P.lv[l];
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x < 6) m[threadIdx.x] = 0;
+  __syncthreads();
+  const int code = L.crow[(long long)(gb - B.b0[l]) * 128 + threadIdx.x];
+  int gx = 0, gy = 0, gz = 0, par = 0;
+  if (code >= 0) {
+    par = code >> 28;
+    const int pos = code & 0x0FFFFFFF;
+    const int hx = pos % L.HX, hy = (pos / L.HX) % L.HY, hz = pos / (L.HX * L.HY);
+    gx = 2 * hx + ((par >> 2) & 1);
+    gy = 2 * hy + ((par >> 1) & 1);
+    gz = 2 * hz + (par & 1);
+  }
+  const unsigned any = __ballot_sync(0xffffffffu, code >= 0);
+  // every row of a block has the same parity; rows without a cell take the first valid row's
+  par = __shfl_sync(0xffffffffu, par, any ? __ffs(any) - 1 : 0);
+  for (int e = 0; e < 189; ++e) {
+    bool occ = false;
+    if (code >= 0) {
+      const int sx = gx + P.off[par][e][0], sy = gy + P.off[par][e][1], sz = gz + P.off[par][e][2];
+      occ = sx >= 0 && sx < L.side && sy >= 0 && sy < L.side && sz >= 0 && sz < L.side &&
+            L.grid[((long long)sz * L.side + sy) * L.side + sx] >= 0;
+    }
+    const unsigned v = __ballot_sync(0xffffffffu, occ);
+    if (lane == 0 && v) atomicOr(&m[e >> 5], 1u << (e & 31));
+  }
+  if (lane == 0 && any) atomicOr(&m[5], 1u << 31);
+  __syncthreads();
+  if (threadIdx.x < 6) cbusy[6LL * gb + threadIdx.x] = m[threadIdx.x];
 }
 // zero the Y rows (every chunk of the row's parity) of the cells a compacted level wrote for an earlier tree
 __global__ void cclear_kernel(const int *__restrict__ crow, long long plane, const __grid_constant__ CPlace B,
@@ -1664,8 +1946,16 @@ struct DenseTC {
   int *ccell[kMaxHeight] = {};            // [rows]: cell index, or -1
   __half *Chi[kMaxHeight] = {}, *Clo[kMaxHeight] = {};  // compacted multipoles [rows][KP]
   long long ccap[kMaxHeight] = {};        // rows allocated
+  long long chcap[kMaxHeight] = {};       // rows allocated in Chi / Clo
   int crows[kMaxHeight] = {};             // rows of the current tree (128-row blocks of each parity)
-  int *ccnt = nullptr;                    // [kMaxHeight][16]: cells of each parity, then placement cursors
+  int *ccnt = nullptr;                    // [kMaxHeight][8]: cells of each parity
+  int *cgrp = nullptr;                    // per level and group of 1024 cells: counts, then offsets, per parity
+  long long cgrp_cap = 0;
+  // second product on compacted levels: the tile-mode unit count of each level, the blocks' busy masks
+  int tunits[kMaxHeight] = {};
+  unsigned *cbusy = nullptr;
+  long long cbusy_cap = 0;
+  int prefix_cap = 0;                     // entries allocated in prefix
 };
 
 static b200fmm_status encode(CUtensorMap *map, void *base, int rank, const cuuint64_t *dims, const cuuint64_t *strides,
@@ -1985,9 +2275,9 @@ b200fmm_status tc_init(Context &c) {
 #define B200_TC_OCC(NPV, CWV, NHV)                 \
   case NPV:                                        \
     if (lr)                                        \
-      occ(m2l_tc_kernel<CWV, NHV, true, true>);    \
+      occ(m2l_tc_kernel<CWV, NHV, true, true, true>);  \
     else                                           \
-      occ(m2l_tc_kernel<CWV, NHV, true, false>);   \
+      occ(m2l_tc_kernel<CWV, NHV, true, false, true>); \
     break;
       B200_TC_OCC(32, 16, 1)
       B200_TC_OCC(64, 32, 1)
@@ -2015,14 +2305,22 @@ b200fmm_status tc_init(Context &c) {
     };
     check_regs(lr_y_kernel<true>);
     check_regs(lr_y_kernel<false>);
-    check_regs(m2l_tc_kernel<176, 2, true, true>);
-    check_regs(m2l_tc_kernel<176, 2, true, false>);
-    check_regs(m2l_tc_kernel<176, 2, false, true>);
-    check_regs(m2l_tc_kernel<176, 2, false, false>);
-    check_regs(m2l_tc_kernel<112, 1, true, true>);
-    check_regs(m2l_tc_kernel<112, 1, true, false>);
-    check_regs(m2l_tc_kernel<112, 1, false, true>);
-    check_regs(m2l_tc_kernel<112, 1, false, false>);
+    check_regs(m2l_tc_kernel<176, 2, true, true, false>);
+    check_regs(m2l_tc_kernel<176, 2, true, false, false>);
+    check_regs(m2l_tc_kernel<176, 2, false, true, false>);
+    check_regs(m2l_tc_kernel<176, 2, false, false, false>);
+    check_regs(m2l_tc_kernel<112, 1, true, true, false>);
+    check_regs(m2l_tc_kernel<112, 1, true, false, false>);
+    check_regs(m2l_tc_kernel<112, 1, false, true, false>);
+    check_regs(m2l_tc_kernel<112, 1, false, false, false>);
+    check_regs(m2l_tc_kernel<176, 2, true, true, true>);
+    check_regs(m2l_tc_kernel<176, 2, true, false, true>);
+    check_regs(m2l_tc_kernel<176, 2, false, true, true>);
+    check_regs(m2l_tc_kernel<176, 2, false, false, true>);
+    check_regs(m2l_tc_kernel<112, 1, true, true, true>);
+    check_regs(m2l_tc_kernel<112, 1, true, false, true>);
+    check_regs(m2l_tc_kernel<112, 1, false, true, true>);
+    check_regs(m2l_tc_kernel<112, 1, false, false, true>);
     if (!regs_ok) {
       cudaGetLastError();
       return fail(B200FMM_ERR_UNSUPPORTED, "tensor-core M2L: kernels not compiled to the register count their "
@@ -2053,7 +2351,8 @@ void tc_free(Context &c) {
     for (void *q : {(void *)t->crow[l], (void *)t->ccell[l], (void *)t->Chi[l], (void *)t->Clo[l]})
       if (q) cudaFree(q);
   }
-  if (t->ccnt) cudaFree(t->ccnt);
+  for (void *q : {(void *)t->ccnt, (void *)t->cgrp, (void *)t->cbusy})
+    if (q) cudaFree(q);
   if (t->sat) cudaFree(t->sat);
   if (t->ydirty) cudaFree(t->ydirty);
   delete t->params;
@@ -2140,6 +2439,11 @@ static b200fmm_status tc_prepare(Context &c) {
     P.lv[l].TZu = t->pair ? (TZ + 1) / 2 : TZ;
     P.lv[l].unit0 = nunits;
     P.lv[l].nunits = c.R * 8 * P.lv[l].TZu * (t->HY[l] / TILE_Y) * (t->HX[l] / TILE_X);
+    t->tunits[l] = P.lv[l].nunits;
+    P.lv[l].cmode = 0;
+    P.lv[l].plane = (long long)t->HX[l] * t->HY[l] * t->HZ[l];
+    P.lv[l].ghi = t->lr ? t->Yhi[l] : t->Ahi[l];
+    P.lv[l].glo = t->lr ? t->Ylo[l] : t->Alo[l];
     nunits += P.lv[l].nunits;
   }
   t->nunits_all = nunits;
@@ -2192,7 +2496,9 @@ static b200fmm_status tc_prepare(Context &c) {
   if (t->lr) t->yparams->busy = t->busy;
   if (t->prefix) cudaFree(t->prefix);
   B200_CUDA(cudaMalloc(&t->prefix, sizeof(int) * (nunits + 1)));
+  t->prefix_cap = nunits + 1;
   P.prefix = t->prefix;
+  P.growlen = t->lr ? 16 : t->KP;
   P.ranges_per_cta = ns;
   P.pair = t->pair ? 1 : 0;
   P.R = c.R;
@@ -2218,95 +2524,187 @@ static b200fmm_status tc_prepare(Context &c) {
   return B200FMM_OK;
 }
 
-// Per tree, low-rank form: which levels the first product runs compacted (a level less than half full, one
-// right-hand side, single CTAs), their cells grouped by parity into 128-row blocks, the tensor maps of their
-// compacted multipoles and the item numbering.  Y must read as zero wherever no cell is: rows that an earlier
-// tree's compacted level wrote are cleared here, and a level that turns compacted after tile-mode runs has its
-// Y and tile flags cleared (tile mode keeps clearing its own rows through the flags).  One host synchronisation
-// (the per-parity counts) when some level is compacted.
-static b200fmm_status y_compact_setup(Context &c, DenseTC &t) {
-  LrYParams &Y = *t.yparams;
+// Per tree: which sparse levels run compacted, and their cells grouped by parity into 128-row blocks.
+//   * A level is sparse when fewer than half of its cells exist; compaction needs one right-hand side.
+//   * The second product (U Y, or K M in the dense form) runs a compacted level's units over blocks (pairs of
+//     blocks of one parity on CTA pairs) instead of grid tiles: the unit numbering of every level is redone
+//     here, and the blocks get their busy masks.  B200FMM_TC_TCOMPACT=0 keeps the tiles.
+//   * Low-rank form, single CTAs: the first product (Y = V^T M) of a compacted level runs over the same blocks,
+//     with the compacted multipoles' tensor maps and its item numbering (B200FMM_TC_YCOMPACT=0 keeps the
+//     tiles).  Y must read as zero wherever no cell is: rows that an earlier tree's compacted first product
+//     wrote are cleared here, and a level whose first product turns compacted after tile-mode runs has its Y
+//     and tile flags cleared (tile mode keeps clearing its own rows through the flags).
+// One host synchronisation (the per-parity counts) when some level is compacted.
+static b200fmm_status compact_setup(Context &c, DenseTC &t) {
+  TcParams &P = *t.params;
   const int LL = c.H - 1;
-  const char *env = getenv("B200FMM_TC_YCOMPACT");
-  const bool allow = !t.ypair && c.R == 1 && !(env && atoi(env) == 0);
-  unsigned mask = 0;
+  const char *ye = getenv("B200FMM_TC_YCOMPACT"), *te = getenv("B200FMM_TC_TCOMPACT");
+  const bool yallow = t.lr && !t.ypair && c.R == 1 && !(ye && atoi(ye) == 0);
+  const bool tallow = c.R == 1 && !(te && atoi(te) == 0);
+  unsigned ymask = 0, tmask = 0;
   for (int l = 2; l <= LL; ++l) {
     const long long plane = (long long)t.HX[l] * t.HY[l] * t.HZ[l];
-    const bool sparse = c.lv[l].n > 0 && 2 * c.lv[l].n < (1LL << (3 * l));
-    if (allow && sparse && plane < (1LL << 28)) mask |= 1u << l;
+    const bool sparse = c.lv[l].n > 0 && 2 * c.lv[l].n < (1LL << (3 * l)) && plane < (1LL << 28);
+    // the gathers number the rows of a level's source grid in 32 bits
+    const long long grid_rows = (long long)c.R * (t.lr ? t.ycht : 8) * plane;
+    if (yallow && sparse) ymask |= 1u << l;
+    if (tallow && sparse && grid_rows < (1LL << 31)) tmask |= 1u << l;
   }
-  CPlace chunks{};
-  for (int p = 0; p <= 8; ++p) chunks.blk0[p] = p < 8 ? t.ybase[p] : t.ycht;
-  for (int l = 2; l <= LL; ++l) {
-    const long long plane = (long long)t.HX[l] * t.HY[l] * t.HZ[l];
-    if (t.ymode[l] == 2 && t.crows[l] > 0) {
-      cclear_kernel<<<(unsigned)t.crows[l], 64, 0, c.stream>>>(t.crow[l], plane, chunks, t.Yhi[l], t.Ylo[l]);
-      ++c.launches;
+  const unsigned mask = ymask | tmask;
+  if (t.lr) {
+    LrYParams &Y = *t.yparams;
+    CPlace chunks{};
+    for (int p = 0; p <= 8; ++p) chunks.blk0[p] = p < 8 ? t.ybase[p] : t.ycht;
+    for (int l = 2; l <= LL; ++l) {
+      const long long plane = (long long)t.HX[l] * t.HY[l] * t.HZ[l];
+      if (t.ymode[l] == 2 && t.crows[l] > 0) {
+        cclear_kernel<<<(unsigned)t.crows[l], 64, 0, c.stream>>>(t.crow[l], plane, chunks, t.Yhi[l], t.Ylo[l]);
+        ++c.launches;
+      }
+      if (((ymask >> l) & 1u) && t.ymode[l] == 1) {
+        B200_CUDA(cudaMemsetAsync(t.Yhi[l], 0, t.Ybytes[l], c.stream));
+        B200_CUDA(cudaMemsetAsync(t.Ylo[l], 0, t.Ybytes[l], c.stream));
+        B200_CUDA(cudaMemsetAsync(t.ydirty + 16 * (size_t)t.titem0[l], 0, 16 * (size_t)t.tnitems[l], c.stream));
+      }
     }
-    if (((mask >> l) & 1u) && t.ymode[l] == 1) {
-      B200_CUDA(cudaMemsetAsync(t.Yhi[l], 0, t.Ybytes[l], c.stream));
-      B200_CUDA(cudaMemsetAsync(t.Ylo[l], 0, t.Ybytes[l], c.stream));
-      B200_CUDA(cudaMemsetAsync(t.ydirty + 16 * (size_t)t.titem0[l], 0, 16 * (size_t)t.tnitems[l], c.stream));
-    }
-    t.crows[l] = 0;
+    (void)Y;
   }
-  int cnt[kMaxHeight][16] = {};
+  for (int l = 2; l <= LL; ++l) t.crows[l] = 0;
+  // per-parity counts of every placed level, in groups of 1024 cells
+  int cnt[kMaxHeight][8] = {};
+  long long g0[kMaxHeight + 1] = {};
   if (mask) {
-    if (!t.ccnt) B200_CUDA(cudaMalloc(&t.ccnt, sizeof(int) * kMaxHeight * 16));
-    B200_CUDA(cudaMemsetAsync(t.ccnt, 0, sizeof(int) * kMaxHeight * 16, c.stream));
+    for (int l = 2; l <= LL; ++l) g0[l + 1] = g0[l] + (((mask >> l) & 1u) ? (c.lv[l].n + 1023) / 1024 : 0);
+    const long long ng = g0[LL + 1];
+    if (t.cgrp_cap < 8 * ng) {
+      if (t.cgrp) cudaFree(t.cgrp);
+      t.cgrp = nullptr;
+      t.cgrp_cap = 0;
+      B200_CUDA(cudaMalloc(&t.cgrp, sizeof(int) * 8 * ng));
+      t.cgrp_cap = 8 * ng;
+    }
+    if (!t.ccnt) B200_CUDA(cudaMalloc(&t.ccnt, sizeof(int) * kMaxHeight * 8));
+    B200_CUDA(cudaMemsetAsync(t.ccnt, 0, sizeof(int) * kMaxHeight * 8, c.stream));
     for (int l = 2; l <= LL; ++l)
       if ((mask >> l) & 1u) {
-        ccount_kernel<<<grid_for(c.lv[l].n, 256), 256, 0, c.stream>>>(c.lv[l].keys, c.lv[l].n, t.ccnt + 16 * l);
-        ++c.launches;
+        const int ngl = (int)(g0[l + 1] - g0[l]);
+        cgroup_count_kernel<<<ngl, 1024, 0, c.stream>>>(c.lv[l].keys, c.lv[l].n, t.cgrp + 8 * g0[l]);
+        cgroup_scan_kernel<<<1, 256, 0, c.stream>>>(ngl, t.cgrp + 8 * g0[l], t.ccnt + 8 * l);
+        c.launches += 2;
       }
     B200_CUDA(cudaMemcpyAsync(cnt, t.ccnt, sizeof(cnt), cudaMemcpyDeviceToHost, c.stream));
     B200_CUDA(cudaStreamSynchronize(c.stream));
   }
-  int n = 0;
-  for (int l = LL; l >= 2; --l) {
-    Y.item0[l] = n;
-    if (!((mask >> l) & 1u)) {
-      Y.nitems[l] = t.tnitems[l];
-      n += Y.nitems[l];
-      t.ymode[l] = 1;
-      continue;
-    }
+  // blocks of every placed level (an even count per parity for CTA pairs), their rows and cells
+  CBlocks B{};
+  B.l0 = 2;
+  B.l1 = LL;
+  int nblocks[kMaxHeight] = {};
+  for (int l = 2; l <= LL; ++l) {
+    P.lv[l].cmode = 0;
+    B.b0[l + 1] = B.b0[l];
+    if (!((mask >> l) & 1u)) continue;
     CPlace C{};
     C.blk0[0] = 0;
-    for (int p = 0; p < 8; ++p) C.blk0[p + 1] = C.blk0[p] + (cnt[l][p] + 127) / 128;
+    for (int p = 0; p < 8; ++p) {
+      int nb = (cnt[l][p] + 127) / 128;
+      if (t.pair && ((tmask >> l) & 1u)) nb += nb & 1;
+      C.blk0[p + 1] = C.blk0[p] + nb;
+    }
     C.HX = t.HX[l];
     C.HY = t.HY[l];
+    nblocks[l] = C.blk0[8];
     const long long rows = 128LL * C.blk0[8];
     if (t.ccap[l] < rows) {
-      for (void *q : {(void *)t.crow[l], (void *)t.ccell[l], (void *)t.Chi[l], (void *)t.Clo[l]})
+      for (void *q : {(void *)t.crow[l], (void *)t.ccell[l]})
         if (q) cudaFree(q);
       t.crow[l] = t.ccell[l] = nullptr;
-      t.Chi[l] = t.Clo[l] = nullptr;
       t.ccap[l] = 0;
       B200_CUDA(cudaMalloc(&t.crow[l], sizeof(int) * rows));
       B200_CUDA(cudaMalloc(&t.ccell[l], sizeof(int) * rows));
-      B200_CUDA(cudaMalloc(&t.Chi[l], sizeof(__half) * rows * t.KP));
-      B200_CUDA(cudaMalloc(&t.Clo[l], sizeof(__half) * rows * t.KP));
       t.ccap[l] = rows;
     }
     B200_CUDA(cudaMemsetAsync(t.crow[l], 0xFF, sizeof(int) * rows, c.stream));
     B200_CUDA(cudaMemsetAsync(t.ccell[l], 0xFF, sizeof(int) * rows, c.stream));
-    cplace_kernel<<<grid_for(c.lv[l].n, 256), 256, 0, c.stream>>>(c.lv[l].keys, c.lv[l].n, C, t.ccnt + 16 * l + 8,
-                                                                   t.crow[l], t.ccell[l]);
+    const int ngl = (int)(g0[l + 1] - g0[l]);
+    cgroup_place_kernel<<<ngl, 1024, 0, c.stream>>>(c.lv[l].keys, c.lv[l].n, C, t.cgrp + 8 * g0[l], t.crow[l],
+                                                    t.ccell[l]);
     ++c.launches;
-    cuuint64_t dims[2] = {(cuuint64_t)t.KP, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)t.KP * 2};
-    cuuint32_t box[2] = {KCHUNK, 128};
-    B200_CHECK(encode(&Y.mapC_hi[l], t.Chi[l], 2, dims, strides, box));
-    B200_CHECK(encode(&Y.mapC_lo[l], t.Clo[l], 2, dims, strides, box));
-    Y.crow[l] = t.crow[l];
-    for (int p = 0; p <= 8; ++p) Y.cblk0[l][p] = C.blk0[p];
     t.crows[l] = (int)rows;
-    Y.nitems[l] = C.blk0[8] * t.nblk;
-    n += Y.nitems[l];
-    t.ymode[l] = 2;
+    P.lv[l].crow = t.crow[l];
+    P.lv[l].ccell = t.ccell[l];
+    for (int p = 0; p <= 8; ++p) P.lv[l].cblk0[p] = C.blk0[p];
+    if ((tmask >> l) & 1u) {
+      P.lv[l].cmode = 1;
+      P.lv[l].cb0 = B.b0[l];
+      B.b0[l + 1] = B.b0[l] + C.blk0[8];
+    }
+    if (t.lr && ((ymask >> l) & 1u)) {
+      LrYParams &Y = *t.yparams;
+      if (t.chcap[l] < rows) {
+        for (void *q : {(void *)t.Chi[l], (void *)t.Clo[l]})
+          if (q) cudaFree(q);
+        t.Chi[l] = t.Clo[l] = nullptr;
+        t.chcap[l] = 0;
+        B200_CUDA(cudaMalloc(&t.Chi[l], sizeof(__half) * rows * t.KP));
+        B200_CUDA(cudaMalloc(&t.Clo[l], sizeof(__half) * rows * t.KP));
+        t.chcap[l] = rows;
+      }
+      cuuint64_t dims[2] = {(cuuint64_t)t.KP, (cuuint64_t)rows};
+      cuuint64_t strides[1] = {(cuuint64_t)t.KP * 2};
+      cuuint32_t box[2] = {KCHUNK, 128};
+      B200_CHECK(encode(&Y.mapC_hi[l], t.Chi[l], 2, dims, strides, box));
+      B200_CHECK(encode(&Y.mapC_lo[l], t.Clo[l], 2, dims, strides, box));
+      Y.crow[l] = t.crow[l];
+      for (int p = 0; p <= 8; ++p) Y.cblk0[l][p] = C.blk0[p];
+    }
   }
-  Y.compact_levels = mask;
+  // first-product items (low rank), finest level first
+  if (t.lr) {
+    LrYParams &Y = *t.yparams;
+    int n = 0;
+    for (int l = LL; l >= 2; --l) {
+      Y.item0[l] = n;
+      if ((ymask >> l) & 1u) {
+        Y.nitems[l] = nblocks[l] * t.nblk;
+        t.ymode[l] = 2;
+      } else {
+        Y.nitems[l] = t.tnitems[l];
+        t.ymode[l] = 1;
+      }
+      n += Y.nitems[l];
+    }
+    Y.compact_levels = ymask;
+  }
+  // second-product units, finest level first, and the busy masks of the compacted blocks
+  int nunits = 0;
+  for (int l = LL; l >= 2; --l) {
+    P.lv[l].unit0 = nunits;
+    P.lv[l].nunits = P.lv[l].cmode ? nblocks[l] / (t.pair ? 2 : 1) : t.tunits[l];
+    nunits += P.lv[l].nunits;
+  }
+  t.nunits_all = nunits;
+  if (t.prefix_cap < nunits + 1) {
+    if (t.prefix) cudaFree(t.prefix);
+    t.prefix = nullptr;
+    t.prefix_cap = 0;
+    B200_CUDA(cudaMalloc(&t.prefix, sizeof(int) * (nunits + 1)));
+    t.prefix_cap = nunits + 1;
+    P.prefix = t.prefix;
+  }
+  const int nb_all = B.b0[LL + 1];
+  if (nb_all > 0) {
+    if (t.cbusy_cap < nb_all) {
+      if (t.cbusy) cudaFree(t.cbusy);
+      t.cbusy = nullptr;
+      t.cbusy_cap = 0;
+      B200_CUDA(cudaMalloc(&t.cbusy, sizeof(unsigned) * 6 * nb_all));
+      t.cbusy_cap = nb_all;
+    }
+    P.cbusy = t.cbusy;
+    cbusy_kernel<<<nb_all, 128, 0, c.stream>>>(P, B, t.cbusy);
+    ++c.launches;
+  }
   return B200FMM_OK;
 }
 
@@ -2352,15 +2750,17 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
     }
     busy_mask_kernel<<<grid_for(t->ntiles_all * 189, 256), 256, 0, c.stream>>>(P0, 2, LL, t->ntiles_all, full_levels,
                                                                                  t->busy);
+    ++c.launches;
+    // compacted levels: placement, unit numbering and block masks
+    B200_CHECK(compact_setup(c, *t));
     // the work of every unit of every level and its prefix sums, from which each launch splits its units
     // into ranges of equal work
-    TcParams Pw = P0;
+    TcParams Pw = *t->params;
     Pw.l0 = 2;
     Pw.l1 = LL;
     unit_work_kernel<<<grid_for(t->nunits_all, 256), 256, 0, c.stream>>>(Pw, t->nunits_all, t->prefix);
     unit_scan_kernel<<<1, 1024, 0, c.stream>>>(t->nunits_all, t->prefix);
-    c.launches += 3;
-    if (t->lr) B200_CHECK(y_compact_setup(c, *t));
+    c.launches += 2;
     t->sat_serial = c.tree_serial;
   }
   const int l0 = level == -1 ? 2 : level, l1 = level == -1 ? LL : level;
@@ -2417,6 +2817,9 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
   P.l1 = l1;
   P.u_begin = P.lv[l1].unit0;
   P.u_end = P.lv[l0].unit0 + P.lv[l0].nunits;
+  P.gather = 0;
+  for (int l = l0; l <= l1; ++l)
+    if (P.lv[l].cmode) P.gather = 1;
   if (P.u_end <= P.u_begin) return B200FMM_OK;
   const size_t smem = (size_t)t->stages * t->stage_bytes + TV_BYTES + 1024;
   const int grid = t->grid;  // persistent: one CTA (pair) per SM (pair of SMs)
@@ -2467,13 +2870,15 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
     return cudaLaunchKernelEx(&cfg, kern, P);
   };
   switch (t->NP) {
+  // one instance per (pair, form, gathers): launches without compacted levels run the tile form alone
+#define B200_TC_PICK(CWV, NHV, PR, LRV)                                                             \
+  (P.gather ? launch(m2l_tc_kernel<CWV, NHV, PR, LRV, true>) : launch(m2l_tc_kernel<CWV, NHV, PR, LRV, false>))
 #define B200_TC_CASE(NPV, CWV, NHV)                                                                \
   case NPV:                                                                                          \
     if (t->pair)                                                                                     \
-      B200_CUDA(t->lr ? launch(m2l_tc_kernel<CWV, NHV, true, true>) : launch(m2l_tc_kernel<CWV, NHV, true, false>)); \
+      B200_CUDA(t->lr ? B200_TC_PICK(CWV, NHV, true, true) : B200_TC_PICK(CWV, NHV, true, false));   \
     else                                                                                             \
-      B200_CUDA(t->lr ? launch(m2l_tc_kernel<CWV, NHV, false, true>)                                 \
-                      : launch(m2l_tc_kernel<CWV, NHV, false, false>));                              \
+      B200_CUDA(t->lr ? B200_TC_PICK(CWV, NHV, false, true) : B200_TC_PICK(CWV, NHV, false, false)); \
     break;
     B200_TC_CASE(32, 16, 1)
     B200_TC_CASE(64, 32, 1)
@@ -2481,6 +2886,7 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
     B200_TC_CASE(224, 112, 1)
     B200_TC_CASE(352, 176, 2)
 #undef B200_TC_CASE
+#undef B200_TC_PICK
     default:
       return fail(B200FMM_ERR_UNSUPPORTED, "no tensor-core M2L instance for this order");
   }

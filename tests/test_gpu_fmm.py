@@ -579,7 +579,7 @@ def test_batch_matches_single_problems(kernel, precision, tol):
     b = S.Batch(kernel, precision, nstreams=3, device=0)
     for _ in range(2):
         outs = b.run(problems)
-        assert b.last_time_ms() > 0
+        assert b.last_time_ms() > 0 and b.last_device_ms() > 0
         for pr, out in zip(problems, outs):
             f = S.FMM(kernel, pr["order"], pr["height"], precision=precision)
             f.set_particles(pr["x"], pr["y"], pr["z"], pr["q"])
@@ -642,11 +642,11 @@ def test_mixed_handle_reused_from_dense_to_sparse_tree():
         assert S.rel_l2(got[k], want[k]) < 1e-12, (k, S.rel_l2(got[k], want[k]))
 
 
-def _mixed_eval(x, y, z, q, H, env=None, order=6):
+def _mixed_eval(x, y, z, q, H, env=None, order=6, kernel="cheb_sym", precision="mixed"):
     old = {k: os.environ.get(k) for k in (env or {})}
     os.environ.update(env or {})
     try:
-        f = S.FMM("cheb_sym", order, H, precision="mixed")
+        f = S.FMM(kernel, order, H, precision=precision)
         f.set_particles(x, y, z, q)
         f.execute()
         r = f.results()
@@ -673,6 +673,33 @@ def test_compacted_first_product_matches_tile_mode(order):
     want = _mixed_eval(x, y, z, q, 6, {"B200FMM_TC_YCOMPACT": "0"}, order=order)
     for k in FIELDS:
         assert np.array_equal(got[k], want[k]), (k, S.rel_l2(got[k], want[k]))
+
+
+@pytest.mark.parametrize("kernel,order,pair", [("cheb_sym", 5, "0"), ("cheb_sym", 6, "0"), ("cheb_sym", 6, "1"),
+                                               ("cheb_sym", 7, "1"), ("lagrange", 6, "0"), ("lagrange", 5, "1")])
+def test_compacted_second_product_matches_tile_mode(kernel, order, pair):
+    """A level less than half full runs the second M2L product (U Y, or K M in the dense form) over blocks of
+    128 cells of one parity whose A rows are gathered, instead of the parity grid's tiles, on single CTAs and
+    on CTA pairs.  The accumulator segments are cut where the block's busy transfer vectors put them, so the
+    results agree with the tile mode (B200FMM_TC_TCOMPACT=0) to the mixed-precision level rather than bitwise;
+    both agree with FP64, and two fresh handles give identical results (the placement is deterministic)."""
+    from distributions import ellipsoid_surface, plummer
+
+    if kernel == "lagrange":
+        x, y, z = ellipsoid_surface(40000, seed=44)
+    else:
+        x, y, z = plummer(30000, seed=43)
+    q = np.random.default_rng(45).uniform(-1.0, 1.0, x.size)
+    env = {"B200FMM_TC_PAIR": pair}
+    got = _mixed_eval(x, y, z, q, 6, env, order=order, kernel=kernel)
+    again = _mixed_eval(x, y, z, q, 6, env, order=order, kernel=kernel)
+    tiles = _mixed_eval(x, y, z, q, 6, {**env, "B200FMM_TC_TCOMPACT": "0"}, order=order, kernel=kernel)
+    ref = _mixed_eval(x, y, z, q, 6, order=order, kernel=kernel, precision="fp64")
+    for k in FIELDS:
+        assert np.array_equal(got[k], again[k]), k
+        assert S.rel_l2(got[k], tiles[k]) < 2e-6, (k, S.rel_l2(got[k], tiles[k]))
+        e_c, e_t = S.rel_l2(got[k], ref[k]), S.rel_l2(tiles[k], ref[k])
+        assert e_c < 2e-6 and e_c < 1.5 * e_t + 1e-8, (k, e_c, e_t)
 
 
 def test_mixed_handle_reused_across_sparse_and_dense_trees():
