@@ -229,6 +229,36 @@ def test_level_batched_operators_equal_execute(golden):
     f.close()
 
 
+@pytest.mark.parametrize("order", [6, 7])
+def test_level_batched_mixed_on_compacted_levels(order):
+    """MIXED level-batched operators on a clustered tree whose sparse levels run the tensor-core M2L on
+    compacted blocks: one M2L launch per level gives the results of execute() (whose single launch covers every
+    level) to the mixed level; the FP32 partial sums are only grouped differently."""
+    from distributions import plummer
+
+    x, y, z = plummer(30000, seed=71)
+    q = np.random.default_rng(72).uniform(-1.0, 1.0, x.size)
+    H = 6
+    f = S.FMM("cheb_sym", order, H, precision="mixed")
+    f.set_particles(x, y, z, q)
+    f.execute()
+    want = f.results()
+    f.reset_expansions()
+    f.p2m()
+    for lvl in range(H - 2, 1, -1):
+        f.m2m(lvl)
+    for lvl in range(2, H):
+        f.m2l(lvl)
+    for lvl in range(2, H - 1):
+        f.l2l(lvl)
+    f.l2p()
+    f.p2p(0)
+    got = f.results()
+    f.close()
+    for k in FIELDS:
+        assert S.rel_l2(got[k], want[k]) < 2e-6, (k, S.rel_l2(got[k], want[k]))
+
+
 def test_edge_cases():
     # one particle: no interactions at all
     f = S.FMM("cheb_sym", 4, 3)
