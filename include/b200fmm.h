@@ -151,6 +151,17 @@ B200FMM_API b200fmm_status b200fmm_p2p(b200fmm_handle h, int variant);
 /* Results in the caller's original particle order, [rhs][particle]; host memory unless on_device. */
 B200FMM_API b200fmm_status b200fmm_get_results(b200fmm_handle h, double *phi, double *fx, double *fy, double *fz,
                                    int on_device);
+/* The same into host memory without waiting (no counterpart in the reference): the results are staged on the
+ * handle's stream and copied on a stream of their own, so the copies overlap what the caller queues next
+ * (set_particles of the next step uploads and builds its tree meanwhile).  The host arrays hold the results
+ * once b200fmm_synchronize() has returned; page-locked arrays make the copies asynchronous.  Any array may be
+ * NULL.  A later call of this function waits on the device for the earlier copies before it stages again. */
+B200FMM_API b200fmm_status b200fmm_get_results_async(b200fmm_handle h, double *phi, double *fx, double *fy,
+                                                     double *fz);
+/* Makes the handle's stream wait (on the device, without blocking the host) for the result copies queued by
+ * b200fmm_get_results_async, so that work or events queued on that stream afterwards follow them. */
+B200FMM_API b200fmm_status b200fmm_join_results(b200fmm_handle h);
+/* Blocks until the handle's work and its result copies are done; reports a device-side failure. */
 B200FMM_API b200fmm_status b200fmm_synchronize(b200fmm_handle h);
 
 /* Tree inspection (host memory).  ncells: height entries.  get_cells returns the cells of one level in

@@ -29,7 +29,7 @@ EXPORTS = (
     "b200fmm_create", "b200fmm_destroy", "b200fmm_last_error", "b200fmm_version", "b200fmm_set_sym_operators",
     "b200fmm_get_sym_operators", "b200fmm_set_particles", "b200fmm_set_charges", "b200fmm_execute",
     "b200fmm_reset_expansions", "b200fmm_zero_results", "b200fmm_p2m", "b200fmm_m2m", "b200fmm_m2l", "b200fmm_l2l", "b200fmm_l2p",
-    "b200fmm_p2p", "b200fmm_get_results", "b200fmm_synchronize", "b200fmm_tree_info", "b200fmm_get_cells",
+    "b200fmm_p2p", "b200fmm_get_results", "b200fmm_get_results_async", "b200fmm_join_results", "b200fmm_synchronize", "b200fmm_tree_info", "b200fmm_get_cells",
     "b200fmm_get_permutation", "b200fmm_last_timings", "b200fmm_last_kernel_times", "b200fmm_tree_stats",
     "b200fmm_last_launch_count", "b200fmm_autotune", "b200fmm_p2p_noalloc", "b200fmm_batch_create", "b200fmm_batch_execute",
     "b200fmm_batch_last_time", "b200fmm_batch_last_device_time", "b200fmm_batch_destroy", "b200fmm_direct", "b200fmm_m2l_flops",
@@ -99,11 +99,12 @@ def lib():
         L.b200fmm_set_charges.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
         L.b200fmm_execute.argtypes = [ctypes.c_void_p, ctypes.c_uint]
         for n in ("b200fmm_reset_expansions", "b200fmm_zero_results", "b200fmm_p2m", "b200fmm_l2p",
-                  "b200fmm_synchronize"):
+                  "b200fmm_synchronize", "b200fmm_join_results"):
             getattr(L, n).argtypes = [ctypes.c_void_p]
         for n in ("b200fmm_m2m", "b200fmm_m2l", "b200fmm_l2l", "b200fmm_p2p"):
             getattr(L, n).argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.b200fmm_get_results.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 4 + [ctypes.c_int]
+        L.b200fmm_get_results_async.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 4
         L.b200fmm_tree_info.argtypes = [ctypes.c_void_p, _lp, _lp]
         L.b200fmm_get_cells.argtypes = [ctypes.c_void_p, ctypes.c_int, _lp, _dp, _dp]
         L.b200fmm_get_permutation.argtypes = [ctypes.c_void_p, _lp]
@@ -270,6 +271,18 @@ class FMM:
         """Write the results into four tensors (CUDA tensors, or pinned host tensors)."""
         _check(lib().b200fmm_get_results(self._h, *[ctypes.c_void_p(t.data_ptr()) for t in (phi, fx, fy, fz)],
                                          1 if phi.is_cuda else 0), "get_results")
+
+    def results_into_async(self, phi, fx, fy, fz):
+        """Queue the results' copy into four pinned host tensors without waiting; they hold the results once
+        synchronize() has returned."""
+        if any(t.is_cuda for t in (phi, fx, fy, fz)):
+            raise ValueError("results_into_async writes host tensors")
+        _check(lib().b200fmm_get_results_async(self._h, *[ctypes.c_void_p(t.data_ptr()) for t in (phi, fx, fy, fz)]),
+               "get_results_async")
+
+    def join_results(self):
+        """Make the handle's stream wait on the device for the queued result copies."""
+        _check(lib().b200fmm_join_results(self._h), "join_results")
 
     def tree_info(self):
         nc = np.zeros(self.height, np.int64)

@@ -146,6 +146,7 @@ b200fmm_status run_m2l(Context &c, int level) {
 void destroy_context(b200fmm_context *c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->stream_out) cudaStreamSynchronize(c->stream_out);
   drop_graph(*c);
   free_tree(*c);
   tc_free(*c);
@@ -154,7 +155,7 @@ void destroy_context(b200fmm_context *c) {
                   (void *)c->d_symU, (void *)c->d_symV, (void *)c->d_symoff, (void *)c->d_symrank,
                   (void *)c->d_dense, (void *)c->d_itab, (void *)c->d_class_order, (void *)c->d_cls_bounds,
                   (void *)c->d_cls_slots, (void *)c->d_status, (void *)c->d_mmax, (void *)c->d_Ut, (void *)c->d_Vt,
-                  (void *)c->d_toff, (void *)c->d_trank, c->d_scratch})
+                  (void *)c->d_toff, (void *)c->d_trank, c->d_scratch, (void *)c->d_out})
     if (p) cudaFree(p);
   if (c->events_ready)
     for (auto &e : c->ev) cudaEventDestroy(e);
@@ -162,6 +163,9 @@ void destroy_context(b200fmm_context *c) {
   if (c->stream2) cudaStreamDestroy(c->stream2);
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->stream_out) cudaStreamDestroy(c->stream_out);
+  if (c->ev_scat) cudaEventDestroy(c->ev_scat);
+  if (c->ev_out) cudaEventDestroy(c->ev_out);
   delete c;
 }
 
@@ -214,7 +218,10 @@ b200fmm_status b200fmm_create(const b200fmm_config *cfg, b200fmm_handle *out) {
   if (st == B200FMM_OK) {
     if (cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->stream_out, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_scat, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_out, cudaEventDisableTiming) != cudaSuccess)
       st = fail(B200FMM_ERR_CUDA, "stream creation failed");
   }
   if (st == B200FMM_OK) {
@@ -627,10 +634,50 @@ b200fmm_status b200fmm_get_results(b200fmm_handle h, double *phi, double *fx, do
   return check_status(c);
 }
 
+// Results to the host without waiting: staged in the caller's order on the handle's stream, then copied on a
+// stream of their own, so that the copies overlap whatever the caller queues next (the next tree's upload and
+// build, in a time-stepping loop).  The staging buffer is rewritten only after the previous copies have read it.
+b200fmm_status b200fmm_get_results_async(b200fmm_handle h, double *phi, double *fx, double *fy, double *fz) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  B200_CHECK(need_particles(c));
+  B200_CHECK(set_device(c));
+  const long long n = c.N;
+  const size_t bytes = sizeof(double) * n * c.R;
+  if (c.out_cap < 4 * bytes) {
+    B200_CUDA(cudaStreamSynchronize(c.stream_out));
+    if (c.d_out) cudaFree(c.d_out);
+    c.d_out = nullptr;
+    c.out_cap = 0;
+    B200_CUDA(cudaMalloc(&c.d_out, 4 * bytes));
+    c.out_cap = 4 * bytes;
+  }
+  double *o = c.d_out;
+  B200_CUDA(cudaStreamWaitEvent(c.stream, c.ev_out, 0));
+  scatter_to_original<<<grid_for(n, 256), 256, 0, c.stream>>>(n, c.R, c.d_perm, c.d_phi, c.d_fx, c.d_fy, c.d_fz, o,
+                                                              o + n * c.R, o + 2 * n * c.R, o + 3 * n * c.R);
+  B200_CUDA(cudaGetLastError());
+  B200_CUDA(cudaEventRecord(c.ev_scat, c.stream));
+  B200_CUDA(cudaStreamWaitEvent(c.stream_out, c.ev_scat, 0));
+  double *dst[4] = {phi, fx, fy, fz};
+  for (int k = 0; k < 4; ++k)
+    if (dst[k]) B200_CUDA(cudaMemcpyAsync(dst[k], o + k * n * c.R, bytes, cudaMemcpyDeviceToHost, c.stream_out));
+  B200_CUDA(cudaEventRecord(c.ev_out, c.stream_out));
+  return B200FMM_OK;
+}
+
+b200fmm_status b200fmm_join_results(b200fmm_handle h) {
+  B200_CHECK(check_handle(h));
+  B200_CHECK(set_device(*h));
+  B200_CUDA(cudaStreamWaitEvent(h->stream, h->ev_out, 0));
+  return B200FMM_OK;
+}
+
 b200fmm_status b200fmm_synchronize(b200fmm_handle h) {
   B200_CHECK(check_handle(h));
   B200_CHECK(set_device(*h));
   B200_CUDA(cudaStreamSynchronize(h->stream));
+  B200_CUDA(cudaStreamSynchronize(h->stream_out));
   return check_status(*h);
 }
 

@@ -77,6 +77,11 @@ struct Context {
   bool own_stream = false;
   cudaStream_t stream2 = nullptr;              // the near field, concurrent with the upward pass
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // asynchronous results: the caller-order results are staged in d_out and copied to the host on stream_out
+  cudaStream_t stream_out = nullptr;
+  cudaEvent_t ev_scat = nullptr, ev_out = nullptr;  // staged on the main stream / copies done on stream_out
+  double *d_out = nullptr;
+  size_t out_cap = 0;                          // bytes of d_out
   bool p2p_overlapped = false;                 // the last execute() ran P2P on stream2
   int device = 0;
 

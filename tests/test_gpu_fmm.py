@@ -259,6 +259,37 @@ def test_level_batched_mixed_on_compacted_levels(order):
         assert S.rel_l2(got[k], want[k]) < 2e-6, (k, S.rel_l2(got[k], want[k]))
 
 
+def test_async_results_overlap_the_next_tree():
+    """get_results_async queues each step's results on a copy stream of their own while the next step uploads
+    and builds its tree (trees of different sizes and shapes, one set of host buffers written twice); after
+    synchronize() every step's host arrays hold that step's results, as the blocking get_results gives them."""
+    import torch
+    from distributions import plummer
+
+    rng = np.random.default_rng(81)
+    trees = [tuple(rng.random((3, 30000))), plummer(25000, seed=82), tuple(rng.random((3, 40000))),
+             tuple(rng.random((3, 30000)))]
+    charges = [rng.uniform(-1.0, 1.0, t[0].size) for t in trees]
+    f = S.FMM("cheb_sym", 5, 5, precision="mixed")
+    shared = [torch.empty(30000, dtype=torch.float64).pin_memory() for _ in range(4)]
+    bufs = []
+    for i, ((x, y, z), q) in enumerate(zip(trees, charges)):
+        f.set_particles(x, y, z, q)
+        f.execute()
+        # steps 0 and 3 write the same host buffers: the later copy must land last
+        b = shared if i in (0, 3) else [torch.empty(x.size, dtype=torch.float64).pin_memory() for _ in range(4)]
+        f.results_into_async(*b)
+        bufs.append(b)
+    f.synchronize()
+    f.close()
+    for i, ((x, y, z), q, b) in enumerate(zip(trees, charges, bufs)):
+        if i == 0:
+            continue
+        want = _mixed_eval(x, y, z, q, 5, order=5)
+        for k, t in zip(FIELDS, b):
+            assert S.rel_l2(t.numpy(), want[k]) < 1e-12, (i, k)
+
+
 def test_edge_cases():
     # one particle: no interactions at all
     f = S.FMM("cheb_sym", 4, 3)
