@@ -353,12 +353,16 @@ def run_gpu(args):
         ev[3].record(stream)
         phases.append(ev)
 
-    def timed(fn, sampler_index=None):
+    def timed(fn, idle_start=False):
         ms = []
         kernel = []
         launches = 0
         for _ in range(args.steps):
             flush.fill_(1.0)
+            if idle_start:
+                # the library's host-input copies run on a stream of their own: none may begin before the start
+                # event, so the stream is idle when it is recorded
+                stream.synchronize()
             s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             s.record(stream)
             fn()
@@ -376,6 +380,7 @@ def run_gpu(args):
         # steps and the last step's copy are inside the region
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         launches = 0
+        stream.synchronize()
         s.record(stream)
         for _ in range(args.steps):
             flush.fill_(1.0)
@@ -402,7 +407,7 @@ def run_gpu(args):
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
-        ms_e2e, _, launches_e2e = timed(step_e2e_phased)
+        ms_e2e, _, launches_e2e = timed(step_e2e_phased, idle_start=True)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()

@@ -147,6 +147,7 @@ void destroy_context(b200fmm_context *c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->stream_out) cudaStreamSynchronize(c->stream_out);
+  if (c->stream_in) cudaStreamSynchronize(c->stream_in);
   drop_graph(*c);
   free_tree(*c);
   tc_free(*c);
@@ -166,6 +167,9 @@ void destroy_context(b200fmm_context *c) {
   if (c->stream_out) cudaStreamDestroy(c->stream_out);
   if (c->ev_scat) cudaEventDestroy(c->ev_scat);
   if (c->ev_out) cudaEventDestroy(c->ev_out);
+  if (c->stream_in) cudaStreamDestroy(c->stream_in);
+  for (cudaEvent_t e : {c->ev_in_xyz, c->ev_in_q, c->ev_stage_free})
+    if (e) cudaEventDestroy(e);
   delete c;
 }
 
@@ -221,7 +225,11 @@ b200fmm_status b200fmm_create(const b200fmm_config *cfg, b200fmm_handle *out) {
         cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->stream_out, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->ev_scat, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->ev_out, cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&c->ev_out, cudaEventDisableTiming) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->stream_in, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_in_xyz, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_in_q, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_stage_free, cudaEventDisableTiming) != cudaSuccess)
       st = fail(B200FMM_ERR_CUDA, "stream creation failed");
   }
   if (st == B200FMM_OK) {

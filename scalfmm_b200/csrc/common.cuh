@@ -80,6 +80,10 @@ struct Context {
   // asynchronous results: the caller-order results are staged in d_out and copied to the host on stream_out
   cudaStream_t stream_out = nullptr;
   cudaEvent_t ev_scat = nullptr, ev_out = nullptr;  // staged on the main stream / copies done on stream_out
+  // host inputs of set_particles: uploaded on stream_in, so that the upload overlaps work still queued on the
+  // main stream; ev_stage_free follows the last main-stream reader of the staging buffer
+  cudaStream_t stream_in = nullptr;
+  cudaEvent_t ev_in_xyz = nullptr, ev_in_q = nullptr, ev_stage_free = nullptr;
   double *d_out = nullptr;
   size_t out_cap = 0;                          // bytes of d_out
   bool p2p_overlapped = false;                 // the last execute() ran P2P on stream2

@@ -655,6 +655,7 @@ b200fmm_status upload_charges(Context &c, const double *q, bool on_device) {
   }
   gather_charges<<<grid_for(n, 256), 256, 0, c.stream>>>(n, c.R, c.d_perm, q, c.d_q);
   B200_CUDA(cudaGetLastError());
+  B200_CUDA(cudaEventRecord(c.ev_stage_free, c.stream));  // the staging buffer's last reader
   c.packed32 = false;
   return B200FMM_OK;
 }
@@ -725,26 +726,20 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
   if (!c.d_err) B200_CUDA(cudaMalloc(&c.d_err, 32 + sizeof(unsigned long long) * kMaxHeight));
   // inputs on the device
   const double *dx = x, *dy = y, *dz = z, *dq = q;
-  bool q_forked = false;  // the charge copy runs on the second stream
   if (!on_device) {
     B200_CHECK(grow(c, c.d_stage, c.cap_stage, (size_t)n * (3 + c.R)));
-    B200_CUDA(cudaMemcpyAsync(c.d_stage, x, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    B200_CUDA(cudaMemcpyAsync(c.d_stage + n, y, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    B200_CUDA(cudaMemcpyAsync(c.d_stage + 2 * n, z, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-    // the charges are first read by the gather after the sort.  From page-locked memory their copy runs on
-    // the second stream beside the keys and the sort (forked after the coordinates, joined before the
-    // gather); a pageable buffer is copied in order, since such a copy is staged by the host anyway.
-    cudaPointerAttributes qa{};
-    q_forked = cudaPointerGetAttributes(&qa, q) == cudaSuccess && qa.type == cudaMemoryTypeHost;
-    cudaGetLastError();
-    if (q_forked) {
-      B200_CUDA(cudaEventRecord(c.ev_fork, s));
-      B200_CUDA(cudaStreamWaitEvent(c.stream2, c.ev_fork, 0));
-      B200_CUDA(cudaMemcpyAsync(c.d_stage + 3 * n, q, sizeof(double) * n * c.R, cudaMemcpyHostToDevice, c.stream2));
-      B200_CUDA(cudaEventRecord(c.ev_join, c.stream2));
-    } else {
-      B200_CUDA(cudaMemcpyAsync(c.d_stage + 3 * n, q, sizeof(double) * n * c.R, cudaMemcpyHostToDevice, s));
-    }
+    // The inputs travel on a copy stream of their own: in a time-stepping loop this upload runs while the
+    // previous evaluation is still executing on the main stream.  The staging buffer is rewritten only after
+    // its last main-stream reader (the previous build's gather, or set_charges' gather) has run.  The keys wait
+    // for the coordinates; the charges, first read by the gather after the sort, arrive meanwhile.
+    B200_CUDA(cudaStreamWaitEvent(c.stream_in, c.ev_stage_free, 0));
+    B200_CUDA(cudaMemcpyAsync(c.d_stage, x, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream_in));
+    B200_CUDA(cudaMemcpyAsync(c.d_stage + n, y, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream_in));
+    B200_CUDA(cudaMemcpyAsync(c.d_stage + 2 * n, z, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream_in));
+    B200_CUDA(cudaEventRecord(c.ev_in_xyz, c.stream_in));
+    B200_CUDA(cudaMemcpyAsync(c.d_stage + 3 * n, q, sizeof(double) * n * c.R, cudaMemcpyHostToDevice, c.stream_in));
+    B200_CUDA(cudaEventRecord(c.ev_in_q, c.stream_in));
+    B200_CUDA(cudaStreamWaitEvent(s, c.ev_in_xyz, 0));
     dx = c.d_stage;
     dy = c.d_stage + n;
     dz = c.d_stage + 2 * n;
@@ -770,8 +765,9 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
     std::swap(k0, k1);
     std::swap(v0, v1);
   }
-  if (q_forked) B200_CUDA(cudaStreamWaitEvent(s, c.ev_join, 0));
+  if (!on_device) B200_CUDA(cudaStreamWaitEvent(s, c.ev_in_q, 0));
   gather_particles<<<grid_for(n, 256), 256, 0, s>>>(n, c.R, v0, dx, dy, dz, dq, c.d_x, c.d_y, c.d_z, c.d_q, c.d_perm);
+  B200_CUDA(cudaEventRecord(c.ev_stage_free, s));  // the last reader of the staging buffer
   // the cell count of every level at once (and the leaf heads), then the build's one synchronisation
   unsigned long long *counts = (unsigned long long *)(c.d_err + 4);
   B200_CUDA(cudaMemsetAsync(counts, 0, sizeof(unsigned long long) * kMaxHeight, s));
