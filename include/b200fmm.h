@@ -219,7 +219,7 @@ B200FMM_API b200fmm_status b200fmm_last_launch_count(b200fmm_handle h, long long
  * the result of that check back before the near field runs, and the status of the near field's bounded waits
  * before it returns.
  * The first call on a device looks up that array's device address (cudaGetSymbolAddress) with the device
- * current; make that first call before any stream capture.  All calls share the one array and its status
+ * current.  All calls share the one array and its status
  * words, and it keeps the last call's contents; calls whose executions overlap on the GPU race on it:
  * serialise them (one stream, or events). */
 #define B200FMM_NOALLOC_MAX_PARTICLES 262144LL
