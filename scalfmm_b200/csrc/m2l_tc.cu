@@ -85,6 +85,10 @@ struct TcLevel {
   const int *ccell;    // [blocks * 128]: cell index, or -1
   const __half *ghi, *glo;
   long long plane;     // positions of one parity grid: HX * HY * HZ
+  // low-rank form: ypr > 0 when Y of this level is stored by compacted row ([R * ycht][ypr][16], rows counted
+  // from each parity's first block); rowmap[parity * plane + position] gives a cell's row, -1 where none is
+  int ypr;
+  const int *rowmap;
 };
 
 // Occupied cells of parity grid `par` in the box [x0, x0+nx) x [y0, y0+ny) x [z0, z0+nz) (clipped).
@@ -915,6 +919,23 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
         if (rank_e++ < r0) continue;
         const TvRec tr = tvs[w.parity * 189 + e];
         const int nk = LR ? (int)tr.nk : P.NK;
+        // this lane's source rows under e: a grid position, or (Y stored by compacted row) the cell's row;
+        // -1 where the source lies outside the grid or holds no cell
+        int srow[4];
+        {
+          const int c = w.parity;
+          const int sp = ((((c >> 2) & 1) + P.off[c][e][0]) & 1) << 2 | ((((c >> 1) & 1) + P.off[c][e][1]) & 1) << 1 |
+                         (((c & 1) + P.off[c][e][2]) & 1);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int x = (int)(hc[i] & 1023u) + tr.ox, y = (int)((hc[i] >> 10) & 1023u) + tr.oy,
+                      z = (int)(hc[i] >> 20) + tr.oz;
+            const bool in = hc[i] != ~0u && x >= 0 && x < Lv.HX && y >= 0 && y < Lv.HY && z >= 0 && z < Lv.HZ;
+            const int pos = (z * Lv.HY + y) * Lv.HX + x;
+            srow[i] = in ? pos : -1;
+            if (LR && Lv.ypr > 0 && in) srow[i] = Lv.rowmap[(long long)sp * Lv.plane + pos];
+          }
+        }
         for (int kc = 0; kc < nk; ++kc) {
           // lane 0 waits for the stage to be free; the warp follows its outcome
           int ok = 1;
@@ -928,17 +949,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
           const unsigned bar = su32(&gbar[stage]);
           if (cmp) {
             const unsigned sa = su32(smem + (size_t)stage * P.stage_bytes);
-            // the grid rows of this K chunk: Y chunk tr.ya + kc of the source parity (low rank), or the source
-            // parity's multipoles at K offset kc * 32 (dense); row numbers fit 32 bits (checked on the host)
-            const int grow0 = (w.rhs * (LR ? P.ycht : 8) + tr.ya + (LR ? kc : 0)) * (int)Lv.plane;
+            // the rows of this K chunk: Y chunk tr.ya + kc of the source parity (low rank; by grid position or
+            // by compacted row), or the source parity's multipoles at K offset kc * 32 (dense); row numbers fit
+            // 32 bits (checked on the host)
+            const int rows_per = (LR && Lv.ypr > 0) ? Lv.ypr : (int)Lv.plane;
+            const int grow0 = (w.rhs * (LR ? P.ycht : 8) + tr.ya + (LR ? kc : 0)) * rows_per;
             const int kel = LR ? 0 : kc * KCHUNK;
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
               const int r = lane + 32 * i;
-              const int x = (int)(hc[i] & 1023u) + tr.ox, y = (int)((hc[i] >> 10) & 1023u) + tr.oy,
-                        z = (int)(hc[i] >> 20) + tr.oz;
-              const bool v = hc[i] != ~0u && x >= 0 && x < Lv.HX && y >= 0 && y < Lv.HY && z >= 0 && z < Lv.HZ;
-              const long long o = v ? (long long)(grow0 + (z * Lv.HY + y) * Lv.HX + x) * P.growlen + kel : 0;
+              const bool v = srow[i] >= 0;
+              const long long o = v ? (long long)(grow0 + srow[i]) * P.growlen + kel : 0;
               const unsigned nb = v ? 16u : 0u;
 #pragma unroll
               for (int j = 0; j < PPR; ++j) {
@@ -1136,6 +1157,9 @@ struct __align__(64) LrYParams {
   CUtensorMap mapC_hi[kMaxHeight], mapC_lo[kMaxHeight];  // compacted multipoles [rows][KP]: 2-D boxes of 32 K x 128 rows
   const int *crow[kMaxHeight];                           // [rows]: (parity << 28) | (hz * HY + hy) * HX + hx, or -1
   int cblk0[kMaxHeight][9];                              // first 128-row block of each parity; [8] = blocks
+  // ypr > 0: this compacted level's Y is stored by compacted row, [R * ycht][ypr][16] with the row counted
+  // from its parity's first block, instead of by grid position (the second product gathers it by row)
+  int ypr[kMaxHeight];
 };
 
 constexpr int YBLK = 256;  // rank rows per item (16 chunks of 16)
@@ -1457,13 +1481,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) lr_y_kernel(const __grid_consta
       if (abort_sh) break;
       // write the 8 chunks of 16 ranks this thread holds, as FP16 hi and lo
       const int l = y.level;
-      const long long plane = (long long)P.HZ[l] * P.HY[l] * P.HX[l];
+      long long plane = (long long)P.HZ[l] * P.HY[l] * P.HX[l];
       long long pos = 0;  // the row's cell in the parity grid: (hz * HY + hy) * HX + hx
       bool real = true;   // false for a padding row of a compacted parity's last block (lanes stay together)
       if (y.blk >= 0) {
         const int code = P.crow[l][y.blk * 128 + row];
         real = code >= 0;
-        pos = real ? (code & 0x0FFFFFFF) : 0;
+        if (P.ypr[l] > 0) {
+          // stored by compacted row: rows of this parity from its first block on
+          plane = P.ypr[l];
+          pos = (long long)(y.blk - P.cblk0[l][y.par]) * 128 + row;
+        } else {
+          pos = real ? (code & 0x0FFFFFFF) : 0;
+        }
       } else {
         if (y.bz >= P.HZ[l] / TILE_Z) continue;  // the missing second tile of a pair at the z edge
         const int hx = y.bx * TILE_X + (row & 7), hy = y.by * TILE_Y + ((row >> 3) & 3), hz = y.bz * TILE_Z + (row >> 5);
@@ -1753,10 +1783,12 @@ struct CPlace {
   int blk0[9];  // first 128-row block of each parity (placement), or first Y chunk of each parity (cclear)
   int HX, HY;
 };
+// rowmap (optional): [parity][position] -> the cell's row counted from its parity's first block
 __global__ void __launch_bounds__(1024) cgroup_place_kernel(const long long *__restrict__ keys, long long n,
                                                             const __grid_constant__ CPlace C,
                                                             const int *__restrict__ goff, int *__restrict__ crow,
-                                                            int *__restrict__ ccell) {
+                                                            int *__restrict__ ccell, int *__restrict__ rowmap,
+                                                            long long plane) {
   __shared__ int wcnt[32][8];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long i = blockIdx.x * 1024LL + threadIdx.x;
@@ -1771,9 +1803,12 @@ __global__ void __launch_bounds__(1024) cgroup_place_kernel(const long long *__r
   if (par < 0) return;
   int before = 0;
   for (int w = 0; w < warp; ++w) before += wcnt[w][par];
-  const int row = C.blk0[par] * 128 + goff[blockIdx.x * 8 + par] + before + rk;
-  crow[row] = (par << 28) | (((iz >> 1) * C.HY + (iy >> 1)) * C.HX + (ix >> 1));
+  const int prow = goff[blockIdx.x * 8 + par] + before + rk;
+  const int row = C.blk0[par] * 128 + prow;
+  const int pos = ((iz >> 1) * C.HY + (iy >> 1)) * C.HX + (ix >> 1);
+  crow[row] = (par << 28) | pos;
   ccell[row] = (int)i;
+  if (rowmap) rowmap[par * plane + pos] = prow;
 }
 // Busy masks of the compacted blocks of every compacted level (one CTA of 128 threads per block, blocks
 // numbered across levels from b0): bit e set when the source of some row under transfer vector e is a cell,
@@ -1941,7 +1976,9 @@ struct DenseTC {
   int lr_rank[343] = {};                  // rank of each far slot
   // first product on compacted levels (sparse levels of a tree): per level
   int titem0[kMaxHeight] = {}, tnitems[kMaxHeight] = {};  // tile-mode item numbering (the ydirty flags)
-  int ymode[kMaxHeight] = {};             // what Y holds besides zeros: 0 nothing, 1 tile-mode rows, 2 compacted rows
+  // what Y holds besides zeros: 0 nothing, 1 tile-mode rows, 2 compacted first product by grid position,
+  // 3 by compacted row
+  int ymode[kMaxHeight] = {};
   int *crow[kMaxHeight] = {};             // [rows]: (parity << 28) | position in the parity grid, or -1
   int *ccell[kMaxHeight] = {};            // [rows]: cell index, or -1
   __half *Chi[kMaxHeight] = {}, *Clo[kMaxHeight] = {};  // compacted multipoles [rows][KP]
@@ -1953,6 +1990,7 @@ struct DenseTC {
   long long cgrp_cap = 0;
   // second product on compacted levels: the tile-mode unit count of each level, the blocks' busy masks
   int tunits[kMaxHeight] = {};
+  int *rowmap[kMaxHeight] = {};           // [8][plane] cell rows of levels whose Y is stored by compacted row
   unsigned *cbusy = nullptr;
   long long cbusy_cap = 0;
   int prefix_cap = 0;                     // entries allocated in prefix
@@ -2348,7 +2386,7 @@ void tc_free(Context &c) {
     if (t->Alo[l]) cudaFree(t->Alo[l]);
     if (t->Yhi[l]) cudaFree(t->Yhi[l]);
     if (t->Ylo[l]) cudaFree(t->Ylo[l]);
-    for (void *q : {(void *)t->crow[l], (void *)t->ccell[l], (void *)t->Chi[l], (void *)t->Clo[l]})
+    for (void *q : {(void *)t->crow[l], (void *)t->ccell[l], (void *)t->Chi[l], (void *)t->Clo[l], (void *)t->rowmap[l]})
       if (q) cudaFree(q);
   }
   for (void *q : {(void *)t->ccnt, (void *)t->cgrp, (void *)t->cbusy})
@@ -2551,25 +2589,6 @@ static b200fmm_status compact_setup(Context &c, DenseTC &t) {
     if (tallow && sparse && grid_rows < (1LL << 31)) tmask |= 1u << l;
   }
   const unsigned mask = ymask | tmask;
-  if (t.lr) {
-    LrYParams &Y = *t.yparams;
-    CPlace chunks{};
-    for (int p = 0; p <= 8; ++p) chunks.blk0[p] = p < 8 ? t.ybase[p] : t.ycht;
-    for (int l = 2; l <= LL; ++l) {
-      const long long plane = (long long)t.HX[l] * t.HY[l] * t.HZ[l];
-      if (t.ymode[l] == 2 && t.crows[l] > 0) {
-        cclear_kernel<<<(unsigned)t.crows[l], 64, 0, c.stream>>>(t.crow[l], plane, chunks, t.Yhi[l], t.Ylo[l]);
-        ++c.launches;
-      }
-      if (((ymask >> l) & 1u) && t.ymode[l] == 1) {
-        B200_CUDA(cudaMemsetAsync(t.Yhi[l], 0, t.Ybytes[l], c.stream));
-        B200_CUDA(cudaMemsetAsync(t.Ylo[l], 0, t.Ybytes[l], c.stream));
-        B200_CUDA(cudaMemsetAsync(t.ydirty + 16 * (size_t)t.titem0[l], 0, 16 * (size_t)t.tnitems[l], c.stream));
-      }
-    }
-    (void)Y;
-  }
-  for (int l = 2; l <= LL; ++l) t.crows[l] = 0;
   // per-parity counts of every placed level, in groups of 1024 cells
   int cnt[kMaxHeight][8] = {};
   long long g0[kMaxHeight + 1] = {};
@@ -2595,24 +2614,65 @@ static b200fmm_status compact_setup(Context &c, DenseTC &t) {
     B200_CUDA(cudaMemcpyAsync(cnt, t.ccnt, sizeof(cnt), cudaMemcpyDeviceToHost, c.stream));
     B200_CUDA(cudaStreamSynchronize(c.stream));
   }
-  // blocks of every placed level (an even count per parity for CTA pairs), their rows and cells
+  // blocks of every placed level (an even count per parity for CTA pairs).  A level compacted in both products
+  // (low rank) stores its Y by compacted row when the largest parity's rows fit the grid layout's rows.
+  CPlace Cl[kMaxHeight] = {};
+  int ypr[kMaxHeight] = {};
+  for (int l = 2; l <= LL; ++l) {
+    if (!((mask >> l) & 1u)) continue;
+    CPlace &C = Cl[l];
+    C.blk0[0] = 0;
+    int most = 0;
+    for (int p = 0; p < 8; ++p) {
+      int nb = (cnt[l][p] + 127) / 128;
+      if (t.pair && ((tmask >> l) & 1u)) nb += nb & 1;
+      C.blk0[p + 1] = C.blk0[p] + nb;
+      most = std::max(most, nb);
+    }
+    C.HX = t.HX[l];
+    C.HY = t.HY[l];
+    const long long plane = (long long)t.HX[l] * t.HY[l] * t.HZ[l];
+    if (t.lr && ((ymask & tmask) >> l & 1u) && 128LL * most <= plane) ypr[l] = 128 * most;
+  }
+  // Low rank: Y must read as zero wherever the second product may read a row that holds no cell of this tree.
+  // Modes of a level's Y: 1 tile-mode rows (kept clear by the tile flags), 2 compacted first product by grid
+  // position, 3 by compacted row (the gathers read only rows of cells, so leftovers elsewhere are never read).
+  // Leaving mode 2 for 1 or 2 clears the earlier tree's rows; leaving mode 3 for 1 or 2, or turning from 1 to 2,
+  // clears Y and the tile flags.
+  if (t.lr) {
+    CPlace chunks{};
+    for (int p = 0; p <= 8; ++p) chunks.blk0[p] = p < 8 ? t.ybase[p] : t.ycht;
+    for (int l = 2; l <= LL; ++l) {
+      const long long plane = (long long)t.HX[l] * t.HY[l] * t.HZ[l];
+      const int next = !((ymask >> l) & 1u) ? 1 : (ypr[l] > 0 ? 3 : 2);
+      const int prev = t.ymode[l];
+      if (prev == 2 && next != 3 && t.crows[l] > 0) {
+        cclear_kernel<<<(unsigned)t.crows[l], 64, 0, c.stream>>>(t.crow[l], plane, chunks, t.Yhi[l], t.Ylo[l]);
+        ++c.launches;
+      }
+      if ((prev == 3 && next != 3) || (prev == 1 && next == 2)) {
+        B200_CUDA(cudaMemsetAsync(t.Yhi[l], 0, t.Ybytes[l], c.stream));
+        B200_CUDA(cudaMemsetAsync(t.Ylo[l], 0, t.Ybytes[l], c.stream));
+        B200_CUDA(cudaMemsetAsync(t.ydirty + 16 * (size_t)t.titem0[l], 0, 16 * (size_t)t.tnitems[l], c.stream));
+      }
+      t.ymode[l] = next;
+    }
+  }
+  for (int l = 2; l <= LL; ++l) t.crows[l] = 0;
+  // rows and cells of every placed level
   CBlocks B{};
   B.l0 = 2;
   B.l1 = LL;
   int nblocks[kMaxHeight] = {};
   for (int l = 2; l <= LL; ++l) {
     P.lv[l].cmode = 0;
+    P.lv[l].ypr = 0;
+    P.lv[l].rowmap = nullptr;
+    if (t.lr) t.yparams->ypr[l] = 0;
     B.b0[l + 1] = B.b0[l];
     if (!((mask >> l) & 1u)) continue;
-    CPlace C{};
-    C.blk0[0] = 0;
-    for (int p = 0; p < 8; ++p) {
-      int nb = (cnt[l][p] + 127) / 128;
-      if (t.pair && ((tmask >> l) & 1u)) nb += nb & 1;
-      C.blk0[p + 1] = C.blk0[p] + nb;
-    }
-    C.HX = t.HX[l];
-    C.HY = t.HY[l];
+    const CPlace &C = Cl[l];
+    const long long plane = (long long)t.HX[l] * t.HY[l] * t.HZ[l];
     nblocks[l] = C.blk0[8];
     const long long rows = 128LL * C.blk0[8];
     if (t.ccap[l] < rows) {
@@ -2626,9 +2686,15 @@ static b200fmm_status compact_setup(Context &c, DenseTC &t) {
     }
     B200_CUDA(cudaMemsetAsync(t.crow[l], 0xFF, sizeof(int) * rows, c.stream));
     B200_CUDA(cudaMemsetAsync(t.ccell[l], 0xFF, sizeof(int) * rows, c.stream));
+    int *rmap = nullptr;
+    if (ypr[l] > 0) {
+      if (!t.rowmap[l]) B200_CUDA(cudaMalloc(&t.rowmap[l], sizeof(int) * 8 * plane));
+      rmap = t.rowmap[l];
+      B200_CUDA(cudaMemsetAsync(rmap, 0xFF, sizeof(int) * 8 * plane, c.stream));
+    }
     const int ngl = (int)(g0[l + 1] - g0[l]);
     cgroup_place_kernel<<<ngl, 1024, 0, c.stream>>>(c.lv[l].keys, c.lv[l].n, C, t.cgrp + 8 * g0[l], t.crow[l],
-                                                    t.ccell[l]);
+                                                    t.ccell[l], rmap, plane);
     ++c.launches;
     t.crows[l] = (int)rows;
     P.lv[l].crow = t.crow[l];
@@ -2638,6 +2704,8 @@ static b200fmm_status compact_setup(Context &c, DenseTC &t) {
       P.lv[l].cmode = 1;
       P.lv[l].cb0 = B.b0[l];
       B.b0[l + 1] = B.b0[l] + C.blk0[8];
+      P.lv[l].ypr = ypr[l];
+      P.lv[l].rowmap = rmap;
     }
     if (t.lr && ((ymask >> l) & 1u)) {
       LrYParams &Y = *t.yparams;
@@ -2657,6 +2725,7 @@ static b200fmm_status compact_setup(Context &c, DenseTC &t) {
       B200_CHECK(encode(&Y.mapC_lo[l], t.Clo[l], 2, dims, strides, box));
       Y.crow[l] = t.crow[l];
       for (int p = 0; p <= 8; ++p) Y.cblk0[l][p] = C.blk0[p];
+      Y.ypr[l] = ypr[l];
     }
   }
   // first-product items (low rank), finest level first
@@ -2665,13 +2734,7 @@ static b200fmm_status compact_setup(Context &c, DenseTC &t) {
     int n = 0;
     for (int l = LL; l >= 2; --l) {
       Y.item0[l] = n;
-      if ((ymask >> l) & 1u) {
-        Y.nitems[l] = nblocks[l] * t.nblk;
-        t.ymode[l] = 2;
-      } else {
-        Y.nitems[l] = t.tnitems[l];
-        t.ymode[l] = 1;
-      }
+      Y.nitems[l] = ((ymask >> l) & 1u) ? nblocks[l] * t.nblk : t.tnitems[l];
       n += Y.nitems[l];
     }
     Y.compact_levels = ymask;
