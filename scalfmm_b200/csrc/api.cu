@@ -393,6 +393,9 @@ static b200fmm_status execute_body(Context &c, unsigned ops) {
     c.stream = main;
     B200_CHECK(st);
   }
+  // the tensor-core M2L's per-tree tables (one host synchronisation on compacted levels) while the near field
+  // runs on the second stream
+  if (c.cfg.precision == B200FMM_MIXED && (ops & B200FMM_M2L)) B200_CHECK(tc_tree_setup(c));
   if (ops & B200FMM_P2M) B200_CHECK(run_p2m(c));
   B200_CHECK(record(c, 2));
   if (ops & B200FMM_M2M)

@@ -236,6 +236,7 @@ bool sym64_fed_ranks(const Context &c, double *fed);
 b200fmm_status tc_init(Context &c);
 void tc_free(Context &c);
 b200fmm_status run_m2l_tc(Context &c, int level);
+b200fmm_status tc_tree_setup(Context &c);
 void tc_set_splits(Context &c, int splits);
 int tc_splits_used(const Context &c);
 // direct.cu

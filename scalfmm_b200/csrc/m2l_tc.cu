@@ -2771,11 +2771,12 @@ static b200fmm_status compact_setup(Context &c, DenseTC &t) {
   return B200FMM_OK;
 }
 
-b200fmm_status run_m2l_tc(Context &c, int level) {
+// The per-tree tables of the tensor-core M2L: occupancy, busy masks, compacted levels and the work units with
+// their prefix sums.  They depend on the tree only; execute() builds them beside the near field, before P2M.
+b200fmm_status tc_tree_setup(Context &c) {
   DenseTC *t = c.tc;
   if (!t) return fail(B200FMM_ERR_STATE, "tensor-core M2L not initialised");
   const int LL = c.H - 1;
-  if (level != -1 && (level < 2 || level > LL)) return fail(B200FMM_ERR_INVALID, "m2l: level out of range");
   if (t->built_for_gen != c.tree_gen) B200_CHECK(tc_prepare(c));
   if (t->sat_serial != c.tree_serial) {
     // which cells of each level are occupied: lets the kernel skip empty target tiles and source boxes
@@ -2826,6 +2827,15 @@ b200fmm_status run_m2l_tc(Context &c, int level) {
     c.launches += 2;
     t->sat_serial = c.tree_serial;
   }
+  return B200FMM_OK;
+}
+
+b200fmm_status run_m2l_tc(Context &c, int level) {
+  DenseTC *t = c.tc;
+  if (!t) return fail(B200FMM_ERR_STATE, "tensor-core M2L not initialised");
+  const int LL = c.H - 1;
+  if (level != -1 && (level < 2 || level > LL)) return fail(B200FMM_ERR_INVALID, "m2l: level out of range");
+  B200_CHECK(tc_tree_setup(c));
   const int l0 = level == -1 ? 2 : level, l1 = level == -1 ? LL : level;
   {
     // the multipoles of all levels of the launch: their maxima, the level scales, then the packed FP16 hi / lo
