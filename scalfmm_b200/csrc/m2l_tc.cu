@@ -2563,7 +2563,7 @@ static b200fmm_status tc_prepare(Context &c) {
 }
 
 // Per tree: which sparse levels run compacted, and their cells grouped by parity into 128-row blocks.
-//   * A level is sparse when fewer than half of its cells exist; compaction needs one right-hand side.
+//   * A level is sparse when fewer than three quarters of its cells exist; compaction needs one right-hand side.
 //   * The second product (U Y, or K M in the dense form) runs a compacted level's units over blocks (pairs of
 //     blocks of one parity on CTA pairs) instead of grid tiles: the unit numbering of every level is redone
 //     here, and the blocks get their busy masks.  B200FMM_TC_TCOMPACT=0 keeps the tiles.
@@ -2579,10 +2579,17 @@ static b200fmm_status compact_setup(Context &c, DenseTC &t) {
   const char *ye = getenv("B200FMM_TC_YCOMPACT"), *te = getenv("B200FMM_TC_TCOMPACT");
   const bool yallow = t.lr && !t.ypair && c.R == 1 && !(ye && atoi(ye) == 0);
   const bool tallow = c.R == 1 && !(te && atoi(te) == 0);
+  // a level runs compacted below this share of occupied cells (B200FMM_TC_COMPACT_BELOW in (0, 1]); on the
+  // Plummer problems of height 7, 0.75 was 2-10 % faster per evaluation than 0.5 and 0.25 clearly slower
+  double below = 0.75;
+  if (const char *e = getenv("B200FMM_TC_COMPACT_BELOW")) {
+    const double v = atof(e);
+    if (v > 0.0 && v <= 1.0) below = v;
+  }
   unsigned ymask = 0, tmask = 0;
   for (int l = 2; l <= LL; ++l) {
     const long long plane = (long long)t.HX[l] * t.HY[l] * t.HZ[l];
-    const bool sparse = c.lv[l].n > 0 && 2 * c.lv[l].n < (1LL << (3 * l)) && plane < (1LL << 28);
+    const bool sparse = c.lv[l].n > 0 && (double)c.lv[l].n < below * (double)(1LL << (3 * l)) && plane < (1LL << 28);
     // the gathers number the rows of a level's source grid in 32 bits
     const long long grid_rows = (long long)c.R * (t.lr ? t.ycht : 8) * plane;
     if (yallow && sparse) ymask |= 1u << l;
