@@ -161,6 +161,15 @@ B200FMM_API b200fmm_status b200fmm_get_results_async(b200fmm_handle h, double *p
 /* Makes the handle's stream wait (on the device, without blocking the host) for the result copies queued by
  * b200fmm_get_results_async, so that work or events queued on that stream afterwards follow them. */
 B200FMM_API b200fmm_status b200fmm_join_results(b200fmm_handle h);
+/* Target shard (the reference's MPI algorithm gives each process a Morton interval of cells per level,
+ * FFmmAlgorithmThreadProc.hpp:84-128, and exchanges the cells its neighbours need).  With count > 1, execute() evaluates only the particles of
+ * shard `rank`: the leaves of a Morton range holding about N / count of the sorted particles (whole leaves).
+ * Every other particle's results stay zero, so the sum over rank = 0 .. count-1 of the results is the whole
+ * evaluation: count processes or GPUs holding the same particles each run one shard and add their results
+ * (an all-reduce).  The near field, L2P and the M2L of the shard's cells and their ancestors are divided; the
+ * tree, P2M, M2M and the low-rank M2L's first product are computed whole by every shard.  count = 1 (the
+ * default) evaluates every particle.  Applies to execute() from the next call on, for every later tree. */
+B200FMM_API b200fmm_status b200fmm_set_shard(b200fmm_handle h, int rank, int count);
 /* Blocks until the handle's work and its result copies are done; reports a device-side failure. */
 B200FMM_API b200fmm_status b200fmm_synchronize(b200fmm_handle h);
 

@@ -29,7 +29,7 @@ EXPORTS = (
     "b200fmm_create", "b200fmm_destroy", "b200fmm_last_error", "b200fmm_version", "b200fmm_set_sym_operators",
     "b200fmm_get_sym_operators", "b200fmm_set_particles", "b200fmm_set_charges", "b200fmm_execute",
     "b200fmm_reset_expansions", "b200fmm_zero_results", "b200fmm_p2m", "b200fmm_m2m", "b200fmm_m2l", "b200fmm_l2l", "b200fmm_l2p",
-    "b200fmm_p2p", "b200fmm_get_results", "b200fmm_get_results_async", "b200fmm_join_results", "b200fmm_synchronize", "b200fmm_tree_info", "b200fmm_get_cells",
+    "b200fmm_p2p", "b200fmm_get_results", "b200fmm_get_results_async", "b200fmm_join_results", "b200fmm_synchronize", "b200fmm_set_shard", "b200fmm_tree_info", "b200fmm_get_cells",
     "b200fmm_get_permutation", "b200fmm_last_timings", "b200fmm_last_kernel_times", "b200fmm_tree_stats",
     "b200fmm_last_launch_count", "b200fmm_autotune", "b200fmm_p2p_noalloc", "b200fmm_batch_create", "b200fmm_batch_execute",
     "b200fmm_batch_last_time", "b200fmm_batch_last_device_time", "b200fmm_batch_destroy", "b200fmm_direct", "b200fmm_m2l_flops",
@@ -105,6 +105,7 @@ def lib():
             getattr(L, n).argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.b200fmm_get_results.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 4 + [ctypes.c_int]
         L.b200fmm_get_results_async.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 4
+        L.b200fmm_set_shard.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.b200fmm_tree_info.argtypes = [ctypes.c_void_p, _lp, _lp]
         L.b200fmm_get_cells.argtypes = [ctypes.c_void_p, ctypes.c_int, _lp, _dp, _dp]
         L.b200fmm_get_permutation.argtypes = [ctypes.c_void_p, _lp]
@@ -280,6 +281,12 @@ class FMM:
         _check(lib().b200fmm_get_results_async(self._h, *[ctypes.c_void_p(t.data_ptr()) for t in (phi, fx, fy, fz)]),
                "get_results_async")
 
+    def set_shard(self, rank, count):
+        """Evaluate only shard `rank` of `count` (a Morton range of leaves with about N / count particles) from
+        the next execute() on; the other particles' results stay zero, so the shards' results add up to the
+        whole evaluation.  count = 1 evaluates every particle."""
+        _check(lib().b200fmm_set_shard(self._h, int(rank), int(count)), "set_shard")
+
     def join_results(self):
         """Make the handle's stream wait on the device for the queued result copies."""
         _check(lib().b200fmm_join_results(self._h), "join_results")
@@ -439,6 +446,38 @@ def write_fma(path, data, box_width=1.0, center=(0.5, 0.5, 0.5)):
     c = _f64(center)
     _check(lib().b200fmm_fma_write(str(path).encode(), data.shape[0], data.shape[1], box_width, _ptr(c), _ptr(data)),
            "fma_write")
+
+
+def shard_indices(x, y, z, height, rank, count, box_width=1.0, center=(0.5, 0.5, 0.5)):
+    """Original indices of the particles that shard `rank` of `count` evaluates (FMM.set_shard): the particles
+    sorted by leaf Morton key (stable), cut at the first leaf boundary at or after N * r / count for r = rank and
+    rank + 1.  Host-side, the same rule as the library's device code, so that a caller knows which results a
+    shard produces."""
+    x, y, z = (np.asarray(a, dtype=np.float64) for a in (x, y, z))
+    n = x.size
+    side = 1 << (height - 1)
+    leaf_w = box_width / side
+    cells = []
+    for a, c in ((x, center[0]), (y, center[1]), (z, center[2])):
+        r = a - (c - box_width / 2)
+        cells.append(np.minimum((r / leaf_w).astype(np.int64), side - 1))
+    key = np.zeros(n, np.int64)
+    for b in range(height - 1):  # z in the lowest bit of each triple, then y, then x
+        key |= ((cells[2] >> b) & 1) << (3 * b)
+        key |= ((cells[1] >> b) & 1) << (3 * b + 1)
+        key |= ((cells[0] >> b) & 1) << (3 * b + 2)
+    order = np.argsort(key, kind="stable")
+    sk = key[order]
+    starts = np.concatenate(([0], np.flatnonzero(sk[1:] != sk[:-1]) + 1, [n]))
+
+    def boundary(r):
+        if r <= 0:
+            return 0
+        if r >= count:
+            return n
+        return int(starts[np.searchsorted(starts, n * r // count, side="left")])
+
+    return order[boundary(rank):boundary(rank + 1)]
 
 
 def rel_l2(a, b):

@@ -156,7 +156,7 @@ void destroy_context(b200fmm_context *c) {
                   (void *)c->d_symU, (void *)c->d_symV, (void *)c->d_symoff, (void *)c->d_symrank,
                   (void *)c->d_dense, (void *)c->d_itab, (void *)c->d_class_order, (void *)c->d_cls_bounds,
                   (void *)c->d_cls_slots, (void *)c->d_status, (void *)c->d_mmax, (void *)c->d_Ut, (void *)c->d_Vt,
-                  (void *)c->d_toff, (void *)c->d_trank, c->d_scratch, (void *)c->d_out})
+                  (void *)c->d_toff, (void *)c->d_trank, c->d_scratch, (void *)c->d_out, (void *)c->d_shard})
     if (p) cudaFree(p);
   if (c->events_ready)
     for (auto &e : c->ev) cudaEventDestroy(e);
@@ -241,6 +241,7 @@ b200fmm_status b200fmm_create(const b200fmm_config *cfg, b200fmm_handle *out) {
   if (st == B200FMM_OK) {
     if (cudaMalloc(&c->d_status, 16 * sizeof(int)) != cudaSuccess ||
         cudaMemset(c->d_status, 0, 16 * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&c->d_shard, sizeof(long long) * (2 + 2 * kMaxHeight)) != cudaSuccess ||
         cudaMalloc(&c->d_mmax, sizeof(unsigned long long) * kMaxHeight * kMmaxSlots) != cudaSuccess)
       st = fail(B200FMM_ERR_OOM, "status allocation failed");
   }
@@ -360,6 +361,12 @@ b200fmm_status b200fmm_zero_results(b200fmm_handle h) {
 
 // The passes of execute(), in the reference's order (FFmmAlgorithmThread::executeCore).
 static b200fmm_status execute_body(Context &c, unsigned ops) {
+  // per-tree tables (the shard's ranges, the tensor-core M2L's tables, which take a host synchronisation) are
+  // built by an eager evaluation, never inside a capture: a capture that finds them pending gives up before it
+  // changes any state, and the caller's evaluation runs eagerly
+  if (c.capturing && ((c.shard_count > 1 && c.shard_serial != c.tree_serial) ||
+                      (c.cfg.precision == B200FMM_MIXED && (ops & B200FMM_M2L) && tc_tables_pending(c))))
+    return fail(B200FMM_ERR_STATE, "per-tree tables pending: the evaluation is not captured");
   c.launches = 0;
   const int LL = c.H - 1;
   B200_CHECK(record(c, 0));
@@ -376,6 +383,12 @@ static b200fmm_status execute_body(Context &c, unsigned ops) {
     c.mmax_out = c.d_mmax;
   }
   B200_CHECK(record(c, 1));
+  // a target shard: the leaf and cell ranges of this tree, read by the near field, L2P and the M2L's units
+  const long long *shard = nullptr;
+  if (c.shard_count > 1) {
+    if (c.shard_serial != c.tree_serial) B200_CHECK(shard_ranges(c));
+    shard = c.d_shard;
+  }
   // The near field needs only the tree: it runs on the second stream beside P2M and M2M and joins before the
   // M2L (a persistent kernel that wants every SM) and before L2P adds into the same results.
   const bool overlap = (ops & B200FMM_P2P) && (ops & (B200FMM_P2M | B200FMM_M2M));
@@ -386,7 +399,7 @@ static b200fmm_status execute_body(Context &c, unsigned ops) {
     cudaStream_t main = c.stream;
     c.stream = c.stream2;
     b200fmm_status st = record(c, 12);
-    if (st == B200FMM_OK) st = run_p2p(c, 0);
+    if (st == B200FMM_OK) st = run_p2p(c, 0, shard);
     if (st == B200FMM_OK) st = record(c, 13);
     if (st == B200FMM_OK && cudaEventRecord(c.ev_join, c.stream2) != cudaSuccess)
       st = fail(B200FMM_ERR_CUDA, "event record failed");
@@ -419,9 +432,9 @@ static b200fmm_status execute_body(Context &c, unsigned ops) {
   if (ops & B200FMM_L2L)
     for (int l = 2; l <= LL - 1; ++l) B200_CHECK(run_l2l(c, l));
   B200_CHECK(record(c, 5));
-  if (ops & B200FMM_L2P) B200_CHECK(run_l2p(c));
+  if (ops & B200FMM_L2P) B200_CHECK(run_l2p(c, shard));
   B200_CHECK(record(c, 6));
-  if ((ops & B200FMM_P2P) && !overlap) B200_CHECK(run_p2p(c, 0));
+  if ((ops & B200FMM_P2P) && !overlap) B200_CHECK(run_p2p(c, 0, shard));
   B200_CHECK(record(c, 7));
   return B200FMM_OK;
 }
@@ -681,6 +694,21 @@ b200fmm_status b200fmm_join_results(b200fmm_handle h) {
   B200_CHECK(check_handle(h));
   B200_CHECK(set_device(*h));
   B200_CUDA(cudaStreamWaitEvent(h->stream, h->ev_out, 0));
+  return B200FMM_OK;
+}
+
+b200fmm_status b200fmm_set_shard(b200fmm_handle h, int rank, int count) {
+  B200_CHECK(check_handle(h));
+  Context &c = *h;
+  if (count < 1 || rank < 0 || rank >= count) return fail(B200FMM_ERR_INVALID, "set_shard: need 0 <= rank < count");
+  B200_CHECK(set_device(c));
+  if (rank == c.shard_rank && count == c.shard_count) return B200FMM_OK;
+  c.shard_rank = count > 1 ? rank : 0;
+  c.shard_count = count;
+  c.shard_serial = -1;
+  drop_graph(c);         // a captured evaluation holds the earlier ranges
+  c.eager_serial = -1;   // the next evaluation runs eagerly and rebuilds the per-tree tables
+  tc_invalidate_units(c);  // the M2L's units are weighted by the shard
   return B200FMM_OK;
 }
 

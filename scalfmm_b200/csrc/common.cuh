@@ -87,6 +87,11 @@ struct Context {
   double *d_out = nullptr;
   size_t out_cap = 0;                          // bytes of d_out
   bool p2p_overlapped = false;                 // the last execute() ran P2P on stream2
+  // target shard of execute(): the particles of a Morton range of leaves holding about N / shard_count of them
+  // (shard_rank of shard_count); shard_count 1 evaluates every particle
+  int shard_rank = 0, shard_count = 1;
+  long long *d_shard = nullptr;                // [2 + 2 * kMaxHeight]: leaf range, then each level's cell range
+  long long shard_serial = -1;                 // tree d_shard was computed for
   int device = 0;
 
   // interpolation tables (device)
@@ -217,9 +222,10 @@ b200fmm_status upload_basis_constants(const Context &c, const double *roots, con
 b200fmm_status run_p2m(Context &c);
 b200fmm_status run_m2m(Context &c, int level);
 b200fmm_status run_l2l(Context &c, int level);
-b200fmm_status run_l2p(Context &c);
+// shard: [first leaf, end leaf) in device memory, or null for every leaf
+b200fmm_status run_l2p(Context &c, const long long *shard = nullptr);
 // p2p.cu
-b200fmm_status run_p2p(Context &c, int variant);
+b200fmm_status run_p2p(Context &c, int variant, const long long *shard = nullptr);
 // Orders the leaves by (x, y) column, z within a column (stable from Morton order), into d_leaf_rank, and
 // lays out the FP32 source records in that order (d_rec_base).  Uses the free tree-build scratch.
 b200fmm_status leaf_column_order(Context &c);
@@ -237,6 +243,9 @@ b200fmm_status tc_init(Context &c);
 void tc_free(Context &c);
 b200fmm_status run_m2l_tc(Context &c, int level);
 b200fmm_status tc_tree_setup(Context &c);
+void tc_invalidate_units(Context &c);  // the work units are recomputed at the next M2L (shard change)
+bool tc_tables_pending(const Context &c);  // the current tree's tables are not built yet
+b200fmm_status shard_ranges(Context &c);  // d_shard for the current tree
 void tc_set_splits(Context &c, int splits);
 int tc_splits_used(const Context &c);
 // direct.cu

@@ -284,13 +284,15 @@ __global__ void __launch_bounds__(L2P_WARPS * 32) l2p_kernel(
     const long long *__restrict__ leaf_start, const double *__restrict__ x, const double *__restrict__ y,
     const double *__restrict__ z, const double *__restrict__ q, double cx0, double cy0, double cz0, double leaf_w,
     const double *__restrict__ L,
-    double *__restrict__ phi, double *__restrict__ fx, double *__restrict__ fy, double *__restrict__ fz) {
+    double *__restrict__ phi, double *__restrict__ fx, double *__restrict__ fy, double *__restrict__ fz,
+    const long long *__restrict__ shard) {
   constexpr int p = P, nn = P * P * P;
   __shared__ double sL[L2P_WARPS][nn];
   __shared__ double sW[L2P_WARPS][32][4 * P + 1];  // wy, dwy, wz, dwz of each lane's particle (+1: banks)
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long long leaf = (long long)blockIdx.x * L2P_WARPS + w;
-  if (leaf >= nleaves) return;
+  // every leaf, or the shard's [shard[0], shard[1])
+  const long long leaf = (shard ? shard[0] : 0) + (long long)blockIdx.x * L2P_WARPS + w;
+  if (leaf >= (shard ? shard[1] : nleaves)) return;
   double *Lw = sL[w];
   double *wy = sW[w][lane], *dwy = wy + P, *wz = wy + 2 * P, *dwz = wy + 3 * P;
   int ix, iy, iz;
@@ -437,7 +439,7 @@ b200fmm_status run_l2l(Context &c, int level) {
   return B200FMM_OK;
 }
 
-b200fmm_status run_l2p(Context &c) {
+b200fmm_status run_l2p(Context &c, const long long *shard) {
   const int LL = c.H - 1;
   const Level &L = c.lv[LL];
   if (L.n == 0) return B200FMM_OK;
@@ -450,11 +452,11 @@ b200fmm_status run_l2p(Context &c) {
     if (lagr)                                                                                                \
       l2p_kernel<PV, true><<<grid_for(L.n, L2P_WARPS), L2P_WARPS * 32, 0, c.stream>>>(                      \
           c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, x0, y0, z0, lw, L.L, c.d_phi,       \
-          c.d_fx, c.d_fy, c.d_fz);                                                 \
+          c.d_fx, c.d_fy, c.d_fz, shard);                                          \
     else                                                                                                     \
       l2p_kernel<PV, false><<<grid_for(L.n, L2P_WARPS), L2P_WARPS * 32, 0, c.stream>>>(                     \
           c.R, c.N, L.n, L.keys, c.d_leaf_start, c.d_x, c.d_y, c.d_z, c.d_q, x0, y0, z0, lw, L.L, c.d_phi,       \
-          c.d_fx, c.d_fy, c.d_fz);                                                 \
+          c.d_fx, c.d_fy, c.d_fz, shard);                                          \
     break;
   switch (c.p) {
     B200_L2P(3) B200_L2P(4) B200_L2P(5) B200_L2P(6) B200_L2P(7) B200_L2P(8)

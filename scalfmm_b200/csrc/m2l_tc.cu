@@ -137,6 +137,8 @@ struct __align__(64) TcParams {
   // compacted; growlen = fp16 per gathered grid row (16 for Y chunks, KP for multipoles)
   const unsigned *cbusy;
   int gather, growlen;
+  // target shard (or null): [2 + 2 l, 3 + 2 l] hold level l's owned cells [a, b); units without one do no work
+  const long long *shard;
 };
 // What the producer and the MMA issuers need of transfer vector e of target parity c: the A box's
 // coordinates (offset of the source tile in half-grid cells; outer coordinate ya + rhs * (ycht or 8)), the B
@@ -1647,13 +1649,41 @@ __global__ void busy_mask_kernel(const __grid_constant__ TcParams P, int l0, int
 // Work of every unit of levels [P.l0, P.l1]: the number of transfer vectors with an occupied source box when
 // the unit's target tile (either tile of a pair) is occupied, else 0.  Written to prefix[u], which the scan
 // below turns into exclusive prefix sums.
+// Whether a unit holds a target cell of the shard (cells [a, b) of its level in Morton order).
+__device__ bool unit_in_shard(const TcParams &P, const TcItem &w) {
+  const long long a = P.shard[2 + 2 * w.level], b = P.shard[3 + 2 * w.level];
+  if (a >= b) return false;
+  const TcLevel &L = P.lv[w.level];
+  const int tiles = P.pair ? 2 : 1;
+  for (int t = 0; t < tiles; ++t) {
+    if (w.blk >= 0) {
+      for (int r = 0; r < 128; ++r) {
+        const int cell = L.ccell[(long long)(w.blk + t) * 128 + r];
+        if (cell >= a && cell < b) return true;
+      }
+      continue;
+    }
+    const int bz = w.bz + t;
+    if (bz >= L.HZ / TILE_Z) continue;
+    const int c = w.parity;
+    for (int r = 0; r < 128; ++r) {
+      const int hx = w.bx * TILE_X + (r & 7), hy = w.by * TILE_Y + ((r >> 3) & 3), hz = bz * TILE_Z + (r >> 5);
+      const int gx = 2 * hx + ((c >> 2) & 1), gy = 2 * hy + ((c >> 1) & 1), gz = 2 * hz + (c & 1);
+      if (gx >= L.side || gy >= L.side || gz >= L.side) continue;
+      const int cell = L.grid[((long long)gz * L.side + gy) * L.side + gx];
+      if (cell >= a && cell < b) return true;
+    }
+  }
+  return false;
+}
+
 __global__ void unit_work_kernel(const __grid_constant__ TcParams P, int nunits, int *__restrict__ prefix) {
   const int u = blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= nunits) return;
   const TcItem w = decode_unit(P, u);
   const BusyMask b = P.pair ? busy_mask_pair(P, w) : busy_mask(P, w);
   int n = 0;
-  if (b.tile()) {
+  if (b.tile() && (!P.shard || unit_in_shard(P, w))) {
 #pragma unroll
     for (int k = 0; k < 5; ++k) n += __popc(b.w[k]);
     n += __popc(b.w[5] & ((1u << (189 - 160)) - 1u));
@@ -2826,6 +2856,7 @@ b200fmm_status tc_tree_setup(Context &c) {
     B200_CHECK(compact_setup(c, *t));
     // the work of every unit of every level and its prefix sums, from which each launch splits its units
     // into ranges of equal work
+    t->params->shard = c.shard_count > 1 ? c.d_shard : nullptr;
     TcParams Pw = *t->params;
     Pw.l0 = 2;
     Pw.l1 = LL;
@@ -2835,6 +2866,14 @@ b200fmm_status tc_tree_setup(Context &c) {
     t->sat_serial = c.tree_serial;
   }
   return B200FMM_OK;
+}
+
+void tc_invalidate_units(Context &c) {
+  if (c.tc) c.tc->sat_serial = -1;
+}
+
+bool tc_tables_pending(const Context &c) {
+  return c.tc && (c.tc->built_for_gen != c.tree_gen || c.tc->sat_serial != c.tree_serial);
 }
 
 b200fmm_status run_m2l_tc(Context &c, int level) {

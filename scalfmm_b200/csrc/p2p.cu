@@ -25,14 +25,16 @@ namespace {
 
 constexpr int P2P64_THREADS = 64;
 
+// shard (optional): [first leaf, end leaf) of the targets to evaluate
 __global__ void p2p_fp64_kernel(int R, long long N, const long long *__restrict__ leaf_start,
                                 const int *__restrict__ nbr, int variant, const double *__restrict__ x,
                                 const double *__restrict__ y, const double *__restrict__ z,
                                 const double *__restrict__ q, double *__restrict__ phi, double *__restrict__ fx,
-                                double *__restrict__ fy, double *__restrict__ fz) {
+                                double *__restrict__ fy, double *__restrict__ fz, const long long *__restrict__ shard) {
   __shared__ double sx[P2P64_THREADS], sy[P2P64_THREADS], sz[P2P64_THREADS], sq[P2P64_THREADS];
   __shared__ long long sidx[P2P64_THREADS];
   const long long leaf = blockIdx.x;
+  if (shard && (leaf < shard[0] || leaf >= shard[1])) return;
   const long long t0 = leaf_start[leaf], t1 = leaf_start[leaf + 1];
   for (int r = 0; r < R; ++r) {
     const double *qr = q + (long long)r * N;
@@ -282,7 +284,8 @@ __device__ __forceinline__ bool p2p_item(long long item, long long nleaves, cons
 __global__ void __launch_bounds__(P2P32_WARPS * 32, 7) p2p_fp32_kernel(
     int R, long long N, long long nleaves, const long long *__restrict__ leaf_start, const int *__restrict__ nbr,
     int variant, const int *__restrict__ rank_of, const long long *__restrict__ rec_base,
-    const long long *__restrict__ chunk_base, int whole, int isize, const float4 *__restrict__ pq,
+    const long long *__restrict__ chunk_base, int whole, int isize, const long long *__restrict__ shard,
+    const float4 *__restrict__ pq,
     const float4 *__restrict__ plo, const float4 *__restrict__ src, double *__restrict__ phi, double *__restrict__ fx, double *__restrict__ fy,
     double *__restrict__ fz, int *__restrict__ status) {
   __shared__ __align__(128) float4 buf[P2P32_WARPS][P2P32_NBUF][4 * P2P32_STAGE];
@@ -296,9 +299,13 @@ __global__ void __launch_bounds__(P2P32_WARPS * 32, 7) p2p_fp32_kernel(
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncwarp();
+  // the work items of the targets' leaves: all, or the shard's [shard[0], shard[1])
+  const long long leaf_lo = shard ? shard[0] : 0, leaf_hi = shard ? shard[1] : nleaves;
+  const long long item0 = chunk_base ? chunk_base[leaf_lo] : leaf_lo;
+  const long long item1 = chunk_base ? chunk_base[leaf_hi] : leaf_hi;
+  const long long item = item0 + (long long)blockIdx.x * P2P32_WARPS + w;
   long long leaf, c0, c1;
-  if (!p2p_item((long long)blockIdx.x * P2P32_WARPS + w, nleaves, leaf_start, chunk_base, whole, isize, leaf, c0, c1))
-    return;
+  if (item >= item1 || !p2p_item(item, nleaves, leaf_start, chunk_base, whole, isize, leaf, c0, c1)) return;
   const long long P = p2p_pairs_capacity(N);
   const long long t0 = leaf_start[leaf];
   const int my_rank = rank_of ? rank_of[leaf] : (int)leaf;
@@ -553,8 +560,9 @@ __device__ __forceinline__ void p2p_record_mrhs(const float4 *__restrict__ s, in
 __global__ void __launch_bounds__(P2P32_WARPS * 32, 4) p2p_fp32_mrhs_kernel(
     int R, long long N, long long nleaves, const long long *__restrict__ leaf_start, const int *__restrict__ nbr,
     int variant, const int *__restrict__ rank_of, const long long *__restrict__ rec_base,
-    const long long *__restrict__ chunk_base, int whole, int isize, const float4 *__restrict__ pq,
-    const float4 *__restrict__ plo, const float *__restrict__ qt, const float4 *__restrict__ src,
+    const long long *__restrict__ chunk_base, int whole, int isize, const long long *__restrict__ shard,
+    const float4 *__restrict__ pq, const float4 *__restrict__ plo, const float *__restrict__ qt,
+    const float4 *__restrict__ src,
     double *__restrict__ phi, double *__restrict__ fx, double *__restrict__ fy, double *__restrict__ fz,
     int *__restrict__ status) {
   __shared__ __align__(128) float4 buf[P2P32_WARPS][P2P32_NBUF][MR_REC * P2P32_STAGE];
@@ -568,9 +576,13 @@ __global__ void __launch_bounds__(P2P32_WARPS * 32, 4) p2p_fp32_mrhs_kernel(
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncwarp();
+  // the work items of the targets' leaves: all, or the shard's [shard[0], shard[1])
+  const long long leaf_lo = shard ? shard[0] : 0, leaf_hi = shard ? shard[1] : nleaves;
+  const long long item0 = chunk_base ? chunk_base[leaf_lo] : leaf_lo;
+  const long long item1 = chunk_base ? chunk_base[leaf_hi] : leaf_hi;
+  const long long item = item0 + (long long)blockIdx.x * P2P32_WARPS + w;
   long long leaf, c0, c1;
-  if (!p2p_item((long long)blockIdx.x * P2P32_WARPS + w, nleaves, leaf_start, chunk_base, whole, isize, leaf, c0, c1))
-    return;
+  if (item >= item1 || !p2p_item(item, nleaves, leaf_start, chunk_base, whole, isize, leaf, c0, c1)) return;
   const long long P = p2p_pairs_capacity(N);
   const long long t0 = leaf_start[leaf];
   const int my_rank = rank_of ? rank_of[leaf] : (int)leaf;
@@ -722,7 +734,7 @@ __global__ void __launch_bounds__(P2P32_WARPS * 32, 4) p2p_fp32_mrhs_kernel(
 
 }  // namespace
 
-b200fmm_status run_p2p(Context &c, int variant) {
+b200fmm_status run_p2p(Context &c, int variant, const long long *shard) {
   const int LL = c.H - 1;
   const Level &L = c.lv[LL];
   if (L.n == 0) return B200FMM_OK;
@@ -749,7 +761,7 @@ b200fmm_status run_p2p(Context &c, int variant) {
     B200_CUDA(record_event(c, 10));
     p2p_fp32_mrhs_kernel<<<blocks, P2P32_WARPS * 32, 0, c.stream>>>(
         c.R, c.N, L.n, c.d_leaf_start, c.d_leaf_nbr, variant, c.d_leaf_rank, c.d_rec_base, c.d_chunk_base, c.p2p_whole,
-        c.p2p_item, hi, lo, qt, src, c.d_phi, c.d_fx, c.d_fy, c.d_fz, c.d_status);
+        c.p2p_item, shard, hi, lo, qt, src, c.d_phi, c.d_fx, c.d_fy, c.d_fz, c.d_status);
     B200_CUDA(record_event(c, 11));
     ++c.launches;
   } else if (c.cfg.precision == B200FMM_MIXED) {
@@ -772,14 +784,14 @@ b200fmm_status run_p2p(Context &c, int variant) {
     B200_CUDA(record_event(c, 10));
     p2p_fp32_kernel<<<blocks, P2P32_WARPS * 32, 0, c.stream>>>(
         c.R, c.N, L.n, c.d_leaf_start, c.d_leaf_nbr, variant, c.d_leaf_rank, c.d_rec_base, c.d_chunk_base, c.p2p_whole,
-        c.p2p_item, hi, lo, src, c.d_phi, c.d_fx, c.d_fy, c.d_fz, status);
+        c.p2p_item, shard, hi, lo, src, c.d_phi, c.d_fx, c.d_fy, c.d_fz, status);
     B200_CUDA(record_event(c, 11));
     ++c.launches;
   } else {
     B200_CUDA(record_event(c, 10));
     p2p_fp64_kernel<<<(unsigned)L.n, P2P64_THREADS, 0, c.stream>>>(c.R, c.N, c.d_leaf_start, c.d_leaf_nbr, variant,
                                                                    c.d_x, c.d_y, c.d_z, c.d_q, c.d_phi, c.d_fx,
-                                                                   c.d_fy, c.d_fz);
+                                                                   c.d_fy, c.d_fz, shard);
     B200_CUDA(record_event(c, 11));
     ++c.launches;
   }
@@ -885,8 +897,8 @@ extern "C" b200fmm_status b200fmm_p2p_noalloc(long long n, const double *x, cons
                                                  center[0] - box_width / 2, center[1] - box_width / 2,
                                                  center[2] - box_width / 2, stage, stage + n, stage + 2 * n);
   p2p_fp32_kernel<<<grid_for(nleaves, P2P32_WARPS), P2P32_WARPS * 32, 0, s>>>(
-      1, n, nleaves, leaf_start, leaf_nbr, variant, nullptr, nullptr, nullptr, 0, 0, stage, stage + n, stage + 2 * n,
-      phi, fx, fy, fz, status);
+      1, n, nleaves, leaf_start, leaf_nbr, variant, nullptr, nullptr, nullptr, 0, 0, nullptr, stage, stage + n,
+      stage + 2 * n, phi, fx, fy, fz, status);
   B200_CUDA(cudaGetLastError());
   B200_CUDA(cudaMemcpyAsync(st, status, sizeof(st), cudaMemcpyDeviceToHost, s));
   B200_CUDA(cudaStreamSynchronize(s));

@@ -860,6 +860,55 @@ b200fmm_status build_tree(Context &c, const double *x, const double *y, const do
   return B200FMM_OK;
 }
 
+// The target shard of execute(): leaves [lo, hi), the Morton range whose particles are those of ranks
+// [rank * N / count, (rank + 1) * N / count) of the sorted order rounded to whole leaves, and at every level the
+// cells [a, b) that are ancestors of those leaves (contiguous in Morton order).  One thread.
+struct ShardLinks {
+  const int *parent[kMaxHeight];
+  int LL;
+};
+__global__ void shard_range_kernel(const long long *__restrict__ leaf_start, long long nleaves, long long N, int rank,
+                                   int count, const __grid_constant__ ShardLinks S, long long *__restrict__ out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  // the first leaf that starts at or after particle t
+  auto first_leaf = [&](long long t) {
+    long long a = 0, b = nleaves;
+    while (a < b) {
+      const long long m = (a + b) >> 1;
+      if (leaf_start[m] < t) a = m + 1; else b = m;
+    }
+    return a;
+  };
+  const long long lo = rank == 0 ? 0 : first_leaf(N * rank / count);
+  const long long hi = rank == count - 1 ? nleaves : first_leaf(N * (rank + 1) / count);
+  out[0] = lo;
+  out[1] = hi;
+  for (int l = 0; l < kMaxHeight; ++l) out[2 + 2 * l] = out[3 + 2 * l] = 0;
+  if (hi <= lo) return;
+  long long a = lo, b = hi - 1;
+  for (int l = S.LL; l >= 0; --l) {
+    out[2 + 2 * l] = a;
+    out[3 + 2 * l] = b + 1;
+    if (l > 0) {
+      a = S.parent[l][a];
+      b = S.parent[l][b];
+    }
+  }
+}
+
+b200fmm_status shard_ranges(Context &c) {
+  const int LL = c.H - 1;
+  ShardLinks S{};
+  S.LL = LL;
+  for (int l = 0; l <= LL; ++l) S.parent[l] = c.lv[l].parent;
+  shard_range_kernel<<<1, 32, 0, c.stream>>>(c.d_leaf_start, c.lv[LL].n, c.N, c.shard_rank, c.shard_count, S,
+                                             c.d_shard);
+  ++c.launches;
+  B200_CUDA(cudaGetLastError());
+  c.shard_serial = c.tree_serial;
+  return B200FMM_OK;
+}
+
 // Interaction lists of levels 2..height-1 of the current tree, if not built yet.
 b200fmm_status build_ilists(Context &c) {
   const int LL = c.H - 1;

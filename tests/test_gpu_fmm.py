@@ -290,6 +290,54 @@ def test_async_results_overlap_the_next_tree():
             assert S.rel_l2(t.numpy(), want[k]) < 1e-12, (i, k)
 
 
+@pytest.mark.parametrize("kernel,precision,order,height,dist,count", [
+    ("cheb_sym", "mixed", 5, 5, "uniform", 3), ("cheb_sym", "fp64", 5, 6, "plummer", 4),
+    ("lagrange", "mixed", 6, 6, "ellipsoid", 2), ("cheb_sym", "mixed", 7, 6, "plummer", 3)])
+def test_shards_add_up_to_the_whole_evaluation(kernel, precision, order, height, dist, count):
+    """Target shards (set_shard): each shard evaluates the particles of its Morton range of leaves and leaves the
+    others at zero, so every particle is evaluated by exactly one shard and the shards' results add up to the
+    whole evaluation (FP64 to rounding; MIXED to the mixed level, the M2L's FP32 partial sums being grouped by
+    other work ranges).  Uniform, clustered (compacted M2L levels, CTA pairs at order 7) and surface trees."""
+    from distributions import ellipsoid_surface, plummer
+
+    rng = np.random.default_rng(91)
+    if dist == "uniform":
+        x, y, z = rng.random((3, 30000))
+    elif dist == "plummer":
+        x, y, z = plummer(30000, seed=92)
+    else:
+        x, y, z = ellipsoid_surface(30000, seed=93)
+    q = rng.uniform(-1.0, 1.0, x.size)
+    f = S.FMM(kernel, order, height, precision=precision)
+    f.set_particles(x, y, z, q)
+    f.execute()
+    whole = f.results()
+    total = {k: np.zeros(x.size) for k in FIELDS}
+    owners = np.zeros(x.size, np.int64)
+    for r in range(count):
+        f.set_shard(r, count)
+        f.execute()
+        part = f.results()
+        owners += part["phi"] != 0.0
+        for k in FIELDS:
+            total[k] += part[k]
+    # the same shard again: the second evaluation is captured into a CUDA graph, the third replays it
+    for _ in range(2):
+        f.execute()
+        rep = f.results()
+        for k in FIELDS:
+            assert S.rel_l2(rep[k], part[k]) < 1e-12, k
+    f.set_shard(0, 1)
+    f.execute()
+    again = f.results()
+    f.close()
+    assert np.all(owners == 1)
+    tol = 1e-12 if precision == "fp64" else 2e-6
+    for k in FIELDS:
+        assert S.rel_l2(total[k], whole[k]) < tol, (k, S.rel_l2(total[k], whole[k]))
+        assert S.rel_l2(again[k], whole[k]) < tol, k
+
+
 def test_edge_cases():
     # one particle: no interactions at all
     f = S.FMM("cheb_sym", 4, 3)
