@@ -888,10 +888,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) m2l_tc_kernel(const __grid_cons
   } else if (GATHER && warp == 3) {
     // ------------------------------------------------ row gathers of compacted blocks (all 32 lanes)
     // A compacted block's A tile holds, for transfer vector e, the source row of each of its 128 cells: the
-    // cell's half-grid position shifted by the box offset of e, in the source parity's grid (rows outside the
-    // grid read as zero, as the TMA boxes of the tile form do).  Lane l copies rows l, l + 32, l + 64, l + 96
-    // in 16-byte pieces, placed where the TMA unit's 32- or 64-byte swizzle would put them, and arrives once
-    // its copies have landed.  Stages of grid tiles (TMA-loaded A) get the 32 arrivals at once.
+    // cell's half-grid position shifted by the box offset of e, in the source parity's grid.  Rows outside the
+    // grid are zero-filled, as the TMA boxes of the tile form read them, and so are, where Y is stored by
+    // compacted row, the positions without a cell.  Lane l copies rows l, l + 32, l + 64, l + 96 in 16-byte
+    // pieces, placed where the TMA unit's 32- or 64-byte swizzle would put them, and arrives once its copies
+    // have landed.  Stages of grid tiles (TMA-loaded A) get the 32 arrivals at once.  Half-grid coordinates
+    // are packed in 10 bits each (levels up to 11).
     constexpr int PPR = ROWB / 16;                     // 16-byte pieces per row: 2 or 4
     constexpr int SWZ_SHIFT = ROWB == 32 ? 2 : 1;      // row bits that select the XOR of the piece index
     unsigned long long *gbar = (PAIR && !leader) ? gfull_bar : full_bar;
