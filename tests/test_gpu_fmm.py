@@ -338,6 +338,69 @@ def test_shards_add_up_to_the_whole_evaluation(kernel, precision, order, height,
         assert S.rel_l2(again[k], whole[k]) < tol, k
 
 
+def _sweep_case(rng):
+    from distributions import ellipsoid_surface, plummer
+
+    kernel = str(rng.choice(["cheb_sym", "cheb_dense", "lagrange"]))
+    order = int(rng.integers(3, 8))
+    height = int(rng.integers(3, 8))
+    n = int(np.exp(rng.uniform(np.log(2000), np.log(60000))))
+    dist = str(rng.choice(["uniform", "plummer", "ellipsoid", "clusters"]))
+    if dist == "uniform":
+        x, y, z = rng.random((3, n))
+    elif dist == "plummer":
+        x, y, z = plummer(n, seed=int(rng.integers(1 << 30)))
+    elif dist == "ellipsoid":
+        x, y, z = ellipsoid_surface(n, seed=int(rng.integers(1 << 30)))
+    else:
+        c = rng.random((4, 3)) * 0.8 + 0.1
+        p = np.clip(c[rng.integers(0, 4, n)] + rng.normal(0.0, 0.02, (n, 3)), 0.0, 1.0 - 1e-12)
+        x, y, z = p[:, 0].copy(), p[:, 1].copy(), p[:, 2].copy()
+    q = rng.uniform(-1.0, 1.0, n)
+    if dist != "plummer":
+        # at least about two particles per leaf (the Plummer core fills deep leaves on its own)
+        height = min(height, max(3, int(np.log(n / 2) / np.log(8)) + 1))
+    return kernel, order, height, dist, (x, y, z, q), str(int(rng.integers(0, 2))), int(rng.choice([1, 1, 2, 3]))
+
+
+@pytest.mark.parametrize("case", range(12))
+def test_seeded_configurations_mixed_vs_fp64(case):
+    """A seeded sweep over kernels (symmetric and dense Chebyshev, Lagrange), orders 3-7, heights 3-7, uniform /
+    clustered / surface / multi-cluster particles, CTA pairs forced on or off and 1-3 target shards: MIXED
+    against FP64 within 3e-6 on every output.  Trees whose leaves hold under about two particles on average
+    are left out (Plummer excepted): there the far field carries nearly all of the forces, and the Lagrange
+    M2L in MIXED reaches 3e-6 at order 6 and 6e-6 at order 7 in every M2L form, tiles and compacted blocks
+    alike."""
+    rng = np.random.default_rng(1000 + case)
+    kernel, order, height, dist, (x, y, z, q), pair, shards = _sweep_case(rng)
+    if kernel == "lagrange" and order == 7:
+        order = 6
+    res = {}
+    old = os.environ.get("B200FMM_TC_PAIR")
+    os.environ["B200FMM_TC_PAIR"] = pair
+    try:
+        for prec in ("fp64", "mixed"):
+            f = S.FMM(kernel, order, height, precision=prec)
+            f.set_particles(x, y, z, q)
+            r = {k: np.zeros(x.size) for k in FIELDS}
+            for s_ in range(shards):
+                f.set_shard(s_, shards)
+                f.execute()
+                part = f.results()
+                for k in FIELDS:
+                    r[k] += part[k]
+            res[prec] = r
+            f.close()
+    finally:
+        if old is None:
+            os.environ.pop("B200FMM_TC_PAIR", None)
+        else:
+            os.environ["B200FMM_TC_PAIR"] = old
+    for k in FIELDS:
+        e = S.rel_l2(res["mixed"][k], res["fp64"][k])
+        assert e < 3e-6, (kernel, order, height, dist, pair, shards, k, e)
+
+
 def test_edge_cases():
     # one particle: no interactions at all
     f = S.FMM("cheb_sym", 4, 3)
