@@ -338,6 +338,40 @@ def test_shards_add_up_to_the_whole_evaluation(kernel, precision, order, height,
         assert S.rel_l2(again[k], whole[k]) < tol, k
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_more_shards_than_leaves(precision):
+    """Shards whose Morton range holds no leaf evaluate nothing (their results are all zero); the others
+    still add up to the whole evaluation.  Also a set_shard before any particles, and one with several
+    right-hand sides."""
+    rng = np.random.default_rng(95)
+    n = 40
+    # two tight clusters: two occupied leaves at height 3, so most of 16 shards hold no leaf
+    c = np.where(np.arange(n) < n // 2, 0.12, 0.82)
+    x, y, z = (c + 0.03 * rng.random(n) for _ in range(3))
+    q = rng.uniform(-1.0, 1.0, (2, n))
+    f = S.FMM("cheb_sym", 4, 3, nrhs=2, precision=precision)
+    f.set_shard(1, 2)
+    f.set_shard(0, 1)
+    f.set_particles(x, y, z, q)
+    f.execute()
+    whole = f.results()
+    count = 16
+    total = {k: np.zeros_like(whole[k]) for k in FIELDS}
+    empty = 0
+    for r in range(count):
+        f.set_shard(r, count)
+        f.execute()
+        part = f.results()
+        empty += int(not np.any(part["phi"]))
+        for k in FIELDS:
+            total[k] += part[k]
+    f.close()
+    assert empty > 0
+    tol = 1e-12 if precision == "fp64" else 2e-6
+    for k in FIELDS:
+        assert S.rel_l2(total[k], whole[k]) < tol, k
+
+
 def _sweep_case(rng):
     from distributions import ellipsoid_surface, plummer
 
